@@ -1,0 +1,324 @@
+"""NUFFT throughput on B200: NU points/s of the 2D type-1 workload (1024^2 modes,
+10^7 uniform points, eps 1e-5), one JSON line on rank 0.
+
+A step is one type-1 execution on prepared points (sort done once by
+set_points), the reference's execute_type1_gpu; `one_shot` adds the sort
+(encode_type1_gpu). Inputs are resident in HBM; L2 is flushed with a 256 MiB
+write between steps, outside the timed events. `e2e` runs the public API with
+host buffers: pinned host -> device copies of points and strengths, one-shot
+execution, device -> host copy of the modes, every step. `--impl reference`
+times the reference's CPU plan (its restatement under oracle/; the reference
+itself needs Rust and wgpu, absent here) on the host cores. With torchrun,
+every rank runs the same workload on its own GPU (independent replicas: weak
+scaling) and the slowest rank's time counts.
+"""
+
+from __future__ import annotations
+
+import argparse
+import json
+import os
+import statistics
+import subprocess
+import sys
+import tempfile
+import time
+from pathlib import Path
+
+import numpy as np
+
+ROOT = Path(__file__).resolve().parent
+sys.path.insert(0, str(ROOT))
+
+MODES = (1024, 1024)
+POINTS = 10_000_000
+EPS = 1e-5
+SEED = 20240601
+WORKLOAD = "2d_type1_modes1024x1024_M1e7_uniform_eps1e-5"
+METRIC = "NU points/s (type-1 2D, 1024^2 modes, 1e7 uniform points, eps 1e-5, rel-l2 vs FP64 direct reported)"
+UNIT = "points/s"
+CPU_SAMPLE = 1_000_000
+
+
+def parse():
+    p = argparse.ArgumentParser()
+    p.add_argument("--gpus", type=int, default=1)
+    p.add_argument("--steps", type=int, default=10)
+    p.add_argument("--warmup", type=int, default=3)
+    p.add_argument("--impl", default="b200", choices=["b200", "reference"])
+    p.add_argument("--no-e2e", action="store_true")
+    p.add_argument("--no-cpu", action="store_true")
+    return p.parse_args()
+
+
+def make_inputs(rng_seed=SEED, count=POINTS):
+    rng = np.random.default_rng(rng_seed)
+    points = rng.uniform(-np.pi, np.pi, (count, 2)).astype(np.float32)
+    strengths = (rng.standard_normal(count) + 1j * rng.standard_normal(count)).astype(np.complex64)
+    return points, strengths
+
+
+def cpu_plan_throughput(points, strengths, repeats=3):
+    """Median NU points/s of the restated CPU plan (one-shot execution) over `repeats` runs."""
+    from oracle import native
+
+    plan = native.CpuPlan(1, MODES, EPS, precision="f32")
+    threads = os.cpu_count() or 1
+    times = []
+    for _ in range(repeats):
+        t0 = time.perf_counter()
+        plan.execute(points, strengths, threads=threads)
+        times.append(time.perf_counter() - t0)
+    return len(points) / statistics.median(times), threads, statistics.median(times)
+
+
+def reference_arm(args):
+    """The reference's CPU implementation (restated) on a bounded sample per step."""
+    rank = int(os.environ.get("RANK", "0"))
+    if rank != 0:
+        return
+    from oracle import native
+
+    points, strengths = make_inputs(count=CPU_SAMPLE)
+    plan = native.CpuPlan(1, MODES, EPS, precision="f32")
+    threads = os.cpu_count() or 1
+    for _ in range(args.warmup):
+        plan.execute(points, strengths, threads=threads)
+    times = []
+    for _ in range(args.steps):
+        t0 = time.perf_counter()
+        plan.execute(points, strengths, threads=threads)
+        times.append(time.perf_counter() - t0)
+    ms = 1e3 * sum(times) / len(times)
+    value = CPU_SAMPLE / (ms / 1e3)
+    sample = (f"{CPU_SAMPLE:,} of the {POINTS:,} uniform points per step on the same 1024^2-mode "
+              f"(2048^2 fine grid) eps 1e-5 plan; one-shot execution incl. sort")
+    line = {
+        "impl": "reference", "metric": METRIC, "value": value, "unit": UNIT, "n_gpus": args.gpus,
+        "steps": args.steps, "warmup": args.warmup, "ms_per_step": ms, "higher_is_better": True,
+        "scaling": "weak", "vs_baseline": None, "dtype": "c64", "data": "synthetic (seeded uniform)",
+        "config": {"workload": WORKLOAD, "modes": list(MODES), "points_per_step": CPU_SAMPLE, "eps": EPS},
+        "cpu_baseline": {"value": value, "unit": UNIT, "cores": threads, "kind": "port", "sample": sample},
+        "e2e": {"value": value, "unit": UNIT, "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0},
+    }
+    print(json.dumps(line), flush=True)
+
+
+class ClockSampler:
+    """nvidia-smi clocks and throttle reasons sampled every 200 ms."""
+
+    FIELDS = ("index,clocks.sm,clocks.max.sm,power.draw,clocks_event_reasons.active,"
+              "clocks_event_reasons.hw_slowdown,clocks_event_reasons.hw_thermal_slowdown,"
+              "clocks_event_reasons.sw_thermal_slowdown,clocks_event_reasons.sw_power_cap")
+
+    def __init__(self, device_index: int):
+        self.device_index = device_index
+        self.file = tempfile.NamedTemporaryFile("w+", suffix=".csv", delete=False)
+        self.proc = None
+
+    def __enter__(self):
+        try:
+            self.proc = subprocess.Popen(
+                ["nvidia-smi", f"--id={self.device_index}", f"--query-gpu={self.FIELDS}",
+                 "--format=csv,noheader,nounits", "-lms", "200"],
+                stdout=self.file, stderr=subprocess.DEVNULL)
+        except OSError:
+            self.proc = None
+        time.sleep(0.3)
+        return self
+
+    def __exit__(self, *exc):
+        if self.proc:
+            self.proc.terminate()
+            try:
+                self.proc.wait(timeout=5)
+            except subprocess.TimeoutExpired:
+                self.proc.kill()
+
+    def summary(self):
+        self.file.flush()
+        rows = [r.split(",") for r in Path(self.file.name).read_text().splitlines() if r.strip()]
+        os.unlink(self.file.name)
+        if not rows:
+            return {"sm_mhz": None, "sm_max_mhz": None, "reasons": ["unsampled"]}
+        sm = [float(r[1]) for r in rows if r[1].strip().replace(".", "").isdigit()]
+        mx = [float(r[2]) for r in rows if r[2].strip().replace(".", "").isdigit()]
+        names = ["hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap"]
+        reasons = sorted({names[i] for r in rows for i, v in enumerate(r[5:9]) if "Active" in v
+                          and "Not" not in v})
+        return {"sm_mhz": statistics.median(sm) if sm else None, "sm_max_mhz": max(mx) if mx else None,
+                "reasons": reasons, "samples": len(rows)}
+
+
+def profile_traffic():
+    """DRAM bytes per spread launch from the committed ncu summary, if present."""
+    path = ROOT / "profiles" / "spread_tiles_2d_1024_M1e7.md"
+    if not path.exists():
+        return None
+    for line in path.read_text().splitlines():
+        if line.startswith("traffic_bytes_per_launch:"):
+            try:
+                return float(line.split(":", 1)[1].strip().split()[0])
+            except ValueError:
+                return None
+    return None
+
+
+def main():
+    args = parse()
+    if args.impl == "reference":
+        reference_arm(args)
+        return
+    import torch
+    import torch.distributed as dist
+
+    world = int(os.environ.get("WORLD_SIZE", "1"))
+    rank = int(os.environ.get("RANK", "0"))
+    local = int(os.environ.get("LOCAL_RANK", "0"))
+    torch.cuda.set_device(local)
+    if world > 1:
+        from datetime import timedelta
+
+        dist.init_process_group("nccl", timeout=timedelta(seconds=300))
+    import wgpunufft_b200 as w
+
+    dev = f"cuda:{local}"
+    points_h, strengths_h = make_inputs()
+    points = torch.from_numpy(points_h).to(dev)
+    strengths = torch.from_numpy(strengths_h.view(np.float32)).to(dev).view(torch.complex64)
+    config = w.NufftConfig(MODES, EPS)
+    plan = w.NufftPlan.type1_gpu(config, device=local)
+    out = torch.empty(config.mode_count(), dtype=torch.complex64, device=dev)
+    flush = torch.empty(256 * 1024 * 1024 // 4, dtype=torch.float32, device=dev)
+    stream = torch.cuda.current_stream()
+
+    def barrier():
+        if world > 1:
+            dist.barrier()
+        torch.cuda.synchronize()
+
+    def timed(step_fn, steps):
+        starts = [torch.cuda.Event(enable_timing=True) for _ in range(steps)]
+        ends = [torch.cuda.Event(enable_timing=True) for _ in range(steps)]
+        for i in range(steps):
+            flush.fill_(float(i))
+            starts[i].record(stream)
+            step_fn()
+            ends[i].record(stream)
+        torch.cuda.synchronize()
+        return sum(s.elapsed_time(e) for s, e in zip(starts, ends))
+
+    # Warm-up: plan scratch, cuFFT plan, the sort.
+    plan.set_points_gpu(points)
+    for _ in range(args.warmup):
+        plan.execute_type1_gpu(strengths, out)
+        plan.encode_type1_gpu(points, strengths, out)
+    plan.synchronize()
+
+    # Prepared executions (the headline value), with stage events.
+    plan.set_points_gpu(points)
+    plan.synchronize()
+    plan.stage_timing(True)
+    plan.stage_report()
+    launches0 = w.launch_count()
+    barrier()
+    with ClockSampler(local) as clocks:
+        total_ms = timed(lambda: plan.execute_type1_gpu(strengths, out), args.steps)
+        launches = w.launch_count() - launches0
+        stages = plan.stage_report()
+        plan.stage_timing(False)
+        one_shot_ms = timed(lambda: plan.encode_type1_gpu(points, strengths, out), args.steps)
+    barrier()
+    clock_summary = clocks.summary()
+    if world > 1:
+        t = torch.tensor([total_ms, one_shot_ms], device=dev)
+        dist.all_reduce(t, op=dist.ReduceOp.MAX)
+        total_ms, one_shot_ms = t.tolist()
+    ms = total_ms / args.steps
+    value = world * POINTS / (ms / 1e3)
+    one_shot = world * POINTS / (one_shot_ms / args.steps / 1e3)
+
+    # Accuracy of this output against FP64 direct sums on 16 seeded modes.
+    rel = None
+    if rank == 0:
+        from oracle import native
+
+        plan.execute_type1_gpu(strengths, out)
+        plan.synchronize()
+        got = out.cpu().numpy()
+        select = np.random.default_rng(1).choice(config.mode_count(), 16, replace=False)
+        ref = native.direct_type1(points_h.astype(np.float64), strengths_h, MODES, select=select)[0]
+        rel = float(np.linalg.norm(got[select] - ref) / np.linalg.norm(ref))
+
+    # End to end through the public API with host buffers.
+    e2e = None
+    if not args.no_e2e:
+        pts_pinned = torch.from_numpy(points_h).pin_memory()
+        str_pinned = torch.from_numpy(strengths_h.view(np.float32)).pin_memory()
+        out_pinned = torch.empty(config.mode_count() * 2, dtype=torch.float32).pin_memory()
+        pts_dev = torch.empty_like(points)
+        str_dev = torch.empty(POINTS * 2, dtype=torch.float32, device=dev)
+
+        def e2e_step():
+            pts_dev.copy_(pts_pinned, non_blocking=True)
+            str_dev.copy_(str_pinned, non_blocking=True)
+            plan.encode_type1_gpu(pts_dev, str_dev.view(torch.complex64), out)
+            out_pinned.copy_(out.view(torch.float32), non_blocking=True)
+
+        for _ in range(2):
+            e2e_step()
+        barrier()
+        e2e_ms = timed(e2e_step, args.steps)
+        if world > 1:
+            t = torch.tensor([e2e_ms], device=dev)
+            dist.all_reduce(t, op=dist.ReduceOp.MAX)
+            e2e_ms = t.item()
+        e2e = {"value": world * POINTS / (e2e_ms / args.steps / 1e3), "unit": UNIT,
+               "h2d_bytes_per_step": POINTS * 8 + POINTS * 8, "d2h_bytes_per_step": config.mode_count() * 8,
+               "path": "NufftPlan.encode_type1_gpu (set_points + execute) with pinned host copies"}
+
+    if rank == 0:
+        peaks = json.loads((ROOT / "MEASURED_PEAKS.json").read_text()) if (ROOT / "MEASURED_PEAKS.json").exists() else {}
+        hbm = peaks.get("hbm_gbs", 6650.0)
+        spread_ms, spread_launches = stages.get("spread", (0.0, 0))
+        per_launch_ms = spread_ms / max(spread_launches, 1)
+        fine = plan.fine_grid_shape()
+        algorithmic = POINTS * (4 * 2 + 8 + 4) + fine[0] * fine[1] * 8
+        achieved = algorithmic / (per_launch_ms / 1e3) / 1e9 if per_launch_ms > 0 else None
+        roofline = {"bound": "hbm", "kernel": "spread_tiles_kernel<2,6>", "achieved": achieved, "peak": hbm,
+                    "unit": "GB/s", "frac": achieved / hbm if achieved else None,
+                    "traffic": profile_traffic(),
+                    "peak_source": "MEASURED_PEAKS.json hbm_gbs (measured)" if peaks else "fallback 6650 GB/s",
+                    "algorithmic_bytes_per_launch": algorithmic}
+        cpu = None
+        if not args.no_cpu:
+            sample_pts, sample_str = points_h[:CPU_SAMPLE], strengths_h[:CPU_SAMPLE]
+            cpu_value, threads, cpu_s = cpu_plan_throughput(sample_pts, sample_str)
+            cpu = {"value": cpu_value, "unit": UNIT, "cores": threads, "kind": "port",
+                   "sample": f"first {CPU_SAMPLE:,} of the {POINTS:,} points, same plan; restated CpuNufftPlan one-shot execute, median of 3 ({cpu_s:.2f} s each)"}
+        line = {
+            "metric": METRIC, "value": value, "unit": UNIT, "n_gpus": world, "steps": args.steps,
+            "warmup": args.warmup, "ms_per_step": ms, "higher_is_better": True, "scaling": "weak",
+            "vs_baseline": None, "dtype": "c64", "data": "synthetic (seeded uniform points, N(0,1) strengths)",
+            "config": {"workload": WORKLOAD, "modes": list(MODES), "points": POINTS, "eps": EPS, "batch": 1,
+                       "fine_grid": list(fine), "kernel_width": plan.kernel_width(),
+                       "l2": "flushed between steps by a 256 MiB write outside the timed events",
+                       "parallelism": f"replicas x{world}"},
+            "one_shot": {"value": one_shot, "unit": UNIT, "ms_per_step": one_shot_ms / args.steps,
+                         "note": "set_points (stable bin sort) + execute per step"},
+            "rel_l2": rel,
+            "stages_ms_per_step": {k: v[0] / args.steps for k, v in stages.items()},
+            "roofline": roofline,
+            "cpu_baseline": cpu,
+            "e2e": e2e,
+            "gpu_launches": launches,
+            "clocks": clock_summary,
+        }
+        print(json.dumps(line), flush=True)
+    if world > 1:
+        dist.barrier()
+        dist.destroy_process_group()
+
+
+if __name__ == "__main__":
+    main()

@@ -1,0 +1,302 @@
+"""GPU parity of the type-1 / type-2 CUDA path against the oracle.
+
+Accuracy bars follow the reference's GPU tests: relative l2 error against the
+FP64 direct sums within 4 eps in 1D (tests/gpu_nufft.rs:14-18), 20 eps in 2D
+(tests/gpu_nufft_2d.rs:15-16) and 32 eps in 3D (tests/gpu_nufft_3d.rs:14-15),
+at f32's floor of 1e-5 relative. The stable bin order, the bin offsets and
+the prepared slots are compared bit for bit with the oracle's restatement of
+the reference's binning.
+"""
+
+from __future__ import annotations
+
+import numpy as np
+import pytest
+
+from oracle import binsort, es_kernel, layout, native
+from tests.conftest import clustered_points, complex_normal, rel_l2, uniform_points
+
+pytestmark = pytest.mark.gpu
+
+torch = pytest.importorskip("torch")
+if not torch.cuda.is_available():  # pragma: no cover - CPU containers
+    pytest.skip("needs a CUDA device", allow_module_level=True)
+
+import wgpunufft_b200 as w  # noqa: E402
+
+DEV = "cuda:0"
+
+
+def tolerance(d: int, eps: float) -> float:
+    factor = {1: 4.0, 2: 20.0, 3: 32.0}[d]
+    return max(factor * eps, 2e-5 if d < 3 else 3e-5)
+
+
+def to_gpu(array):
+    return torch.from_numpy(np.ascontiguousarray(array)).to(DEV)
+
+
+def run_type1(n_modes, eps, points, strengths, isign=1, order=0, batch=1, plan=None):
+    config = w.NufftConfig(n_modes, eps, isign=isign, mode_order=order, batch=batch)
+    plan = plan or w.NufftPlan.type1_gpu(config)
+    n = config.mode_count()
+    out = torch.empty((batch, n), dtype=torch.complex64, device=DEV)
+    plan.encode_type1_gpu(to_gpu(points), to_gpu(strengths.reshape(batch, -1)), out)
+    plan.synchronize()
+    return out.cpu().numpy(), plan
+
+
+def run_type2(n_modes, eps, points, coefficients, isign=1, order=0, batch=1, plan=None):
+    config = w.NufftConfig(n_modes, eps, isign=isign, mode_order=order, batch=batch)
+    plan = plan or w.NufftPlan.type2_gpu(config)
+    m = points.shape[0]
+    out = torch.empty((batch, m), dtype=torch.complex64, device=DEV)
+    plan.encode_type2_gpu(to_gpu(points), to_gpu(coefficients.reshape(batch, -1)), out)
+    plan.synchronize()
+    return out.cpu().numpy(), plan
+
+
+SHAPES = [(11,), (64,), (200,), (6, 5), (16, 12), (64, 64), (4, 3, 5), (16, 12, 10), (24, 20, 16)]
+
+
+@pytest.mark.parametrize("n_modes", SHAPES)
+@pytest.mark.parametrize("eps", [1e-3, 1e-6])
+def test_type1_and_type2_match_direct_sums(n_modes, eps):
+    d = len(n_modes)
+    rng = np.random.default_rng([d, int(-np.log10(eps)), int(np.prod(n_modes))])
+    points = uniform_points(rng, 3000, d)
+    strengths = complex_normal(rng, 3000)
+    coefficients = complex_normal(rng, int(np.prod(n_modes)))
+    for isign in (1, -1):
+        for order in (0, 1):
+            got1, _ = run_type1(n_modes, eps, points, strengths, isign, order)
+            ref1 = native.direct_type1(points.astype(np.float64), strengths, n_modes, isign, order)
+            assert rel_l2(got1, ref1) < tolerance(d, eps), (isign, order)
+            got2, _ = run_type2(n_modes, eps, points, coefficients, isign, order)
+            ref2 = native.direct_type2(points.astype(np.float64), coefficients, n_modes, isign, order)
+            assert rel_l2(got2, ref2) < tolerance(d, eps), (isign, order)
+
+
+@pytest.mark.parametrize("eps", [1e-2, 1e-4, 1e-5])
+def test_accuracy_sweep_2d(eps):
+    rng = np.random.default_rng(7)
+    n_modes = (32, 24)
+    points = uniform_points(rng, 4000, 2)
+    strengths = complex_normal(rng, 4000)
+    got, _ = run_type1(n_modes, eps, points, strengths)
+    ref = native.direct_type1(points.astype(np.float64), strengths, n_modes)
+    assert rel_l2(got, ref) < tolerance(2, eps)
+
+
+def oracle_order(points, fine, eps, kind):
+    width = es_kernel.es_parameters(eps, 2.0)[0]
+    if kind == 1:
+        lay = layout.Layout(width, list(fine), "F32")
+        side = lay.geometries[lay.choose_geometry(points.shape[0])].side
+        keys, bins = binsort.type1_keys(points, fine, width, side)
+    else:
+        side = None
+        keys, bins = binsort.type2_keys(points, fine)
+    perm, offsets = binsort.stable_order(keys, bins)
+    return perm, offsets, keys, side, width
+
+
+def point_sets(d, rng):
+    m = 20_000
+    special = uniform_points(rng, m, d)
+    special[::97, 0] = np.float32(np.pi)
+    special[1::97, -1] = np.float32(-np.pi)
+    special[2::97, 0] = np.float32(3 * np.pi)
+    special[3::97, 0] = np.float32(-3 * np.pi)
+    special[4::131] = special[5::131][: len(special[4::131])]  # duplicates
+    special[6::211, 0] = np.nan
+    special[7::211, -1] = np.inf
+    special[8::211, 0] = np.float32(1e30)
+    special[9::211, 0] = np.float32(5 * np.pi)
+    special[10::211, 0] = np.float32(-40.0)
+    return {
+        "uniform": uniform_points(rng, m, d),
+        "clustered": clustered_points(rng, m, d),
+        "edges_and_invalid": special,
+        "single_point": clustered_points(rng, 5000, d, centres=1, spread=0.0),
+    }
+
+
+@pytest.mark.parametrize("n_modes", [(64,), (1000,), (64, 64), (200, 150), (16, 12, 10), (40, 40, 40)])
+@pytest.mark.parametrize("kind", [1, 2])
+def test_bin_order_is_bit_exact(n_modes, kind):
+    d = len(n_modes)
+    rng = np.random.default_rng([kind, d, n_modes[0]])
+    eps = 1e-5
+    for name, points in point_sets(d, rng).items():
+        config = w.NufftConfig(n_modes, eps)
+        plan = w.NufftPlan.type1_gpu(config) if kind == 1 else w.NufftPlan.type2_gpu(config)
+        gpu_points = to_gpu(points)
+        plan.set_points_gpu(gpu_points)
+        perm, offsets = plan.bin_order()
+        fine = plan.fine_grid_shape()
+        ref_perm, ref_offsets, keys, side, width = oracle_order(points, fine, eps, kind)
+        assert np.array_equal(offsets.numpy(), ref_offsets), name
+        assert np.array_equal(perm.numpy(), ref_perm), name
+        if kind == 1:
+            assert plan.info().chosen_geometry == layout.Layout(width, list(fine), "F32").choose_geometry(len(points))
+            starts, offs = plan.prepared_slots()
+            ref_starts, ref_offs = binsort.prepared_slots(points, fine, width, side, ref_perm, keys)
+            assert np.array_equal(starts.numpy().reshape(-1, d + 1), ref_starts), name
+            assert np.array_equal(offs.numpy().view(np.uint32).reshape(-1),
+                                  ref_offs.reshape(-1).view(np.uint32)), name
+
+
+def test_large_sort_matches_oracle():
+    """A multi-tile sort (several look-back tiles and all three radix passes)."""
+    rng = np.random.default_rng(11)
+    for points, n_modes in [(uniform_points(rng, 3_000_000, 2), (1024, 1024)),
+                            (clustered_points(rng, 2_000_000, 2), (1024, 1024)),
+                            (uniform_points(rng, 1_500_000, 3), (128, 128, 128))]:
+        plan = w.NufftPlan.type1_gpu(w.NufftConfig(n_modes, 1e-5))
+        plan.set_points_gpu(to_gpu(points))
+        perm, offsets = plan.bin_order()
+        ref_perm, ref_offsets, *_ = oracle_order(points, plan.fine_grid_shape(), 1e-5, 1)
+        assert np.array_equal(offsets.numpy(), ref_offsets)
+        assert np.array_equal(perm.numpy(), ref_perm)
+
+
+@pytest.mark.parametrize("n_modes", [(256,), (128, 128), (32, 32, 32)])
+def test_bitwise_repeatable(n_modes):
+    d = len(n_modes)
+    rng = np.random.default_rng(5)
+    points = clustered_points(rng, 200_000, d)
+    strengths = complex_normal(rng, 200_000)
+    coefficients = complex_normal(rng, int(np.prod(n_modes)))
+    first1, plan1 = run_type1(n_modes, 1e-5, points, strengths)
+    first2, plan2 = run_type2(n_modes, 1e-5, points, coefficients)
+    for _ in range(10):
+        again1, _ = run_type1(n_modes, 1e-5, points, strengths, plan=plan1)
+        again2, _ = run_type2(n_modes, 1e-5, points, coefficients, plan=plan2)
+        assert np.array_equal(first1.view(np.uint32), again1.view(np.uint32))
+        assert np.array_equal(first2.view(np.uint32), again2.view(np.uint32))
+
+
+@pytest.mark.parametrize("n_modes", [(128,), (48, 40), (16, 16, 12)])
+def test_batch_matches_single_vectors(n_modes):
+    d = len(n_modes)
+    rng = np.random.default_rng(9)
+    m, batch = 5000, 3
+    points = uniform_points(rng, m, d)
+    strengths = complex_normal(rng, (batch, m))
+    coefficients = complex_normal(rng, (batch, int(np.prod(n_modes))))
+    many1, _ = run_type1(n_modes, 1e-5, points, strengths, batch=batch)
+    many2, _ = run_type2(n_modes, 1e-5, points, coefficients, batch=batch)
+    for b in range(batch):
+        one1, _ = run_type1(n_modes, 1e-5, points, strengths[b])
+        one2, _ = run_type2(n_modes, 1e-5, points, coefficients[b])
+        assert rel_l2(many1[b], one1[0]) < 1e-6
+        assert rel_l2(many2[b], one2[0]) < 1e-6
+        ref = native.direct_type1(points.astype(np.float64), strengths[b], n_modes)[0]
+        assert rel_l2(many1[b], ref) < tolerance(d, 1e-5)
+
+
+def test_active_batch_below_capacity_and_set_points_reuse():
+    rng = np.random.default_rng(12)
+    n_modes = (40, 36)
+    m = 6000
+    points = uniform_points(rng, m, 2)
+    strengths = complex_normal(rng, (4, m))
+    config = w.NufftConfig(n_modes, 1e-5, batch=4)
+    plan = w.NufftPlan.type1_gpu(config)
+    plan.set_points_gpu(to_gpu(points))
+    out = torch.empty((2, config.mode_count()), dtype=torch.complex64, device=DEV)
+    plan.execute_type1_gpu_batch(2, to_gpu(strengths[:2]), out)
+    plan.synchronize()
+    executed = out.cpu().numpy()
+    encoded, _ = run_type1(n_modes, 1e-5, points, strengths[:2], batch=2)
+    assert np.array_equal(executed.view(np.uint32), encoded.view(np.uint32))
+    with pytest.raises(w.NufftError, match="InvalidBatch"):
+        plan.execute_type1_gpu_batch(5, to_gpu(strengths), out)
+
+
+def test_zero_points():
+    n_modes = (16, 12)
+    plan = w.NufftPlan.type1_gpu(w.NufftConfig(n_modes, 1e-6))
+    out = torch.full((1, 192), 7.0 + 1j, dtype=torch.complex64, device=DEV)
+    empty = torch.empty((0, 2), dtype=torch.float32, device=DEV)
+    plan.encode_type1_gpu(empty, torch.empty((1, 0), dtype=torch.complex64, device=DEV), out)
+    plan.synchronize()
+    assert torch.count_nonzero(out).item() == 0
+    plan2 = w.NufftPlan.type2_gpu(w.NufftConfig(n_modes, 1e-6))
+    out2 = torch.empty((1, 0), dtype=torch.complex64, device=DEV)
+    plan2.encode_type2_gpu(empty, torch.ones((1, 192), dtype=torch.complex64, device=DEV), out2)
+    plan2.synchronize()
+
+
+def test_execute_before_points_and_wrong_kind_fail():
+    plan = w.NufftPlan.type1_gpu(w.NufftConfig((8,), 1e-6))
+    out = torch.empty((1, 8), dtype=torch.complex64, device=DEV)
+    with pytest.raises(w.NufftError, match="GpuExecutionUnavailable"):
+        plan.execute_type1_gpu(out, out)
+    with pytest.raises(w.NufftError, match="GpuExecutionUnavailable"):
+        plan.execute_type2_gpu(out, out)
+
+
+@pytest.mark.parametrize("n_modes", [(64,), (24, 20), (16, 16, 12)])
+def test_invalid_points_leave_other_points_intact(n_modes):
+    """tests/gpu_invalid_points.rs: non-finite and far coordinates get zero
+    weight; type-2 values at the other points are unchanged bit for bit and
+    zero at the invalid ones; type-1 modes match those of the valid points."""
+    d = len(n_modes)
+    rng = np.random.default_rng(21)
+    valid = uniform_points(rng, 300, d)
+    invalid_values = [np.nan, np.inf, -np.inf, 1e30, -1e30, -40.0, 5 * np.pi]
+    mixed, index = [], []
+    k = 0
+    for i, p in enumerate(valid):
+        mixed.append(p)
+        index.append(i)
+        if (i + 1) % 25 == 0:
+            q = p.copy()
+            q[k % d] = invalid_values[k % len(invalid_values)]
+            mixed.append(q)
+            index.append(-1)
+            k += 1
+    mixed = np.array(mixed, dtype=np.float32)
+    index = np.array(index)
+    coefficients = complex_normal(rng, int(np.prod(n_modes)))
+    only, _ = run_type2(n_modes, 1e-6, valid, coefficients)
+    both, _ = run_type2(n_modes, 1e-6, mixed, coefficients)
+    assert np.array_equal(both[0, index >= 0].view(np.uint32), only[0].view(np.uint32))
+    assert np.all(both[0, index < 0] == 0)
+    strengths = complex_normal(rng, len(mixed))
+    with_invalid, _ = run_type1(n_modes, 1e-6, mixed, strengths)
+    without, _ = run_type1(n_modes, 1e-6, valid, strengths[index >= 0])
+    assert rel_l2(with_invalid, without) < 1e-6
+
+
+def test_clustered_and_heavy_tiles_match_direct():
+    """Dense clusters split tiles into many parts; the sums stay accurate."""
+    rng = np.random.default_rng(31)
+    n_modes = (64, 64)
+    points = clustered_points(rng, 400_000, 2, centres=2, spread=0.003)
+    strengths = complex_normal(rng, 400_000)
+    got, _ = run_type1(n_modes, 1e-5, points, strengths)
+    select = rng.choice(64 * 64, 300, replace=False)
+    ref = native.direct_type1(points.astype(np.float64), strengths, n_modes, select=select)
+    assert rel_l2(got[0, select], ref[0]) < tolerance(2, 1e-5)
+
+
+def test_2d_1024_ten_million_points_against_direct_subsets():
+    """The 2D 1024^2, 10^7-point workload: a seeded subset of modes (type 1)
+    and of points (type 2) against FP64 direct sums over all inputs."""
+    rng = np.random.default_rng(2024)
+    n_modes = (1024, 1024)
+    m = 10_000_000
+    for points in (uniform_points(rng, m, 2), clustered_points(rng, m, 2)):
+        strengths = complex_normal(rng, m)
+        got, plan = run_type1(n_modes, 1e-5, points, strengths)
+        select = rng.choice(1024 * 1024, 48, replace=False)
+        ref = native.direct_type1(points.astype(np.float64), strengths, n_modes, select=select)
+        assert rel_l2(got[0, select], ref[0]) < tolerance(2, 1e-5)
+        coefficients = complex_normal(rng, 1024 * 1024)
+        got2, _ = run_type2(n_modes, 1e-5, points, coefficients)
+        pick = rng.choice(m, 48, replace=False)
+        ref2 = native.direct_type2(points.astype(np.float64), coefficients, n_modes, select=pick)
+        assert rel_l2(got2[0, pick], ref2[0]) < tolerance(2, 1e-5)

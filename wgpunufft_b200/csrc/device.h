@@ -1,0 +1,86 @@
+// Device memory, launch accounting and the parameter blocks that the host
+// passes to the kernels.
+#pragma once
+
+#include <cuda_runtime.h>
+
+#include <atomic>
+#include <cstdint>
+#include <string>
+
+#include "es_kernel.h"
+#include "fold.cuh"
+#include "stage_timer.h"
+#include "status.h"
+
+namespace b200nufft {
+
+// Throws NufftFailure for a failed CUDA runtime call.
+void check_cuda(cudaError_t error, const char* what);
+
+// Counts this library's kernel launches (b200nufft_launch_count).
+void note_launch(int count = 1);
+
+// A grow-only device allocation, the analogue of the reference's
+// GrowOnlyBuffer (src/gpu_point_bins.rs:53-90).
+class DeviceBuffer {
+ public:
+  DeviceBuffer() = default;
+  DeviceBuffer(const DeviceBuffer&) = delete;
+  DeviceBuffer& operator=(const DeviceBuffer&) = delete;
+  ~DeviceBuffer();
+  // Ensures at least `bytes` bytes; contents are lost when it grows.
+  void* reserve(size_t bytes, const char* label);
+  void* get() const { return ptr_; }
+  size_t size() const { return bytes_; }
+  void release();
+
+ private:
+  void* ptr_ = nullptr;
+  size_t bytes_ = 0;
+};
+
+// Fine-grid geometry and window of an F32 plan as the kernels see it.
+struct GridParams {
+  int32_t dimensions;
+  int32_t width;
+  float half_width;
+  float beta;
+  FoldAxis axis[3];
+  int64_t fine[3];       // fine-grid cells per axis
+  int64_t fine_count;    // cells of one transform's grid
+};
+
+// Stable sort of the points by bin key. Launches on `stream`; all pointers
+// are device pointers owned by the caller.
+struct SortBuffers {
+  uint32_t* keys_a;
+  uint32_t* keys_b;
+  uint32_t* vals_b;
+  uint32_t* vals_a;
+  uint32_t* hist;        // 4 passes x 256 counts
+  uint32_t* status;      // tiles x 256 look-back words
+  uint32_t* counters;    // 4 tile tickets + 1 error flag
+};
+
+// Key kinds: the reference's type-1 stable bins of support starts
+// (src/gpu_nd_bins.rs:474-554), or its type-2 grouped bins of plain-f32
+// position cells (src/gpu_point_bins.rs:422-465).
+enum class KeyKind { SupportStart, ApproximateCell };
+
+// Sorts `count` points; on return `*perm` and `*sorted_keys` point into the
+// buffers at the permutation and the sorted keys. Writes bin offsets
+// (bins + 1 words) to `offsets`.
+void sort_points(const float* points, int64_t count, const GridParams& grid, KeyKind kind,
+                 uint64_t bins, SortBuffers buffers, uint32_t* offsets, uint32_t** perm,
+                 uint32_t** sorted_keys, cudaStream_t stream, StageTimer* timer = nullptr);
+
+// Bytes of look-back status words a sort of `count` points needs.
+size_t sort_status_bytes(int64_t count);
+
+// Reference-layout prepared slots of the stable type-1 binning.
+void prepare_reference_slots(const float* points, int64_t count, const GridParams& grid,
+                             const uint32_t* perm, const uint32_t* sorted_keys, int32_t* starts,
+                             float* offsets, cudaStream_t stream);
+
+}  // namespace b200nufft

@@ -1,0 +1,127 @@
+// Deconvolution around the fine-grid FFT.
+//
+// Type 1 truncates the transformed fine grid to the requested modes and
+// scales every mode by its deconvolution amplitude prod_a 1/phi_hat_a(|k_a|)
+// (the reference's deconvolution shader, src/gpu_type1_nd.rs:617-687). Type 2
+// writes every fine-grid cell once: the deconvolved mode that maps to it, or
+// zero, so the clearing pass of the reference (src/gpu_2d.rs:640-648, 896-957)
+// is fused into the scatter.
+#include <cuda_runtime.h>
+
+#include "device.h"
+#include "modes.h"
+
+namespace b200nufft {
+
+namespace {
+
+// Fine-grid index of mode storage index k along an axis of N modes and n
+// cells (src/gpu_type1_nd.rs:642-652).
+__device__ __forceinline__ int64_t fine_index(int64_t k, int64_t N, int64_t n, bool centered) {
+  if (centered) {
+    const int64_t half = N / 2;
+    return k < half ? n - (half - k) : k - half;
+  }
+  const int64_t nonnegative = (N + 1) / 2;
+  return k < nonnegative ? k : n - (N - k);
+}
+
+// Mode storage index of fine-grid cell c, or -1 when no mode maps to it.
+__device__ __forceinline__ int64_t mode_index(int64_t c, int64_t N, int64_t n, bool centered) {
+  if (centered) {
+    const int64_t half = N / 2;
+    if (c < N - half) return c + half;
+    if (c >= n - half) return c - n + half;
+    return -1;
+  }
+  const int64_t nonnegative = (N + 1) / 2;
+  if (c < nonnegative) return c;
+  if (c >= n - (N - nonnegative)) return c - n + N;
+  return -1;
+}
+
+template <typename Real, typename Complex>
+__global__ void deconvolve_kernel(ModeParams mp, int batch, const Complex* __restrict__ fine,
+                                  const Real* __restrict__ amplitudes,
+                                  Complex* __restrict__ output) {
+  const int64_t k = static_cast<int64_t>(blockIdx.x) * blockDim.x + threadIdx.x;
+  if (k >= mp.mode_count) return;
+  int64_t rest = k, flat = 0, stride = 1;
+  for (int a = 0; a < mp.dimensions; ++a) {
+    const int64_t index = rest % mp.modes[a];
+    rest /= mp.modes[a];
+    flat += fine_index(index, mp.modes[a], mp.fine[a], mp.centered) * stride;
+    stride *= mp.fine[a];
+  }
+  const Real amplitude = amplitudes[k];
+  for (int b = 0; b < batch; ++b) {
+    const Complex v = fine[static_cast<int64_t>(b) * mp.fine_count + flat];
+    Complex o;
+    o.x = v.x * amplitude;
+    o.y = v.y * amplitude;
+    output[static_cast<int64_t>(b) * mp.mode_count + k] = o;
+  }
+}
+
+template <typename Real, typename Complex>
+__global__ void predeconvolve_kernel(ModeParams mp, int batch, const Complex* __restrict__ input,
+                                     const Real* __restrict__ amplitudes,
+                                     Complex* __restrict__ fine) {
+  const int64_t c = static_cast<int64_t>(blockIdx.x) * blockDim.x + threadIdx.x;
+  if (c >= mp.fine_count) return;
+  int64_t rest = c, flat = 0, stride = 1;
+  bool mapped = true;
+  for (int a = 0; a < mp.dimensions; ++a) {
+    const int64_t cell = rest % mp.fine[a];
+    rest /= mp.fine[a];
+    const int64_t index = mode_index(cell, mp.modes[a], mp.fine[a], mp.centered);
+    mapped = mapped && index >= 0;
+    flat += index * stride;
+    stride *= mp.modes[a];
+  }
+  const Real amplitude = mapped ? amplitudes[flat] : Real(0);
+  for (int b = 0; b < batch; ++b) {
+    Complex o;
+    o.x = Real(0);
+    o.y = Real(0);
+    if (mapped) {
+      const Complex v = input[static_cast<int64_t>(b) * mp.mode_count + flat];
+      o.x = v.x * amplitude;
+      o.y = v.y * amplitude;
+    }
+    fine[static_cast<int64_t>(b) * mp.fine_count + c] = o;
+  }
+}
+
+}  // namespace
+
+void deconvolve_f32(const ModeParams& mp, int batch, const float2* fine, const float* amplitudes,
+                    float2* output, cudaStream_t stream) {
+  const unsigned blocks = static_cast<unsigned>((mp.mode_count + 255) / 256);
+  deconvolve_kernel<float, float2><<<blocks, 256, 0, stream>>>(mp, batch, fine, amplitudes, output);
+  note_launch();
+}
+
+void predeconvolve_f32(const ModeParams& mp, int batch, const float2* input,
+                       const float* amplitudes, float2* fine, cudaStream_t stream) {
+  const unsigned blocks = static_cast<unsigned>((mp.fine_count + 255) / 256);
+  predeconvolve_kernel<float, float2><<<blocks, 256, 0, stream>>>(mp, batch, input, amplitudes, fine);
+  note_launch();
+}
+
+void deconvolve_f64(const ModeParams& mp, int batch, const double2* fine,
+                    const double* amplitudes, double2* output, cudaStream_t stream) {
+  const unsigned blocks = static_cast<unsigned>((mp.mode_count + 255) / 256);
+  deconvolve_kernel<double, double2><<<blocks, 256, 0, stream>>>(mp, batch, fine, amplitudes, output);
+  note_launch();
+}
+
+void predeconvolve_f64(const ModeParams& mp, int batch, const double2* input,
+                       const double* amplitudes, double2* fine, cudaStream_t stream) {
+  const unsigned blocks = static_cast<unsigned>((mp.fine_count + 255) / 256);
+  predeconvolve_kernel<double, double2><<<blocks, 256, 0, stream>>>(mp, batch, input, amplitudes,
+                                                                   fine);
+  note_launch();
+}
+
+}  // namespace b200nufft

@@ -1,0 +1,579 @@
+// Type-1 / type-2 plan: creation (src/plan.rs:658-694), point preparation
+// (src/plan.rs:890-925) and execution (src/plan.rs:931-977, 1183-1229).
+#include "plan.h"
+
+#include <algorithm>
+#include <cmath>
+#include <cstring>
+#include <limits>
+
+#include "util.h"
+
+namespace b200nufft {
+
+namespace {
+
+constexpr double kTwoPi = 6.28318530717958647692;
+// Records of one spreading subproblem, at most.
+constexpr int32_t kPartCap = 4096;
+// Padded tile bytes a spreading CTA may hold, so that two fit on an SM.
+constexpr int64_t kTileBytesTarget = 100 * 1024;
+// Points one plan can bin: look-back words hold 30-bit counts.
+constexpr int64_t kMaxPoints = (int64_t(1) << 30) - 1;
+
+int64_t mode_for_storage_index(int order, int64_t index, int64_t length) {
+  // src/direct.rs:120-131
+  if (order == B200NUFFT_MODE_ORDER_CENTERED) return index - length / 2;
+  return index < (length + 1) / 2 ? index : index - length;
+}
+
+int64_t pow2_ceil(int64_t v) {
+  int64_t p = 1;
+  while (p < v) p <<= 1;
+  return p;
+}
+
+int ilog2(int64_t v) {
+  int s = 0;
+  while ((int64_t(1) << s) < v) ++s;
+  return s;
+}
+
+// config.rs:252-284: an F32 plan whose rounding, amplified by deconvolution,
+// would miss the tolerance by far is rejected.
+void validate_f32_rounding(const int64_t* modes, int dim, double eps, double sigma,
+                           const std::vector<std::vector<double>>& coefficients) {
+  double estimate = static_cast<double>(std::numeric_limits<float>::epsilon()) / 2.0;
+  for (int a = 0; a < dim; ++a) {
+    const auto& axis = coefficients[a];
+    if (axis.empty()) continue;
+    const double center = axis[0];
+    const int64_t half = modes[a] / 2;
+    double sum = 0.0;
+    for (int64_t index = 0; index < modes[a]; ++index) {
+      const int64_t magnitude = index > half ? index - half : half - index;
+      const double value =
+          magnitude < static_cast<int64_t>(axis.size()) ? std::fabs(axis[magnitude]) : 0.0;
+      sum += value > 0.0 ? (center / value) * (center / value)
+                         : std::numeric_limits<double>::infinity();
+    }
+    estimate *= std::sqrt(sum / static_cast<double>(modes[a]));
+  }
+  if (estimate > 10.0 * eps && estimate > 1.0e-5) {
+    throw NufftFailure{B200NUFFT_F32_TOLERANCE_UNREACHABLE,
+                       "f32 rounding amplified by the deconvolution (estimated error " +
+                           std::to_string(estimate) + ") misses eps " + std::to_string(eps) +
+                           " at sigma " + std::to_string(sigma) +
+                           "; use sigma = 2, a larger tolerance, or f64"};
+  }
+}
+
+}  // namespace
+
+NufftPlan::NufftPlan(const b200nufft_config& c, bool with_device) : has_device_(with_device) {
+  if (c.type != 1 && c.type != 2) {
+    throw NufftFailure{B200NUFFT_INVALID_ARGUMENT, "plan type must be 1 or 2"};
+  }
+  type_ = c.type;
+  if (c.batch <= 0) {
+    throw NufftFailure{B200NUFFT_INVALID_BATCH, "batch must be at least one"};
+  }
+  if (c.dimensions < 1 || c.dimensions > 8) {
+    throw NufftFailure{B200NUFFT_INVALID_DIMENSIONS, "dimensions must lie in 1..8"};
+  }
+  if (c.dimensions > B200NUFFT_MAX_DIMENSIONS) {
+    throw NufftFailure{B200NUFFT_GPU_DIMENSIONS_UNSUPPORTED,
+                       "GPU plans support 1 to 3 dimensions"};
+  }
+  dim_ = c.dimensions;
+  batch_ = c.batch;
+  mode_count_ = 1;
+  for (int a = 0; a < dim_; ++a) {
+    if (c.n_modes[a] <= 0) {
+      throw NufftFailure{B200NUFFT_ZERO_MODE, "axis " + std::to_string(a) + " has no modes"};
+    }
+    modes_[a] = c.n_modes[a];
+    if (mode_count_ > std::numeric_limits<int64_t>::max() / modes_[a]) {
+      throw NufftFailure{B200NUFFT_LENGTH_OVERFLOW, "total Fourier mode count"};
+    }
+    mode_count_ *= modes_[a];
+  }
+  if (mode_count_ > std::numeric_limits<int64_t>::max() / batch_) {
+    throw NufftFailure{B200NUFFT_LENGTH_OVERFLOW, "batched Fourier mode count"};
+  }
+  eps_ = c.eps;
+  isign_ = c.isign >= 0 ? 1 : -1;
+  if (c.mode_order != B200NUFFT_MODE_ORDER_CENTERED && c.mode_order != B200NUFFT_MODE_ORDER_FFT) {
+    throw NufftFailure{B200NUFFT_INVALID_ARGUMENT, "mode order must be 0 (centered) or 1 (FFT)"};
+  }
+  mode_order_ = c.mode_order;
+  sigma_ = c.sigma == 0.0 ? 2.0 : c.sigma;
+  precision_ = c.precision == 0 ? B200NUFFT_PRECISION_F32 : c.precision;
+  if (precision_ != B200NUFFT_PRECISION_F32) {
+    throw NufftFailure{B200NUFFT_PRECISION_UNSUPPORTED,
+                       "this build runs F32 type-1/type-2 plans; f64 plans are not built yet"};
+  }
+  kernel_ = EsKernel::for_tolerance(eps_, sigma_);
+  fine_count_ = 1;
+  for (int a = 0; a < dim_; ++a) {
+    const uint64_t n = select_fine_grid_size(static_cast<uint64_t>(modes_[a]), sigma_, kernel_.width);
+    fine_.push_back(static_cast<int64_t>(n));
+  }
+  const bool horner = precision_ != B200NUFFT_PRECISION_F32;
+  if (horner) horner_ = EsHornerTable::fit(kernel_);
+  for (int a = 0; a < dim_; ++a) {
+    phi_hat_.push_back(centered_fourier_coefficients(kernel_, static_cast<size_t>(fine_[a]),
+                                                     horner ? &horner_ : nullptr));
+  }
+  if (precision_ == B200NUFFT_PRECISION_F32) {
+    validate_f32_rounding(modes_, dim_, eps_, sigma_, phi_hat_);
+    // src/gpu_type1_nd.rs:68-73: support indices must stay exact in f32.
+    const int64_t maximum = (int64_t(1) << 24) - kernel_.width;
+    for (int a = 0; a < dim_; ++a) {
+      if (fine_[a] > maximum) {
+        throw NufftFailure{B200NUFFT_GPU_FINE_GRID_INDEX_UNSUPPORTED,
+                           "fine-grid axis of " + std::to_string(fine_[a]) +
+                               " cells exceeds the f32-exact maximum " + std::to_string(maximum)};
+      }
+    }
+  }
+  for (int a = 0; a < dim_; ++a) {
+    if (fine_count_ > std::numeric_limits<int64_t>::max() / fine_[a]) {
+      throw NufftFailure{B200NUFFT_LENGTH_OVERFLOW, "fine-grid element count"};
+    }
+    fine_count_ *= fine_[a];
+  }
+  layout_ = SpreadLayout::for_grid(kernel_.width, fine_,
+                                   precision_ == B200NUFFT_PRECISION_F32 ? LayoutPrecision::F32
+                                   : precision_ == B200NUFFT_PRECISION_F64 ? LayoutPrecision::F64
+                                                                           : LayoutPrecision::Df64);
+
+  // Deconvolution amplitudes prod_a 1 / phi_hat_a(|k_a|), divided in f64 in
+  // axis order and rounded once (mode_amplitudes_nd, src/gpu_nd.rs:910-951).
+  std::vector<float> amplitudes(static_cast<size_t>(mode_count_));
+  for (int64_t flat = 0; flat < mode_count_; ++flat) {
+    int64_t rest = flat;
+    double amplitude = 1.0;
+    for (int a = 0; a < dim_; ++a) {
+      const int64_t index = rest % modes_[a];
+      rest /= modes_[a];
+      const int64_t mode = mode_for_storage_index(mode_order_, index, modes_[a]);
+      const double coefficient = phi_hat_[a][static_cast<size_t>(mode < 0 ? -mode : mode)];
+      if (!std::isfinite(coefficient) || coefficient == 0.0) {
+        throw NufftFailure{B200NUFFT_INVALID_KERNEL_FOURIER_COEFFICIENT,
+                           "kernel Fourier coefficient of mode " + std::to_string(mode) +
+                               " is zero or not finite"};
+      }
+      amplitude /= coefficient;
+    }
+    const float rounded = static_cast<float>(amplitude);
+    if (!std::isfinite(rounded)) {
+      throw NufftFailure{B200NUFFT_INVALID_KERNEL_FOURIER_COEFFICIENT,
+                         "deconvolution amplitude overflows f32"};
+    }
+    amplitudes[static_cast<size_t>(flat)] = rounded;
+  }
+  amplitudes_host_ = std::move(amplitudes);
+  if (!with_device) return;
+  int current = 0;
+  check_cuda(cudaGetDevice(&current), "current device");
+  device_ = c.device < 0 ? current : c.device;
+  make_current();
+  void* amp = amplitudes_.reserve(amplitudes_host_.size() * sizeof(float), "deconvolution amplitudes");
+  check_cuda(cudaMemcpy(amp, amplitudes_host_.data(), amplitudes_host_.size() * sizeof(float),
+                        cudaMemcpyHostToDevice),
+             "upload deconvolution amplitudes");
+
+  std::memset(&grid_, 0, sizeof(grid_));
+  grid_.dimensions = dim_;
+  grid_.width = kernel_.width;
+  grid_.half_width = static_cast<float>(kernel_.half_width());
+  grid_.beta = static_cast<float>(kernel_.beta);
+  grid_.fine_count = fine_count_;
+  for (int a = 0; a < dim_; ++a) {
+    const double scale = static_cast<double>(fine_[a]) / kTwoPi;
+    FoldAxis& axis = grid_.axis[a];
+    axis.scale_hi = static_cast<float>(scale);
+    axis.scale_lo = static_cast<float>(scale - static_cast<double>(axis.scale_hi));
+    axis.origin = static_cast<float>(fine_[a] / 2);
+    axis.length_f = static_cast<float>(fine_[a]);
+    axis.length = static_cast<int32_t>(fine_[a]);
+    grid_.fine[a] = fine_[a];
+  }
+  std::memset(&modes_params_, 0, sizeof(modes_params_));
+  modes_params_.dimensions = dim_;
+  modes_params_.centered = mode_order_ == B200NUFFT_MODE_ORDER_CENTERED ? 1 : 0;
+  modes_params_.mode_count = mode_count_;
+  modes_params_.fine_count = fine_count_;
+  for (int a = 0; a < dim_; ++a) {
+    modes_params_.modes[a] = modes_[a];
+    modes_params_.fine[a] = fine_[a];
+  }
+  fine_grid_.reserve(static_cast<size_t>(batch_) * fine_count_ * 2 * scalar_bytes(), "fine grid");
+  counters_.reserve(8 * sizeof(uint32_t), "sort tickets");
+  check_cuda(cudaMemset(counters_.get(), 0, 8 * sizeof(uint32_t)), "clear sort tickets");
+  hist_.reserve(4 * 256 * sizeof(uint32_t), "digit histograms");
+  max_bits_.reserve(static_cast<size_t>(batch_) * sizeof(uint32_t), "strength maxima");
+}
+
+NufftPlan::~NufftPlan() {
+  if (!has_device_) return;
+  cudaSetDevice(device_);
+  cudaDeviceSynchronize();
+  for (auto& entry : ffts_) cufftDestroy(entry.second);
+}
+
+void NufftPlan::make_current() const { check_cuda(cudaSetDevice(device_), "select plan device"); }
+
+size_t NufftPlan::scalar_bytes() const {
+  return precision_ == B200NUFFT_PRECISION_F32 ? 4 : 8;
+}
+
+void NufftPlan::validate_active_batch(int64_t active_batch) const {
+  if (active_batch <= 0 || active_batch > batch_) {
+    throw NufftFailure{B200NUFFT_INVALID_BATCH, "active batch " + std::to_string(active_batch) +
+                                                    " outside 1.." + std::to_string(batch_)};
+  }
+}
+
+uint64_t NufftPlan::required_point_bytes(int64_t count) const {
+  if (count < 0) throw NufftFailure{B200NUFFT_INVALID_ARGUMENT, "negative point count"};
+  const size_t coord = precision_ == B200NUFFT_PRECISION_F32 ? 4 : 8;
+  return static_cast<uint64_t>(count) * dim_ * coord;
+}
+
+uint64_t NufftPlan::required_input_bytes(int64_t count, int64_t active_batch) const {
+  validate_active_batch(active_batch);
+  const uint64_t elements = type_ == 1 ? static_cast<uint64_t>(count) : static_cast<uint64_t>(mode_count_);
+  return elements * active_batch * 2 * (precision_ == B200NUFFT_PRECISION_F32 ? 4 : 8);
+}
+
+uint64_t NufftPlan::required_output_bytes(int64_t count, int64_t active_batch) const {
+  validate_active_batch(active_batch);
+  const uint64_t elements = type_ == 1 ? static_cast<uint64_t>(mode_count_) : static_cast<uint64_t>(count);
+  return elements * active_batch * 2 * (precision_ == B200NUFFT_PRECISION_F32 ? 4 : 8);
+}
+
+void NufftPlan::configure_bins(int geometry) {
+  const BinGeometry& g = layout_.geometries[static_cast<size_t>(geometry)];
+  uint64_t stride = 1;
+  for (int a = 0; a < dim_; ++a) {
+    grid_.axis[a].shift = ilog2(g.side[a]);
+    grid_.axis[a].bins = static_cast<uint32_t>(g.bins[a]);
+    grid_.axis[a].stride = static_cast<uint32_t>(stride);
+    stride *= static_cast<uint64_t>(g.bins[a]);
+  }
+  bins_ = stride;
+}
+
+void NufftPlan::configure_type2_bins() {
+  // Interpolation bins of 8 cells per axis in 1D and 2D and 4 in 3D
+  // (src/gpu.rs:19, src/gpu_2d.rs:22, src/gpu_3d.rs:25).
+  const int side = dim_ == 3 ? 4 : 8;
+  uint64_t stride = 1;
+  for (int a = 0; a < dim_; ++a) {
+    const int64_t bins = (fine_[a] + side - 1) / side;
+    grid_.axis[a].shift = ilog2(side);
+    grid_.axis[a].bins = static_cast<uint32_t>(bins);
+    grid_.axis[a].stride = static_cast<uint32_t>(stride);
+    stride *= static_cast<uint64_t>(bins);
+  }
+  bins_ = stride;
+}
+
+void NufftPlan::configure_tiles() {
+  SpreadParams& sp = spread_;
+  std::memset(&sp, 0, sizeof(sp));
+  sp.grid = grid_;
+  const int w = kernel_.width;
+  int64_t tile[3] = {1, 1, 1};
+  if (dim_ == 1) tile[0] = 1024;
+  if (dim_ == 2) tile[0] = tile[1] = 32;
+  if (dim_ == 3) tile[0] = tile[1] = tile[2] = 16;
+  for (int a = 0; a < dim_; ++a) tile[a] = std::min(tile[a], pow2_ceil(fine_[a]));
+  auto padded_bytes = [&]() {
+    int64_t cells = 1;
+    for (int a = 0; a < dim_; ++a) cells *= tile[a] + w - 1;
+    return cells * 16;
+  };
+  while (padded_bytes() > kTileBytesTarget) {
+    int largest = dim_ - 1;
+    for (int a = dim_ - 1; a >= 0; --a) {
+      if (tile[a] > tile[largest]) largest = a;
+    }
+    if (tile[largest] == 1) break;
+    tile[largest] /= 2;
+  }
+  sp.tile_count = 1;
+  sp.padded_cells = 1;
+  int64_t tiles_per_bin = 1;
+  int64_t rows = 1;
+  for (int a = 0; a < dim_; ++a) {
+    sp.tile[a] = static_cast<int32_t>(tile[a]);
+    sp.pad[a] = static_cast<int32_t>(tile[a] + w - 1);
+    sp.ntiles[a] = static_cast<int32_t>((fine_[a] + tile[a] - 1) / tile[a]);
+    sp.tile_count *= sp.ntiles[a];
+    sp.padded_cells *= sp.pad[a];
+    const int64_t side = int64_t(1) << grid_.axis[a].shift;
+    if (side > tile[a]) tiles_per_bin *= side / tile[a];
+    if (a > 0) rows *= std::max<int64_t>(1, tile[a] / side);
+  }
+  for (int a = dim_; a < 3; ++a) {
+    sp.tile[a] = 1;
+    sp.pad[a] = 1;
+    sp.ntiles[a] = 1;
+  }
+  if (rows > kMaxTileRows) {
+    throw NufftFailure{B200NUFFT_INTERNAL, "spreading tile spans too many bin rows"};
+  }
+  sp.part_cap = kPartCap;
+  sp.headroom = ilog2(static_cast<int64_t>(kPartCap) + 1);
+  // Candidate (tile, local) pairs of every coordinate of every axis: tile t
+  // covers cells (t * tile + l) mod n for l < pad.
+  host_candidates_.clear();
+  for (int a = 0; a < dim_; ++a) {
+    const int64_t n = fine_[a];
+    std::vector<std::vector<int2>> lists(static_cast<size_t>(n));
+    for (int64_t t = 0; t < sp.ntiles[a]; ++t) {
+      for (int64_t l = 0; l < sp.pad[a]; ++l) {
+        const int64_t cell = (t * tile[a] + l) % n;
+        lists[static_cast<size_t>(cell)].push_back(make_int2(static_cast<int>(t), static_cast<int>(l)));
+      }
+    }
+    size_t most = 1;
+    for (const auto& list : lists) most = std::max(most, list.size());
+    sp.candidate_base[a] = static_cast<int64_t>(host_candidates_.size());
+    sp.candidate_count[a] = static_cast<int32_t>(most);
+    for (const auto& list : lists) {
+      for (size_t k = 0; k < most; ++k) {
+        host_candidates_.push_back(k < list.size() ? list[k] : make_int2(-1, -1));
+      }
+    }
+  }
+  void* cand = candidates_.reserve(host_candidates_.size() * sizeof(int2), "fold candidates");
+  check_cuda(cudaMemcpy(cand, host_candidates_.data(), host_candidates_.size() * sizeof(int2),
+                        cudaMemcpyHostToDevice),
+             "upload fold candidates");
+  (void)tiles_per_bin;
+  spread_.grid = grid_;
+  part_upper_bound_ = sp.tile_count + (std::max<int64_t>(point_count_, 0) * tiles_per_bin +
+                                       kPartCap - 1) / kPartCap + 1;
+}
+
+int NufftPlan::choose_geometry(int64_t point_count) const {
+  if (type_ != 1) throw NufftFailure{B200NUFFT_INVALID_ARGUMENT, "type-2 plans bin in one geometry"};
+  if (point_count < 0) throw NufftFailure{B200NUFFT_INVALID_ARGUMENT, "negative point count"};
+  return layout_.choose_geometry(point_count);
+}
+
+void NufftPlan::set_points(int64_t count, const void* points, cudaStream_t stream) {
+  if (!has_device_) {
+    throw NufftFailure{B200NUFFT_GPU_EXECUTION_UNAVAILABLE,
+                       "the plan was created without device resources"};
+  }
+  make_current();
+  if (count < 0) throw NufftFailure{B200NUFFT_INVALID_ARGUMENT, "negative point count"};
+  if (count > kMaxPoints) {
+    throw NufftFailure{B200NUFFT_LENGTH_OVERFLOW, "more than 2^30 - 1 points in one point set"};
+  }
+  if (count > 0 && points == nullptr) {
+    throw NufftFailure{B200NUFFT_INVALID_ARGUMENT, "null point buffer"};
+  }
+  point_count_ = count;
+  points_ = points;
+  if (type_ == 1) {
+    geometry_ = layout_.choose_geometry(count);
+    configure_bins(geometry_);
+  } else {
+    geometry_ = -1;
+    configure_type2_bins();
+  }
+  const size_t words = static_cast<size_t>(std::max<int64_t>(count, 1)) * sizeof(uint32_t);
+  SortBuffers buf;
+  buf.keys_a = static_cast<uint32_t*>(keys_a_.reserve(words, "bin keys"));
+  buf.keys_b = static_cast<uint32_t*>(keys_b_.reserve(words, "bin keys"));
+  buf.vals_a = static_cast<uint32_t*>(vals_a_.reserve(words, "point permutation"));
+  buf.vals_b = static_cast<uint32_t*>(vals_b_.reserve(words, "point permutation"));
+  buf.hist = static_cast<uint32_t*>(hist_.get());
+  buf.status = static_cast<uint32_t*>(status_.reserve(sort_status_bytes(count), "look-back words"));
+  buf.counters = static_cast<uint32_t*>(counters_.get());
+  uint32_t* offsets =
+      static_cast<uint32_t*>(offsets_.reserve((bins_ + 1) * sizeof(uint32_t), "bin offsets"));
+  sort_points(static_cast<const float*>(points), count, grid_,
+              type_ == 1 ? KeyKind::SupportStart : KeyKind::ApproximateCell, bins_, buf, offsets,
+              &perm_, &sorted_keys_, stream, &timer_);
+  if (type_ == 1) {
+    configure_tiles();
+    parts_.reserve(static_cast<size_t>(spread_.tile_count) * sizeof(uint32_t), "tile parts");
+    part_start_.reserve(static_cast<size_t>(spread_.tile_count + 1) * sizeof(uint32_t),
+                        "tile part offsets");
+    spread_count_parts(spread_, offsets, static_cast<uint32_t*>(parts_.get()),
+                       static_cast<uint32_t*>(part_start_.get()), stream, &timer_);
+  }
+  check_cuda(cudaGetLastError(), "set points launch");
+}
+
+cufftHandle NufftPlan::fft_for(int batch) {
+  auto found = ffts_.find(batch);
+  if (found != ffts_.end()) return found->second;
+  int n[3];
+  for (int a = 0; a < dim_; ++a) n[a] = static_cast<int>(fine_[dim_ - 1 - a]);
+  cufftHandle handle;
+  const cufftType kind = precision_ == B200NUFFT_PRECISION_F32 ? CUFFT_C2C : CUFFT_Z2Z;
+  const cufftResult r = cufftPlanMany(&handle, dim_, n, nullptr, 1, static_cast<int>(fine_count_),
+                                      nullptr, 1, static_cast<int>(fine_count_), kind, batch);
+  if (r != CUFFT_SUCCESS) {
+    throw NufftFailure{B200NUFFT_FFT_SHAPE_UNSUPPORTED,
+                       "cuFFT plan creation failed with code " + std::to_string(static_cast<int>(r))};
+  }
+  ffts_[batch] = handle;
+  return handle;
+}
+
+void NufftPlan::run_fft(void* fine, int batch, int direction, cudaStream_t stream) {
+  StageScope scope(&timer_, kStageFft, stream);
+  cufftHandle h = fft_for(batch);
+  cufftSetStream(h, stream);
+  const cufftResult r =
+      precision_ == B200NUFFT_PRECISION_F32
+          ? cufftExecC2C(h, static_cast<cufftComplex*>(fine), static_cast<cufftComplex*>(fine), direction)
+          : cufftExecZ2Z(h, static_cast<cufftDoubleComplex*>(fine),
+                         static_cast<cufftDoubleComplex*>(fine), direction);
+  if (r != CUFFT_SUCCESS) {
+    throw NufftFailure{B200NUFFT_FFT_EXECUTION_FAILED,
+                       "cuFFT execution failed with code " + std::to_string(static_cast<int>(r))};
+  }
+}
+
+void NufftPlan::execute(int64_t active_batch, const void* input, void* output, cudaStream_t stream) {
+  if (!has_device_) {
+    throw NufftFailure{B200NUFFT_GPU_EXECUTION_UNAVAILABLE,
+                       "the plan was created without device resources"};
+  }
+  make_current();
+  validate_active_batch(active_batch);
+  if (point_count_ < 0) {
+    throw NufftFailure{B200NUFFT_GPU_EXECUTION_UNAVAILABLE,
+                       "call b200nufft_set_points (or b200nufft_encode) before executing"};
+  }
+  if (output == nullptr || (input == nullptr && (type_ == 2 || point_count_ > 0))) {
+    throw NufftFailure{B200NUFFT_INVALID_ARGUMENT, "null input or output buffer"};
+  }
+  const uint64_t in_bytes = required_input_bytes(point_count_, active_batch);
+  const uint64_t out_bytes = required_output_bytes(point_count_, active_batch);
+  const char* in_lo = static_cast<const char*>(input);
+  const char* out_lo = static_cast<const char*>(output);
+  if (input && in_bytes && out_bytes && in_lo < out_lo + out_bytes && out_lo < in_lo + in_bytes) {
+    throw NufftFailure{B200NUFFT_GPU_BUFFER_ALIAS_UNSUPPORTED, "input and output overlap"};
+  }
+  const int batch = static_cast<int>(active_batch);
+  float2* fine = static_cast<float2*>(fine_grid_.get());
+  const int direction = isign_ >= 0 ? CUFFT_INVERSE : CUFFT_FORWARD;
+  if (type_ == 1) {
+    if (point_count_ == 0) {
+      check_cuda(cudaMemsetAsync(output, 0, out_bytes, stream), "zero type-1 output");
+      return;
+    }
+    const size_t scratch_bytes = static_cast<size_t>(part_upper_bound_) * batch *
+                                 spread_.padded_cells * sizeof(float2);
+    SpreadLaunch l;
+    l.points = static_cast<const float*>(points_);
+    l.strengths = static_cast<const float2*>(input);
+    l.point_count = point_count_;
+    l.batch = batch;
+    l.perm = perm_;
+    l.offsets = static_cast<const uint32_t*>(offsets_.get());
+    l.part_start = static_cast<const uint32_t*>(part_start_.get());
+    l.part_upper_bound = part_upper_bound_;
+    l.max_bits = static_cast<uint32_t*>(max_bits_.get());
+    l.scratch = static_cast<float2*>(scratch_.reserve(scratch_bytes, "spreading tiles"));
+    l.candidates = static_cast<const int2*>(candidates_.get());
+    l.fine = fine;
+    spread_execute(spread_, l, stream, &timer_);
+    run_fft(fine, batch, direction, stream);
+    StageScope scope(&timer_, kStageDeconvolution, stream);
+    deconvolve_f32(modes_params_, batch, fine, static_cast<const float*>(amplitudes_.get()),
+                   static_cast<float2*>(output), stream);
+  } else {
+    {
+      StageScope scope(&timer_, kStagePredeconvolution, stream);
+      predeconvolve_f32(modes_params_, batch, static_cast<const float2*>(input),
+                        static_cast<const float*>(amplitudes_.get()), fine, stream);
+    }
+    run_fft(fine, batch, direction, stream);
+    InterpLaunch l;
+    l.points = static_cast<const float*>(points_);
+    l.point_count = point_count_;
+    l.perm = perm_;
+    l.fine = fine;
+    l.batch = batch;
+    l.output = static_cast<float2*>(output);
+    StageScope scope(&timer_, kStageInterpolation, stream);
+    interpolate_execute(grid_, l, stream);
+  }
+  check_cuda(cudaGetLastError(), "execute launch");
+}
+
+void NufftPlan::copy_bin_order(uint32_t* permutation, uint32_t* bin_offsets, cudaStream_t stream) {
+  make_current();
+  if (point_count_ < 0) {
+    throw NufftFailure{B200NUFFT_GPU_EXECUTION_UNAVAILABLE, "no point set"};
+  }
+  if (permutation && point_count_ > 0) {
+    check_cuda(cudaMemcpyAsync(permutation, perm_, point_count_ * sizeof(uint32_t),
+                               cudaMemcpyDeviceToDevice, stream),
+               "copy permutation");
+  }
+  if (bin_offsets) {
+    check_cuda(cudaMemcpyAsync(bin_offsets, offsets_.get(), (bins_ + 1) * sizeof(uint32_t),
+                               cudaMemcpyDeviceToDevice, stream),
+               "copy bin offsets");
+  }
+}
+
+void NufftPlan::copy_prepared_slots(int32_t* starts, float* offsets, cudaStream_t stream) {
+  make_current();
+  if (point_count_ < 0 || type_ != 1) {
+    throw NufftFailure{B200NUFFT_GPU_EXECUTION_UNAVAILABLE, "no type-1 point set"};
+  }
+  if (!starts || !offsets) throw NufftFailure{B200NUFFT_INVALID_ARGUMENT, "null buffer"};
+  prepare_reference_slots(static_cast<const float*>(points_), point_count_, grid_, perm_,
+                          sorted_keys_, starts, offsets, stream);
+}
+
+void NufftPlan::synchronize(cudaStream_t stream) {
+  make_current();
+  check_cuda(cudaStreamSynchronize(stream), "synchronize");
+  uint32_t flag = 0;
+  check_cuda(cudaMemcpy(&flag, static_cast<uint32_t*>(counters_.get()) + 7, sizeof(uint32_t),
+                        cudaMemcpyDeviceToHost),
+             "read device flags");
+  if (flag != 0) {
+    cudaMemset(static_cast<uint32_t*>(counters_.get()) + 7, 0, sizeof(uint32_t));
+    throw NufftFailure{B200NUFFT_DEVICE_TIMEOUT,
+                       "a bin-sort tile gave up waiting for its predecessor; results are invalid"};
+  }
+}
+
+void NufftPlan::info(b200nufft_plan_info* out) const {
+  std::memset(out, 0, sizeof(*out));
+  out->type = type_;
+  out->dimensions = dim_;
+  out->precision = precision_;
+  out->kernel_width = kernel_.width;
+  out->kernel_beta = kernel_.beta;
+  for (int a = 0; a < dim_; ++a) out->fine_shape[a] = fine_[a];
+  out->mode_count = mode_count_;
+  out->batch = batch_;
+  out->geometry_count = static_cast<int32_t>(std::min<size_t>(layout_.geometries.size(), 16));
+  for (int g = 0; g < out->geometry_count; ++g) {
+    for (int a = 0; a < dim_; ++a) {
+      out->geometry_sides[g][a] = static_cast<int32_t>(layout_.geometries[static_cast<size_t>(g)].side[a]);
+    }
+  }
+  out->point_count = point_count_;
+  out->chosen_geometry = geometry_;
+  out->bin_count = static_cast<int64_t>(bins_);
+}
+
+}  // namespace b200nufft

@@ -1,0 +1,102 @@
+// Type-1 / type-2 plans (the NufftPlan mirror) as the C++ host sees them.
+#pragma once
+
+#include <cufft.h>
+
+#include <map>
+#include <memory>
+#include <vector>
+
+#include "device.h"
+#include "es_kernel.h"
+#include "interp.h"
+#include "layout.h"
+#include "modes.h"
+#include "spread.h"
+
+namespace b200nufft {
+
+class NufftPlan {
+ public:
+  // Without a device only the host-side metadata is built (the reference's
+  // NufftPlan::type1 / type2 plans without GPU resources, src/plan.rs:449-455).
+  explicit NufftPlan(const b200nufft_config& config, bool with_device = true);
+  ~NufftPlan();
+
+  void set_points(int64_t count, const void* points, cudaStream_t stream);
+  void execute(int64_t active_batch, const void* input, void* output, cudaStream_t stream);
+  void info(b200nufft_plan_info* out) const;
+  int choose_geometry(int64_t point_count) const;
+  const std::vector<double>& phi_hat(int axis) const { return phi_hat_[axis]; }
+  uint64_t required_point_bytes(int64_t count) const;
+  uint64_t required_input_bytes(int64_t count, int64_t active_batch) const;
+  uint64_t required_output_bytes(int64_t count, int64_t active_batch) const;
+  void copy_bin_order(uint32_t* permutation, uint32_t* bin_offsets, cudaStream_t stream);
+  void copy_prepared_slots(int32_t* starts, float* offsets, cudaStream_t stream);
+  // Waits for the plan's work on `stream` and reports a device wait that gave up.
+  void synchronize(cudaStream_t stream);
+  StageTimer& timer() { return timer_; }
+
+  int type() const { return type_; }
+  int dimensions() const { return dim_; }
+  int precision() const { return precision_; }
+  int64_t batch() const { return batch_; }
+  int64_t mode_count() const { return mode_count_; }
+  int device() const { return device_; }
+  const std::vector<int64_t>& fine_shape() const { return fine_; }
+  const EsKernel& kernel() const { return kernel_; }
+
+ private:
+  void make_current() const;
+  void validate_active_batch(int64_t active_batch) const;
+  void configure_bins(int geometry);
+  void configure_type2_bins();
+  void configure_tiles();
+  cufftHandle fft_for(int batch);
+  void run_fft(void* fine, int batch, int direction, cudaStream_t stream);
+  size_t scalar_bytes() const;
+
+  int type_ = 1;
+  int dim_ = 1;
+  int64_t modes_[3] = {1, 1, 1};
+  int64_t batch_ = 1;
+  double eps_ = 1e-6;
+  int isign_ = 1;
+  int mode_order_ = 0;
+  double sigma_ = 2.0;
+  int precision_ = B200NUFFT_PRECISION_F32;
+  int device_ = 0;
+  EsKernel kernel_;
+  EsHornerTable horner_;
+  std::vector<int64_t> fine_;
+  std::vector<std::vector<double>> phi_hat_;
+  SpreadLayout layout_;
+  int64_t mode_count_ = 1;
+  int64_t fine_count_ = 1;
+  GridParams grid_{};
+  ModeParams modes_params_{};
+  SpreadParams spread_{};
+
+  bool has_device_ = true;
+  StageTimer timer_;
+  std::vector<float> amplitudes_host_;
+  DeviceBuffer amplitudes_;
+  DeviceBuffer fine_grid_;
+  std::map<int, cufftHandle> ffts_;
+
+  // Remembered points and their bin order.
+  int64_t point_count_ = -1;
+  const void* points_ = nullptr;
+  int geometry_ = -1;
+  uint64_t bins_ = 0;
+  uint32_t* perm_ = nullptr;
+  uint32_t* sorted_keys_ = nullptr;
+  DeviceBuffer keys_a_, keys_b_, vals_a_, vals_b_, hist_, status_, counters_, offsets_;
+
+  // Spreading state.
+  DeviceBuffer parts_, part_start_, max_bits_, scratch_, candidates_;
+  int64_t part_upper_bound_ = 0;
+  std::vector<int2> host_candidates_;
+};
+
+}  // namespace b200nufft

@@ -1,0 +1,447 @@
+// Stable binning of the nonuniform points.
+//
+// The reference bins points with u32 atomics, a prefix scan, a scatter, a
+// merge sort of bins above 64 points and an O(bin^2) ranking of the smaller
+// ones (src/gpu_nd_bins.rs:336-709, src/gpu_bin_sort.rs, src/gpu_scan.rs);
+// its result is the points sorted by bin key, ties in original index order,
+// plus the exclusive scan of the bin counts with a trailing total. Here the
+// same order comes from a least-significant-digit radix sort whose passes are
+// single kernels with a decoupled look-back across tiles (one pass per 8 key
+// bits), which is stable by construction, so no bin needs a second sort
+// however clustered the points are. Bin offsets then follow from the sorted
+// keys without atomics: the first slot of every bin is where its key begins.
+#include <cuda_runtime.h>
+
+#include <algorithm>
+#include <cstdio>
+
+#include "device.h"
+
+namespace b200nufft {
+
+namespace {
+
+constexpr int kSortThreads = 256;
+constexpr int kSortWarps = kSortThreads / 32;
+constexpr int kItemsPerThread = 16;
+constexpr int kSortTile = kSortThreads * kItemsPerThread;
+constexpr int kRadix = 256;
+constexpr uint32_t kFlagAggregate = 1u << 30;
+constexpr uint32_t kFlagInclusive = 2u << 30;
+constexpr uint32_t kValueMask = (1u << 30) - 1;
+// Polls of a predecessor's look-back word before a tile gives up and flags
+// an error (about a second with the back-off below).
+constexpr uint32_t kLookbackPollLimit = 1u << 24;
+
+// ---------------------------------------------------------------------------
+// Keys.
+
+// Bin key of a point from its support starts (src/gpu_nd_bins.rs:474-554):
+// every axis's start is computed only when all coordinates lie within the
+// fold's reach; otherwise the point lands in bin 0 of every axis.
+template <int D>
+__device__ __forceinline__ uint32_t support_start_key(const float* p, const GridParams& g) {
+  bool reach = true;
+#pragma unroll
+  for (int a = 0; a < D; ++a) reach = reach && in_fold_reach(p[a]);
+  uint32_t key = 0;
+#pragma unroll
+  for (int a = 0; a < D; ++a) {
+    int32_t start = 0;
+    if (reach) {
+      Df64 offset;
+      support_of(p[a], g.axis[a], g.half_width, start, offset);
+    }
+    const int32_t wrapped = wrap_start(start, g.axis[a].length);
+    key += (static_cast<uint32_t>(wrapped) >> g.axis[a].shift) * g.axis[a].stride;
+  }
+  return key;
+}
+
+// Grid cell of a coordinate folded in plain f32 and clamped onto the grid
+// (approximate_cell, src/gpu_point_bins.rs:460-464), with the reference's
+// operations kept separate.
+__device__ __forceinline__ uint32_t approximate_cell(float x, const FoldAxis& a) {
+  const float position = __fadd_rn(__fmul_rn(x, a.scale_hi), a.origin);
+  const float wrapped =
+      __fsub_rn(position, __fmul_rn(a.length_f, floorf(__fdiv_rn(position, a.length_f))));
+  const float clamped = fmaxf(wrapped, 0.0f);
+  uint32_t cell = clamped >= 4294967040.0f ? 0xFFFFFFFFu : static_cast<uint32_t>(clamped);
+  const uint32_t last = static_cast<uint32_t>(a.length - 1);
+  return cell < last ? cell : last;
+}
+
+template <int D>
+__device__ __forceinline__ uint32_t approximate_cell_key(const float* p, const GridParams& g) {
+  uint32_t key = 0;
+#pragma unroll
+  for (int a = 0; a < D; ++a) {
+    key += (approximate_cell(p[a], g.axis[a]) >> g.axis[a].shift) * g.axis[a].stride;
+  }
+  return key;
+}
+
+// Computes every point's key and the digit histograms of all passes.
+template <int D, KeyKind K>
+__global__ void __launch_bounds__(256) bin_keys_kernel(const float* __restrict__ points,
+                                                       int64_t count, GridParams g,
+                                                       uint32_t* __restrict__ keys,
+                                                       uint32_t* __restrict__ hist, int passes) {
+  __shared__ uint32_t local[4][kRadix];
+  for (int i = threadIdx.x; i < 4 * kRadix; i += blockDim.x) (&local[0][0])[i] = 0;
+  __syncthreads();
+  const int64_t stride = static_cast<int64_t>(gridDim.x) * blockDim.x;
+  for (int64_t i = static_cast<int64_t>(blockIdx.x) * blockDim.x + threadIdx.x; i < count;
+       i += stride) {
+    float p[D];
+#pragma unroll
+    for (int a = 0; a < D; ++a) p[a] = points[i * D + a];
+    const uint32_t key =
+        K == KeyKind::SupportStart ? support_start_key<D>(p, g) : approximate_cell_key<D>(p, g);
+    keys[i] = key;
+    for (int pass = 0; pass < passes; ++pass) {
+      atomicAdd(&local[pass][(key >> (8 * pass)) & 0xFF], 1u);
+    }
+  }
+  __syncthreads();
+  for (int i = threadIdx.x; i < passes * kRadix; i += blockDim.x) {
+    const uint32_t v = (&local[0][0])[i];
+    if (v) atomicAdd(&hist[i], v);
+  }
+}
+
+// Exclusive scan of every pass's 256 digit counts, in place.
+__global__ void digit_scan_kernel(uint32_t* hist, int passes) {
+  __shared__ uint32_t buffer[kRadix];
+  for (int pass = 0; pass < passes; ++pass) {
+    const uint32_t v = hist[pass * kRadix + threadIdx.x];
+    buffer[threadIdx.x] = v;
+    __syncthreads();
+    for (int offset = 1; offset < kRadix; offset <<= 1) {
+      const uint32_t add = threadIdx.x >= offset ? buffer[threadIdx.x - offset] : 0u;
+      __syncthreads();
+      buffer[threadIdx.x] += add;
+      __syncthreads();
+    }
+    hist[pass * kRadix + threadIdx.x] = buffer[threadIdx.x] - v;
+    __syncthreads();
+  }
+}
+
+// ---------------------------------------------------------------------------
+// One stable counting pass over 8 key bits.
+//
+// Tiles take their index from a ticket so that every earlier tile has already
+// started; each tile ranks its items within warps (match on the digit, in
+// item order), publishes its digit counts, then adds its predecessors'
+// counts by looking back until it meets an inclusive prefix. Items go
+// through shared memory so that the global stores of one digit are
+// contiguous.
+__global__ void __launch_bounds__(kSortThreads) onesweep_pass_kernel(
+    const uint32_t* __restrict__ keys_in, const uint32_t* __restrict__ vals_in,
+    uint32_t* __restrict__ keys_out, uint32_t* __restrict__ vals_out, int64_t count, int shift,
+    const uint32_t* __restrict__ digit_base, uint32_t* status, uint32_t* ticket,
+    uint32_t* error_flag, int write_keys) {
+  __shared__ uint32_t s_tile;
+  __shared__ uint32_t warp_counts[kSortWarps][kRadix];
+  __shared__ uint32_t s_local_start[kRadix];
+  __shared__ uint32_t s_global_start[kRadix];
+  __shared__ uint32_t s_keys[kSortTile];
+  __shared__ uint32_t s_vals[kSortTile];
+
+  const int tid = threadIdx.x;
+  const int warp = tid >> 5;
+  const int lane = tid & 31;
+  if (tid == 0) s_tile = atomicAdd(ticket, 1u);
+  for (int i = tid; i < kSortWarps * kRadix; i += kSortThreads) (&warp_counts[0][0])[i] = 0;
+  __syncthreads();
+  const uint32_t tile = s_tile;
+  const int64_t tile_base = static_cast<int64_t>(tile) * kSortTile;
+  const int64_t warp_base = tile_base + static_cast<int64_t>(warp) * 32 * kItemsPerThread;
+
+  uint32_t key[kItemsPerThread];
+  uint32_t val[kItemsPerThread];
+  uint32_t rank[kItemsPerThread];
+#pragma unroll
+  for (int i = 0; i < kItemsPerThread; ++i) {
+    const int64_t index = warp_base + i * 32 + lane;
+    const bool valid = index < count;
+    key[i] = valid ? keys_in[index] : 0u;
+    val[i] = valid ? (vals_in ? vals_in[index] : static_cast<uint32_t>(index)) : 0u;
+  }
+  const uint32_t lane_below = (1u << lane) - 1u;
+#pragma unroll
+  for (int i = 0; i < kItemsPerThread; ++i) {
+    const int64_t index = warp_base + i * 32 + lane;
+    const bool valid = index < count;
+    const uint32_t active = __ballot_sync(0xFFFFFFFFu, valid);
+    const uint32_t digit = (key[i] >> shift) & 0xFFu;
+    uint32_t peers = 0, before = 0;
+    if (valid) {
+      peers = __match_any_sync(active, digit);
+      before = warp_counts[warp][digit];
+      rank[i] = before + __popc(peers & lane_below);
+    }
+    __syncwarp();
+    if (valid && (31 - __clz(peers)) == lane) warp_counts[warp][digit] = before + __popc(peers);
+    __syncwarp();
+  }
+  __syncthreads();
+
+  // Per digit: the tile's count, and each warp's exclusive prefix.
+  const int digit = tid;
+  uint32_t total = 0;
+#pragma unroll
+  for (int w = 0; w < kSortWarps; ++w) {
+    const uint32_t c = warp_counts[w][digit];
+    warp_counts[w][digit] = total;
+    total += c;
+  }
+  // Publish the aggregate (or the inclusive prefix of the first tile).
+  volatile uint32_t* my_status = status + static_cast<size_t>(tile) * kRadix + digit;
+  if (tile == 0) {
+    *my_status = kFlagInclusive | total;
+  } else {
+    *my_status = kFlagAggregate | total;
+  }
+  // Exclusive scan of the tile's digit counts: where each digit starts in the
+  // tile's shared-memory order.
+  s_local_start[digit] = total;
+  __syncthreads();
+  for (int offset = 1; offset < kRadix; offset <<= 1) {
+    const uint32_t add = digit >= offset ? s_local_start[digit - offset] : 0u;
+    __syncthreads();
+    s_local_start[digit] += add;
+    __syncthreads();
+  }
+  const uint32_t local_start = s_local_start[digit] - total;
+  __syncthreads();
+  s_local_start[digit] = local_start;
+
+  // Look back over the predecessors.
+  uint32_t exclusive = 0;
+  if (tile > 0) {
+    int64_t j = static_cast<int64_t>(tile) - 1;
+    uint32_t polls = 0;
+    bool failed = false;
+    while (j >= 0) {
+      const uint32_t word = *(volatile uint32_t*)(status + static_cast<size_t>(j) * kRadix + digit);
+      const uint32_t flag = word & ~kValueMask;
+      if (flag == 0u) {
+        if (++polls > kLookbackPollLimit) {
+          failed = true;
+          break;
+        }
+        __nanosleep(64);
+        continue;
+      }
+      exclusive += word & kValueMask;
+      if (flag == kFlagInclusive) break;
+      --j;
+    }
+    if (failed) atomicExch(error_flag, 1u);
+    __threadfence();
+    *my_status = kFlagInclusive | ((exclusive + total) & kValueMask);
+  }
+  s_global_start[digit] = digit_base[digit] + exclusive;
+  __syncthreads();
+
+#pragma unroll
+  for (int i = 0; i < kItemsPerThread; ++i) {
+    const int64_t index = warp_base + i * 32 + lane;
+    if (index < count) {
+      const uint32_t d = (key[i] >> shift) & 0xFFu;
+      const uint32_t position = s_local_start[d] + warp_counts[warp][d] + rank[i];
+      s_keys[position] = key[i];
+      s_vals[position] = val[i];
+    }
+  }
+  __syncthreads();
+  const int64_t remaining = count - tile_base;
+  const int valid_items = remaining < kSortTile ? static_cast<int>(remaining) : kSortTile;
+  for (int p = tid; p < valid_items; p += kSortThreads) {
+    const uint32_t k = s_keys[p];
+    const uint32_t d = (k >> shift) & 0xFFu;
+    const uint32_t out = s_global_start[d] + (p - s_local_start[d]);
+    if (write_keys) keys_out[out] = k;
+    vals_out[out] = s_vals[p];
+  }
+}
+
+// First slot of every bin from the sorted keys: bins (key[i-1], key[i]]
+// start at slot i, and bins past the last key start at `count`.
+__global__ void bin_offsets_kernel(const uint32_t* __restrict__ keys, int64_t count,
+                                   uint64_t bins, uint32_t* __restrict__ offsets) {
+  const int64_t i = static_cast<int64_t>(blockIdx.x) * blockDim.x + threadIdx.x;
+  if (i > count) return;
+  const uint64_t low = i == 0 ? 0ull : static_cast<uint64_t>(keys[i - 1]) + 1ull;
+  const uint64_t high = i == count ? bins : static_cast<uint64_t>(keys[i]);
+  for (uint64_t b = low; b <= high && b <= bins; ++b) offsets[b] = static_cast<uint32_t>(i);
+}
+
+__global__ void identity_kernel(uint32_t* __restrict__ perm, uint32_t* __restrict__ keys,
+                                int64_t count) {
+  const int64_t i = static_cast<int64_t>(blockIdx.x) * blockDim.x + threadIdx.x;
+  if (i < count) {
+    perm[i] = static_cast<uint32_t>(i);
+    keys[i] = 0u;
+  }
+}
+
+// Reference start_in_bin (src/gpu_nd_bins.rs:658-670): a start binned one
+// cell across the edge of its bin is moved to the nearest start of the bin.
+__device__ __forceinline__ int32_t start_in_bin(int32_t start, int32_t low, int32_t side,
+                                                int32_t n) {
+  const int32_t span = min(low + side, n) - 1 - low;
+  int32_t delta = (start < 0 ? start + n : start) - low;
+  if (delta < 0) delta += n;
+  if (delta > span && n - delta < delta - span) delta -= n;
+  const int32_t clamped = delta < 0 ? 0 : (delta > span ? span : delta);
+  return start + clamped - delta;
+}
+
+template <int D>
+__global__ void prepare_slots_kernel(const float* __restrict__ points, int64_t count, GridParams g,
+                                     const uint32_t* __restrict__ perm,
+                                     const uint32_t* __restrict__ sorted_keys,
+                                     int32_t* __restrict__ starts, float* __restrict__ offsets) {
+  const int64_t slot = static_cast<int64_t>(blockIdx.x) * blockDim.x + threadIdx.x;
+  if (slot >= count) return;
+  const uint32_t point = perm[slot];
+  float p[D];
+#pragma unroll
+  for (int a = 0; a < D; ++a) p[a] = points[static_cast<int64_t>(point) * D + a];
+  bool reach = true;
+#pragma unroll
+  for (int a = 0; a < D; ++a) reach = reach && in_fold_reach(p[a]);
+  uint32_t rest = sorted_keys[slot];
+#pragma unroll
+  for (int a = 0; a < D; ++a) {
+    uint32_t bin_a;
+    if (a == D - 1) {
+      bin_a = rest;
+    } else {
+      bin_a = rest % g.axis[a].bins;
+      rest /= g.axis[a].bins;
+    }
+    const int32_t side = 1 << g.axis[a].shift;
+    int32_t start = 0;
+    Df64 offset{1024.0f, 0.0f};
+    if (reach) support_of(p[a], g.axis[a], g.half_width, start, offset);
+    start = start_in_bin(start, static_cast<int32_t>(bin_a) * side, side, g.axis[a].length);
+    starts[(D + 1) * slot + a] = start;
+    offsets[2 * (D * slot + a)] = offset.hi;
+    offsets[2 * (D * slot + a) + 1] = offset.lo;
+  }
+  starts[(D + 1) * slot + D] = static_cast<int32_t>(point);
+}
+
+template <int D>
+void launch_keys(const float* points, int64_t count, const GridParams& g, KeyKind kind,
+                 uint32_t* keys, uint32_t* hist, int passes, cudaStream_t stream) {
+  const int blocks = static_cast<int>(std::min<int64_t>((count + 255) / 256, 148 * 16));
+  if (kind == KeyKind::SupportStart) {
+    bin_keys_kernel<D, KeyKind::SupportStart>
+        <<<blocks, 256, 0, stream>>>(points, count, g, keys, hist, passes);
+  } else {
+    bin_keys_kernel<D, KeyKind::ApproximateCell>
+        <<<blocks, 256, 0, stream>>>(points, count, g, keys, hist, passes);
+  }
+  note_launch();
+}
+
+}  // namespace
+
+size_t sort_status_bytes(int64_t count) {
+  const int64_t tiles = (count + kSortTile - 1) / kSortTile;
+  return static_cast<size_t>(std::max<int64_t>(tiles, 1)) * kRadix * sizeof(uint32_t);
+}
+
+void sort_points(const float* points, int64_t count, const GridParams& g, KeyKind kind,
+                 uint64_t bins, SortBuffers buf, uint32_t* offsets, uint32_t** perm,
+                 uint32_t** sorted_keys, cudaStream_t stream, StageTimer* timer) {
+  int key_bits = 0;
+  while (key_bits < 32 && (uint64_t(1) << key_bits) < bins) ++key_bits;
+  const int passes = (key_bits + 7) / 8;
+  if (count == 0) {
+    check_cuda(cudaMemsetAsync(offsets, 0, (bins + 1) * sizeof(uint32_t), stream), "clear offsets");
+    *perm = buf.vals_a;
+    *sorted_keys = buf.keys_a;
+    return;
+  }
+  {
+    StageScope scope(timer, kStageBinKeys, stream);
+    check_cuda(cudaMemsetAsync(buf.hist, 0, 4 * kRadix * sizeof(uint32_t), stream), "clear histogram");
+    check_cuda(cudaMemsetAsync(buf.counters, 0, 7 * sizeof(uint32_t), stream), "clear tickets");
+    switch (g.dimensions) {
+      case 1: launch_keys<1>(points, count, g, kind, buf.keys_a, buf.hist, passes, stream); break;
+      case 2: launch_keys<2>(points, count, g, kind, buf.keys_a, buf.hist, passes, stream); break;
+      default: launch_keys<3>(points, count, g, kind, buf.keys_a, buf.hist, passes, stream); break;
+    }
+  }
+  if (passes == 0) {
+    identity_kernel<<<static_cast<unsigned>((count + 255) / 256), 256, 0, stream>>>(buf.vals_a,
+                                                                                 buf.keys_a, count);
+    note_launch();
+    *perm = buf.vals_a;
+    *sorted_keys = buf.keys_a;
+  } else {
+    {
+      StageScope scope(timer, kStageDigitScan, stream);
+      digit_scan_kernel<<<1, kRadix, 0, stream>>>(buf.hist, passes);
+      note_launch();
+    }
+    StageScope scope(timer, kStageRadixPasses, stream);
+    const int64_t tiles = (count + kSortTile - 1) / kSortTile;
+    uint32_t* keys_in = buf.keys_a;
+    uint32_t* vals_in = nullptr;
+    uint32_t* keys_out = buf.keys_b;
+    uint32_t* vals_out = buf.vals_b;
+    for (int pass = 0; pass < passes; ++pass) {
+      check_cuda(cudaMemsetAsync(buf.status, 0, static_cast<size_t>(tiles) * kRadix * sizeof(uint32_t),
+                                 stream),
+                 "clear look-back words");
+      onesweep_pass_kernel<<<static_cast<unsigned>(tiles), kSortThreads, 0, stream>>>(
+          keys_in, vals_in, keys_out, vals_out, count, 8 * pass, buf.hist + pass * kRadix,
+          buf.status, buf.counters + pass, buf.counters + 7, 1);
+      note_launch();
+      // Ping-pong: the next pass reads what this one wrote.
+      uint32_t* next_keys_out = keys_in;
+      uint32_t* next_vals_out = (vals_out == buf.vals_b) ? buf.vals_a : buf.vals_b;
+      keys_in = keys_out;
+      vals_in = vals_out;
+      keys_out = next_keys_out;
+      vals_out = next_vals_out;
+    }
+    *perm = vals_in;
+    *sorted_keys = keys_in;
+  }
+  StageScope scope(timer, kStageBinOffsets, stream);
+  bin_offsets_kernel<<<static_cast<unsigned>((count + 1 + 255) / 256), 256, 0, stream>>>(
+      *sorted_keys, count, bins, offsets);
+  note_launch();
+}
+
+void prepare_reference_slots(const float* points, int64_t count, const GridParams& g,
+                             const uint32_t* perm, const uint32_t* sorted_keys, int32_t* starts,
+                             float* offsets, cudaStream_t stream) {
+  if (count == 0) return;
+  const unsigned blocks = static_cast<unsigned>((count + 255) / 256);
+  switch (g.dimensions) {
+    case 1:
+      prepare_slots_kernel<1><<<blocks, 256, 0, stream>>>(points, count, g, perm, sorted_keys,
+                                                          starts, offsets);
+      break;
+    case 2:
+      prepare_slots_kernel<2><<<blocks, 256, 0, stream>>>(points, count, g, perm, sorted_keys,
+                                                          starts, offsets);
+      break;
+    default:
+      prepare_slots_kernel<3><<<blocks, 256, 0, stream>>>(points, count, g, perm, sorted_keys,
+                                                          starts, offsets);
+      break;
+  }
+  note_launch();
+}
+
+}  // namespace b200nufft
