@@ -104,7 +104,13 @@ def df64_ceil(h, l):
 
 
 def support(x, axis: AxisFold, width: int):
-    """Support start ceil(position - w/2) and offset start - position as (hi, lo)."""
+    """Support start ceil(position - w/2) and offset start - position as (hi, lo).
+    Coordinates outside the fold's reach give unspecified values; callers mask them."""
+    with np.errstate(invalid="ignore", over="ignore"):
+        return _support(x, axis, width)
+
+
+def _support(x, axis: AxisFold, width: int):
     ph, pl = fold_position(x, axis)
     hw = np.full_like(ph, F(0.5 * width))
     sh, sl = df64_sub(ph, pl, hw, np.zeros_like(ph))

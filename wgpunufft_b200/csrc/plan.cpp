@@ -456,11 +456,13 @@ void NufftPlan::execute(int64_t active_batch, const void* input, void* output, c
     throw NufftFailure{B200NUFFT_GPU_EXECUTION_UNAVAILABLE,
                        "call b200nufft_set_points (or b200nufft_encode) before executing"};
   }
-  if (output == nullptr || (input == nullptr && (type_ == 2 || point_count_ > 0))) {
-    throw NufftFailure{B200NUFFT_INVALID_ARGUMENT, "null input or output buffer"};
-  }
   const uint64_t in_bytes = required_input_bytes(point_count_, active_batch);
   const uint64_t out_bytes = required_output_bytes(point_count_, active_batch);
+  // Empty buffers (zero points) may be null.
+  if ((output == nullptr && out_bytes > 0) || (input == nullptr && in_bytes > 0)) {
+    throw NufftFailure{B200NUFFT_INVALID_ARGUMENT, "null input or output buffer"};
+  }
+  if (out_bytes == 0) return;
   const char* in_lo = static_cast<const char*>(input);
   const char* out_lo = static_cast<const char*>(output);
   if (input && in_bytes && out_bytes && in_lo < out_lo + out_bytes && out_lo < in_lo + in_bytes) {

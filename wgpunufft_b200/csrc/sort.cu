@@ -263,6 +263,10 @@ __global__ void __launch_bounds__(kSortThreads) onesweep_pass_kernel(
     const uint32_t k = s_keys[p];
     const uint32_t d = (k >> shift) & 0xFFu;
     const uint32_t out = s_global_start[d] + (p - s_local_start[d]);
+    if (out >= count) {  // only after a look-back that gave up
+      atomicExch(error_flag, 1u);
+      continue;
+    }
     if (write_keys) keys_out[out] = k;
     vals_out[out] = s_vals[p];
   }

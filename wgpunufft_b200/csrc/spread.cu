@@ -58,7 +58,9 @@ __global__ void strength_magnitude_kernel(const float2* __restrict__ values, int
 // below 2^(62 - headroom): the sum of up to 2^headroom of them fits in 63 bits.
 __device__ __forceinline__ int fixed_point_exponent(uint32_t max_bits, int headroom) {
   if (max_bits == 0u) return 0;
-  const int e = ilogbf(__uint_as_float(max_bits)) + 1;  // max < 2^e
+  // Non-finite strengths (bits at or above infinity) leave the outputs
+  // unspecified but the exponent bounded.
+  const int e = max_bits >= 0x7f800000u ? 128 : ilogbf(__uint_as_float(max_bits)) + 1;  // max < 2^e
   return 62 - headroom - e;
 }
 
@@ -332,7 +334,7 @@ __global__ void __launch_bounds__(kSpreadThreads) spread_tiles_kernel(
 // parts that cover it.
 template <int D>
 __global__ void fold_tiles_kernel(SpreadParams sp, int batch, const float2* __restrict__ scratch,
-                                  const uint32_t* __restrict__ part_start,
+                                  const uint32_t* __restrict__ part_start, int64_t part_limit,
                                   const int2* __restrict__ candidates,
                                   float2* __restrict__ fine) {
   const int64_t cell = static_cast<int64_t>(blockIdx.x) * blockDim.x + threadIdx.x;
@@ -376,7 +378,7 @@ __global__ void fold_tiles_kernel(SpreadParams sp, int batch, const float2* __re
             e.x + static_cast<int64_t>(sp.ntiles[0]) * (t1 + static_cast<int64_t>(sp.ntiles[1]) * t2);
         const int local = e.y + sp.pad[0] * (l1 + sp.pad[1] * l2);
         const uint32_t first = part_start[tile];
-        const uint32_t last = part_start[tile + 1];
+        const uint32_t last = min(part_start[tile + 1], static_cast<uint32_t>(part_limit));
         for (uint32_t part = first; part < last; ++part) {
           const float2 v = scratch[(static_cast<int64_t>(part) * batch + b) * sp.padded_cells + local];
           re += v.x;
@@ -463,15 +465,15 @@ void spread_execute(const SpreadParams& sp, const SpreadLaunch& l, cudaStream_t 
   switch (sp.grid.dimensions) {
     case 1:
       fold_tiles_kernel<1><<<grid, 256, 0, stream>>>(sp, l.batch, l.scratch, l.part_start,
-                                                     l.candidates, l.fine);
+                                                     l.part_upper_bound, l.candidates, l.fine);
       break;
     case 2:
       fold_tiles_kernel<2><<<grid, 256, 0, stream>>>(sp, l.batch, l.scratch, l.part_start,
-                                                     l.candidates, l.fine);
+                                                     l.part_upper_bound, l.candidates, l.fine);
       break;
     default:
       fold_tiles_kernel<3><<<grid, 256, 0, stream>>>(sp, l.batch, l.scratch, l.part_start,
-                                                     l.candidates, l.fine);
+                                                     l.part_upper_bound, l.candidates, l.fine);
       break;
   }
   note_launch();
