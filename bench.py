@@ -238,6 +238,30 @@ def main():
     value = world * POINTS / (ms / 1e3)
     one_shot = world * POINTS / (one_shot_ms / args.steps / 1e3)
 
+    # Type 2 on the same points (reported beside the headline, same timing rules).
+    plan2 = w.NufftPlan.type2_gpu(config, device=local)
+    coefficients = torch.complex(torch.randn(config.mode_count(), device=dev),
+                                 torch.randn(config.mode_count(), device=dev))
+    values = torch.empty(POINTS, dtype=torch.complex64, device=dev)
+    plan2.set_points_gpu(points)
+    for _ in range(args.warmup):
+        plan2.execute_type2_gpu(coefficients, values)
+    plan2.synchronize()
+    plan2.stage_timing(True)
+    plan2.stage_report()
+    type2_ms = timed(lambda: plan2.execute_type2_gpu(coefficients, values), args.steps)
+    stages2 = plan2.stage_report()
+    plan2.stage_timing(False)
+    type2_one_shot_ms = timed(lambda: plan2.encode_type2_gpu(points, coefficients, values), args.steps)
+    if world > 1:
+        t = torch.tensor([type2_ms, type2_one_shot_ms], device=dev)
+        dist.all_reduce(t, op=dist.ReduceOp.MAX)
+        type2_ms, type2_one_shot_ms = t.tolist()
+    type2 = {"value": world * POINTS / (type2_ms / args.steps / 1e3), "unit": UNIT,
+             "ms_per_step": type2_ms / args.steps,
+             "one_shot_value": world * POINTS / (type2_one_shot_ms / args.steps / 1e3),
+             "stages_ms_per_step": {k: v[0] / args.steps for k, v in stages2.items()}}
+
     # Accuracy of this output against FP64 direct sums on 16 seeded modes.
     rel = None
     if rank == 0:
@@ -308,6 +332,7 @@ def main():
                          "note": "set_points (stable bin sort) + execute per step"},
             "rel_l2": rel,
             "stages_ms_per_step": {k: v[0] / args.steps for k, v in stages.items()},
+            "type2": type2,
             "roofline": roofline,
             "cpu_baseline": cpu,
             "e2e": e2e,

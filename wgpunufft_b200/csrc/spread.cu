@@ -7,10 +7,11 @@
 // fine grid (or one part of a crowded tile), read from the bins of the stable
 // sort. Every point evaluates its window per axis into registers and adds
 // its w^d contributions to a padded copy of the tile in shared memory. The
-// contributions are accumulated as 64-bit fixed-point integers, scaled by a
-// power of two derived from the largest strength, so the sum of a cell is the
-// exact integer sum of its rounded contributions whatever order the threads
-// add them in: the accumulation is deterministic without ordering the
+// contributions are accumulated as fixed-point integers (each rounded to a
+// 32-bit integer after scaling by a power of two derived from the largest
+// strength, and summed exactly in two 32-bit halves), so the sum of a cell is
+// the exact integer sum of its rounded contributions whatever order the
+// threads add them in: the accumulation is deterministic without ordering the
 // threads, and it carries more bits than an f32 sum. Each padded tile is then
 // converted to f32 and written out, and a fold pass adds, for every fine-grid
 // cell, the padded tiles and parts that cover it in a fixed order (halos
@@ -54,14 +55,31 @@ __global__ void strength_magnitude_kernel(const float2* __restrict__ values, int
   if ((threadIdx.x & 31) == 0 && m) atomicMax(&max_bits[b], m);
 }
 
-// Power-of-two exponent S so that every contribution scaled by 2^S stays
-// below 2^(62 - headroom): the sum of up to 2^headroom of them fits in 63 bits.
-__device__ __forceinline__ int fixed_point_exponent(uint32_t max_bits, int headroom) {
+// Power-of-two exponent S that scales every contribution, at most the largest
+// strength magnitude, below 2^30 in magnitude: each then rounds to a 32-bit
+// integer with a resolution of 2^-30 of the largest strength.
+__device__ __forceinline__ int fixed_point_exponent(uint32_t max_bits) {
   if (max_bits == 0u) return 0;
   // Non-finite strengths (bits at or above infinity) leave the outputs
   // unspecified but the exponent bounded.
   const int e = max_bits >= 0x7f800000u ? 128 : ilogbf(__uint_as_float(max_bits)) + 1;  // max < 2^e
-  return 62 - headroom - e;
+  return 30 - e;
+}
+
+// Adds a fixed-point contribution v (|v| < 2^31) to cell c as two exact
+// 32-bit sums: its low 16 bits, unsigned, and its arithmetic high part. Both
+// stay exact for up to 2^16 contributions per cell, and the cell's value is
+// hi * 2^16 + lo. Integer addition is associative, so the sums do not depend
+// on the order in which threads add.
+__device__ __forceinline__ void add_fixed(uint32_t* lo, int32_t* hi, int c, float value) {
+  const int32_t v = __float2int_rn(value);
+  atomicAdd(&lo[c], static_cast<uint32_t>(v) & 0xFFFFu);
+  atomicAdd(&hi[c], v >> 16);
+}
+
+__device__ __forceinline__ float fixed_to_float(uint32_t lo, int32_t hi, int S) {
+  const long long total = static_cast<long long>(hi) * 65536ll + static_cast<long long>(lo);
+  return ldexpf(__ll2float_rn(total), -S);
 }
 
 // Records in the reach of every tile's bins, and the parts of every tile.
@@ -144,7 +162,7 @@ __global__ void __launch_bounds__(kSpreadThreads) spread_tiles_kernel(
     int64_t point_count, int batch, const uint32_t* __restrict__ perm,
     const uint32_t* __restrict__ offsets, const uint32_t* __restrict__ part_start,
     const uint32_t* __restrict__ max_bits, float2* __restrict__ scratch) {
-  extern __shared__ unsigned long long acc[];
+  extern __shared__ uint32_t acc[];
   __shared__ uint32_t row_begin[kMaxTileRows];
   __shared__ uint32_t row_prefix[kMaxTileRows + 1];
   __shared__ int64_t s_tile;
@@ -165,7 +183,7 @@ __global__ void __launch_bounds__(kSpreadThreads) spread_tiles_kernel(
     s_tile = low;
   }
   const int padded = sp.padded_cells;
-  for (int c = tid; c < 2 * padded; c += kSpreadThreads) acc[c] = 0ull;
+  for (int c = tid; c < 4 * padded; c += kSpreadThreads) acc[c] = 0u;
   __syncthreads();
   const int64_t tile = s_tile;
   const uint32_t part_in_tile = part - part_start[tile];
@@ -236,11 +254,13 @@ __global__ void __launch_bounds__(kSpreadThreads) spread_tiles_kernel(
   const uint32_t tile_total = row_prefix[rows];
   const uint32_t record_begin = part_in_tile * static_cast<uint32_t>(sp.part_cap);
   const uint32_t record_end = min(tile_total, record_begin + static_cast<uint32_t>(sp.part_cap));
-  const int S = fixed_point_exponent(max_bits[b], sp.headroom);
+  const int S = fixed_point_exponent(max_bits[b]);
   const float width_f = static_cast<float>(W);
   const float2* sv = strengths + static_cast<int64_t>(b) * point_count;
-  unsigned long long* acc_re = acc;
-  unsigned long long* acc_im = acc + padded;
+  uint32_t* re_lo = acc;
+  int32_t* re_hi = reinterpret_cast<int32_t*>(acc + padded);
+  uint32_t* im_lo = acc + 2 * padded;
+  int32_t* im_hi = reinterpret_cast<int32_t*>(acc + 3 * padded);
 
   int row = 0;
   for (uint32_t r = record_begin + tid; r < record_end; r += kSpreadThreads) {
@@ -287,8 +307,8 @@ __global__ void __launch_bounds__(kSpreadThreads) spread_tiles_kernel(
 #pragma unroll
       for (int i = 0; i < W; ++i) {
         const int c = local_start[0] + i;
-        atomicAdd(&acc_re[c], static_cast<unsigned long long>(__float2ll_rn(sr * w[0][i])));
-        atomicAdd(&acc_im[c], static_cast<unsigned long long>(__float2ll_rn(si * w[0][i])));
+        add_fixed(re_lo, re_hi, c, sr * w[0][i]);
+        add_fixed(im_lo, im_hi, c, si * w[0][i]);
       }
     } else if (D == 2) {
 #pragma unroll
@@ -298,8 +318,8 @@ __global__ void __launch_bounds__(kSpreadThreads) spread_tiles_kernel(
         const int base = (local_start[1] + j) * sp.pad[0] + local_start[0];
 #pragma unroll
         for (int i = 0; i < W; ++i) {
-          atomicAdd(&acc_re[base + i], static_cast<unsigned long long>(__float2ll_rn(wr * w[0][i])));
-          atomicAdd(&acc_im[base + i], static_cast<unsigned long long>(__float2ll_rn(wi * w[0][i])));
+          add_fixed(re_lo, re_hi, base + i, wr * w[0][i]);
+          add_fixed(im_lo, im_hi, base + i, wi * w[0][i]);
         }
       }
     } else {
@@ -314,8 +334,8 @@ __global__ void __launch_bounds__(kSpreadThreads) spread_tiles_kernel(
               ((local_start[2] + k) * sp.pad[1] + local_start[1] + j) * sp.pad[0] + local_start[0];
 #pragma unroll
           for (int i = 0; i < W; ++i) {
-            atomicAdd(&acc_re[base + i], static_cast<unsigned long long>(__float2ll_rn(wr * w[0][i])));
-            atomicAdd(&acc_im[base + i], static_cast<unsigned long long>(__float2ll_rn(wi * w[0][i])));
+            add_fixed(re_lo, re_hi, base + i, wr * w[0][i]);
+            add_fixed(im_lo, im_hi, base + i, wi * w[0][i]);
           }
         }
       }
@@ -324,9 +344,7 @@ __global__ void __launch_bounds__(kSpreadThreads) spread_tiles_kernel(
   __syncthreads();
   float2* out = scratch + (static_cast<int64_t>(part) * batch + b) * padded;
   for (int c = tid; c < padded; c += kSpreadThreads) {
-    const float re = ldexpf(__ll2float_rn(static_cast<long long>(acc_re[c])), -S);
-    const float im = ldexpf(__ll2float_rn(static_cast<long long>(acc_im[c])), -S);
-    out[c] = make_float2(re, im);
+    out[c] = make_float2(fixed_to_float(re_lo[c], re_hi[c], S), fixed_to_float(im_lo[c], im_hi[c], S));
   }
 }
 
@@ -392,7 +410,7 @@ __global__ void fold_tiles_kernel(SpreadParams sp, int batch, const float2* __re
 
 template <int D, int W>
 void launch_spread_width(const SpreadParams& sp, const SpreadLaunch& l, cudaStream_t stream) {
-  const size_t smem = static_cast<size_t>(2) * sp.padded_cells * sizeof(unsigned long long);
+  const size_t smem = static_cast<size_t>(4) * sp.padded_cells * sizeof(uint32_t);
   auto kernel = spread_tiles_kernel<D, W>;
   check_cuda(cudaFuncSetAttribute(kernel, cudaFuncAttributeMaxDynamicSharedMemorySize,
                                   static_cast<int>(smem)),
