@@ -75,6 +75,10 @@ void sort_points(const float* points, int64_t count, const GridParams& grid, Key
                  uint64_t bins, SortBuffers buffers, uint32_t* offsets, uint32_t** perm,
                  uint32_t** sorted_keys, cudaStream_t stream, StageTimer* timer = nullptr);
 
+// The coordinates of `count` points in the bin order `perm`.
+void gather_sorted_points(const float* points, const uint32_t* perm, int64_t count, int dimensions,
+                          float* sorted, cudaStream_t stream, StageTimer* timer = nullptr);
+
 // Bytes of look-back status words a sort of `count` points needs.
 size_t sort_status_bytes(int64_t count);
 

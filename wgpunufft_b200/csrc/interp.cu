@@ -25,8 +25,15 @@ __device__ __forceinline__ float es_weight(float distance, float beta, float wid
   return expf(beta * (sqrtf(fmaxf(0.0f, 1.0f - squared)) - 1.0f));
 }
 
+// Resident blocks per SM the register budget is tuned for: narrow 1D and 2D
+// windows fit three 256-thread blocks without spilling, wider ones two.
 template <int D, int W>
-__global__ void __launch_bounds__(256) interpolate_kernel(GridParams g,
+struct InterpBlocks {
+  static constexpr int value = (D <= 2 && W <= 6) ? 3 : 2;
+};
+
+template <int D, int W>
+__global__ void __launch_bounds__(256, InterpBlocks<D, W>::value) interpolate_kernel(GridParams g,
                                                           const float* __restrict__ points,
                                                           int64_t count,
                                                           const uint32_t* __restrict__ perm,
@@ -37,7 +44,7 @@ __global__ void __launch_bounds__(256) interpolate_kernel(GridParams g,
   const uint32_t point = perm[slot];
   float p[D];
 #pragma unroll
-  for (int a = 0; a < D; ++a) p[a] = points[static_cast<int64_t>(point) * D + a];
+  for (int a = 0; a < D; ++a) p[a] = points[slot * D + a];
   bool reach = true;
 #pragma unroll
   for (int a = 0; a < D; ++a) reach = reach && in_fold_reach(p[a]);

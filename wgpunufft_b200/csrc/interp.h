@@ -10,7 +10,7 @@
 namespace b200nufft {
 
 struct InterpLaunch {
-  const float* points;
+  const float* points;    // coordinates in bin (slot) order
   int64_t point_count;
   const uint32_t* perm;   // slot -> original point, in bin order
   const float2* fine;     // batch * fine_count

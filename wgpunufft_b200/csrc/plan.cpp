@@ -402,6 +402,10 @@ void NufftPlan::set_points(int64_t count, const void* points, cudaStream_t strea
   sort_points(static_cast<const float*>(points), count, grid_,
               type_ == 1 ? KeyKind::SupportStart : KeyKind::ApproximateCell, bins_, buf, offsets,
               &perm_, &sorted_keys_, stream, &timer_);
+  float* sorted = static_cast<float*>(
+      sorted_points_.reserve(static_cast<size_t>(std::max<int64_t>(count, 1)) * dim_ * sizeof(float),
+                             "sorted coordinates"));
+  gather_sorted_points(static_cast<const float*>(points), perm_, count, dim_, sorted, stream, &timer_);
   if (type_ == 1) {
     configure_tiles();
     parts_.reserve(static_cast<size_t>(spread_.tile_count) * sizeof(uint32_t), "tile parts");
@@ -479,7 +483,7 @@ void NufftPlan::execute(int64_t active_batch, const void* input, void* output, c
     const size_t scratch_bytes = static_cast<size_t>(part_upper_bound_) * batch *
                                  spread_.padded_cells * sizeof(float2);
     SpreadLaunch l;
-    l.points = static_cast<const float*>(points_);
+    l.points = static_cast<const float*>(sorted_points_.get());
     l.strengths = static_cast<const float2*>(input);
     l.point_count = point_count_;
     l.batch = batch;
@@ -504,7 +508,7 @@ void NufftPlan::execute(int64_t active_batch, const void* input, void* output, c
     }
     run_fft(fine, batch, direction, stream);
     InterpLaunch l;
-    l.points = static_cast<const float*>(points_);
+    l.points = static_cast<const float*>(sorted_points_.get());
     l.point_count = point_count_;
     l.perm = perm_;
     l.fine = fine;

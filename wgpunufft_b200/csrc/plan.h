@@ -92,6 +92,7 @@ class NufftPlan {
   uint32_t* perm_ = nullptr;
   uint32_t* sorted_keys_ = nullptr;
   DeviceBuffer keys_a_, keys_b_, vals_a_, vals_b_, hist_, status_, counters_, offsets_;
+  DeviceBuffer sorted_points_;
 
   // Spreading state.
   DeviceBuffer parts_, part_start_, max_bits_, scratch_, candidates_;

@@ -283,6 +283,19 @@ __global__ void bin_offsets_kernel(const uint32_t* __restrict__ keys, int64_t co
   for (uint64_t b = low; b <= high && b <= bins; ++b) offsets[b] = static_cast<uint32_t>(i);
 }
 
+// Coordinates in bin order: sorted[slot] = points[perm[slot]], so that the
+// spreading and interpolation kernels read them contiguously.
+template <int D>
+__global__ void gather_points_kernel(const float* __restrict__ points,
+                                     const uint32_t* __restrict__ perm, int64_t count,
+                                     float* __restrict__ sorted) {
+  const int64_t slot = static_cast<int64_t>(blockIdx.x) * blockDim.x + threadIdx.x;
+  if (slot >= count) return;
+  const int64_t point = perm[slot];
+#pragma unroll
+  for (int a = 0; a < D; ++a) sorted[slot * D + a] = points[point * D + a];
+}
+
 __global__ void identity_kernel(uint32_t* __restrict__ perm, uint32_t* __restrict__ keys,
                                 int64_t count) {
   const int64_t i = static_cast<int64_t>(blockIdx.x) * blockDim.x + threadIdx.x;
@@ -355,6 +368,19 @@ void launch_keys(const float* points, int64_t count, const GridParams& g, KeyKin
 }
 
 }  // namespace
+
+void gather_sorted_points(const float* points, const uint32_t* perm, int64_t count, int dimensions,
+                          float* sorted, cudaStream_t stream, StageTimer* timer) {
+  if (count == 0) return;
+  StageScope scope(timer, kStageBinOffsets, stream);
+  const unsigned blocks = static_cast<unsigned>((count + 255) / 256);
+  switch (dimensions) {
+    case 1: gather_points_kernel<1><<<blocks, 256, 0, stream>>>(points, perm, count, sorted); break;
+    case 2: gather_points_kernel<2><<<blocks, 256, 0, stream>>>(points, perm, count, sorted); break;
+    default: gather_points_kernel<3><<<blocks, 256, 0, stream>>>(points, perm, count, sorted); break;
+  }
+  note_launch();
+}
 
 size_t sort_status_bytes(int64_t count) {
   const int64_t tiles = (count + kSortTile - 1) / kSortTile;

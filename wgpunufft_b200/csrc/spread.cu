@@ -274,10 +274,9 @@ __global__ void __launch_bounds__(kSpreadThreads) spread_tiles_kernel(
       row = low;
     }
     const uint32_t slot = row_begin[row] + (r - row_prefix[row]);
-    const uint32_t point = perm[slot];
     float p[D];
 #pragma unroll
-    for (int a = 0; a < D; ++a) p[a] = points[static_cast<int64_t>(point) * D + a];
+    for (int a = 0; a < D; ++a) p[a] = points[static_cast<int64_t>(slot) * D + a];
     bool reach = true;
 #pragma unroll
     for (int a = 0; a < D; ++a) reach = reach && in_fold_reach(p[a]);
@@ -300,7 +299,7 @@ __global__ void __launch_bounds__(kSpreadThreads) spread_tiles_kernel(
       }
     }
     if (!inside) continue;  // a bin wider than the tile: another tile owns it
-    const float2 s = sv[point];
+    const float2 s = sv[perm[slot]];
     const float sr = ldexpf(s.x, S);
     const float si = ldexpf(s.y, S);
     if (D == 1) {

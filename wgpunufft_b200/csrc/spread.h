@@ -32,7 +32,7 @@ struct SpreadParams {
 };
 
 struct SpreadLaunch {
-  const float* points;
+  const float* points;    // coordinates in bin (slot) order
   const float2* strengths;
   int64_t point_count;
   int batch;
