@@ -234,6 +234,32 @@ int b200nufft_plan_stage_report(b200nufft_plan plan, b200nufft_stage_report *rep
 int b200nufft_copy_prepared_slots(b200nufft_plan plan, int32_t *starts, float *offsets,
                                   void *stream);
 
+/* Stable bin order without any device allocation. This entry point has no
+ * counterpart in the reference. It is for callers that cannot call
+ * cudaMalloc: code running while another framework owns every byte of device
+ * memory through its own pool, and real-time or callback code where an
+ * allocation may block or fail. It writes the same `permutation`
+ * (point_count words) and `bin_offsets` (bins + 1 words, bins = prod_a
+ * ceil(fine_shape[a] / bin_sides[a])) as b200nufft_set_points followed by
+ * b200nufft_copy_bin_order on an F32 type-1 plan whose chosen bin geometry
+ * has the sides `bin_sides` (b200nufft_plan_info.geometry_sides[chosen_geometry]);
+ * `points` are point-major float coordinates. All scratch lives in a fixed
+ * array of about 4.3 MB in the library's device image, which every GPU that
+ * loads the library holds until the process exits; point counts above
+ * B200NUFFT_NOALLOC_MAX_POINTS are rejected with B200NUFFT_LENGTH_OVERFLOW.
+ * The call allocates nothing: no cudaMalloc, no cudaFree, no library that
+ * allocates. Its first call on a device looks up the array's device address
+ * (cudaGetSymbolAddress, with that device current); make that first call
+ * before any stream capture. Every call shares the one array and starts by
+ * clearing what must start at zero, so calls that overlap on the GPU (on
+ * different streams, or from different threads) race and must be ordered by
+ * the caller. */
+#define B200NUFFT_NOALLOC_MAX_POINTS 262144
+int b200nufft_bin_order_noalloc(int32_t dimensions, const int64_t *fine_shape,
+                                int32_t kernel_width, const int32_t *bin_sides,
+                                int64_t point_count, const float *points, uint32_t *permutation,
+                                uint32_t *bin_offsets, void *stream);
+
 /* ------------------------------------------------------------------------ */
 /* Type 3 (NufftType3Plan, src/type3.rs)                                     */
 /* ------------------------------------------------------------------------ */

@@ -134,6 +134,8 @@ SIGNATURES: dict[str, tuple] = {
     "b200nufft_type3_get_info": (c_int, [PLAN, P(Type3Info)]),
     "b200nufft_type3_set_points": (c_int, [PLAN, c_int64, c_void_p, c_int64, c_void_p, c_void_p]),
     "b200nufft_type3_execute": (c_int, [PLAN, c_int64, c_void_p, c_void_p, c_void_p]),
+    "b200nufft_bin_order_noalloc": (c_int, [c_int32, P(c_int64), c_int32, P(c_int32), c_int64,
+                                            c_void_p, c_void_p, c_void_p, c_void_p]),
     "b200nufft_last_error": (c_char_p, []),
     "b200nufft_version": (c_char_p, []),
     "b200nufft_launch_count": (c_uint64, []),
