@@ -144,6 +144,50 @@ def type1_keys(points: np.ndarray, fine, width: int, sides):
     return key, stride
 
 
+FOLD_REACH64 = 4.0 * math.pi
+
+
+def support64(x, n: int, width: int):
+    """The F64 fold of src/gpu_nd_wgsl.rs:311-365 in numpy float64 (separate
+    multiply and add): support start and offset start - position."""
+    x = np.asarray(x, dtype=np.float64)
+    with np.errstate(invalid="ignore", over="ignore"):
+        position = x * (n / (2.0 * math.pi)) + float(n // 2)
+        for _ in range(2):
+            position = np.where(position < 0.0, position + n, position)
+        for _ in range(2):
+            position = np.where(position >= n, position - n, position)
+        start = np.ceil(position - 0.5 * width)
+        offset = start - position
+    return start, offset
+
+
+def type1_keys64(points: np.ndarray, fine, width: int, sides):
+    """Support-start bin keys of f64 coordinates (native f64 fold)."""
+    points = np.asarray(points, dtype=np.float64).reshape(-1, len(fine))
+    reach = np.all(np.abs(points) <= FOLD_REACH64, axis=1)
+    key = np.zeros(points.shape[0], dtype=np.int64)
+    stride = 1
+    for a, n in enumerate(fine):
+        start, _ = support64(points[:, a], n, width)
+        start = np.where(reach, start, 0).astype(np.int64)
+        wrapped = np.clip(np.where(start < 0, start + n, start), 0, n - 1)
+        key += (wrapped >> _ilog2(sides[a])) * stride
+        stride *= -(-n // sides[a])
+    return key, stride
+
+
+def type2_sides64(fine):
+    """type2_bin_shape (src/gpu_nd.rs:566-586): 4 cells per axis, doubled from
+    the last axis backwards while there are more than 2^24 bins."""
+    sides = [4] * len(fine)
+    axis = len(fine)
+    while math.prod(-(-n // s) for n, s in zip(fine, sides)) > (1 << 24):
+        axis = len(fine) - 1 if axis == 0 else axis - 1
+        sides[axis] *= 2
+    return sides
+
+
 def approximate_cell(x, axis: AxisFold):
     """approximate_cell (src/gpu_point_bins.rs:460-464) in plain f32."""
     x = np.asarray(x, dtype=F)

@@ -49,6 +49,11 @@ struct GridParams {
   FoldAxis axis[3];
   int64_t fine[3];       // fine-grid cells per axis
   int64_t fine_count;    // cells of one transform's grid
+  // f64 plans: the native fold and the Horner table of the window.
+  FoldAxis64 axis64[3];
+  double half_width64;
+  const double* horner;  // device, rows x width
+  int32_t horner_rows;
 };
 
 // Stable sort of the points by bin key. Launches on `stream`; all pointers
@@ -75,9 +80,22 @@ void sort_points(const float* points, int64_t count, const GridParams& grid, Key
                  uint64_t bins, SortBuffers buffers, uint32_t* offsets, uint32_t** perm,
                  uint32_t** sorted_keys, cudaStream_t stream, StageTimer* timer = nullptr);
 
+// The same for f64 coordinates folded in native f64 (support-start keys).
+void sort_points64(const double* points, int64_t count, const GridParams& grid, uint64_t bins,
+                   SortBuffers buffers, uint32_t* offsets, uint32_t** perm, uint32_t** sorted_keys,
+                   cudaStream_t stream, StageTimer* timer = nullptr);
+
 // The coordinates of `count` points in the bin order `perm`.
 void gather_sorted_points(const float* points, const uint32_t* perm, int64_t count, int dimensions,
                           float* sorted, cudaStream_t stream, StageTimer* timer = nullptr);
+void gather_sorted_points64(const double* points, const uint32_t* perm, int64_t count,
+                            int dimensions, double* sorted, cudaStream_t stream,
+                            StageTimer* timer = nullptr);
+
+// Df64 storage (a (hi, lo) pair of floats per scalar, the reference's
+// double-float format) to and from f64, `count` scalars.
+void df64_to_f64(const float* pairs, int64_t count, double* out, cudaStream_t stream);
+void f64_to_df64(const double* values, int64_t count, float* pairs, cudaStream_t stream);
 
 // Bytes of look-back status words a sort of `count` points needs.
 size_t sort_status_bytes(int64_t count);

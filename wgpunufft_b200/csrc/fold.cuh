@@ -126,6 +126,53 @@ __device__ __forceinline__ void support_of(float x, const FoldAxis& a, float hal
   offset = df64_sub(Df64{static_cast<float>(start), 0.0f}, position);
 }
 
+// ---------------------------------------------------------------------------
+// f64 plans fold in native f64 (the F64 branch of src/gpu_nd_wgsl.rs:311-365):
+// position = x * n/(2 pi) + floor(n/2), folded by at most two periods each
+// way, start = ceil(position - w/2), offset = start - position. The products
+// and sums are kept separate (no fused multiply-add).
+
+struct FoldAxis64 {
+  double scale;
+  double origin;
+  double length;
+};
+
+// 4 pi in f64: the magnitude the fold brings onto the grid.
+constexpr double kFoldReach64 = 12.566370614359172953850573533118;
+
+__device__ __forceinline__ bool in_fold_reach64(double x) { return fabs(x) <= kFoldReach64; }
+
+__device__ __forceinline__ double fold_position64(double x, const FoldAxis64& a) {
+  double position = __dadd_rn(__dmul_rn(x, a.scale), a.origin);
+  if (position < 0.0) position = __dadd_rn(position, a.length);
+  if (position < 0.0) position = __dadd_rn(position, a.length);
+  if (position >= a.length) position = __dsub_rn(position, a.length);
+  if (position >= a.length) position = __dsub_rn(position, a.length);
+  return position;
+}
+
+__device__ __forceinline__ void support_of64(double x, const FoldAxis64& a, double half_width,
+                                             int32_t& start, double& offset) {
+  const double position = fold_position64(x, a);
+  start = static_cast<int32_t>(ceil(__dsub_rn(position, half_width)));
+  offset = __dsub_rn(static_cast<double>(start), position);
+}
+
+// Weight of support cell start + j for a point with prepared offset
+// start - position, from the host-fitted Horner table (coefficient-major,
+// highest degree first): panel j at local coordinate 2 offset + w - 1 in
+// [-1, 1] (the F64 support_weight of src/gpu_nd_wgsl.rs:399-440). An offset
+// past the support weighs zero.
+__device__ __forceinline__ double horner_weight(double offset, int j, int width,
+                                                const double* __restrict__ table, int rows) {
+  const double local = 2.0 * offset + static_cast<double>(width - 1);
+  if (!(fabs(local) <= 1.0)) return 0.0;
+  double value = 0.0;
+  for (int r = 0; r < rows; ++r) value = fma(value, local, __ldg(&table[r * width + j]));
+  return value;
+}
+
 // Support start wrapped onto [0, n): the bin coordinate of a point
 // (src/gpu_nd_bins.rs:524-528).
 __device__ __forceinline__ int32_t wrap_start(int32_t start, int32_t n) {

@@ -18,6 +18,16 @@ struct InterpLaunch {
   float2* output;         // batch * point_count, input order
 };
 
+struct InterpLaunch64 {
+  const double* points;   // coordinates in bin (slot) order
+  int64_t point_count;
+  const uint32_t* perm;
+  const double2* fine;
+  int batch;
+  double2* output;
+};
+
 void interpolate_execute(const GridParams& g, const InterpLaunch& launch, cudaStream_t stream);
+void interpolate_execute64(const GridParams& g, const InterpLaunch64& launch, cudaStream_t stream);
 
 }  // namespace b200nufft

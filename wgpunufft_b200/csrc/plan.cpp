@@ -109,9 +109,9 @@ NufftPlan::NufftPlan(const b200nufft_config& c, bool with_device) : has_device_(
   mode_order_ = c.mode_order;
   sigma_ = c.sigma == 0.0 ? 2.0 : c.sigma;
   precision_ = c.precision == 0 ? B200NUFFT_PRECISION_F32 : c.precision;
-  if (precision_ != B200NUFFT_PRECISION_F32) {
-    throw NufftFailure{B200NUFFT_PRECISION_UNSUPPORTED,
-                       "this build runs F32 type-1/type-2 plans; f64 plans are not built yet"};
+  if (precision_ != B200NUFFT_PRECISION_F32 && precision_ != B200NUFFT_PRECISION_F64 &&
+      precision_ != B200NUFFT_PRECISION_DF64) {
+    throw NufftFailure{B200NUFFT_INVALID_ARGUMENT, "precision must be F64 (1), DF64 (2) or F32 (3)"};
   }
   kernel_ = EsKernel::for_tolerance(eps_, sigma_);
   fine_count_ = 1;
@@ -149,8 +149,9 @@ NufftPlan::NufftPlan(const b200nufft_config& c, bool with_device) : has_device_(
                                                                            : LayoutPrecision::Df64);
 
   // Deconvolution amplitudes prod_a 1 / phi_hat_a(|k_a|), divided in f64 in
-  // axis order and rounded once (mode_amplitudes_nd, src/gpu_nd.rs:910-951).
-  std::vector<float> amplitudes(static_cast<size_t>(mode_count_));
+  // axis order and, for f32 plans, rounded once (mode_amplitudes_nd and
+  // mode_amplitudes_nd_f64, src/gpu_nd.rs:910-990).
+  std::vector<double> amplitudes(static_cast<size_t>(mode_count_));
   for (int64_t flat = 0; flat < mode_count_; ++flat) {
     int64_t rest = flat;
     double amplitude = 1.0;
@@ -166,23 +167,36 @@ NufftPlan::NufftPlan(const b200nufft_config& c, bool with_device) : has_device_(
       }
       amplitude /= coefficient;
     }
-    const float rounded = static_cast<float>(amplitude);
-    if (!std::isfinite(rounded)) {
+    if (precision_ == B200NUFFT_PRECISION_F32 && !std::isfinite(static_cast<float>(amplitude))) {
       throw NufftFailure{B200NUFFT_INVALID_KERNEL_FOURIER_COEFFICIENT,
                          "deconvolution amplitude overflows f32"};
     }
-    amplitudes[static_cast<size_t>(flat)] = rounded;
+    if (!std::isfinite(amplitude)) {
+      throw NufftFailure{B200NUFFT_INVALID_KERNEL_FOURIER_COEFFICIENT,
+                         "deconvolution amplitude is not finite"};
+    }
+    amplitudes[static_cast<size_t>(flat)] = amplitude;
   }
-  amplitudes_host_ = std::move(amplitudes);
   if (!with_device) return;
   int current = 0;
   check_cuda(cudaGetDevice(&current), "current device");
   device_ = c.device < 0 ? current : c.device;
   make_current();
-  void* amp = amplitudes_.reserve(amplitudes_host_.size() * sizeof(float), "deconvolution amplitudes");
-  check_cuda(cudaMemcpy(amp, amplitudes_host_.data(), amplitudes_host_.size() * sizeof(float),
-                        cudaMemcpyHostToDevice),
-             "upload deconvolution amplitudes");
+  if (precision_ == B200NUFFT_PRECISION_F32) {
+    std::vector<float> rounded(amplitudes.begin(), amplitudes.end());
+    void* amp = amplitudes_.reserve(rounded.size() * sizeof(float), "deconvolution amplitudes");
+    check_cuda(cudaMemcpy(amp, rounded.data(), rounded.size() * sizeof(float), cudaMemcpyHostToDevice),
+               "upload deconvolution amplitudes");
+  } else {
+    void* amp = amplitudes_.reserve(amplitudes.size() * sizeof(double), "deconvolution amplitudes");
+    check_cuda(cudaMemcpy(amp, amplitudes.data(), amplitudes.size() * sizeof(double),
+                          cudaMemcpyHostToDevice),
+               "upload deconvolution amplitudes");
+    void* table = horner_device_.reserve(horner_.coefficients.size() * sizeof(double), "Horner table");
+    check_cuda(cudaMemcpy(table, horner_.coefficients.data(),
+                          horner_.coefficients.size() * sizeof(double), cudaMemcpyHostToDevice),
+               "upload Horner table");
+  }
 
   std::memset(&grid_, 0, sizeof(grid_));
   grid_.dimensions = dim_;
@@ -190,6 +204,9 @@ NufftPlan::NufftPlan(const b200nufft_config& c, bool with_device) : has_device_(
   grid_.half_width = static_cast<float>(kernel_.half_width());
   grid_.beta = static_cast<float>(kernel_.beta);
   grid_.fine_count = fine_count_;
+  grid_.half_width64 = kernel_.half_width();
+  grid_.horner = horner ? static_cast<const double*>(horner_device_.get()) : nullptr;
+  grid_.horner_rows = horner ? horner_.coefficient_count : 0;
   for (int a = 0; a < dim_; ++a) {
     const double scale = static_cast<double>(fine_[a]) / kTwoPi;
     FoldAxis& axis = grid_.axis[a];
@@ -198,6 +215,9 @@ NufftPlan::NufftPlan(const b200nufft_config& c, bool with_device) : has_device_(
     axis.origin = static_cast<float>(fine_[a] / 2);
     axis.length_f = static_cast<float>(fine_[a]);
     axis.length = static_cast<int32_t>(fine_[a]);
+    grid_.axis64[a].scale = scale;
+    grid_.axis64[a].origin = static_cast<double>(fine_[a] / 2);
+    grid_.axis64[a].length = static_cast<double>(fine_[a]);
     grid_.fine[a] = fine_[a];
   }
   std::memset(&modes_params_, 0, sizeof(modes_params_));
@@ -213,7 +233,7 @@ NufftPlan::NufftPlan(const b200nufft_config& c, bool with_device) : has_device_(
   counters_.reserve(8 * sizeof(uint32_t), "sort tickets");
   check_cuda(cudaMemset(counters_.get(), 0, 8 * sizeof(uint32_t)), "clear sort tickets");
   hist_.reserve(4 * 256 * sizeof(uint32_t), "digit histograms");
-  max_bits_.reserve(static_cast<size_t>(batch_) * sizeof(uint32_t), "strength maxima");
+  max_bits_.reserve(static_cast<size_t>(batch_) * sizeof(uint64_t), "strength maxima");
 }
 
 NufftPlan::~NufftPlan() {
@@ -267,11 +287,29 @@ void NufftPlan::configure_bins(int geometry) {
 }
 
 void NufftPlan::configure_type2_bins() {
-  // Interpolation bins of 8 cells per axis in 1D and 2D and 4 in 3D
-  // (src/gpu.rs:19, src/gpu_2d.rs:22, src/gpu_3d.rs:25).
-  const int side = dim_ == 3 ? 4 : 8;
+  // f32: interpolation bins of 8 cells per axis in 1D and 2D and 4 in 3D
+  // (src/gpu.rs:19, src/gpu_2d.rs:22, src/gpu_3d.rs:25). f64 and Df64: the
+  // rank-generic bins of type2_bin_shape (src/gpu_nd.rs:566-586), 4 cells per
+  // axis, doubled from the last axis backwards while above 2^24 bins.
+  int64_t sides[3] = {1, 1, 1};
+  if (precision_ == B200NUFFT_PRECISION_F32) {
+    for (int a = 0; a < dim_; ++a) sides[a] = dim_ == 3 ? 4 : 8;
+  } else {
+    for (int a = 0; a < dim_; ++a) sides[a] = 4;
+    auto count = [&]() {
+      int64_t total = 1;
+      for (int a = 0; a < dim_; ++a) total *= (fine_[a] + sides[a] - 1) / sides[a];
+      return total;
+    };
+    int axis = dim_;
+    while (count() > (int64_t(1) << 24)) {
+      axis = axis == 0 ? dim_ - 1 : axis - 1;
+      sides[axis] *= 2;
+    }
+  }
   uint64_t stride = 1;
   for (int a = 0; a < dim_; ++a) {
+    const int64_t side = sides[a];
     const int64_t bins = (fine_[a] + side - 1) / side;
     grid_.axis[a].shift = ilog2(side);
     grid_.axis[a].bins = static_cast<uint32_t>(bins);
@@ -399,13 +437,26 @@ void NufftPlan::set_points(int64_t count, const void* points, cudaStream_t strea
   buf.counters = static_cast<uint32_t*>(counters_.get());
   uint32_t* offsets =
       static_cast<uint32_t*>(offsets_.reserve((bins_ + 1) * sizeof(uint32_t), "bin offsets"));
-  sort_points(static_cast<const float*>(points), count, grid_,
-              type_ == 1 ? KeyKind::SupportStart : KeyKind::ApproximateCell, bins_, buf, offsets,
-              &perm_, &sorted_keys_, stream, &timer_);
-  float* sorted = static_cast<float*>(
-      sorted_points_.reserve(static_cast<size_t>(std::max<int64_t>(count, 1)) * dim_ * sizeof(float),
-                             "sorted coordinates"));
-  gather_sorted_points(static_cast<const float*>(points), perm_, count, dim_, sorted, stream, &timer_);
+  const size_t sorted_bytes = static_cast<size_t>(std::max<int64_t>(count, 1)) * dim_ * scalar_bytes();
+  if (precision_ == B200NUFFT_PRECISION_F32) {
+    sort_points(static_cast<const float*>(points), count, grid_,
+                type_ == 1 ? KeyKind::SupportStart : KeyKind::ApproximateCell, bins_, buf, offsets,
+                &perm_, &sorted_keys_, stream, &timer_);
+    float* sorted = static_cast<float*>(sorted_points_.reserve(sorted_bytes, "sorted coordinates"));
+    gather_sorted_points(static_cast<const float*>(points), perm_, count, dim_, sorted, stream,
+                         &timer_);
+  } else {
+    const double* points64 = static_cast<const double*>(points);
+    if (precision_ == B200NUFFT_PRECISION_DF64 && count > 0) {
+      double* converted = static_cast<double*>(points64_.reserve(sorted_bytes, "f64 coordinates"));
+      df64_to_f64(static_cast<const float*>(points), count * dim_, converted, stream);
+      points64 = converted;
+    }
+    sort_points64(points64, count, grid_, bins_, buf, offsets, &perm_, &sorted_keys_, stream,
+                  &timer_);
+    double* sorted = static_cast<double*>(sorted_points_.reserve(sorted_bytes, "sorted coordinates"));
+    gather_sorted_points64(points64, perm_, count, dim_, sorted, stream, &timer_);
+  }
   if (type_ == 1) {
     configure_tiles();
     parts_.reserve(static_cast<size_t>(spread_.tile_count) * sizeof(uint32_t), "tile parts");
@@ -473,6 +524,16 @@ void NufftPlan::execute(int64_t active_batch, const void* input, void* output, c
     throw NufftFailure{B200NUFFT_GPU_BUFFER_ALIAS_UNSUPPORTED, "input and output overlap"};
   }
   const int batch = static_cast<int>(active_batch);
+  if (precision_ == B200NUFFT_PRECISION_F32) {
+    execute_f32(batch, input, output, out_bytes, stream);
+  } else {
+    execute_f64(batch, input, output, in_bytes, out_bytes, stream);
+  }
+  check_cuda(cudaGetLastError(), "execute launch");
+}
+
+void NufftPlan::execute_f32(int batch, const void* input, void* output, uint64_t out_bytes,
+                            cudaStream_t stream) {
   float2* fine = static_cast<float2*>(fine_grid_.get());
   const int direction = isign_ >= 0 ? CUFFT_INVERSE : CUFFT_FORWARD;
   if (type_ == 1) {
@@ -517,7 +578,124 @@ void NufftPlan::execute(int64_t active_batch, const void* input, void* output, c
     StageScope scope(&timer_, kStageInterpolation, stream);
     interpolate_execute(grid_, l, stream);
   }
-  check_cuda(cudaGetLastError(), "execute launch");
+}
+
+void NufftPlan::execute_f64(int batch, const void* input, void* output, uint64_t in_bytes,
+                            uint64_t out_bytes, cudaStream_t stream) {
+  double2* fine = static_cast<double2*>(fine_grid_.get());
+  const int direction = isign_ >= 0 ? CUFFT_INVERSE : CUFFT_FORWARD;
+  // Df64 values arrive as (hi, lo) float pairs per scalar; the pipeline runs
+  // in f64 on converted copies.
+  const bool df64 = precision_ == B200NUFFT_PRECISION_DF64;
+  const double2* in = static_cast<const double2*>(input);
+  double2* out = static_cast<double2*>(output);
+  if (df64) {
+    double* converted = static_cast<double*>(input64_.reserve(std::max<uint64_t>(in_bytes, 16), "f64 input"));
+    if (in_bytes) df64_to_f64(static_cast<const float*>(input), static_cast<int64_t>(in_bytes / 8), converted, stream);
+    in = reinterpret_cast<const double2*>(converted);
+    out = static_cast<double2*>(output64_.reserve(std::max<uint64_t>(out_bytes, 16), "f64 output"));
+  }
+  if (type_ == 1) {
+    if (point_count_ == 0) {
+      check_cuda(cudaMemsetAsync(output, 0, out_bytes, stream), "zero type-1 output");
+      return;
+    }
+    const size_t scratch_bytes = static_cast<size_t>(part_upper_bound_) * batch *
+                                 spread_.padded_cells * sizeof(double2);
+    SpreadLaunch64 l;
+    l.points = static_cast<const double*>(sorted_points_.get());
+    l.strengths = in;
+    l.point_count = point_count_;
+    l.batch = batch;
+    l.perm = perm_;
+    l.offsets = static_cast<const uint32_t*>(offsets_.get());
+    l.part_start = static_cast<const uint32_t*>(part_start_.get());
+    l.part_upper_bound = part_upper_bound_;
+    l.max_bits = static_cast<unsigned long long*>(max_bits_.get());
+    l.scratch = static_cast<double2*>(scratch_.reserve(scratch_bytes, "spreading tiles"));
+    l.candidates = static_cast<const int2*>(candidates_.get());
+    l.fine = fine;
+    spread_execute64(spread_, l, stream, &timer_);
+    run_fft(fine, batch, direction, stream);
+    StageScope scope(&timer_, kStageDeconvolution, stream);
+    deconvolve_f64(modes_params_, batch, fine, static_cast<const double*>(amplitudes_.get()), out,
+                   stream);
+  } else {
+    {
+      StageScope scope(&timer_, kStagePredeconvolution, stream);
+      predeconvolve_f64(modes_params_, batch, in, static_cast<const double*>(amplitudes_.get()),
+                        fine, stream);
+    }
+    run_fft(fine, batch, direction, stream);
+    InterpLaunch64 l;
+    l.points = static_cast<const double*>(sorted_points_.get());
+    l.point_count = point_count_;
+    l.perm = perm_;
+    l.fine = fine;
+    l.batch = batch;
+    l.output = out;
+    StageScope scope(&timer_, kStageInterpolation, stream);
+    interpolate_execute64(grid_, l, stream);
+  }
+  if (df64 && out_bytes) {
+    f64_to_df64(reinterpret_cast<const double*>(out), static_cast<int64_t>(out_bytes / 8),
+                static_cast<float*>(output), stream);
+  }
+}
+
+void NufftPlan::spread_to(int64_t active_batch, const void* strengths, void* grid,
+                          cudaStream_t stream) {
+  if (!has_device_ || type_ != 1) {
+    throw NufftFailure{B200NUFFT_GPU_EXECUTION_UNAVAILABLE, "spreading needs a type-1 GPU plan"};
+  }
+  make_current();
+  validate_active_batch(active_batch);
+  if (point_count_ < 0) {
+    throw NufftFailure{B200NUFFT_GPU_EXECUTION_UNAVAILABLE, "no point set"};
+  }
+  const int batch = static_cast<int>(active_batch);
+  if (point_count_ == 0) {
+    check_cuda(cudaMemsetAsync(grid, 0, static_cast<size_t>(batch) * fine_count_ * 2 * scalar_bytes(),
+                               stream),
+               "zero spread grid");
+    return;
+  }
+  if (precision_ == B200NUFFT_PRECISION_F32) {
+    SpreadLaunch l;
+    l.points = static_cast<const float*>(sorted_points_.get());
+    l.strengths = static_cast<const float2*>(strengths);
+    l.point_count = point_count_;
+    l.batch = batch;
+    l.perm = perm_;
+    l.offsets = static_cast<const uint32_t*>(offsets_.get());
+    l.part_start = static_cast<const uint32_t*>(part_start_.get());
+    l.part_upper_bound = part_upper_bound_;
+    l.max_bits = static_cast<uint32_t*>(max_bits_.get());
+    l.scratch = static_cast<float2*>(scratch_.reserve(
+        static_cast<size_t>(part_upper_bound_) * batch * spread_.padded_cells * sizeof(float2),
+        "spreading tiles"));
+    l.candidates = static_cast<const int2*>(candidates_.get());
+    l.fine = static_cast<float2*>(grid);
+    spread_execute(spread_, l, stream, &timer_);
+  } else {
+    SpreadLaunch64 l;
+    l.points = static_cast<const double*>(sorted_points_.get());
+    l.strengths = static_cast<const double2*>(strengths);
+    l.point_count = point_count_;
+    l.batch = batch;
+    l.perm = perm_;
+    l.offsets = static_cast<const uint32_t*>(offsets_.get());
+    l.part_start = static_cast<const uint32_t*>(part_start_.get());
+    l.part_upper_bound = part_upper_bound_;
+    l.max_bits = static_cast<unsigned long long*>(max_bits_.get());
+    l.scratch = static_cast<double2*>(scratch_.reserve(
+        static_cast<size_t>(part_upper_bound_) * batch * spread_.padded_cells * sizeof(double2),
+        "spreading tiles"));
+    l.candidates = static_cast<const int2*>(candidates_.get());
+    l.fine = static_cast<double2*>(grid);
+    spread_execute64(spread_, l, stream, &timer_);
+  }
+  check_cuda(cudaGetLastError(), "spread launch");
 }
 
 void NufftPlan::copy_bin_order(uint32_t* permutation, uint32_t* bin_offsets, cudaStream_t stream) {

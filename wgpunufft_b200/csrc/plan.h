@@ -25,6 +25,11 @@ class NufftPlan {
 
   void set_points(int64_t count, const void* points, cudaStream_t stream);
   void execute(int64_t active_batch, const void* input, void* output, cudaStream_t stream);
+  // Type-1 plans: spreads the strengths of the remembered points onto `grid`
+  // (active_batch fine grids of the plan's precision), with no FFT and no
+  // deconvolution (Type1GpuPlanNd::encode_spread_batch, src/gpu_type1_nd.rs:477).
+  void spread_to(int64_t active_batch, const void* strengths, void* grid, cudaStream_t stream);
+  int64_t fine_count() const { return fine_count_; }
   void info(b200nufft_plan_info* out) const;
   int choose_geometry(int64_t point_count) const;
   const std::vector<double>& phi_hat(int axis) const { return phi_hat_[axis]; }
@@ -54,6 +59,10 @@ class NufftPlan {
   void configure_tiles();
   cufftHandle fft_for(int batch);
   void run_fft(void* fine, int batch, int direction, cudaStream_t stream);
+  void execute_f32(int batch, const void* input, void* output, uint64_t out_bytes,
+                   cudaStream_t stream);
+  void execute_f64(int batch, const void* input, void* output, uint64_t in_bytes,
+                   uint64_t out_bytes, cudaStream_t stream);
   size_t scalar_bytes() const;
 
   int type_ = 1;
@@ -79,8 +88,10 @@ class NufftPlan {
 
   bool has_device_ = true;
   StageTimer timer_;
-  std::vector<float> amplitudes_host_;
   DeviceBuffer amplitudes_;
+  DeviceBuffer horner_device_;
+  // Df64 plans: f64 copies of the caller's double-float coordinates and values.
+  DeviceBuffer points64_, input64_, output64_;
   DeviceBuffer fine_grid_;
   std::map<int, cufftHandle> ffts_;
 

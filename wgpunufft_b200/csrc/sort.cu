@@ -110,6 +110,49 @@ __global__ void __launch_bounds__(256) bin_keys_kernel(const float* __restrict__
   }
 }
 
+// Bin keys of f64 coordinates: the support starts of the native f64 fold,
+// with the same reach rule and wrapping as the f32 keys.
+template <int D>
+__global__ void __launch_bounds__(256) bin_keys64_kernel(const double* __restrict__ points,
+                                                         int64_t count, GridParams g,
+                                                         uint32_t* __restrict__ keys,
+                                                         uint32_t* __restrict__ hist, int passes) {
+  __shared__ uint32_t local[4][kRadix];
+  for (int i = threadIdx.x; i < 4 * kRadix; i += blockDim.x) (&local[0][0])[i] = 0;
+  __syncthreads();
+  const int64_t stride = static_cast<int64_t>(gridDim.x) * blockDim.x;
+  for (int64_t i = static_cast<int64_t>(blockIdx.x) * blockDim.x + threadIdx.x; i < count;
+       i += stride) {
+    double p[D];
+    bool reach = true;
+#pragma unroll
+    for (int a = 0; a < D; ++a) {
+      p[a] = points[i * D + a];
+      reach = reach && in_fold_reach64(p[a]);
+    }
+    uint32_t key = 0;
+#pragma unroll
+    for (int a = 0; a < D; ++a) {
+      int32_t start = 0;
+      if (reach) {
+        double offset;
+        support_of64(p[a], g.axis64[a], g.half_width64, start, offset);
+      }
+      const int32_t wrapped = wrap_start(start, g.axis[a].length);
+      key += (static_cast<uint32_t>(wrapped) >> g.axis[a].shift) * g.axis[a].stride;
+    }
+    keys[i] = key;
+    for (int pass = 0; pass < passes; ++pass) {
+      atomicAdd(&local[pass][(key >> (8 * pass)) & 0xFF], 1u);
+    }
+  }
+  __syncthreads();
+  for (int i = threadIdx.x; i < passes * kRadix; i += blockDim.x) {
+    const uint32_t v = (&local[0][0])[i];
+    if (v) atomicAdd(&hist[i], v);
+  }
+}
+
 // Exclusive scan of every pass's 256 digit counts, in place.
 __global__ void digit_scan_kernel(uint32_t* hist, int passes) {
   __shared__ uint32_t buffer[kRadix];
@@ -285,10 +328,10 @@ __global__ void bin_offsets_kernel(const uint32_t* __restrict__ keys, int64_t co
 
 // Coordinates in bin order: sorted[slot] = points[perm[slot]], so that the
 // spreading and interpolation kernels read them contiguously.
-template <int D>
-__global__ void gather_points_kernel(const float* __restrict__ points,
+template <int D, typename T>
+__global__ void gather_points_kernel(const T* __restrict__ points,
                                      const uint32_t* __restrict__ perm, int64_t count,
-                                     float* __restrict__ sorted) {
+                                     T* __restrict__ sorted) {
   const int64_t slot = static_cast<int64_t>(blockIdx.x) * blockDim.x + threadIdx.x;
   if (slot >= count) return;
   const int64_t point = perm[slot];
@@ -375,9 +418,9 @@ void gather_sorted_points(const float* points, const uint32_t* perm, int64_t cou
   StageScope scope(timer, kStageBinOffsets, stream);
   const unsigned blocks = static_cast<unsigned>((count + 255) / 256);
   switch (dimensions) {
-    case 1: gather_points_kernel<1><<<blocks, 256, 0, stream>>>(points, perm, count, sorted); break;
-    case 2: gather_points_kernel<2><<<blocks, 256, 0, stream>>>(points, perm, count, sorted); break;
-    default: gather_points_kernel<3><<<blocks, 256, 0, stream>>>(points, perm, count, sorted); break;
+    case 1: gather_points_kernel<1, float><<<blocks, 256, 0, stream>>>(points, perm, count, sorted); break;
+    case 2: gather_points_kernel<2, float><<<blocks, 256, 0, stream>>>(points, perm, count, sorted); break;
+    default: gather_points_kernel<3, float><<<blocks, 256, 0, stream>>>(points, perm, count, sorted); break;
   }
   note_launch();
 }
@@ -387,12 +430,51 @@ size_t sort_status_bytes(int64_t count) {
   return static_cast<size_t>(std::max<int64_t>(tiles, 1)) * kRadix * sizeof(uint32_t);
 }
 
+namespace {
+
+int radix_passes(uint64_t bins) {
+  int key_bits = 0;
+  while (key_bits < 32 && (uint64_t(1) << key_bits) < bins) ++key_bits;
+  return (key_bits + 7) / 8;
+}
+
+// The radix passes and bin offsets once buf.keys_a and buf.hist hold the
+// keys and their digit histograms.
+void sort_from_keys(int64_t count, uint64_t bins, int passes, SortBuffers buf, uint32_t* offsets,
+                    uint32_t** perm, uint32_t** sorted_keys, cudaStream_t stream,
+                    StageTimer* timer);
+
+}  // namespace
+
+void sort_points64(const double* points, int64_t count, const GridParams& g, uint64_t bins,
+                   SortBuffers buf, uint32_t* offsets, uint32_t** perm, uint32_t** sorted_keys,
+                   cudaStream_t stream, StageTimer* timer) {
+  const int passes = radix_passes(bins);
+  if (count == 0) {
+    check_cuda(cudaMemsetAsync(offsets, 0, (bins + 1) * sizeof(uint32_t), stream), "clear offsets");
+    *perm = buf.vals_a;
+    *sorted_keys = buf.keys_a;
+    return;
+  }
+  {
+    StageScope scope(timer, kStageBinKeys, stream);
+    check_cuda(cudaMemsetAsync(buf.hist, 0, 4 * kRadix * sizeof(uint32_t), stream), "clear histogram");
+    check_cuda(cudaMemsetAsync(buf.counters, 0, 7 * sizeof(uint32_t), stream), "clear tickets");
+    const int blocks = static_cast<int>(std::min<int64_t>((count + 255) / 256, 148 * 16));
+    switch (g.dimensions) {
+      case 1: bin_keys64_kernel<1><<<blocks, 256, 0, stream>>>(points, count, g, buf.keys_a, buf.hist, passes); break;
+      case 2: bin_keys64_kernel<2><<<blocks, 256, 0, stream>>>(points, count, g, buf.keys_a, buf.hist, passes); break;
+      default: bin_keys64_kernel<3><<<blocks, 256, 0, stream>>>(points, count, g, buf.keys_a, buf.hist, passes); break;
+    }
+    note_launch();
+  }
+  sort_from_keys(count, bins, passes, buf, offsets, perm, sorted_keys, stream, timer);
+}
+
 void sort_points(const float* points, int64_t count, const GridParams& g, KeyKind kind,
                  uint64_t bins, SortBuffers buf, uint32_t* offsets, uint32_t** perm,
                  uint32_t** sorted_keys, cudaStream_t stream, StageTimer* timer) {
-  int key_bits = 0;
-  while (key_bits < 32 && (uint64_t(1) << key_bits) < bins) ++key_bits;
-  const int passes = (key_bits + 7) / 8;
+  const int passes = radix_passes(bins);
   if (count == 0) {
     check_cuda(cudaMemsetAsync(offsets, 0, (bins + 1) * sizeof(uint32_t), stream), "clear offsets");
     *perm = buf.vals_a;
@@ -409,6 +491,14 @@ void sort_points(const float* points, int64_t count, const GridParams& g, KeyKin
       default: launch_keys<3>(points, count, g, kind, buf.keys_a, buf.hist, passes, stream); break;
     }
   }
+  sort_from_keys(count, bins, passes, buf, offsets, perm, sorted_keys, stream, timer);
+}
+
+namespace {
+
+void sort_from_keys(int64_t count, uint64_t bins, int passes, SortBuffers buf, uint32_t* offsets,
+                    uint32_t** perm, uint32_t** sorted_keys, cudaStream_t stream,
+                    StageTimer* timer) {
   if (passes == 0) {
     identity_kernel<<<static_cast<unsigned>((count + 255) / 256), 256, 0, stream>>>(buf.vals_a,
                                                                                  buf.keys_a, count);
@@ -449,6 +539,22 @@ void sort_points(const float* points, int64_t count, const GridParams& g, KeyKin
   StageScope scope(timer, kStageBinOffsets, stream);
   bin_offsets_kernel<<<static_cast<unsigned>((count + 1 + 255) / 256), 256, 0, stream>>>(
       *sorted_keys, count, bins, offsets);
+  note_launch();
+}
+
+}  // namespace
+
+void gather_sorted_points64(const double* points, const uint32_t* perm, int64_t count,
+                            int dimensions, double* sorted, cudaStream_t stream,
+                            StageTimer* timer) {
+  if (count == 0) return;
+  StageScope scope(timer, kStageBinOffsets, stream);
+  const unsigned blocks = static_cast<unsigned>((count + 255) / 256);
+  switch (dimensions) {
+    case 1: gather_points_kernel<1, double><<<blocks, 256, 0, stream>>>(points, perm, count, sorted); break;
+    case 2: gather_points_kernel<2, double><<<blocks, 256, 0, stream>>>(points, perm, count, sorted); break;
+    default: gather_points_kernel<3, double><<<blocks, 256, 0, stream>>>(points, perm, count, sorted); break;
+  }
   note_launch();
 }
 

@@ -7,15 +7,17 @@
 // fine grid (or one part of a crowded tile), read from the bins of the stable
 // sort. Every point evaluates its window per axis into registers and adds
 // its w^d contributions to a padded copy of the tile in shared memory. The
-// contributions are accumulated as fixed-point integers (each rounded to a
-// 32-bit integer after scaling by a power of two derived from the largest
-// strength, and summed exactly in two 32-bit halves), so the sum of a cell is
-// the exact integer sum of its rounded contributions whatever order the
-// threads add them in: the accumulation is deterministic without ordering the
-// threads, and it carries more bits than an f32 sum. Each padded tile is then
-// converted to f32 and written out, and a fold pass adds, for every fine-grid
-// cell, the padded tiles and parts that cover it in a fixed order (halos
-// wrap periodically). Nothing is accumulated with floating-point atomics.
+// contributions are accumulated as fixed-point integers, scaled by a power of
+// two derived from the largest strength (f32 plans: each rounded to a 32-bit
+// integer and summed exactly in two 32-bit halves; f64 plans: 64-bit integers
+// with 2^-50 resolution), so the sum of a cell is the exact integer sum of its
+// rounded contributions whatever order the threads add them in: the
+// accumulation is deterministic without ordering the threads, and it carries
+// more bits than a floating-point sum. Each padded tile is then converted back
+// to floating point and written out, and a fold pass adds, for every
+// fine-grid cell, the padded tiles and parts that cover it in a fixed order
+// (halos wrap periodically). Nothing is accumulated with floating-point
+// atomics.
 #include <cuda_runtime.h>
 
 #include <algorithm>
@@ -37,49 +39,130 @@ __device__ __forceinline__ float es_weight(float distance, float beta, float wid
   return expf(beta * (sqrtf(fmaxf(0.0f, 1.0f - squared)) - 1.0f));
 }
 
-// Largest |re| or |im| of every strength vector, as float bits.
-__global__ void strength_magnitude_kernel(const float2* __restrict__ values, int64_t count,
-                                          int batch, uint32_t* __restrict__ max_bits) {
+// ---------------------------------------------------------------------------
+// Precision traits: coordinates, window, fixed-point accumulator.
+
+struct F32Traits {
+  using Real = float;
+  using Complex = float2;
+  using Bits = uint32_t;
+  // Shared-memory words per padded cell: re lo, re hi, im lo, im hi.
+  static constexpr int kWordsPerCell = 4;
+  using Word = uint32_t;
+
+  static __device__ __forceinline__ Bits magnitude_bits(float v) {
+    return __float_as_uint(v) & 0x7fffffffu;
+  }
+  // S so that every contribution, at most the largest strength, scales below
+  // 2^30: each then rounds to a 32-bit integer with a resolution of 2^-30 of
+  // the largest strength. Non-finite strengths leave the outputs unspecified
+  // but the exponent bounded.
+  static __device__ __forceinline__ int exponent(Bits max_bits) {
+    if (max_bits == 0u) return 0;
+    const int e = max_bits >= 0x7f800000u ? 128 : ilogbf(__uint_as_float(max_bits)) + 1;
+    return 30 - e;
+  }
+  static __device__ __forceinline__ bool in_reach(float x) { return in_fold_reach(x); }
+  static __device__ __forceinline__ void window(float x, const GridParams& g, int a, int32_t& wrapped,
+                                                float* w, int W) {
+    int32_t start;
+    Df64 off;
+    support_of(x, g.axis[a], g.half_width, start, off);
+    wrapped = wrap_start(start, g.axis[a].length);
+    const float width_f = static_cast<float>(W);
+    for (int j = 0; j < W; ++j) {
+      const float d = __fadd_rn(__fadd_rn(static_cast<float>(j), off.hi), off.lo);
+      w[j] = es_weight(d, g.beta, width_f);
+    }
+  }
+  static __device__ __forceinline__ float scale(float s, int S) { return ldexpf(s, S); }
+  // Adds a contribution (|v| < 2^31 after rounding) as two exact 32-bit sums:
+  // its low 16 bits, unsigned, and its arithmetic high part. Both stay exact
+  // for up to 2^16 contributions per cell; the cell's value is hi 2^16 + lo.
+  static __device__ __forceinline__ void add(Word* acc, int padded, int part, int c, float value) {
+    const int32_t v = __float2int_rn(value);
+    atomicAdd(&acc[(2 * part) * padded + c], static_cast<uint32_t>(v) & 0xFFFFu);
+    atomicAdd(reinterpret_cast<int32_t*>(&acc[(2 * part + 1) * padded + c]), v >> 16);
+  }
+  static __device__ __forceinline__ float value(const Word* acc, int padded, int part, int c, int S) {
+    const uint32_t lo = acc[(2 * part) * padded + c];
+    const int32_t hi = static_cast<int32_t>(acc[(2 * part + 1) * padded + c]);
+    const long long total = static_cast<long long>(hi) * 65536ll + static_cast<long long>(lo);
+    return ldexpf(__ll2float_rn(total), -S);
+  }
+};
+
+struct F64Traits {
+  using Real = double;
+  using Complex = double2;
+  using Bits = unsigned long long;
+  // Shared-memory words per padded cell: re, im (64-bit).
+  static constexpr int kWordsPerCell = 2;
+  using Word = unsigned long long;
+
+  static __device__ __forceinline__ Bits magnitude_bits(double v) {
+    return static_cast<unsigned long long>(__double_as_longlong(v)) & 0x7fffffffffffffffull;
+  }
+  // S so that every contribution scales below 2^50; a part of at most 4096
+  // records then sums below 2^62 in every cell, with a resolution of 2^-50 of
+  // the largest strength.
+  static __device__ __forceinline__ int exponent(Bits max_bits) {
+    if (max_bits == 0ull) return 0;
+    const int e = max_bits >= 0x7ff0000000000000ull ? 1024 : ilogb(__longlong_as_double(static_cast<long long>(max_bits))) + 1;
+    return 50 - e;
+  }
+  static __device__ __forceinline__ bool in_reach(double x) { return in_fold_reach64(x); }
+  static __device__ __forceinline__ void window(double x, const GridParams& g, int a,
+                                                int32_t& wrapped, double* w, int W) {
+    int32_t start;
+    double offset;
+    support_of64(x, g.axis64[a], g.half_width64, start, offset);
+    wrapped = wrap_start(start, g.axis[a].length);
+    for (int j = 0; j < W; ++j) w[j] = horner_weight(offset, j, W, g.horner, g.horner_rows);
+  }
+  static __device__ __forceinline__ double scale(double s, int S) { return ldexp(s, S); }
+  static __device__ __forceinline__ void add(Word* acc, int padded, int part, int c, double value) {
+    atomicAdd(&acc[part * padded + c], static_cast<unsigned long long>(__double2ll_rn(value)));
+  }
+  static __device__ __forceinline__ double value(const Word* acc, int padded, int part, int c, int S) {
+    return ldexp(__ll2double_rn(static_cast<long long>(acc[part * padded + c])), -S);
+  }
+};
+
+template <typename T>
+struct SpreadLaunchT {
+  const typename T::Real* points;
+  const typename T::Complex* strengths;
+  int64_t point_count;
+  int batch;
+  const uint32_t* perm;
+  const uint32_t* offsets;
+  const uint32_t* part_start;
+  int64_t part_upper_bound;
+  typename T::Bits* max_bits;
+  typename T::Complex* scratch;
+  const int2* candidates;
+  typename T::Complex* fine;
+};
+
+// Largest |re| or |im| of every strength vector, as magnitude bits.
+template <typename T>
+__global__ void strength_magnitude_kernel(const typename T::Complex* __restrict__ values,
+                                          int64_t count, int batch,
+                                          typename T::Bits* __restrict__ max_bits) {
   const int b = blockIdx.y;
-  const float2* v = values + static_cast<int64_t>(b) * count;
-  uint32_t m = 0;
+  const typename T::Complex* v = values + static_cast<int64_t>(b) * count;
+  typename T::Bits m = 0;
   const int64_t stride = static_cast<int64_t>(gridDim.x) * blockDim.x;
   for (int64_t i = static_cast<int64_t>(blockIdx.x) * blockDim.x + threadIdx.x; i < count;
        i += stride) {
-    const float2 s = v[i];
-    m = max(m, __float_as_uint(s.x) & 0x7fffffffu);
-    m = max(m, __float_as_uint(s.y) & 0x7fffffffu);
+    const typename T::Complex s = v[i];
+    m = max(m, T::magnitude_bits(s.x));
+    m = max(m, T::magnitude_bits(s.y));
   }
 #pragma unroll
   for (int offset = 16; offset > 0; offset >>= 1) m = max(m, __shfl_xor_sync(0xFFFFFFFFu, m, offset));
   if ((threadIdx.x & 31) == 0 && m) atomicMax(&max_bits[b], m);
-}
-
-// Power-of-two exponent S that scales every contribution, at most the largest
-// strength magnitude, below 2^30 in magnitude: each then rounds to a 32-bit
-// integer with a resolution of 2^-30 of the largest strength.
-__device__ __forceinline__ int fixed_point_exponent(uint32_t max_bits) {
-  if (max_bits == 0u) return 0;
-  // Non-finite strengths (bits at or above infinity) leave the outputs
-  // unspecified but the exponent bounded.
-  const int e = max_bits >= 0x7f800000u ? 128 : ilogbf(__uint_as_float(max_bits)) + 1;  // max < 2^e
-  return 30 - e;
-}
-
-// Adds a fixed-point contribution v (|v| < 2^31) to cell c as two exact
-// 32-bit sums: its low 16 bits, unsigned, and its arithmetic high part. Both
-// stay exact for up to 2^16 contributions per cell, and the cell's value is
-// hi * 2^16 + lo. Integer addition is associative, so the sums do not depend
-// on the order in which threads add.
-__device__ __forceinline__ void add_fixed(uint32_t* lo, int32_t* hi, int c, float value) {
-  const int32_t v = __float2int_rn(value);
-  atomicAdd(&lo[c], static_cast<uint32_t>(v) & 0xFFFFu);
-  atomicAdd(&hi[c], v >> 16);
-}
-
-__device__ __forceinline__ float fixed_to_float(uint32_t lo, int32_t hi, int S) {
-  const long long total = static_cast<long long>(hi) * 65536ll + static_cast<long long>(lo);
-  return ldexpf(__ll2float_rn(total), -S);
 }
 
 // Records in the reach of every tile's bins, and the parts of every tile.
@@ -155,14 +238,18 @@ __global__ void __launch_bounds__(1024) part_scan_kernel(const uint32_t* __restr
 }
 
 // One CTA per (part, vector): spreads the part's records into a padded tile
-// of 64-bit fixed-point sums and writes the tile out as f32.
-template <int D, int W>
+// of fixed-point sums and writes the tile out in floating point.
+template <int D, int W, typename T>
 __global__ void __launch_bounds__(kSpreadThreads) spread_tiles_kernel(
-    SpreadParams sp, const float* __restrict__ points, const float2* __restrict__ strengths,
-    int64_t point_count, int batch, const uint32_t* __restrict__ perm,
-    const uint32_t* __restrict__ offsets, const uint32_t* __restrict__ part_start,
-    const uint32_t* __restrict__ max_bits, float2* __restrict__ scratch) {
-  extern __shared__ uint32_t acc[];
+    SpreadParams sp, const typename T::Real* __restrict__ points,
+    const typename T::Complex* __restrict__ strengths, int64_t point_count, int batch,
+    const uint32_t* __restrict__ perm, const uint32_t* __restrict__ offsets,
+    const uint32_t* __restrict__ part_start, const typename T::Bits* __restrict__ max_bits,
+    typename T::Complex* __restrict__ scratch) {
+  using Real = typename T::Real;
+  using Word = typename T::Word;
+  extern __shared__ __align__(16) unsigned char shared_bytes[];
+  Word* acc = reinterpret_cast<Word*>(shared_bytes);
   __shared__ uint32_t row_begin[kMaxTileRows];
   __shared__ uint32_t row_prefix[kMaxTileRows + 1];
   __shared__ int64_t s_tile;
@@ -183,7 +270,7 @@ __global__ void __launch_bounds__(kSpreadThreads) spread_tiles_kernel(
     s_tile = low;
   }
   const int padded = sp.padded_cells;
-  for (int c = tid; c < 4 * padded; c += kSpreadThreads) acc[c] = 0u;
+  for (int c = tid; c < T::kWordsPerCell * padded; c += kSpreadThreads) acc[c] = Word(0);
   __syncthreads();
   const int64_t tile = s_tile;
   const uint32_t part_in_tile = part - part_start[tile];
@@ -254,13 +341,8 @@ __global__ void __launch_bounds__(kSpreadThreads) spread_tiles_kernel(
   const uint32_t tile_total = row_prefix[rows];
   const uint32_t record_begin = part_in_tile * static_cast<uint32_t>(sp.part_cap);
   const uint32_t record_end = min(tile_total, record_begin + static_cast<uint32_t>(sp.part_cap));
-  const int S = fixed_point_exponent(max_bits[b]);
-  const float width_f = static_cast<float>(W);
-  const float2* sv = strengths + static_cast<int64_t>(b) * point_count;
-  uint32_t* re_lo = acc;
-  int32_t* re_hi = reinterpret_cast<int32_t*>(acc + padded);
-  uint32_t* im_lo = acc + 2 * padded;
-  int32_t* im_hi = reinterpret_cast<int32_t*>(acc + 3 * padded);
+  const int S = T::exponent(max_bits[b]);
+  const typename T::Complex* sv = strengths + static_cast<int64_t>(b) * point_count;
 
   int row = 0;
   for (uint32_t r = record_begin + tid; r < record_end; r += kSpreadThreads) {
@@ -274,51 +356,44 @@ __global__ void __launch_bounds__(kSpreadThreads) spread_tiles_kernel(
       row = low;
     }
     const uint32_t slot = row_begin[row] + (r - row_prefix[row]);
-    float p[D];
+    Real p[D];
 #pragma unroll
     for (int a = 0; a < D; ++a) p[a] = points[static_cast<int64_t>(slot) * D + a];
     bool reach = true;
 #pragma unroll
-    for (int a = 0; a < D; ++a) reach = reach && in_fold_reach(p[a]);
+    for (int a = 0; a < D; ++a) reach = reach && T::in_reach(p[a]);
     if (!reach) continue;  // weighed zero by the reference
     int local_start[D];
-    float w[D][W];
+    Real w[D][W];
     bool inside = true;
 #pragma unroll
     for (int a = 0; a < D; ++a) {
-      int32_t start;
-      Df64 off;
-      support_of(p[a], sp.grid.axis[a], sp.grid.half_width, start, off);
-      const int32_t wrapped = wrap_start(start, sp.grid.axis[a].length);
+      int32_t wrapped;
+      T::window(p[a], sp.grid, a, wrapped, w[a], W);
       local_start[a] = wrapped - origin[a];
       inside = inside && local_start[a] >= 0 && local_start[a] < sp.tile[a];
-#pragma unroll
-      for (int j = 0; j < W; ++j) {
-        const float d = __fadd_rn(__fadd_rn(static_cast<float>(j), off.hi), off.lo);
-        w[a][j] = es_weight(d, sp.grid.beta, width_f);
-      }
     }
     if (!inside) continue;  // a bin wider than the tile: another tile owns it
-    const float2 s = sv[perm[slot]];
-    const float sr = ldexpf(s.x, S);
-    const float si = ldexpf(s.y, S);
+    const typename T::Complex s = sv[perm[slot]];
+    const Real sr = T::scale(s.x, S);
+    const Real si = T::scale(s.y, S);
     if (D == 1) {
 #pragma unroll
       for (int i = 0; i < W; ++i) {
         const int c = local_start[0] + i;
-        add_fixed(re_lo, re_hi, c, sr * w[0][i]);
-        add_fixed(im_lo, im_hi, c, si * w[0][i]);
+        T::add(acc, padded, 0, c, sr * w[0][i]);
+        T::add(acc, padded, 1, c, si * w[0][i]);
       }
     } else if (D == 2) {
 #pragma unroll
       for (int j = 0; j < W; ++j) {
-        const float wr = sr * w[1][j];
-        const float wi = si * w[1][j];
+        const Real wr = sr * w[1][j];
+        const Real wi = si * w[1][j];
         const int base = (local_start[1] + j) * sp.pad[0] + local_start[0];
 #pragma unroll
         for (int i = 0; i < W; ++i) {
-          add_fixed(re_lo, re_hi, base + i, wr * w[0][i]);
-          add_fixed(im_lo, im_hi, base + i, wi * w[0][i]);
+          T::add(acc, padded, 0, base + i, wr * w[0][i]);
+          T::add(acc, padded, 1, base + i, wi * w[0][i]);
         }
       }
     } else {
@@ -326,34 +401,37 @@ __global__ void __launch_bounds__(kSpreadThreads) spread_tiles_kernel(
       for (int k = 0; k < W; ++k) {
 #pragma unroll
         for (int j = 0; j < W; ++j) {
-          const float wyz = w[1][j] * w[2][k];
-          const float wr = sr * wyz;
-          const float wi = si * wyz;
+          const Real wyz = w[1][j] * w[2][k];
+          const Real wr = sr * wyz;
+          const Real wi = si * wyz;
           const int base =
               ((local_start[2] + k) * sp.pad[1] + local_start[1] + j) * sp.pad[0] + local_start[0];
 #pragma unroll
           for (int i = 0; i < W; ++i) {
-            add_fixed(re_lo, re_hi, base + i, wr * w[0][i]);
-            add_fixed(im_lo, im_hi, base + i, wi * w[0][i]);
+            T::add(acc, padded, 0, base + i, wr * w[0][i]);
+            T::add(acc, padded, 1, base + i, wi * w[0][i]);
           }
         }
       }
     }
   }
   __syncthreads();
-  float2* out = scratch + (static_cast<int64_t>(part) * batch + b) * padded;
+  typename T::Complex* out = scratch + (static_cast<int64_t>(part) * batch + b) * padded;
   for (int c = tid; c < padded; c += kSpreadThreads) {
-    out[c] = make_float2(fixed_to_float(re_lo[c], re_hi[c], S), fixed_to_float(im_lo[c], im_hi[c], S));
+    typename T::Complex v;
+    v.x = T::value(acc, padded, 0, c, S);
+    v.y = T::value(acc, padded, 1, c, S);
+    out[c] = v;
   }
 }
 
 // Every fine-grid cell as the sum, in a fixed order, of the padded tiles and
 // parts that cover it.
-template <int D>
-__global__ void fold_tiles_kernel(SpreadParams sp, int batch, const float2* __restrict__ scratch,
+template <int D, typename Complex>
+__global__ void fold_tiles_kernel(SpreadParams sp, int batch, const Complex* __restrict__ scratch,
                                   const uint32_t* __restrict__ part_start, int64_t part_limit,
                                   const int2* __restrict__ candidates,
-                                  float2* __restrict__ fine) {
+                                  Complex* __restrict__ fine) {
   const int64_t cell = static_cast<int64_t>(blockIdx.x) * blockDim.x + threadIdx.x;
   if (cell >= sp.grid.fine_count) return;
   const int b = blockIdx.y;
@@ -371,7 +449,9 @@ __global__ void fold_tiles_kernel(SpreadParams sp, int batch, const float2* __re
   const int2* c2 = D > 2 ? candidates + sp.candidate_base[2] + coord[2] * sp.candidate_count[2] : nullptr;
   const int k2n = D > 2 ? sp.candidate_count[2] : 1;
   const int k1n = D > 1 ? sp.candidate_count[1] : 1;
-  float re = 0.0f, im = 0.0f;
+  Complex sum;
+  sum.x = 0;
+  sum.y = 0;
   for (int k2 = 0; k2 < k2n; ++k2) {
     int t2 = 0, l2 = 0;
     if (D > 2) {
@@ -396,21 +476,22 @@ __global__ void fold_tiles_kernel(SpreadParams sp, int batch, const float2* __re
         const int local = e.y + sp.pad[0] * (l1 + sp.pad[1] * l2);
         const uint32_t first = part_start[tile];
         const uint32_t last = min(part_start[tile + 1], static_cast<uint32_t>(part_limit));
-        for (uint32_t part = first; part < last; ++part) {
-          const float2 v = scratch[(static_cast<int64_t>(part) * batch + b) * sp.padded_cells + local];
-          re += v.x;
-          im += v.y;
+        for (uint32_t p = first; p < last; ++p) {
+          const Complex v = scratch[(static_cast<int64_t>(p) * batch + b) * sp.padded_cells + local];
+          sum.x += v.x;
+          sum.y += v.y;
         }
       }
     }
   }
-  fine[static_cast<int64_t>(b) * sp.grid.fine_count + cell] = make_float2(re, im);
+  fine[static_cast<int64_t>(b) * sp.grid.fine_count + cell] = sum;
 }
 
-template <int D, int W>
-void launch_spread_width(const SpreadParams& sp, const SpreadLaunch& l, cudaStream_t stream) {
-  const size_t smem = static_cast<size_t>(4) * sp.padded_cells * sizeof(uint32_t);
-  auto kernel = spread_tiles_kernel<D, W>;
+template <int D, int W, typename T>
+void launch_spread_width(const SpreadParams& sp, const SpreadLaunchT<T>& l, cudaStream_t stream) {
+  const size_t smem =
+      static_cast<size_t>(T::kWordsPerCell) * sp.padded_cells * sizeof(typename T::Word);
+  auto kernel = spread_tiles_kernel<D, W, T>;
   check_cuda(cudaFuncSetAttribute(kernel, cudaFuncAttributeMaxDynamicSharedMemorySize,
                                   static_cast<int>(smem)),
              "spread shared memory");
@@ -421,25 +502,67 @@ void launch_spread_width(const SpreadParams& sp, const SpreadLaunch& l, cudaStre
   note_launch();
 }
 
-template <int D>
-void launch_spread_dim(const SpreadParams& sp, const SpreadLaunch& l, cudaStream_t stream) {
+template <int D, typename T>
+void launch_spread_dim(const SpreadParams& sp, const SpreadLaunchT<T>& l, cudaStream_t stream) {
   switch (sp.grid.width) {
-    case 2: launch_spread_width<D, 2>(sp, l, stream); break;
-    case 3: launch_spread_width<D, 3>(sp, l, stream); break;
-    case 4: launch_spread_width<D, 4>(sp, l, stream); break;
-    case 5: launch_spread_width<D, 5>(sp, l, stream); break;
-    case 6: launch_spread_width<D, 6>(sp, l, stream); break;
-    case 7: launch_spread_width<D, 7>(sp, l, stream); break;
-    case 8: launch_spread_width<D, 8>(sp, l, stream); break;
-    case 9: launch_spread_width<D, 9>(sp, l, stream); break;
-    case 10: launch_spread_width<D, 10>(sp, l, stream); break;
-    case 11: launch_spread_width<D, 11>(sp, l, stream); break;
-    case 12: launch_spread_width<D, 12>(sp, l, stream); break;
-    case 13: launch_spread_width<D, 13>(sp, l, stream); break;
-    case 14: launch_spread_width<D, 14>(sp, l, stream); break;
-    case 15: launch_spread_width<D, 15>(sp, l, stream); break;
-    default: launch_spread_width<D, 16>(sp, l, stream); break;
+    case 2: launch_spread_width<D, 2, T>(sp, l, stream); break;
+    case 3: launch_spread_width<D, 3, T>(sp, l, stream); break;
+    case 4: launch_spread_width<D, 4, T>(sp, l, stream); break;
+    case 5: launch_spread_width<D, 5, T>(sp, l, stream); break;
+    case 6: launch_spread_width<D, 6, T>(sp, l, stream); break;
+    case 7: launch_spread_width<D, 7, T>(sp, l, stream); break;
+    case 8: launch_spread_width<D, 8, T>(sp, l, stream); break;
+    case 9: launch_spread_width<D, 9, T>(sp, l, stream); break;
+    case 10: launch_spread_width<D, 10, T>(sp, l, stream); break;
+    case 11: launch_spread_width<D, 11, T>(sp, l, stream); break;
+    case 12: launch_spread_width<D, 12, T>(sp, l, stream); break;
+    case 13: launch_spread_width<D, 13, T>(sp, l, stream); break;
+    case 14: launch_spread_width<D, 14, T>(sp, l, stream); break;
+    case 15: launch_spread_width<D, 15, T>(sp, l, stream); break;
+    default: launch_spread_width<D, 16, T>(sp, l, stream); break;
   }
+}
+
+template <typename T>
+void spread_execute_impl(const SpreadParams& sp, const SpreadLaunchT<T>& l, cudaStream_t stream,
+                         StageTimer* timer) {
+  if (l.point_count > 0) {
+    {
+      StageScope scope(timer, kStageStrengthScale, stream);
+      check_cuda(cudaMemsetAsync(l.max_bits, 0, sizeof(typename T::Bits) * l.batch, stream),
+                 "clear maxima");
+      const unsigned blocks =
+          static_cast<unsigned>(std::min<int64_t>((l.point_count + 255) / 256, 148 * 8));
+      strength_magnitude_kernel<T><<<dim3(blocks, l.batch), 256, 0, stream>>>(
+          l.strengths, l.point_count, l.batch, l.max_bits);
+      note_launch();
+    }
+    StageScope scope(timer, kStageSpread, stream);
+    switch (sp.grid.dimensions) {
+      case 1: launch_spread_dim<1, T>(sp, l, stream); break;
+      case 2: launch_spread_dim<2, T>(sp, l, stream); break;
+      default: launch_spread_dim<3, T>(sp, l, stream); break;
+    }
+  }
+  StageScope scope(timer, kStageFold, stream);
+  const dim3 grid(static_cast<unsigned>((sp.grid.fine_count + 255) / 256),
+                  static_cast<unsigned>(l.batch));
+  using Complex = typename T::Complex;
+  switch (sp.grid.dimensions) {
+    case 1:
+      fold_tiles_kernel<1, Complex><<<grid, 256, 0, stream>>>(sp, l.batch, l.scratch, l.part_start,
+                                                              l.part_upper_bound, l.candidates, l.fine);
+      break;
+    case 2:
+      fold_tiles_kernel<2, Complex><<<grid, 256, 0, stream>>>(sp, l.batch, l.scratch, l.part_start,
+                                                              l.part_upper_bound, l.candidates, l.fine);
+      break;
+    default:
+      fold_tiles_kernel<3, Complex><<<grid, 256, 0, stream>>>(sp, l.batch, l.scratch, l.part_start,
+                                                              l.part_upper_bound, l.candidates, l.fine);
+      break;
+  }
+  note_launch();
 }
 
 }  // namespace
@@ -459,41 +582,18 @@ void spread_count_parts(const SpreadParams& sp, const uint32_t* offsets, uint32_
 
 void spread_execute(const SpreadParams& sp, const SpreadLaunch& l, cudaStream_t stream,
                     StageTimer* timer) {
-  if (l.point_count > 0) {
-    {
-      StageScope scope(timer, kStageStrengthScale, stream);
-      check_cuda(cudaMemsetAsync(l.max_bits, 0, sizeof(uint32_t) * l.batch, stream), "clear maxima");
-      const unsigned blocks =
-          static_cast<unsigned>(std::min<int64_t>((l.point_count + 255) / 256, 148 * 8));
-      strength_magnitude_kernel<<<dim3(blocks, l.batch), 256, 0, stream>>>(
-          l.strengths, l.point_count, l.batch, l.max_bits);
-      note_launch();
-    }
-    StageScope scope(timer, kStageSpread, stream);
-    switch (sp.grid.dimensions) {
-      case 1: launch_spread_dim<1>(sp, l, stream); break;
-      case 2: launch_spread_dim<2>(sp, l, stream); break;
-      default: launch_spread_dim<3>(sp, l, stream); break;
-    }
-  }
-  StageScope scope(timer, kStageFold, stream);
-  const dim3 grid(static_cast<unsigned>((sp.grid.fine_count + 255) / 256),
-                  static_cast<unsigned>(l.batch));
-  switch (sp.grid.dimensions) {
-    case 1:
-      fold_tiles_kernel<1><<<grid, 256, 0, stream>>>(sp, l.batch, l.scratch, l.part_start,
-                                                     l.part_upper_bound, l.candidates, l.fine);
-      break;
-    case 2:
-      fold_tiles_kernel<2><<<grid, 256, 0, stream>>>(sp, l.batch, l.scratch, l.part_start,
-                                                     l.part_upper_bound, l.candidates, l.fine);
-      break;
-    default:
-      fold_tiles_kernel<3><<<grid, 256, 0, stream>>>(sp, l.batch, l.scratch, l.part_start,
-                                                     l.part_upper_bound, l.candidates, l.fine);
-      break;
-  }
-  note_launch();
+  SpreadLaunchT<F32Traits> t{l.points,   l.strengths,        l.point_count, l.batch,
+                             l.perm,     l.offsets,          l.part_start,  l.part_upper_bound,
+                             l.max_bits, l.scratch,          l.candidates,  l.fine};
+  spread_execute_impl<F32Traits>(sp, t, stream, timer);
+}
+
+void spread_execute64(const SpreadParams& sp, const SpreadLaunch64& l, cudaStream_t stream,
+                      StageTimer* timer) {
+  SpreadLaunchT<F64Traits> t{l.points,   l.strengths,        l.point_count, l.batch,
+                             l.perm,     l.offsets,          l.part_start,  l.part_upper_bound,
+                             l.max_bits, l.scratch,          l.candidates,  l.fine};
+  spread_execute_impl<F64Traits>(sp, t, stream, timer);
 }
 
 }  // namespace b200nufft

@@ -46,6 +46,22 @@ struct SpreadLaunch {
   float2* fine;          // batch * fine_count
 };
 
+// The f64 plan's launch: double coordinates and complex128 values.
+struct SpreadLaunch64 {
+  const double* points;    // coordinates in bin (slot) order
+  const double2* strengths;
+  int64_t point_count;
+  int batch;
+  const uint32_t* perm;
+  const uint32_t* offsets;
+  const uint32_t* part_start;
+  int64_t part_upper_bound;
+  unsigned long long* max_bits;  // batch words
+  double2* scratch;
+  const int2* candidates;
+  double2* fine;
+};
+
 // Parts of every tile and their exclusive scan (tile_count + 1 words).
 void spread_count_parts(const SpreadParams& sp, const uint32_t* offsets, uint32_t* parts,
                         uint32_t* part_start, cudaStream_t stream, StageTimer* timer = nullptr);
@@ -53,5 +69,7 @@ void spread_count_parts(const SpreadParams& sp, const uint32_t* offsets, uint32_
 // Spreads `batch` strength vectors onto `fine`, overwriting every cell.
 void spread_execute(const SpreadParams& sp, const SpreadLaunch& launch, cudaStream_t stream,
                     StageTimer* timer = nullptr);
+void spread_execute64(const SpreadParams& sp, const SpreadLaunch64& launch, cudaStream_t stream,
+                      StageTimer* timer = nullptr);
 
 }  // namespace b200nufft
