@@ -139,7 +139,49 @@ SIGNATURES: dict[str, tuple] = {
     "b200nufft_last_error": (c_char_p, []),
     "b200nufft_version": (c_char_p, []),
     "b200nufft_launch_count": (c_uint64, []),
+    # wgpu_nufft.h
+    "wgpu_nufft_default_opts": (None, [P(WgpuOpts)]),
+    "wgpu_nufft_list_adapters": (c_int, [c_void_p, c_int32, P(c_int32)]),
+    "wgpu_nufft_last_error": (c_char_p, []),
+    "wgpu_nufft_version": (c_char_p, []),
+    "wgpu_nufft_gpu_name": (c_char_p, []),
+    "wgpu_nufft_shutdown": (None, []),
+    "b200nufft_resolve_adapter": (c_int, [P(c_char_p), P(c_char_p), c_int32, P(WgpuOpts), P(c_int32)]),
 }
+
+# The two host-array families differ only in their prefix; array arguments
+# are raw addresses (numpy .ctypes.data), so both share the signatures.
+_A = c_void_p
+_O = P(WgpuOpts)
+for _prefix in ("wgpu_nufft", "wgpu_nufftf"):
+    SIGNATURES.update({
+        f"{_prefix}_makeplan": (c_int, [c_int32, c_int32, P(c_int64), c_int32, c_int64, c_double, P(PLAN), _O]),
+        f"{_prefix}_setpts": (c_int, [PLAN, c_int64, _A, _A, _A, c_int64, _A, _A, _A]),
+        f"{_prefix}_setpts_nd": (c_int, [PLAN, c_int64, _A, c_int64, _A]),
+        f"{_prefix}_execute": (c_int, [PLAN, _A, _A]),
+        f"{_prefix}_destroy": (None, [PLAN]),
+        f"{_prefix}_plan_backend": (c_int, [PLAN]),
+        f"{_prefix}_plan_precision": (c_int, [PLAN]),
+        f"{_prefix}1d1": (c_int, [c_int64, _A, _A, c_int32, c_double, c_int64, _A, _O]),
+        f"{_prefix}1d2": (c_int, [c_int64, _A, _A, c_int32, c_double, c_int64, _A, _O]),
+        f"{_prefix}1d3": (c_int, [c_int64, _A, _A, c_int32, c_double, c_int64, _A, _A, _O]),
+        f"{_prefix}2d1": (c_int, [c_int64, _A, _A, _A, c_int32, c_double, c_int64, c_int64, _A, _O]),
+        f"{_prefix}2d2": (c_int, [c_int64, _A, _A, _A, c_int32, c_double, c_int64, c_int64, _A, _O]),
+        f"{_prefix}2d3": (c_int, [c_int64, _A, _A, _A, c_int32, c_double, c_int64, _A, _A, _A, _O]),
+        f"{_prefix}3d1": (c_int, [c_int64, _A, _A, _A, _A, c_int32, c_double, c_int64, c_int64, c_int64, _A, _O]),
+        f"{_prefix}3d2": (c_int, [c_int64, _A, _A, _A, _A, c_int32, c_double, c_int64, c_int64, c_int64, _A, _O]),
+        f"{_prefix}3d3": (c_int, [c_int64, _A, _A, _A, _A, c_int32, c_double, c_int64, _A, _A, _A, _A, _O]),
+    })
+
+
+class WgpuAdapter(ctypes.Structure):
+    _fields_ = [
+        ("name", ctypes.c_char * 256),
+        ("backend", ctypes.c_char * 16),
+        ("device_type", ctypes.c_char * 16),
+        ("pci_bus_id", ctypes.c_char * 32),
+        ("is_default", c_int32),
+    ]
 
 _lib: ctypes.CDLL | None = None
 
