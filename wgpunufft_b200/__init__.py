@@ -223,7 +223,7 @@ class NufftPlan:
 
     def __del__(self):
         handle = getattr(self, "_handle", None)
-        if handle:
+        if handle and _native is not None:  # module globals are gone at interpreter exit
             _native.library().b200nufft_plan_destroy(handle)
             self._handle = None
 
@@ -419,7 +419,7 @@ class NufftType3Plan:
 
     def __del__(self):
         handle = getattr(self, "_handle", None)
-        if handle:
+        if handle and _native is not None:  # module globals are gone at interpreter exit
             _native.library().b200nufft_type3_plan_destroy(handle)
             self._handle = None
 

@@ -321,6 +321,12 @@ void NufftPlan::configure_type2_bins() {
 
 void NufftPlan::configure_tiles() {
   SpreadParams& sp = spread_;
+  int64_t kept_candidate_base[3];
+  int32_t kept_candidate_count[3];
+  for (int a = 0; a < 3; ++a) {
+    kept_candidate_base[a] = sp.candidate_base[a];
+    kept_candidate_count[a] = sp.candidate_count[a];
+  }
   std::memset(&sp, 0, sizeof(sp));
   sp.grid = grid_;
   const int w = kernel_.width;
@@ -364,11 +370,25 @@ void NufftPlan::configure_tiles() {
   if (rows > kMaxTileRows) {
     throw NufftFailure{B200NUFFT_INTERNAL, "spreading tile spans too many bin rows"};
   }
-  sp.part_cap = kPartCap;
+  // Parts of at most kPartCap records, fewer for small point sets so that
+  // about four CTAs per SM have work.
+  const int64_t spread_ctas = 4 * 148;
+  int64_t cap = (std::max<int64_t>(point_count_, 1) + spread_ctas - 1) / spread_ctas;
+  cap = std::min<int64_t>(kPartCap, std::max<int64_t>(256, (cap + 255) / 256 * 256));
+  sp.part_cap = static_cast<int32_t>(cap);
   sp.headroom = ilog2(static_cast<int64_t>(kPartCap) + 1);
   // Candidate (tile, local) pairs of every coordinate of every axis: tile t
-  // covers cells (t * tile + l) mod n for l < pad.
-  host_candidates_.clear();
+  // covers cells (t * tile + l) mod n for l < pad. They depend on the grid
+  // and tile shape only, so later point sets reuse them.
+  if (!host_candidates_.empty()) {
+    for (int a = 0; a < 3; ++a) {
+      sp.candidate_base[a] = kept_candidate_base[a];
+      sp.candidate_count[a] = kept_candidate_count[a];
+    }
+    part_upper_bound_ = sp.tile_count + (std::max<int64_t>(point_count_, 0) * tiles_per_bin +
+                                         sp.part_cap - 1) / sp.part_cap + 1;
+    return;
+  }
   for (int a = 0; a < dim_; ++a) {
     const int64_t n = fine_[a];
     std::vector<std::vector<int2>> lists(static_cast<size_t>(n));
@@ -395,7 +415,7 @@ void NufftPlan::configure_tiles() {
   (void)tiles_per_bin;
   spread_.grid = grid_;
   part_upper_bound_ = sp.tile_count + (std::max<int64_t>(point_count_, 0) * tiles_per_bin +
-                                       kPartCap - 1) / kPartCap + 1;
+                                       sp.part_cap - 1) / sp.part_cap + 1;
 }
 
 int NufftPlan::choose_geometry(int64_t point_count) const {

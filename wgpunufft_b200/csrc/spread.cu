@@ -75,7 +75,7 @@ struct F32Traits {
       w[j] = es_weight(d, g.beta, width_f);
     }
   }
-  static __device__ __forceinline__ float scale(float s, int S) { return ldexpf(s, S); }
+  static __device__ __forceinline__ float power_of_two(int e) { return ldexpf(1.0f, e); }
   // Adds a contribution (|v| < 2^31 after rounding) as two exact 32-bit sums:
   // its low 16 bits, unsigned, and its arithmetic high part. Both stay exact
   // for up to 2^16 contributions per cell; the cell's value is hi 2^16 + lo.
@@ -120,7 +120,7 @@ struct F64Traits {
     wrapped = wrap_start(start, g.axis[a].length);
     for (int j = 0; j < W; ++j) w[j] = horner_weight(offset, j, W, g.horner, g.horner_rows);
   }
-  static __device__ __forceinline__ double scale(double s, int S) { return ldexp(s, S); }
+  static __device__ __forceinline__ double power_of_two(int e) { return ldexp(1.0, e); }
   static __device__ __forceinline__ void add(Word* acc, int padded, int part, int c, double value) {
     atomicAdd(&acc[part * padded + c], static_cast<unsigned long long>(__double2ll_rn(value)));
   }
@@ -237,10 +237,78 @@ __global__ void __launch_bounds__(1024) part_scan_kernel(const uint32_t* __restr
   if (threadIdx.x == 0) part_start[tile_count] = carry_shared;
 }
 
+// Records per register run of a thread: one for 3D and for windows whose
+// w^2 complex accumulators would not fit in registers.
+constexpr int kRunBits = 3;
+template <int D, int W, typename T>
+__host__ __device__ constexpr int spread_run() {
+  return (D == 1 || (D == 2 && 2 * W * W * sizeof(typename T::Real) < 400)) ? (1 << kRunBits) : 1;
+}
+
+// Record r of the tile's bin rows: its support start relative to the tile,
+// its window weights and its strength. False when the point lies outside the
+// fold reach (weighed zero by the reference) or starts in another tile (a bin
+// wider than the tile).
+template <int D, int W, typename T>
+__device__ __forceinline__ bool tile_record(const SpreadParams& sp, const typename T::Real* points,
+                                            const typename T::Complex* sv, const uint32_t* perm,
+                                            const uint32_t* row_begin, const uint32_t* row_prefix,
+                                            int rows, const int* origin, uint32_t r, int& row,
+                                            int* local_start, typename T::Real (*w)[W],
+                                            typename T::Complex& s) {
+  using Real = typename T::Real;
+  // Advance to the row holding record r (rows are visited in order).
+  if (r >= row_prefix[row + 1] || r < row_prefix[row]) {
+    int low = 0, high = rows - 1;
+    while (low < high) {
+      const int mid = (low + high + 1) >> 1;
+      if (row_prefix[mid] <= r) low = mid; else high = mid - 1;
+    }
+    row = low;
+  }
+  const uint32_t slot = row_begin[row] + (r - row_prefix[row]);
+  Real p[D];
+#pragma unroll
+  for (int a = 0; a < D; ++a) p[a] = points[static_cast<int64_t>(slot) * D + a];
+  bool reach = true;
+#pragma unroll
+  for (int a = 0; a < D; ++a) reach = reach && T::in_reach(p[a]);
+  if (!reach) return false;
+  bool inside = true;
+#pragma unroll
+  for (int a = 0; a < D; ++a) {
+    int32_t wrapped;
+    T::window(p[a], sp.grid, a, wrapped, w[a], W);
+    local_start[a] = wrapped - origin[a];
+    inside = inside && local_start[a] >= 0 && local_start[a] < sp.tile[a];
+  }
+  if (!inside) return false;
+  s = sv[perm[slot]];
+  return true;
+}
+
+// Adds a run's register sums to the fixed-point tile and clears them.
+template <int D, int W, typename T>
+__device__ __forceinline__ void flush_run(typename T::Word* acc, int padded, int pad0, int x, int y,
+                                          typename T::Real (*ar)[W], typename T::Real (*ai)[W],
+                                          typename T::Real scale_lo, typename T::Real scale_hi) {
+  constexpr int R = D == 2 ? W : 1;
+#pragma unroll
+  for (int j = 0; j < R; ++j) {
+    const int base = (y + j) * pad0 + x;
+#pragma unroll
+    for (int i = 0; i < W; ++i) {
+      T::add(acc, padded, 0, base + i, (ar[j][i] * scale_lo) * scale_hi);
+      T::add(acc, padded, 1, base + i, (ai[j][i] * scale_lo) * scale_hi);
+      ar[j][i] = ai[j][i] = typename T::Real(0);
+    }
+  }
+}
+
 // One CTA per (part, vector): spreads the part's records into a padded tile
 // of fixed-point sums and writes the tile out in floating point.
 template <int D, int W, typename T>
-__global__ void __launch_bounds__(kSpreadThreads) spread_tiles_kernel(
+__global__ void __launch_bounds__(kSpreadThreads, (spread_run<D, W, T>() > 1 || sizeof(typename T::Real) == 8 ? 2 : 3)) spread_tiles_kernel(
     SpreadParams sp, const typename T::Real* __restrict__ points,
     const typename T::Complex* __restrict__ strengths, int64_t point_count, int batch,
     const uint32_t* __restrict__ perm, const uint32_t* __restrict__ offsets,
@@ -341,78 +409,109 @@ __global__ void __launch_bounds__(kSpreadThreads) spread_tiles_kernel(
   const uint32_t tile_total = row_prefix[rows];
   const uint32_t record_begin = part_in_tile * static_cast<uint32_t>(sp.part_cap);
   const uint32_t record_end = min(tile_total, record_begin + static_cast<uint32_t>(sp.part_cap));
-  const int S = T::exponent(max_bits[b]);
+  // Runs of records with one support start add up in registers first (a
+  // fixed order within the run) and reach the fixed-point tile once per run,
+  // which leaves that much headroom in the scale.
+  constexpr int kRun = spread_run<D, W, T>();
+  const int S = T::exponent(max_bits[b]) - (kRun > 1 ? kRunBits : 0);
+  const Real scale_lo = T::power_of_two(S / 2);
+  const Real scale_hi = T::power_of_two(S - S / 2);
   const typename T::Complex* sv = strengths + static_cast<int64_t>(b) * point_count;
 
   int row = 0;
-  for (uint32_t r = record_begin + tid; r < record_end; r += kSpreadThreads) {
-    // Advance to the row holding record r (rows are visited in order).
-    if (r >= row_prefix[row + 1] || r < row_prefix[row]) {
-      int low = 0, high = rows - 1;
-      while (low < high) {
-        const int mid = (low + high + 1) >> 1;
-        if (row_prefix[mid] <= r) low = mid; else high = mid - 1;
+  if constexpr (kRun == 1) {
+    for (uint32_t r = record_begin + tid; r < record_end; r += kSpreadThreads) {
+      int local_start[D];
+      Real w[D][W];
+      typename T::Complex s;
+      if (!tile_record<D, W, T>(sp, points, sv, perm, row_begin, row_prefix, rows, origin, r, row,
+                                local_start, w, s)) {
+        continue;
       }
-      row = low;
-    }
-    const uint32_t slot = row_begin[row] + (r - row_prefix[row]);
-    Real p[D];
-#pragma unroll
-    for (int a = 0; a < D; ++a) p[a] = points[static_cast<int64_t>(slot) * D + a];
-    bool reach = true;
-#pragma unroll
-    for (int a = 0; a < D; ++a) reach = reach && T::in_reach(p[a]);
-    if (!reach) continue;  // weighed zero by the reference
-    int local_start[D];
-    Real w[D][W];
-    bool inside = true;
-#pragma unroll
-    for (int a = 0; a < D; ++a) {
-      int32_t wrapped;
-      T::window(p[a], sp.grid, a, wrapped, w[a], W);
-      local_start[a] = wrapped - origin[a];
-      inside = inside && local_start[a] >= 0 && local_start[a] < sp.tile[a];
-    }
-    if (!inside) continue;  // a bin wider than the tile: another tile owns it
-    const typename T::Complex s = sv[perm[slot]];
-    const Real sr = T::scale(s.x, S);
-    const Real si = T::scale(s.y, S);
-    if (D == 1) {
-#pragma unroll
-      for (int i = 0; i < W; ++i) {
-        const int c = local_start[0] + i;
-        T::add(acc, padded, 0, c, sr * w[0][i]);
-        T::add(acc, padded, 1, c, si * w[0][i]);
-      }
-    } else if (D == 2) {
-#pragma unroll
-      for (int j = 0; j < W; ++j) {
-        const Real wr = sr * w[1][j];
-        const Real wi = si * w[1][j];
-        const int base = (local_start[1] + j) * sp.pad[0] + local_start[0];
+      const Real sr = (s.x * scale_lo) * scale_hi;
+      const Real si = (s.y * scale_lo) * scale_hi;
+      if (D == 1) {
 #pragma unroll
         for (int i = 0; i < W; ++i) {
-          T::add(acc, padded, 0, base + i, wr * w[0][i]);
-          T::add(acc, padded, 1, base + i, wi * w[0][i]);
+          const int c = local_start[0] + i;
+          T::add(acc, padded, 0, c, sr * w[0][i]);
+          T::add(acc, padded, 1, c, si * w[0][i]);
         }
-      }
-    } else {
-#pragma unroll 1
-      for (int k = 0; k < W; ++k) {
+      } else if (D == 2) {
 #pragma unroll
         for (int j = 0; j < W; ++j) {
-          const Real wyz = w[1][j] * w[2][k];
-          const Real wr = sr * wyz;
-          const Real wi = si * wyz;
-          const int base =
-              ((local_start[2] + k) * sp.pad[1] + local_start[1] + j) * sp.pad[0] + local_start[0];
+          const Real wr = sr * w[1][j];
+          const Real wi = si * w[1][j];
+          const int base = (local_start[1] + j) * sp.pad[0] + local_start[0];
 #pragma unroll
           for (int i = 0; i < W; ++i) {
             T::add(acc, padded, 0, base + i, wr * w[0][i]);
             T::add(acc, padded, 1, base + i, wi * w[0][i]);
           }
         }
+      } else {
+#pragma unroll 1
+        for (int k = 0; k < W; ++k) {
+#pragma unroll
+          for (int j = 0; j < W; ++j) {
+            const Real wyz = w[1][j] * w[2][k];
+            const Real wr = sr * wyz;
+            const Real wi = si * wyz;
+            const int base =
+                ((local_start[2] + k) * sp.pad[1] + local_start[1] + j) * sp.pad[0] + local_start[0];
+#pragma unroll
+            for (int i = 0; i < W; ++i) {
+              T::add(acc, padded, 0, base + i, wr * w[0][i]);
+              T::add(acc, padded, 1, base + i, wi * w[0][i]);
+            }
+          }
+        }
       }
+    }
+  } else {
+    // Each thread takes runs of up to kRun consecutive records (consecutive
+    // slots of one bin row share starts when bins are one cell wide), sized so
+    // that every pass gives every thread the same number of records.
+    constexpr int R = D == 2 ? W : 1;
+    const uint32_t count = record_end - record_begin;
+    const uint32_t per_thread = (count + kSpreadThreads - 1) / kSpreadThreads;
+    const uint32_t passes = (per_thread + kRun - 1) / kRun;
+    const uint32_t run = passes ? (count + kSpreadThreads * passes - 1) / (kSpreadThreads * passes) : 1u;
+    for (uint32_t first = record_begin + tid * run; first < record_end; first += kSpreadThreads * run) {
+      const uint32_t stop = min(first + run, record_end);
+      Real ar[R][W], ai[R][W];
+#pragma unroll
+      for (int j = 0; j < R; ++j) {
+#pragma unroll
+        for (int i = 0; i < W; ++i) ar[j][i] = ai[j][i] = Real(0);
+      }
+      int run0 = -1, run1 = 0;
+      for (uint32_t r = first; r < stop; ++r) {
+        int local_start[D];
+        Real w[D][W];
+        typename T::Complex s;
+        if (!tile_record<D, W, T>(sp, points, sv, perm, row_begin, row_prefix, rows, origin, r, row,
+                                  local_start, w, s)) {
+          continue;
+        }
+        const int l1 = D == 2 ? local_start[D - 1] : 0;
+        if (local_start[0] != run0 || l1 != run1) {
+          if (run0 >= 0) flush_run<D, W, T>(acc, padded, sp.pad[0], run0, run1, ar, ai, scale_lo, scale_hi);
+          run0 = local_start[0];
+          run1 = l1;
+        }
+#pragma unroll
+        for (int j = 0; j < R; ++j) {
+          const Real wr = D == 2 ? s.x * w[D - 1][j] : s.x;
+          const Real wi = D == 2 ? s.y * w[D - 1][j] : s.y;
+#pragma unroll
+          for (int i = 0; i < W; ++i) {
+            ar[j][i] += wr * w[0][i];
+            ai[j][i] += wi * w[0][i];
+          }
+        }
+      }
+      if (run0 >= 0) flush_run<D, W, T>(acc, padded, sp.pad[0], run0, run1, ar, ai, scale_lo, scale_hi);
     }
   }
   __syncthreads();
