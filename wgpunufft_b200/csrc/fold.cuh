@@ -181,4 +181,30 @@ __device__ __forceinline__ int32_t wrap_start(int32_t start, int32_t n) {
   return s > n - 1 ? n - 1 : s;
 }
 
+// The F32 window of the reference's shaders (src/gpu_nd_wgsl.rs:383-395):
+// exp(beta (sqrt(1 - (2 d / w)^2) - 1)) inside the support, zero outside.
+__device__ __forceinline__ float es_weight(float distance, float beta, float width_f) {
+  const float scaled = (2.0f * fabsf(distance)) / width_f;
+  const float squared = scaled * scaled;
+  if (squared >= 1.0f) return 0.0f;
+  return expf(beta * (sqrtf(fmaxf(0.0f, 1.0f - squared)) - 1.0f));
+}
+
+// Wrapped support start and the W window weights of an f32 coordinate on one
+// axis (the F32 plans' per-axis window, src/gpu_nd_wgsl.rs:263-298,383-395).
+template <int W>
+__device__ __forceinline__ void f32_window(float x, const FoldAxis& axis, float half_width, float beta,
+                                           int32_t& wrapped, float* w) {
+  int32_t start;
+  Df64 off;
+  support_of(x, axis, half_width, start, off);
+  wrapped = wrap_start(start, axis.length);
+  const float width_f = static_cast<float>(W);
+#pragma unroll
+  for (int j = 0; j < W; ++j) {
+    const float d = __fadd_rn(__fadd_rn(static_cast<float>(j), off.hi), off.lo);
+    w[j] = es_weight(d, beta, width_f);
+  }
+}
+
 }  // namespace b200nufft

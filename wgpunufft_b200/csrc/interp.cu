@@ -20,13 +20,6 @@ namespace b200nufft {
 
 namespace {
 
-__device__ __forceinline__ float es_weight(float distance, float beta, float width_f) {
-  const float scaled = (2.0f * fabsf(distance)) / width_f;
-  const float squared = scaled * scaled;
-  if (squared >= 1.0f) return 0.0f;
-  return expf(beta * (sqrtf(fmaxf(0.0f, 1.0f - squared)) - 1.0f));
-}
-
 struct F32Window {
   using Real = float;
   using Complex = float2;

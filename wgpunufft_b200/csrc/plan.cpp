@@ -114,6 +114,8 @@ NufftPlan::NufftPlan(const b200nufft_config& c, bool with_device) : has_device_(
     throw NufftFailure{B200NUFFT_INVALID_ARGUMENT, "precision must be F64 (1), DF64 (2) or F32 (3)"};
   }
   kernel_ = EsKernel::for_tolerance(eps_, sigma_);
+  tc_enabled_ = type_ == 1 && dim_ == 2 && precision_ == B200NUFFT_PRECISION_F32 &&
+                kernel_.width <= kTcMaxWidth && batch_ >= kTcMinBatch;
   fine_count_ = 1;
   for (int a = 0; a < dim_; ++a) {
     const uint64_t n = select_fine_grid_size(static_cast<uint64_t>(modes_[a]), sigma_, kernel_.width);
@@ -335,12 +337,19 @@ void NufftPlan::configure_tiles() {
   if (dim_ == 2) tile[0] = tile[1] = 32;
   if (dim_ == 3) tile[0] = tile[1] = tile[2] = 16;
   for (int a = 0; a < dim_; ++a) tile[a] = std::min(tile[a], pow2_ceil(fine_[a]));
+  // The tensor-core spreader needs one-cell bin rows, column bins of at most
+  // 8 cells, and its own tile shape (16 cells x 22 - w rows).
+  tc_active_ = tc_enabled_ && grid_.axis[1].shift == 0 && grid_.axis[0].shift <= 3;
+  if (tc_active_) {
+    tile[0] = kTcTileX;
+    tile[1] = tc_tile_rows(w);
+  }
   auto padded_bytes = [&]() {
     int64_t cells = 1;
     for (int a = 0; a < dim_; ++a) cells *= tile[a] + w - 1;
     return cells * 16;
   };
-  while (padded_bytes() > kTileBytesTarget) {
+  while (!tc_active_ && padded_bytes() > kTileBytesTarget) {
     int largest = dim_ - 1;
     for (int a = dim_ - 1; a >= 0; --a) {
       if (tile[a] > tile[largest]) largest = a;
@@ -380,7 +389,8 @@ void NufftPlan::configure_tiles() {
   // Candidate (tile, local) pairs of every coordinate of every axis: tile t
   // covers cells (t * tile + l) mod n for l < pad. They depend on the grid
   // and tile shape only, so later point sets reuse them.
-  if (!host_candidates_.empty()) {
+  if (!host_candidates_.empty() && candidate_tile_[0] == tile[0] && candidate_tile_[1] == tile[1] &&
+      candidate_tile_[2] == tile[2]) {
     for (int a = 0; a < 3; ++a) {
       sp.candidate_base[a] = kept_candidate_base[a];
       sp.candidate_count[a] = kept_candidate_count[a];
@@ -389,6 +399,8 @@ void NufftPlan::configure_tiles() {
                                          sp.part_cap - 1) / sp.part_cap + 1;
     return;
   }
+  host_candidates_.clear();
+  for (int a = 0; a < 3; ++a) candidate_tile_[a] = tile[a];
   for (int a = 0; a < dim_; ++a) {
     const int64_t n = fine_[a];
     std::vector<std::vector<int2>> lists(static_cast<size_t>(n));
@@ -484,6 +496,28 @@ void NufftPlan::set_points(int64_t count, const void* points, cudaStream_t strea
                         "tile part offsets");
     spread_count_parts(spread_, offsets, static_cast<uint32_t*>(parts_.get()),
                        static_cast<uint32_t*>(part_start_.get()), stream, &timer_);
+    if (tc_active_) {
+      const int64_t tiles = spread_.tile_count;
+      const int64_t chunk_bound = tc_chunk_bound(spread_, count);
+      TcPrepare p;
+      p.sorted_points = static_cast<const float*>(sorted_points_.get());
+      p.count = count;
+      p.perm = perm_;
+      p.offsets = offsets;
+      p.weights = static_cast<TcWeights*>(
+          tc_weights_.reserve(static_cast<size_t>(std::max<int64_t>(count, 1)) * sizeof(TcWeights), "point windows"));
+      p.inverse = static_cast<uint32_t*>(
+          tc_inverse_.reserve(static_cast<size_t>(std::max<int64_t>(count, 1)) * sizeof(uint32_t), "point slots"));
+      p.tile_chunks = static_cast<uint32_t*>(tc_tile_chunks_.reserve(tiles * sizeof(uint32_t), "tile chunks"));
+      p.tile_chunk_start = static_cast<uint32_t*>(
+          tc_tile_chunk_start_.reserve((tiles + 1) * sizeof(uint32_t), "tile chunk offsets"));
+      p.chunks = static_cast<TcChunk*>(tc_chunks_.reserve(chunk_bound * sizeof(TcChunk), "chunk table"));
+      p.parts = static_cast<uint32_t*>(tc_parts_.reserve(tiles * sizeof(uint32_t), "tensor-core parts"));
+      p.part_start = static_cast<uint32_t*>(
+          tc_part_start_.reserve((tiles + 1) * sizeof(uint32_t), "tensor-core part offsets"));
+      tc_prepare(spread_, p, stream, &timer_);
+      tc_part_upper_bound_ = tiles + chunk_bound / kTcChunksPerPart + 1;
+    }
   }
   check_cuda(cudaGetLastError(), "set points launch");
 }
@@ -559,6 +593,33 @@ void NufftPlan::execute_f32(int batch, const void* input, void* output, uint64_t
   if (type_ == 1) {
     if (point_count_ == 0) {
       check_cuda(cudaMemsetAsync(output, 0, out_bytes, stream), "zero type-1 output");
+      return;
+    }
+    if (tc_active_ && batch >= kTcMinBatch) {
+      const int64_t groups = (batch + kTcVectors - 1) / kTcVectors;
+      TcLaunch t;
+      t.strengths = static_cast<const float2*>(input);
+      t.count = point_count_;
+      t.batch = batch;
+      t.inverse = static_cast<const uint32_t*>(tc_inverse_.get());
+      t.weights = static_cast<const TcWeights*>(tc_weights_.get());
+      t.chunks = static_cast<const TcChunk*>(tc_chunks_.get());
+      t.tile_chunk_start = static_cast<const uint32_t*>(tc_tile_chunk_start_.get());
+      t.part_start = static_cast<const uint32_t*>(tc_part_start_.get());
+      t.part_upper_bound = tc_part_upper_bound_;
+      t.packed = static_cast<float*>(tc_packed_.reserve(
+          static_cast<size_t>(groups) * point_count_ * kTcRows * sizeof(float), "packed strengths"));
+      t.scratch = static_cast<float2*>(scratch_.reserve(static_cast<size_t>(tc_part_upper_bound_) * groups *
+                                                            kTcVectors * spread_.padded_cells * sizeof(float2),
+                                                        "spreading tiles"));
+      t.candidates = static_cast<const int2*>(candidates_.get());
+      t.fine = fine;
+      t.error_flag = static_cast<uint32_t*>(counters_.get()) + 7;
+      tc_spread_execute(spread_, t, stream, &timer_);
+      run_fft(fine, batch, direction, stream);
+      StageScope scope(&timer_, kStageDeconvolution, stream);
+      deconvolve_f32(modes_params_, batch, fine, static_cast<const float*>(amplitudes_.get()),
+                     static_cast<float2*>(output), stream);
       return;
     }
     const size_t scratch_bytes = static_cast<size_t>(part_upper_bound_) * batch *

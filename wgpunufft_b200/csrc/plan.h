@@ -13,6 +13,7 @@
 #include "layout.h"
 #include "modes.h"
 #include "spread.h"
+#include "tc_spread.h"
 
 namespace b200nufft {
 
@@ -109,6 +110,15 @@ class NufftPlan {
   DeviceBuffer parts_, part_start_, max_bits_, scratch_, candidates_;
   int64_t part_upper_bound_ = 0;
   std::vector<int2> host_candidates_;
+  int64_t candidate_tile_[3] = {0, 0, 0};
+
+  // Tensor-core spreading (2D f32 type-1 plans of batch >= kTcMinBatch):
+  // enabled by the configuration, active when the chosen bins allow it.
+  bool tc_enabled_ = false;
+  bool tc_active_ = false;
+  DeviceBuffer tc_weights_, tc_inverse_, tc_tile_chunks_, tc_tile_chunk_start_, tc_chunks_;
+  DeviceBuffer tc_parts_, tc_part_start_, tc_packed_;
+  int64_t tc_part_upper_bound_ = 0;
 };
 
 }  // namespace b200nufft

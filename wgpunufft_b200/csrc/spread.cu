@@ -31,14 +31,6 @@ namespace {
 
 constexpr int kSpreadThreads = 256;
 
-__device__ __forceinline__ float es_weight(float distance, float beta, float width_f) {
-  // The F32 window of the reference's spreading shader (src/gpu_nd_wgsl.rs:383-395).
-  const float scaled = (2.0f * fabsf(distance)) / width_f;
-  const float squared = scaled * scaled;
-  if (squared >= 1.0f) return 0.0f;
-  return expf(beta * (sqrtf(fmaxf(0.0f, 1.0f - squared)) - 1.0f));
-}
-
 // ---------------------------------------------------------------------------
 // Precision traits: coordinates, window, fixed-point accumulator.
 
@@ -526,14 +518,16 @@ __global__ void __launch_bounds__(kSpreadThreads, (spread_run<D, W, T>() > 1 || 
 
 // Every fine-grid cell as the sum, in a fixed order, of the padded tiles and
 // parts that cover it.
-template <int D, typename Complex>
+template <int D, int BB, typename Complex>
 __global__ void fold_tiles_kernel(SpreadParams sp, int batch, const Complex* __restrict__ scratch,
                                   const uint32_t* __restrict__ part_start, int64_t part_limit,
                                   const int2* __restrict__ candidates,
                                   Complex* __restrict__ fine) {
+  // Each thread sums one cell of BB consecutive vectors, so the candidate
+  // lookups are shared and the vectors' loads are independent.
   const int64_t cell = static_cast<int64_t>(blockIdx.x) * blockDim.x + threadIdx.x;
   if (cell >= sp.grid.fine_count) return;
-  const int b = blockIdx.y;
+  const int b0 = blockIdx.y * BB;
   int coord[3] = {0, 0, 0};
   {
     int64_t rest = cell;
@@ -548,9 +542,13 @@ __global__ void fold_tiles_kernel(SpreadParams sp, int batch, const Complex* __r
   const int2* c2 = D > 2 ? candidates + sp.candidate_base[2] + coord[2] * sp.candidate_count[2] : nullptr;
   const int k2n = D > 2 ? sp.candidate_count[2] : 1;
   const int k1n = D > 1 ? sp.candidate_count[1] : 1;
-  Complex sum;
-  sum.x = 0;
-  sum.y = 0;
+  const int active = min(BB, batch - b0);
+  Complex sum[BB];
+#pragma unroll
+  for (int i = 0; i < BB; ++i) {
+    sum[i].x = 0;
+    sum[i].y = 0;
+  }
   for (int k2 = 0; k2 < k2n; ++k2) {
     int t2 = 0, l2 = 0;
     if (D > 2) {
@@ -576,14 +574,56 @@ __global__ void fold_tiles_kernel(SpreadParams sp, int batch, const Complex* __r
         const uint32_t first = part_start[tile];
         const uint32_t last = min(part_start[tile + 1], static_cast<uint32_t>(part_limit));
         for (uint32_t p = first; p < last; ++p) {
-          const Complex v = scratch[(static_cast<int64_t>(p) * batch + b) * sp.padded_cells + local];
-          sum.x += v.x;
-          sum.y += v.y;
+          const Complex* v = scratch + (static_cast<int64_t>(p) * batch + b0) * sp.padded_cells + local;
+#pragma unroll
+          for (int i = 0; i < BB; ++i) {
+            if (i < active) {
+              const Complex x = v[static_cast<int64_t>(i) * sp.padded_cells];
+              sum[i].x += x.x;
+              sum[i].y += x.y;
+            }
+          }
         }
       }
     }
   }
-  fine[static_cast<int64_t>(b) * sp.grid.fine_count + cell] = sum;
+#pragma unroll
+  for (int i = 0; i < BB; ++i) {
+    if (i < active) fine[static_cast<int64_t>(b0 + i) * sp.grid.fine_count + cell] = sum[i];
+  }
+}
+
+template <int BB, typename Complex>
+void launch_fold(const SpreadParams& sp, int batch, const Complex* scratch, const uint32_t* part_start,
+                 int64_t part_limit, const int2* candidates, Complex* fine, cudaStream_t stream) {
+  const dim3 grid(static_cast<unsigned>((sp.grid.fine_count + 255) / 256),
+                  static_cast<unsigned>((batch + BB - 1) / BB));
+  switch (sp.grid.dimensions) {
+    case 1:
+      fold_tiles_kernel<1, BB, Complex><<<grid, 256, 0, stream>>>(sp, batch, scratch, part_start, part_limit,
+                                                                  candidates, fine);
+      break;
+    case 2:
+      fold_tiles_kernel<2, BB, Complex><<<grid, 256, 0, stream>>>(sp, batch, scratch, part_start, part_limit,
+                                                                  candidates, fine);
+      break;
+    default:
+      fold_tiles_kernel<3, BB, Complex><<<grid, 256, 0, stream>>>(sp, batch, scratch, part_start, part_limit,
+                                                                  candidates, fine);
+      break;
+  }
+  note_launch();
+}
+
+// Vectors per fold thread: one for a single vector, eight for batches.
+template <typename Complex>
+void fold_any(const SpreadParams& sp, int batch, const Complex* scratch, const uint32_t* part_start,
+              int64_t part_limit, const int2* candidates, Complex* fine, cudaStream_t stream) {
+  if (batch >= 8) {
+    launch_fold<8>(sp, batch, scratch, part_start, part_limit, candidates, fine, stream);
+  } else {
+    launch_fold<1>(sp, batch, scratch, part_start, part_limit, candidates, fine, stream);
+  }
 }
 
 template <int D, int W, typename T>
@@ -644,24 +684,7 @@ void spread_execute_impl(const SpreadParams& sp, const SpreadLaunchT<T>& l, cuda
     }
   }
   StageScope scope(timer, kStageFold, stream);
-  const dim3 grid(static_cast<unsigned>((sp.grid.fine_count + 255) / 256),
-                  static_cast<unsigned>(l.batch));
-  using Complex = typename T::Complex;
-  switch (sp.grid.dimensions) {
-    case 1:
-      fold_tiles_kernel<1, Complex><<<grid, 256, 0, stream>>>(sp, l.batch, l.scratch, l.part_start,
-                                                              l.part_upper_bound, l.candidates, l.fine);
-      break;
-    case 2:
-      fold_tiles_kernel<2, Complex><<<grid, 256, 0, stream>>>(sp, l.batch, l.scratch, l.part_start,
-                                                              l.part_upper_bound, l.candidates, l.fine);
-      break;
-    default:
-      fold_tiles_kernel<3, Complex><<<grid, 256, 0, stream>>>(sp, l.batch, l.scratch, l.part_start,
-                                                              l.part_upper_bound, l.candidates, l.fine);
-      break;
-  }
-  note_launch();
+  fold_any(sp, l.batch, l.scratch, l.part_start, l.part_upper_bound, l.candidates, l.fine, stream);
 }
 
 }  // namespace
@@ -677,6 +700,18 @@ void spread_count_parts(const SpreadParams& sp, const uint32_t* offsets, uint32_
   }
   part_scan_kernel<<<1, 1024, 0, stream>>>(parts, sp.tile_count, part_start);
   note_launch(2);
+}
+
+void exclusive_scan_u32(const uint32_t* in, int64_t n, uint32_t* out, cudaStream_t stream) {
+  part_scan_kernel<<<1, 1024, 0, stream>>>(in, n, out);
+  note_launch();
+}
+
+void spread_fold(const SpreadParams& sp, int batch, const float2* scratch, const uint32_t* part_start,
+                 int64_t part_limit, const int2* candidates, float2* fine, cudaStream_t stream,
+                 StageTimer* timer) {
+  StageScope scope(timer, kStageFold, stream);
+  fold_any(sp, batch, scratch, part_start, part_limit, candidates, fine, stream);
 }
 
 void spread_execute(const SpreadParams& sp, const SpreadLaunch& l, cudaStream_t stream,
