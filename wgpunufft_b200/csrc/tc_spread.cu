@@ -32,11 +32,13 @@ namespace b200nufft {
 
 namespace {
 
-constexpr int kTcThreads = 256;
-constexpr int kTcCopyStages = 8;     // chunks whose copies are in flight or unread
-constexpr int kTcOperandStages = 4;  // chunks whose MMAs may still read their operands
+constexpr int kTcTeams = 4;          // converter teams, each converting every fourth chunk
+constexpr int kTcTeamThreads = 64;
+constexpr int kTcThreads = 64 + kTcTeams * kTcTeamThreads;  // producer warp, MMA warp, converters
+constexpr int kTcCopyStages = 20;    // chunks whose copies are in flight or unread
+constexpr int kTcOperandStages = 6;  // chunks whose MMAs may still read their operands
 constexpr uint32_t kSpinLimit = 1u << 22;
-constexpr size_t kTcSharedBytes = 116 * 1024;  // one CTA per SM: it holds all 512 columns
+constexpr size_t kTcSharedBytes = 200 * 1024;  // one CTA per SM: it holds all 512 columns
 
 __device__ __forceinline__ uint32_t smem_u32(const void* p) {
   return static_cast<uint32_t>(__cvta_generic_to_shared(p));
@@ -87,13 +89,20 @@ __device__ __forceinline__ bool mbar_try(uint32_t bar, uint32_t parity) {
       : "memory");
   return done != 0;
 }
-// Waits for the phase of the given parity to complete; false when it gave up.
-__device__ __noinline__ bool mbar_wait(uint32_t bar, uint32_t parity) {
+// Waits for the phase of the given parity to complete; false when it gave up
+// or when another role raised the CTA's abort flag (which a failed wait
+// raises).
+__device__ __noinline__ bool mbar_wait(uint32_t bar, uint32_t parity, volatile int* abort_flag) {
   for (uint32_t i = 0; i < kSpinLimit; ++i) {
     if (mbar_try(bar, parity)) return true;
-    if (i >= 32) __nanosleep(64);
+    if (abort_flag != nullptr && *abort_flag) return false;
+    if (i >= 32) __nanosleep(32);
   }
+  if (abort_flag != nullptr) *abort_flag = 1;
   return false;
+}
+__device__ __forceinline__ void mbar_arrive(uint32_t bar) {
+  asm volatile("mbarrier.arrive.shared::cta.b64 _, [%0];" ::"r"(bar) : "memory");
 }
 __device__ __forceinline__ void mbar_expect(uint32_t bar, uint32_t bytes) {
   asm volatile("mbarrier.arrive.expect_tx.shared::cta.b64 _, [%0], %1;" ::"r"(bar), "r"(bytes) : "memory");
@@ -133,16 +142,23 @@ __global__ void tc_weights_kernel(GridParams g, const float* __restrict__ sorted
   r.sx = r.sy = 0;
   r.unused[0] = r.unused[1] = 0;
 #pragma unroll
-  for (int j = 0; j < kTcMaxWidth; ++j) r.wx[j] = r.wy[j] = 0.0f;
+  for (int j = 0; j < kTcMaxWidth; ++j) r.wy[j] = 0.0f;
+#pragma unroll
+  for (int c = 0; c < 2 * kTcTileX; ++c) r.wxs[c] = 0.0f;
   const float x = sorted[2 * s], y = sorted[2 * s + 1];
   if (in_fold_reach(x) && in_fold_reach(y)) {
     float wx[W], wy[W];
     f32_window<W>(x, g.axis[0], g.half_width, g.beta, r.sx, wx);
     f32_window<W>(y, g.axis[1], g.half_width, g.beta, r.sy, wy);
+    // Tiles start at multiples of 8 cells: the column of the first weight.
+    const int dx = r.sx & (kTcTileX - 1);
 #pragma unroll
     for (int j = 0; j < W; ++j) {
-      r.wx[j] = wx[j];
       r.wy[j] = wy[j];
+#pragma unroll
+      for (int d = 0; d < kTcTileX; ++d) {
+        if (d == dx) r.wxs[d + j] = wx[j];
+      }
     }
   }
   out[s] = r;
@@ -257,6 +273,63 @@ struct TcLayout {
   static constexpr int kPadX = kTcTileX + W - 1;
 };
 
+// Converts chunk `ch` from its copy stage into its operand stage with the
+// kTcTeamThreads threads of one team (t = thread index in the team).
+template <int W>
+__device__ __forceinline__ void tc_convert(const TcChunk& ch, const unsigned char* raw, unsigned char* op, int t) {
+  using L = TcLayout<W>;
+  const int cnt = ch.count;
+  const float* raw_c = reinterpret_cast<const float*>(raw + L::kRawC);
+  const TcWeights* raw_w = reinterpret_cast<const TcWeights*>(raw + L::kRawW);
+  // A: row m, points 4h .. 4h + 3 (256 units).
+#pragma unroll
+  for (int i = 0; i < 256 / kTcTeamThreads; ++i) {
+    const int u = t + i * kTcTeamThreads;
+    const int m = u & (kTcRows - 1), h = u >> 7;
+    float v[4];
+#pragma unroll
+    for (int q = 0; q < 4; ++q) {
+      const int k = 4 * h + q;
+      v[q] = k < cnt ? raw_c[k * kTcRows + m] : 0.0f;
+    }
+    float4 hi, lo;
+    split_tf32(v[0], hi.x, lo.x);
+    split_tf32(v[1], hi.y, lo.y);
+    split_tf32(v[2], hi.z, lo.z);
+    split_tf32(v[3], hi.w, lo.w);
+    const int off = kmajor_unit(m, h);
+    *reinterpret_cast<float4*>(op + L::kAHi + off) = hi;
+    *reinterpret_cast<float4*>(op + L::kALo + off) = lo;
+  }
+  // B: accumulator column 16 j + nn (window row j, padded column nn), points
+  // 4h .. 4h + 3 (32 W units).
+#pragma unroll
+  for (int i = 0; i < (32 * W + kTcTeamThreads - 1) / kTcTeamThreads; ++i) {
+    const int u = t + i * kTcTeamThreads;
+    if (u < 32 * W) {
+      const int j = u >> 5, nn = (u >> 1) & 15, h = u & 1;
+      float v[4];
+#pragma unroll
+      for (int q = 0; q < 4; ++q) {
+        const int k = 4 * h + q;
+        v[q] = k < cnt ? raw_w[k].wy[j] * raw_w[k].wxs[nn] : 0.0f;
+      }
+      float4 hi, lo;
+      split_tf32(v[0], hi.x, lo.x);
+      split_tf32(v[1], hi.y, lo.y);
+      split_tf32(v[2], hi.z, lo.z);
+      split_tf32(v[3], hi.w, lo.w);
+      const int off = j * 512 + kmajor_unit(nn, h);
+      *reinterpret_cast<float4*>(op + L::kBHi + off) = hi;
+      *reinterpret_cast<float4*>(op + L::kBLo + off) = lo;
+    }
+  }
+}
+
+// Warp roles: warp 0 issues the bulk copies, warp 1 issues the MMAs, and
+// warps 2 .. 9 convert: four teams of two warps, team t taking chunks
+// c = t (mod 4). Barriers: full (copy landed), copy_free (copy read),
+// op_full (operands written), op_empty (MMAs done with the operands).
 template <int W>
 __global__ void __launch_bounds__(kTcThreads, 1) tc_spread_kernel(
     SpreadParams sp, const float* __restrict__ packed, int64_t count, const TcWeights* __restrict__ weights,
@@ -266,9 +339,12 @@ __global__ void __launch_bounds__(kTcThreads, 1) tc_spread_kernel(
   using L = TcLayout<W>;
   extern __shared__ __align__(1024) unsigned char smem[];
   __shared__ __align__(8) uint64_t full_bar[kTcCopyStages];
-  __shared__ __align__(8) uint64_t mma_bar[kTcOperandStages];
+  __shared__ __align__(8) uint64_t copy_free_bar[kTcCopyStages];
+  __shared__ __align__(8) uint64_t op_full_bar[kTcOperandStages];
+  __shared__ __align__(8) uint64_t op_empty_bar[kTcOperandStages];
   __shared__ uint32_t tmem_base;
   __shared__ int64_t s_tile;
+  __shared__ int s_abort;
   __shared__ TcChunk s_chunks[kTcChunksPerPart];
 
   const uint32_t part = blockIdx.x;
@@ -282,10 +358,17 @@ __global__ void __launch_bounds__(kTcThreads, 1) tc_spread_kernel(
       if (part_start[mid] <= part) low = mid; else high = mid - 1;
     }
     s_tile = low;
+    s_abort = 0;
 #pragma unroll
-    for (int s = 0; s < kTcCopyStages; ++s) mbar_init(&full_bar[s], 1);
+    for (int s = 0; s < kTcCopyStages; ++s) {
+      mbar_init(&full_bar[s], 1);
+      mbar_init(&copy_free_bar[s], kTcTeamThreads);
+    }
 #pragma unroll
-    for (int s = 0; s < kTcOperandStages; ++s) mbar_init(&mma_bar[s], 1);
+    for (int s = 0; s < kTcOperandStages; ++s) {
+      mbar_init(&op_full_bar[s], kTcTeamThreads);
+      mbar_init(&op_empty_bar[s], 1);
+    }
     asm volatile("fence.mbarrier_init.release.cluster;" ::: "memory");
   }
   if (warp == 0) {
@@ -298,16 +381,16 @@ __global__ void __launch_bounds__(kTcThreads, 1) tc_spread_kernel(
   tc_fence_after();
   const uint32_t tm = tmem_base;
   const int64_t tile = s_tile;
-  const int origin_x = static_cast<int>(tile % sp.ntiles[0]) * sp.tile[0];
-  const int origin_y = static_cast<int>(tile / sp.ntiles[0]) * sp.tile[1];
   const uint32_t first = tile_chunk_start[tile] + (part - part_start[tile]) * kTcChunksPerPart;
   const uint32_t stop = min(first + static_cast<uint32_t>(kTcChunksPerPart), tile_chunk_start[tile + 1]);
   const int n = stop > first ? static_cast<int>(stop - first) : 0;
   for (int c = tid; c < n; c += kTcThreads) s_chunks[c] = chunks[first + c];
 
-  // Zero the accumulator: warp w clears 256 columns of the 32 lanes it may access.
-  {
-    const uint32_t base = tm + (static_cast<uint32_t>((warp & 3) * 32) << 16) + static_cast<uint32_t>((warp >> 2) * 256);
+  // Zero the accumulator: the eight converter warps, two per lane quadrant,
+  // clear 256 columns each.
+  if (warp >= 2) {
+    const int cw = warp - 2;
+    const uint32_t base = tm + (static_cast<uint32_t>((warp & 3) * 32) << 16) + static_cast<uint32_t>((cw >> 2) * 256);
     for (int c = 0; c < 256; c += 8) tmem_zero8(base + c);
     asm volatile("tcgen05.wait::st.sync.aligned;" ::: "memory");
   }
@@ -315,123 +398,94 @@ __global__ void __launch_bounds__(kTcThreads, 1) tc_spread_kernel(
   __syncthreads();
   tc_fence_after();
 
-  const float* packed_group = packed + static_cast<int64_t>(group) * count * kTcRows;
-  auto issue_copies = [&](int c) {
-    const TcChunk ch = s_chunks[c];
-    unsigned char* st = smem + (c % kTcCopyStages) * L::kCopyStage;
-    const uint32_t bar = smem_u32(&full_bar[c % kTcCopyStages]);
-    const uint32_t cbytes = static_cast<uint32_t>(ch.count) * kTcRows * 4u;
-    const uint32_t wbytes = static_cast<uint32_t>(ch.count) * static_cast<uint32_t>(sizeof(TcWeights));
-    mbar_expect(bar, cbytes + wbytes);
-    bulk_load(smem_u32(st + L::kRawC), packed_group + static_cast<int64_t>(ch.slot) * kTcRows, cbytes, bar);
-    bulk_load(smem_u32(st + L::kRawW), weights + ch.slot, wbytes, bar);
-  };
-  if (tid == 0) {
-    for (int c = 0; c < min(n, kTcCopyStages - 1); ++c) issue_copies(c);
-  }
-
-  int issued = 0;
-  bool failed = false;
-  for (int c = 0; c < n; ++c) {
-    const int cs = c % kTcCopyStages, os = c % kTcOperandStages;
-    unsigned char* raw = smem + cs * L::kCopyStage;
-    unsigned char* op = smem + L::kOperandBase + os * L::kOperandStage;
-    // The copy stage of chunk c - 1 was read before the last barrier.
-    if (tid == 0 && c + kTcCopyStages - 1 < n) issue_copies(c + kTcCopyStages - 1);
-    bool ok = mbar_wait(smem_u32(&full_bar[cs]), static_cast<uint32_t>(c / kTcCopyStages) & 1u);
-    if (ok && c >= kTcOperandStages) {
-      ok = mbar_wait(smem_u32(&mma_bar[os]), static_cast<uint32_t>(c / kTcOperandStages - 1) & 1u);
-    }
-    const TcChunk ch = s_chunks[c];
-    if (ok) {
-      const int cnt = ch.count;
-      const float* raw_c = reinterpret_cast<const float*>(raw + L::kRawC);
-      const TcWeights* raw_w = reinterpret_cast<const TcWeights*>(raw + L::kRawW);
-      {
-        // A: row m, points 4h .. 4h + 3.
-        const int m = tid & (kTcRows - 1), h = tid >> 7;
-        float4 hi, lo;
-        float v[4];
-#pragma unroll
-        for (int q = 0; q < 4; ++q) {
-          const int k = 4 * h + q;
-          v[q] = k < cnt ? raw_c[k * kTcRows + m] : 0.0f;
+  volatile int* abort_flag = &s_abort;
+  int issued_copies = 0;
+  int issued_mmas = 0;
+  if (warp == 0) {
+    if (lane == 0) {
+      // Producer: chunk c reuses the copy stage of chunk c - kTcCopyStages once it has been read.
+      const float* packed_group = packed + static_cast<int64_t>(group) * count * kTcRows;
+      for (int c = 0; c < n; ++c) {
+        const int cs = c % kTcCopyStages;
+        if (c >= kTcCopyStages &&
+            !mbar_wait(smem_u32(&copy_free_bar[cs]), static_cast<uint32_t>(c / kTcCopyStages - 1) & 1u, abort_flag)) {
+          break;
         }
-        split_tf32(v[0], hi.x, lo.x);
-        split_tf32(v[1], hi.y, lo.y);
-        split_tf32(v[2], hi.z, lo.z);
-        split_tf32(v[3], hi.w, lo.w);
-        const int off = kmajor_unit(m, h);
-        *reinterpret_cast<float4*>(op + L::kAHi + off) = hi;
-        *reinterpret_cast<float4*>(op + L::kALo + off) = lo;
-      }
-      if (tid < 32 * W) {
-        // B: accumulator column 16 j + nn (window row j, padded column nn), points 4h .. 4h + 3.
-        const int j = tid >> 5, nn = (tid >> 1) & 15, h = tid & 1;
-        const int gy = origin_y + ch.row0, gx = origin_x + ch.x0;
-        float v[4];
-#pragma unroll
-        for (int q = 0; q < 4; ++q) {
-          const int k = 4 * h + q;
-          float value = 0.0f;
-          if (k < cnt) {
-            const TcWeights& r = raw_w[k];
-            const int jy = j - (r.sy - gy);
-            const int ix = nn - (r.sx - gx);
-            if (jy >= 0 && jy < W && ix >= 0 && ix < W) value = r.wy[jy] * r.wx[ix];
-          }
-          v[q] = value;
-        }
-        float4 hi, lo;
-        split_tf32(v[0], hi.x, lo.x);
-        split_tf32(v[1], hi.y, lo.y);
-        split_tf32(v[2], hi.z, lo.z);
-        split_tf32(v[3], hi.w, lo.w);
-        const int off = j * 512 + kmajor_unit(nn, h);
-        *reinterpret_cast<float4*>(op + L::kBHi + off) = hi;
-        *reinterpret_cast<float4*>(op + L::kBLo + off) = lo;
+        const TcChunk ch = s_chunks[c];
+        unsigned char* st = smem + cs * L::kCopyStage;
+        const uint32_t bar = smem_u32(&full_bar[cs]);
+        const uint32_t cbytes = static_cast<uint32_t>(ch.count) * kTcRows * 4u;
+        const uint32_t wbytes = static_cast<uint32_t>(ch.count) * static_cast<uint32_t>(sizeof(TcWeights));
+        mbar_expect(bar, cbytes + wbytes);
+        bulk_load(smem_u32(st + L::kRawC), packed_group + static_cast<int64_t>(ch.slot) * kTcRows, cbytes, bar);
+        bulk_load(smem_u32(st + L::kRawW), weights + ch.slot, wbytes, bar);
+        issued_copies = c + 1;
       }
     }
-    asm volatile("fence.proxy.async.shared::cta;" ::: "memory");
-    if (__syncthreads_or(ok ? 0 : 1)) {
-      failed = true;
-      break;
-    }
-    if (tid == 0) {
-      tc_fence_after();
-      const uint64_t ahi = kmajor_desc(smem_u32(op + L::kAHi));
-      const uint64_t alo = kmajor_desc(smem_u32(op + L::kALo));
-      const uint64_t bhi = kmajor_desc(smem_u32(op + L::kBHi));
-      const uint64_t blo = kmajor_desc(smem_u32(op + L::kBLo));
-      const uint32_t d = tm + static_cast<uint32_t>(ch.row0 * kTcPitch);
+  } else if (warp == 1) {
+    if (lane == 0) {
+      // MMA issuer: chunks in order, so the accumulation order is fixed.
       constexpr uint32_t idesc = tc_idesc<W>();
-      mma_tf32(d, ahi, bhi, idesc);
-      mma_tf32(d, ahi, blo, idesc);
-      mma_tf32(d, alo, bhi, idesc);
-      mma_commit(smem_u32(&mma_bar[os]));
+      for (int c = 0; c < n; ++c) {
+        const int os = c % kTcOperandStages;
+        if (!mbar_wait(smem_u32(&op_full_bar[os]), static_cast<uint32_t>(c / kTcOperandStages) & 1u, abort_flag)) {
+          break;
+        }
+        tc_fence_after();
+        const unsigned char* op = smem + L::kOperandBase + os * L::kOperandStage;
+        const uint64_t ahi = kmajor_desc(smem_u32(op + L::kAHi));
+        const uint64_t alo = kmajor_desc(smem_u32(op + L::kALo));
+        const uint64_t bhi = kmajor_desc(smem_u32(op + L::kBHi));
+        const uint64_t blo = kmajor_desc(smem_u32(op + L::kBLo));
+        const uint32_t d = tm + static_cast<uint32_t>(s_chunks[c].row0 * kTcPitch);
+        mma_tf32(d, ahi, bhi, idesc);
+        mma_tf32(d, ahi, blo, idesc);
+        mma_tf32(d, alo, bhi, idesc);
+        mma_commit(smem_u32(&op_empty_bar[os]));
+        issued_mmas = c + 1;
+      }
     }
-    issued = c + 1;
+  } else {
+    // Converters.
+    const int team = (warp - 2) >> 1, t = tid - 64 - team * kTcTeamThreads;
+    for (int c = team; c < n; c += kTcTeams) {
+      const int cs = c % kTcCopyStages, os = c % kTcOperandStages;
+      if (!mbar_wait(smem_u32(&full_bar[cs]), static_cast<uint32_t>(c / kTcCopyStages) & 1u, abort_flag)) break;
+      if (c >= kTcOperandStages &&
+          !mbar_wait(smem_u32(&op_empty_bar[os]), static_cast<uint32_t>(c / kTcOperandStages - 1) & 1u, abort_flag)) {
+        break;
+      }
+      tc_convert<W>(s_chunks[c], smem + cs * L::kCopyStage, smem + L::kOperandBase + os * L::kOperandStage, t);
+      asm volatile("fence.proxy.async.shared::cta;" ::: "memory");
+      mbar_arrive(smem_u32(&op_full_bar[os]));
+      mbar_arrive(smem_u32(&copy_free_bar[cs]));
+    }
   }
 
-  // Drain: the last commit covers every MMA issued before it; after a wait
-  // that gave up, the copies already issued must land before the CTA leaves.
+  // Drain: the producer waits for the copies it issued to land, the MMA
+  // issuer for its last commit (which covers every MMA before it).
   bool drained = true;
-  if (issued > 0) {
-    drained = mbar_wait(smem_u32(&mma_bar[(issued - 1) % kTcOperandStages]),
-                        static_cast<uint32_t>((issued - 1) / kTcOperandStages) & 1u);
-  }
-  if (failed) {
-    for (int c = issued; c < min(n, issued + kTcCopyStages); ++c) {
-      mbar_wait(smem_u32(&full_bar[c % kTcCopyStages]), static_cast<uint32_t>(c / kTcCopyStages) & 1u);
+  if (warp == 0 && lane == 0) {
+    for (int c = max(0, issued_copies - kTcCopyStages); c < issued_copies; ++c) {
+      drained = mbar_wait(smem_u32(&full_bar[c % kTcCopyStages]), static_cast<uint32_t>(c / kTcCopyStages) & 1u,
+                          nullptr) && drained;
     }
   }
+  if (warp == 1 && lane == 0 && issued_mmas > 0) {
+    drained = mbar_wait(smem_u32(&op_empty_bar[(issued_mmas - 1) % kTcOperandStages]),
+                        static_cast<uint32_t>((issued_mmas - 1) / kTcOperandStages) & 1u, nullptr);
+    if (issued_mmas < n) drained = false;
+  }
+  if (!drained) *abort_flag = 1;
+  tc_fence_before();
+  __syncthreads();
   tc_fence_after();
-  const bool good = drained && !failed;
-  {
+  const bool good = *abort_flag == 0;
+  if (warp >= 2) {
     // Accumulator row m = 32 (w % 4) + lane (vector m / 2, real part when m
     // is even) goes to scratch[part][cell][group][m]: a warp stores 128
     // contiguous bytes per cell.
-    const int q = warp & 3, half = warp >> 2;
+    const int q = warp & 3, half = (warp - 2) >> 2;
     const int m = q * 32 + lane;
     const int pad_y = sp.pad[1];
     const int rows_half = (pad_y + 1) / 2;

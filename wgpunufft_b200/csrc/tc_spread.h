@@ -40,15 +40,16 @@ struct TcChunk {
   uint8_t x0;    // padded-tile column of the column group
 };
 
-// The window of one point in slot order: its wrapped support start and
-// per-axis weights (zero for points outside the fold reach).
+// The window of one point in slot order: its wrapped support start, its y
+// weights, and its x weights placed at their padded-tile columns
+// (wxs[c] = wx[c - sx mod 8]); zero for points outside the fold reach.
 struct __align__(16) TcWeights {
   int32_t sx, sy;
   int32_t unused[2];
-  float wx[kTcMaxWidth];
   float wy[kTcMaxWidth];
+  float wxs[2 * kTcTileX];
 };
-static_assert(sizeof(TcWeights) == 80, "TcWeights is copied in 16-byte units");
+static_assert(sizeof(TcWeights) == 112, "TcWeights is copied in 16-byte units");
 
 // Tile rows of the tensor-core geometry for window width w.
 inline int tc_tile_rows(int width) { return kTcColumns / kTcPitch - width + 1; }
