@@ -48,6 +48,7 @@ def parse():
     p.add_argument("--impl", default="b200", choices=["b200", "reference"])
     p.add_argument("--no-e2e", action="store_true")
     p.add_argument("--no-cpu", action="store_true")
+    p.add_argument("--no-batched", action="store_true")
     return p.parse_args()
 
 
@@ -148,6 +149,117 @@ class ClockSampler:
                           and "Not" not in v})
         return {"sm_mhz": statistics.median(sm) if sm else None, "sm_max_mhz": max(mx) if mx else None,
                 "reasons": reasons, "samples": len(rows)}
+
+
+def c_interface_e2e(w, torch, points_h, strengths_h, timed, barrier, world, dev, args):
+    """NU points/s of wgpu_nufftf_setpts + wgpu_nufftf_execute on pinned host arrays."""
+    import ctypes
+
+    from wgpunufft_b200 import _native
+
+    lib = _native.library()
+    x = torch.from_numpy(np.ascontiguousarray(points_h[:, 0])).pin_memory()
+    y = torch.from_numpy(np.ascontiguousarray(points_h[:, 1])).pin_memory()
+    c = torch.from_numpy(strengths_h.view(np.float32)).pin_memory()
+    f = torch.empty(MODES[0] * MODES[1] * 2, dtype=torch.float32).pin_memory()
+    opts = _native.WgpuOpts()
+    lib.wgpu_nufft_default_opts(ctypes.byref(opts))
+    opts.adapter_index = torch.cuda.current_device() + 1
+    plan = ctypes.c_void_p()
+    modes = (ctypes.c_int64 * 2)(*MODES)
+    code = lib.wgpu_nufftf_makeplan(1, 2, modes, 1, 1, EPS, ctypes.byref(plan), ctypes.byref(opts))
+    if code != 0:
+        return {"error": lib.wgpu_nufft_last_error().decode()}
+    failures = []
+
+    def step():
+        rc = lib.wgpu_nufftf_setpts(plan, POINTS, x.data_ptr(), y.data_ptr(), None, 0, None, None, None)
+        rc = rc or lib.wgpu_nufftf_execute(plan, c.data_ptr(), f.data_ptr())
+        if rc:
+            failures.append(lib.wgpu_nufft_last_error().decode())
+
+    try:
+        for _ in range(2):
+            step()
+        barrier()
+        e2e_ms = timed(step, args.steps)
+    finally:
+        lib.wgpu_nufftf_destroy(plan)
+    if failures:
+        return {"error": failures[0]}
+    if world > 1:
+        import torch.distributed as dist
+
+        t = torch.tensor([e2e_ms], device=dev)
+        dist.all_reduce(t, op=dist.ReduceOp.MAX)
+        e2e_ms = t.item()
+    return {"value": world * POINTS / (e2e_ms / args.steps / 1e3), "unit": UNIT,
+            "ms_per_step": e2e_ms / args.steps,
+            "h2d_bytes_per_step": POINTS * 4 * 2 + POINTS * 8, "d2h_bytes_per_step": MODES[0] * MODES[1] * 8,
+            "path": "C interface wgpu_nufftf_setpts (per-axis f32, pinned host) + wgpu_nufftf_execute, "
+                    "plan made once; host-to-device copies, stable bin sort, spread, FFT, deconvolution "
+                    "and device-to-host copy inside every step"}
+
+
+BATCH_MODES = (512, 512)
+BATCH_POINTS = 2_000_000
+BATCH_EPS = 1e-6
+
+
+def batched_comparison(w, torch, timed, barrier, world, dev, args, rank):
+    """Type-1 NU points/s (points x vectors) of 64 and 256 vectors sharing one
+    point set, tensor cores (3xTF32) against CUDA cores, plus rel-l2 against
+    FP64 direct sums on 8 modes x 4 vectors."""
+    g = torch.Generator(device=dev)
+    g.manual_seed(SEED + 4)
+    pts = (torch.rand((BATCH_POINTS, 2), generator=g, device=dev) * (2 * np.pi) - np.pi).float().contiguous()
+    result = {"workload": "2d_type1_modes512x512_M2e6_uniform_eps1e-6", "modes": list(BATCH_MODES),
+              "points": BATCH_POINTS, "eps": BATCH_EPS, "unit": "NU points/s (points x vectors)"}
+    steps = max(1, min(args.steps, 5))
+    select = np.random.default_rng(3).choice(BATCH_MODES[0] * BATCH_MODES[1], 8, replace=False)
+    pts_h = pts.cpu().numpy().astype(np.float64) if rank == 0 else None
+    for batch in (64, 256):
+        c = torch.complex(torch.randn((batch, BATCH_POINTS), generator=g, device=dev),
+                          torch.randn((batch, BATCH_POINTS), generator=g, device=dev))
+        out = torch.empty((batch, BATCH_MODES[0] * BATCH_MODES[1]), dtype=torch.complex64, device=dev)
+        entry = {}
+        for name, method in (("tensor_cores", w.SpreadMethod.TENSOR_CORES), ("cuda_cores", w.SpreadMethod.CUDA_CORES)):
+            plan = w.NufftPlan.type1_gpu(w.NufftConfig(BATCH_MODES, BATCH_EPS, batch=batch, spread_method=method))
+            plan.set_points_gpu(pts)
+            for _ in range(max(1, args.warmup)):
+                plan.execute_gpu_batch(batch, c, out)
+            barrier()
+            plan.stage_timing(True)
+            plan.stage_report()
+            total = timed(lambda: plan.execute_gpu_batch(batch, c, out), steps)
+            stages = plan.stage_report()
+            plan.stage_timing(False)
+            if world > 1:
+                import torch.distributed as dist
+
+                t = torch.tensor([total], device=dev)
+                dist.all_reduce(t, op=dist.ReduceOp.MAX)
+                total = t.item()
+            ms = total / steps
+            item = {"value": world * BATCH_POINTS * batch / (ms / 1e3), "ms_per_step": ms,
+                    "stages_ms_per_step": {k: v[0] / steps for k, v in stages.items()}}
+            if rank == 0:
+                from oracle import native
+
+                got = out[:4].cpu().numpy()[:, select]
+                ref = native.direct_type1(pts_h, c[:4].cpu().numpy().astype(np.complex128), BATCH_MODES,
+                                          select=select)
+                item["rel_l2"] = float(np.linalg.norm(got - ref) / np.linalg.norm(ref))
+            entry[name] = item
+            del plan
+        entry["speedup_tensor_over_cuda_cores"] = entry["tensor_cores"]["value"] / entry["cuda_cores"]["value"]
+        spread_ms = entry["tensor_cores"]["stages_ms_per_step"].get("spread", 0.0)
+        useful = 4.0 * batch * BATCH_POINTS * 7 * 7
+        entry["tensor_core_spread_useful_tflops"] = useful / (spread_ms / 1e3) / 1e12 if spread_ms else None
+        result[f"B{batch}"] = entry
+        del c, out
+        torch.cuda.empty_cache()
+    return result
 
 
 def profile_traffic():
@@ -274,32 +386,19 @@ def main():
         ref = native.direct_type1(points_h.astype(np.float64), strengths_h, MODES, select=select)[0]
         rel = float(np.linalg.norm(got[select] - ref) / np.linalg.norm(ref))
 
-    # End to end through the public API with host buffers.
+    # End to end through the reference-facing C interface with host buffers:
+    # wgpu_nufftf_setpts (per-axis f32 coordinates) + wgpu_nufftf_execute
+    # every step, as a Fortran/MATLAB/Julia caller of the reference would.
     e2e = None
     if not args.no_e2e:
-        pts_pinned = torch.from_numpy(points_h).pin_memory()
-        str_pinned = torch.from_numpy(strengths_h.view(np.float32)).pin_memory()
-        out_pinned = torch.empty(config.mode_count() * 2, dtype=torch.float32).pin_memory()
-        pts_dev = torch.empty_like(points)
-        str_dev = torch.empty(POINTS * 2, dtype=torch.float32, device=dev)
+        e2e = c_interface_e2e(w, torch, points_h, strengths_h, timed, barrier, world, dev, args)
 
-        def e2e_step():
-            pts_dev.copy_(pts_pinned, non_blocking=True)
-            str_dev.copy_(str_pinned, non_blocking=True)
-            plan.encode_type1_gpu(pts_dev, str_dev.view(torch.complex64), out)
-            out_pinned.copy_(out.view(torch.float32), non_blocking=True)
-
-        for _ in range(2):
-            e2e_step()
-        barrier()
-        e2e_ms = timed(e2e_step, args.steps)
-        if world > 1:
-            t = torch.tensor([e2e_ms], device=dev)
-            dist.all_reduce(t, op=dist.ReduceOp.MAX)
-            e2e_ms = t.item()
-        e2e = {"value": world * POINTS / (e2e_ms / args.steps / 1e3), "unit": UNIT,
-               "h2d_bytes_per_step": POINTS * 8 + POINTS * 8, "d2h_bytes_per_step": config.mode_count() * 8,
-               "path": "NufftPlan.encode_type1_gpu (set_points + execute) with pinned host copies"}
+    # Batched vectors on one point set (2D 512^2 modes, 2e6 points, eps 1e-6):
+    # the tensor-core spreader against the CUDA-core spreader on the same plan
+    # shape and inputs.
+    batched = None
+    if not args.no_batched:
+        batched = batched_comparison(w, torch, timed, barrier, world, dev, args, rank)
 
     if rank == 0:
         peaks = json.loads((ROOT / "MEASURED_PEAKS.json").read_text()) if (ROOT / "MEASURED_PEAKS.json").exists() else {}
@@ -333,6 +432,7 @@ def main():
             "rel_l2": rel,
             "stages_ms_per_step": {k: v[0] / args.steps for k, v in stages.items()},
             "type2": type2,
+            "batched": batched,
             "roofline": roofline,
             "cpu_baseline": cpu,
             "e2e": e2e,

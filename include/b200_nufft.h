@@ -89,8 +89,17 @@ typedef enum b200nufft_status {
 
 #define B200NUFFT_MAX_DIMENSIONS 3
 
-/* Mirror of NufftConfig (src/config.rs:66-229) plus the plan's type and the
- * CUDA device. */
+/* Type-1 spreading engines. AUTO runs 2D f32 type-1 plans of batch >= 16 on
+ * the tensor cores (3xTF32 tcgen05 MMAs) when their active batch is at least
+ * 16 and the chosen bins allow it, and everything else on the CUDA cores.
+ * TENSOR_CORES asks for the tensor cores whenever the plan qualifies
+ * (plan creation fails otherwise); CUDA_CORES never uses them. */
+#define B200NUFFT_SPREAD_AUTO 0
+#define B200NUFFT_SPREAD_CUDA_CORES 1
+#define B200NUFFT_SPREAD_TENSOR_CORES 2
+
+/* Mirror of NufftConfig (src/config.rs:66-229) plus the plan's type, the
+ * CUDA device and the spreading engine. */
 typedef struct b200nufft_config {
   int32_t type;        /* 1 or 2 */
   int32_t dimensions;  /* 1..B200NUFFT_MAX_DIMENSIONS */
@@ -102,6 +111,7 @@ typedef struct b200nufft_config {
   double sigma;        /* upsampling factor, > 1; 0 selects 2 */
   int32_t precision;   /* B200NUFFT_PRECISION_*; 0 selects F32 */
   int32_t device;      /* CUDA device ordinal; -1 selects the current device */
+  int32_t spread_method; /* B200NUFFT_SPREAD_*; no counterpart in the reference */
 } b200nufft_config;
 
 /* Fills *config with NufftConfig::default(): one mode, eps 1e-6, batch 1,

@@ -24,6 +24,7 @@ __all__ = [
     "NufftType3Plan",
     "Precision",
     "ModeOrder",
+    "SpreadMethod",
     "NufftSign",
     "launch_count",
     "version",
@@ -96,6 +97,14 @@ class ModeOrder:
     FFT = 1
 
 
+class SpreadMethod:
+    """Type-1 spreading engine (B200NUFFT_SPREAD_*)."""
+
+    AUTO = 0
+    CUDA_CORES = 1
+    TENSOR_CORES = 2
+
+
 class NufftSign:
     POSITIVE = 1
     NEGATIVE = -1
@@ -112,10 +121,11 @@ class NufftConfig:
     sigma: float = DEFAULT_SIGMA
     batch: int = 1
     precision: int = Precision.F32
+    spread_method: int = 0
 
     def __init__(self, n_modes, eps: float = DEFAULT_EPS, *, isign: int = 1,
                  mode_order: int = ModeOrder.CENTERED, sigma: float = DEFAULT_SIGMA,
-                 batch: int = 1, precision: int = Precision.F32):
+                 batch: int = 1, precision: int = Precision.F32, spread_method: int = 0):
         object.__setattr__(self, "n_modes", tuple(int(n) for n in n_modes))
         object.__setattr__(self, "eps", float(eps))
         object.__setattr__(self, "isign", 1 if isign >= 0 else -1)
@@ -123,6 +133,7 @@ class NufftConfig:
         object.__setattr__(self, "sigma", float(sigma))
         object.__setattr__(self, "batch", int(batch))
         object.__setattr__(self, "precision", int(precision))
+        object.__setattr__(self, "spread_method", int(spread_method))
 
     # Builder methods of src/config.rs:91-130.
     def with_isign(self, isign: int) -> "NufftConfig":
@@ -144,6 +155,10 @@ class NufftConfig:
 
     def with_precision(self, precision: int) -> "NufftConfig":
         return replace(self, precision=int(precision))
+
+    def with_spread_method(self, method: int) -> "NufftConfig":
+        """SpreadMethod.AUTO, CUDA_CORES or TENSOR_CORES (no counterpart in the reference)."""
+        return replace(self, spread_method=int(method))
 
     @property
     def dimensions(self) -> int:
@@ -172,6 +187,7 @@ class NufftConfig:
         c.sigma = self.sigma
         c.precision = self.precision
         c.device = device
+        c.spread_method = self.spread_method
         return c
 
 

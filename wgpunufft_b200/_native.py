@@ -33,6 +33,7 @@ class Config(ctypes.Structure):
         ("sigma", c_double),
         ("precision", c_int32),
         ("device", c_int32),
+        ("spread_method", c_int32),
     ]
 
 

@@ -24,10 +24,16 @@
 #include "../../include/wgpu_nufft.h"
 #include "plan.h"
 #include "type3.h"
+#include "capi_io.h"
 #include "util.h"
 
 using b200nufft::DeviceBuffer;
 using b200nufft::NufftFailure;
+using b200nufft::HostScalar;
+using b200nufft::capi_gather_points;
+using b200nufft::capi_convert_values;
+using b200nufft::capi_convert_back;
+using b200nufft::capi_key_value;
 
 namespace {
 
@@ -397,52 +403,12 @@ struct HostPlan {
   std::unique_ptr<b200nufft::NufftPlan> plan12;
   std::unique_ptr<b200nufft::Type3Plan> plan3;
   std::vector<double> source_lo, source_hi, target_lo, target_hi;
-  DeviceBuffer points, targets, input, output;
+  DeviceBuffer points, targets, input, output, staging, checks;
   int64_t point_count = -1;
   int64_t target_count = 0;
 };
 
 size_t scalar_bytes(int precision) { return precision == B200NUFFT_PRECISION_F32 ? 4 : 8; }
-
-// Host doubles in the plan's storage: f32, f64, or Df64 (hi, lo) pairs.
-std::vector<unsigned char> encode(const std::vector<double>& values, int precision) {
-  std::vector<unsigned char> out(values.size() * scalar_bytes(precision));
-  if (precision == B200NUFFT_PRECISION_F32) {
-    float* o = reinterpret_cast<float*>(out.data());
-    for (size_t i = 0; i < values.size(); ++i) o[i] = static_cast<float>(values[i]);
-  } else if (precision == B200NUFFT_PRECISION_F64) {
-    std::memcpy(out.data(), values.data(), out.size());
-  } else {
-    float* o = reinterpret_cast<float*>(out.data());
-    for (size_t i = 0; i < values.size(); ++i) {
-      const float hi = static_cast<float>(values[i]);
-      o[2 * i] = hi;
-      o[2 * i + 1] = static_cast<float>(values[i] - static_cast<double>(hi));
-    }
-  }
-  return out;
-}
-
-std::vector<double> decode(const unsigned char* bytes, size_t count, int precision) {
-  std::vector<double> out(count);
-  if (precision == B200NUFFT_PRECISION_F32) {
-    const float* p = reinterpret_cast<const float*>(bytes);
-    for (size_t i = 0; i < count; ++i) out[i] = p[i];
-  } else if (precision == B200NUFFT_PRECISION_F64) {
-    std::memcpy(out.data(), bytes, count * sizeof(double));
-  } else {
-    const float* p = reinterpret_cast<const float*>(bytes);
-    for (size_t i = 0; i < count; ++i) out[i] = static_cast<double>(p[2 * i]) + static_cast<double>(p[2 * i + 1]);
-  }
-  return out;
-}
-
-void upload(DeviceBuffer& buffer, const std::vector<unsigned char>& bytes, const char* label) {
-  void* d = buffer.reserve(std::max<size_t>(bytes.size(), 16), label);
-  if (!bytes.empty()) {
-    b200nufft::check_cuda(cudaMemcpy(d, bytes.data(), bytes.size(), cudaMemcpyHostToDevice), label);
-  }
-}
 
 b200nufft_type3_config type3_config(const HostPlan& p, const std::vector<double>& slo,
                                     const std::vector<double>& shi, const std::vector<double>& tlo,
@@ -507,64 +473,136 @@ std::unique_ptr<HostPlan> make_host_plan(const Spec& spec) {
   return plan;
 }
 
-// check_type12_points (capi/src/plan.rs:524-536).
-void check_type12_points(const std::vector<double>& points, int dim) {
-  const double limit = 3.0 * kPi;
-  for (size_t i = 0; i < points.size(); ++i) {
-    const double v = points[i];
-    if (std::isnan(v) || std::fabs(v) > limit) {
-      invalid("point " + std::to_string(i / dim) + " has coordinate " + std::to_string(v) +
-              " on axis " + std::to_string(i % dim) + ", outside [-3*pi, 3*pi]");
+bool storage_matches(int precision, HostScalar scalar) {
+  return (precision == B200NUFFT_PRECISION_F32 && scalar == HostScalar::F32) ||
+         (precision == B200NUFFT_PRECISION_F64 && scalar == HostScalar::F64);
+}
+
+template <typename T>
+constexpr HostScalar host_scalar() {
+  return std::is_same<T, float>::value ? HostScalar::F32 : HostScalar::F64;
+}
+
+// A point set as the caller passes it: one array per axis or one point-major array.
+template <typename T>
+struct HostPoints {
+  int64_t count = 0;
+  const T* axes[3] = {nullptr, nullptr, nullptr};
+  const T* interleaved = nullptr;
+  const char* const* names = nullptr;  // per-axis argument names, or the point-major one
+};
+
+template <typename T>
+void validate_points(const HostPoints<T>& h, int dim) {
+  if (h.count < 0) invalid("M must not be negative");
+  if (h.count == 0) return;
+  if (h.names && dim <= 3 && !h.interleaved) {
+    for (int a = 0; a < dim; ++a) {
+      if (!h.axes[a]) invalid(std::string(h.names[a]) + " is null");
     }
+  } else if (!h.interleaved) {
+    invalid("the point array is null");
   }
 }
 
-void check_finite(const char* set, const std::vector<double>& points, int dim) {
-  for (size_t i = 0; i < points.size(); ++i) {
-    if (!std::isfinite(points[i])) {
-      invalid(std::string(set) + " " + std::to_string(i / dim) + " has a coordinate that is not finite on axis " +
-              std::to_string(i % dim));
+template <typename T>
+double host_coordinate(const HostPoints<T>& h, int dim, int64_t i, int a) {
+  return h.interleaved ? static_cast<double>(h.interleaved[i * dim + a]) : static_cast<double>(h.axes[a][i]);
+}
+
+// Copies the caller's coordinates to `staging` as they are and converts them
+// to point-major storage in `out` on the device.
+template <typename T>
+void upload_points(HostPlan& p, const HostPoints<T>& h, DeviceBuffer& out, int check,
+                   unsigned long long* first_bad, unsigned long long* bounds, size_t staging_offset) {
+  const int dim = p.spec.dim;
+  const size_t bytes = static_cast<size_t>(h.count) * dim * sizeof(T);
+  const size_t storage = static_cast<size_t>(h.count) * dim * scalar_bytes(p.precision);
+  void* dst = out.reserve(std::max<size_t>(storage, 16), "coordinates");
+  if (h.count == 0) return;
+  unsigned char* stage = static_cast<unsigned char*>(p.staging.get()) + staging_offset;
+  if (h.interleaved) {
+    b200nufft::check_cuda(cudaMemcpyAsync(stage, h.interleaved, bytes, cudaMemcpyHostToDevice, nullptr),
+                          "copy points");
+    capi_gather_points(host_scalar<T>(), stage, 1, dim, dim, h.count, p.precision, check, dst, first_bad, bounds,
+                       nullptr);
+  } else {
+    for (int a = 0; a < dim; ++a) {
+      b200nufft::check_cuda(cudaMemcpyAsync(stage + a * h.count * sizeof(T), h.axes[a], h.count * sizeof(T),
+                                            cudaMemcpyHostToDevice, nullptr),
+                            "copy points");
     }
+    capi_gather_points(host_scalar<T>(), stage, h.count, 1, dim, h.count, p.precision, check, dst, first_bad,
+                       bounds, nullptr);
   }
 }
 
-// f32 plans see rounded coordinates, which the type-3 bounds must hold.
-void round_if_f32(std::vector<double>& values, int precision) {
-  if (precision != B200NUFFT_PRECISION_F32) return;
-  for (double& v : values) v = static_cast<double>(static_cast<float>(v));
+double rounded(double v, int precision) {
+  return precision == B200NUFFT_PRECISION_F32 ? static_cast<double>(static_cast<float>(v)) : v;
 }
 
-void intervals(const std::vector<double>& points, int dim, std::vector<double>& lo, std::vector<double>& hi) {
-  lo.assign(dim, INFINITY);
-  hi.assign(dim, -INFINITY);
-  for (size_t i = 0; i < points.size(); ++i) {
-    const int a = static_cast<int>(i % dim);
-    lo[a] = std::min(lo[a], points[i]);
-    hi[a] = std::max(hi[a], points[i]);
-  }
-  for (int a = 0; a < dim; ++a) {
-    if (lo[a] > hi[a]) lo[a] = hi[a] = 0.0;
-  }
+std::string number(double v) {
+  char buffer[64];
+  std::snprintf(buffer, sizeof(buffer), "%.17g", v);
+  return buffer;
 }
 
-void set_points(HostPlan& p, std::vector<double> points, std::vector<double> targets) {
+// Plan::set_points (capi/src/plan.rs:478-523) with the checks of
+// check_type12_points / check_finite (:524-545) on the device.
+template <typename T>
+void set_points(HostPlan& p, const HostPoints<T>& pts, const HostPoints<T>& tgs) {
   b200nufft::check_cuda(cudaSetDevice(p.device), "select device");
   const int dim = p.spec.dim;
-  const int64_t m = static_cast<int64_t>(points.size()) / dim;
-  const int64_t n = static_cast<int64_t>(targets.size()) / dim;
+  validate_points(pts, dim);
+  const bool type3 = p.spec.kind == 3;
+  if (type3) validate_points(tgs, dim);
   p.point_count = -1;
-  round_if_f32(points, p.precision);
-  round_if_f32(targets, p.precision);
-  if (p.spec.kind != 3) {
-    check_type12_points(points, dim);
-    upload(p.points, encode(points, p.precision), "points");
-    p.plan12->set_points(m, p.points.get(), nullptr);
+  const size_t point_bytes = static_cast<size_t>(pts.count) * dim * sizeof(T);
+  const size_t target_bytes = type3 ? static_cast<size_t>(tgs.count) * dim * sizeof(T) : 0;
+  const size_t target_offset = (point_bytes + 255) / 256 * 256;
+  p.staging.reserve(std::max<size_t>(target_offset + target_bytes, 16), "host copies");
+  // checks: [0] first bad point element, [1] first bad target element,
+  // [2 .. 2 + 2 dim) point bounds, [2 + 2 dim .. 2 + 4 dim) target bounds.
+  unsigned long long init[16];
+  init[0] = init[1] = ~0ull;
+  for (int a = 0; a < dim; ++a) {
+    init[2 + 2 * a] = init[2 + 2 * dim + 2 * a] = ~0ull;
+    init[3 + 2 * a] = init[3 + 2 * dim + 2 * a] = 0ull;
+  }
+  unsigned long long* checks = static_cast<unsigned long long*>(p.checks.reserve(sizeof(init), "checks"));
+  b200nufft::check_cuda(cudaMemcpyAsync(checks, init, sizeof(init), cudaMemcpyHostToDevice, nullptr), "reset checks");
+  upload_points(p, pts, p.points, type3 ? 1 : 0, checks, type3 ? checks + 2 : nullptr, 0);
+  if (type3) upload_points(p, tgs, p.targets, 1, checks + 1, checks + 2 + 2 * dim, target_offset);
+  unsigned long long result[16];
+  b200nufft::check_cuda(cudaMemcpy(result, checks, sizeof(result), cudaMemcpyDeviceToHost), "read checks");
+  if (type3 && result[1] != ~0ull) {
+    const int64_t i = static_cast<int64_t>(result[1] / dim);
+    invalid("target " + std::to_string(i) + " has a coordinate that is not finite on axis " +
+            std::to_string(result[1] % dim));
+  }
+  if (result[0] != ~0ull) {
+    const int64_t i = static_cast<int64_t>(result[0] / dim);
+    const int a = static_cast<int>(result[0] % dim);
+    if (type3) {
+      invalid("point " + std::to_string(i) + " has a coordinate that is not finite on axis " + std::to_string(a));
+    }
+    invalid("point " + std::to_string(i) + " has coordinate " +
+            number(rounded(host_coordinate(pts, dim, i, a), p.precision)) + " on axis " + std::to_string(a) +
+            ", outside [-3*pi, 3*pi]");
+  }
+  if (!type3) {
+    p.plan12->set_points(pts.count, p.points.get(), nullptr);
   } else {
-    check_finite("target", targets, dim);
-    check_finite("point", points, dim);
-    std::vector<double> slo, shi, tlo, thi;
-    intervals(points, dim, slo, shi);
-    intervals(targets, dim, tlo, thi);
+    // The smallest interval per axis holding every point, [0, 0] without any
+    // (intervals, capi/src/plan.rs:377-397).
+    std::vector<double> slo(dim), shi(dim), tlo(dim), thi(dim);
+    for (int a = 0; a < dim; ++a) {
+      const bool any_s = pts.count > 0, any_t = tgs.count > 0;
+      slo[a] = any_s ? capi_key_value(result[2 + 2 * a]) : 0.0;
+      shi[a] = any_s ? capi_key_value(result[3 + 2 * a]) : 0.0;
+      tlo[a] = any_t ? capi_key_value(result[2 + 2 * dim + 2 * a]) : 0.0;
+      thi[a] = any_t ? capi_key_value(result[3 + 2 * dim + 2 * a]) : 0.0;
+    }
     bool contained = p.plan3 != nullptr;
     for (int a = 0; contained && a < dim; ++a) {
       contained = p.source_lo[a] <= slo[a] && shi[a] <= p.source_hi[a] && p.target_lo[a] <= tlo[a] &&
@@ -578,12 +616,10 @@ void set_points(HostPlan& p, std::vector<double> points, std::vector<double> tar
       p.target_lo = tlo;
       p.target_hi = thi;
     }
-    upload(p.points, encode(points, p.precision), "sources");
-    upload(p.targets, encode(targets, p.precision), "targets");
-    p.plan3->set_points(m, p.points.get(), n, p.targets.get(), nullptr);
+    p.plan3->set_points(pts.count, p.points.get(), tgs.count, p.targets.get(), nullptr);
   }
-  p.point_count = m;
-  p.target_count = n;
+  p.point_count = pts.count;
+  p.target_count = type3 ? tgs.count : 0;
 }
 
 void lengths(const HostPlan& p, int64_t& in_complex, int64_t& out_complex) {
@@ -596,54 +632,56 @@ void lengths(const HostPlan& p, int64_t& in_complex, int64_t& out_complex) {
   }
 }
 
-void execute(HostPlan& p, const std::vector<double>& input, std::vector<double>& output) {
+// Plan::execute (capi/src/plan.rs:547-570): the input copied as it is and
+// checked on the device; the output copied back when every value was finite.
+template <typename T>
+void execute(HostPlan& p, const T* in, T* out, const char* in_name, const char* out_name) {
   b200nufft::check_cuda(cudaSetDevice(p.device), "select device");
-  for (size_t i = 0; i < input.size(); ++i) {
-    if (!std::isfinite(input[i])) {
-      invalid("the input holds a value that is not finite at complex index " + std::to_string(i / 2));
-    }
+  int64_t in_complex, out_complex;
+  lengths(p, in_complex, out_complex);
+  const int64_t in_scalars = 2 * in_complex, out_scalars = 2 * out_complex;
+  if (in_scalars > 0 && !in) invalid(std::string(in_name) + " is null");
+  if (out_scalars > 0 && !out) invalid(std::string(out_name) + " is null");
+  const HostScalar scalar = host_scalar<T>();
+  const bool direct = storage_matches(p.precision, scalar);
+  const size_t in_storage = static_cast<size_t>(in_scalars) * scalar_bytes(p.precision);
+  const size_t out_storage = static_cast<size_t>(out_scalars) * scalar_bytes(p.precision);
+  void* d_in = p.input.reserve(std::max<size_t>(in_storage, 16), "input");
+  void* d_out = p.output.reserve(std::max<size_t>(out_storage, 16), "output");
+  if (!direct) {
+    p.staging.reserve(std::max<size_t>(static_cast<size_t>(std::max(in_scalars, out_scalars)) * sizeof(T), 16),
+                      "host copies");
   }
-  upload(p.input, encode(input, p.precision), "input");
-  const size_t out_bytes = output.size() * scalar_bytes(p.precision);
-  void* d_out = p.output.reserve(std::max<size_t>(out_bytes, 16), "output");
+  unsigned long long* checks = static_cast<unsigned long long*>(p.checks.reserve(16 * sizeof(unsigned long long), "checks"));
+  b200nufft::check_cuda(cudaMemsetAsync(checks, 0xFF, sizeof(unsigned long long), nullptr), "reset checks");
+  if (in_scalars > 0) {
+    void* landing = direct ? d_in : p.staging.get();
+    b200nufft::check_cuda(cudaMemcpyAsync(landing, in, static_cast<size_t>(in_scalars) * sizeof(T),
+                                          cudaMemcpyHostToDevice, nullptr),
+                          "copy input");
+    capi_convert_values(scalar, landing, in_scalars, p.precision, direct ? nullptr : d_in, checks, nullptr);
+  }
   if (p.spec.kind != 3) {
-    p.plan12->execute(p.spec.ntrans, p.input.get(), d_out, nullptr);
-    p.plan12->synchronize(nullptr);
+    p.plan12->execute(p.spec.ntrans, d_in, d_out, nullptr);
   } else {
-    p.plan3->execute(p.spec.ntrans, p.input.get(), d_out, nullptr);
-    b200nufft::check_cuda(cudaStreamSynchronize(nullptr), "synchronize");
+    p.plan3->execute(p.spec.ntrans, d_in, d_out, nullptr);
   }
-  std::vector<unsigned char> bytes(out_bytes);
-  if (out_bytes) {
-    b200nufft::check_cuda(cudaMemcpy(bytes.data(), d_out, out_bytes, cudaMemcpyDeviceToHost), "read output");
+  unsigned long long first_bad = 0;
+  b200nufft::check_cuda(cudaMemcpy(&first_bad, checks, sizeof(first_bad), cudaMemcpyDeviceToHost), "read checks");
+  if (p.spec.kind != 3) p.plan12->synchronize(nullptr);
+  if (first_bad != ~0ull) {
+    invalid("the input holds a value that is not finite at complex index " + std::to_string(first_bad / 2));
   }
-  output = decode(bytes.data(), output.size(), p.precision);
-}
-
-template <typename T>
-std::vector<double> widened(const T* values, int64_t count, const char* name) {
-  if (count < 0) invalid(std::string(name) + " length must not be negative");
-  if (count > 0 && !values) invalid(std::string(name) + " is null");
-  std::vector<double> out(static_cast<size_t>(count));
-  for (int64_t i = 0; i < count; ++i) out[static_cast<size_t>(i)] = static_cast<double>(values[i]);
-  return out;
-}
-
-template <typename T>
-std::vector<double> per_axis(int64_t m, const T* const* axes, int dim, const char* const* names) {
-  if (m < 0) invalid("M must not be negative");
-  std::vector<double> points(static_cast<size_t>(m) * dim);
-  for (int a = 0; a < dim; ++a) {
-    if (m > 0 && !axes[a]) invalid(std::string(names[a]) + " is null");
-    for (int64_t j = 0; j < m; ++j) points[static_cast<size_t>(j) * dim + a] = static_cast<double>(axes[a][j]);
+  if (out_scalars > 0) {
+    const void* source = d_out;
+    if (!direct) {
+      capi_convert_back(p.precision, d_out, out_scalars, scalar, p.staging.get(), nullptr);
+      source = p.staging.get();
+    }
+    b200nufft::check_cuda(cudaMemcpy(out, source, static_cast<size_t>(out_scalars) * sizeof(T),
+                                     cudaMemcpyDeviceToHost),
+                          "read output");
   }
-  return points;
-}
-
-template <typename T>
-void narrow_into(const std::vector<double>& values, T* out, const char* name) {
-  if (!values.empty() && !out) invalid(std::string(name) + " is null");
-  for (size_t i = 0; i < values.size(); ++i) out[i] = static_cast<T>(values[i]);
 }
 
 // ---------------------------------------------------------------------------
@@ -660,12 +698,19 @@ int one_call(int kind, int dim, int64_t m, const T* const* axes, int32_t isign, 
     const Spec spec = make_spec(kind, dim, modes, isign, 1, eps, data, opts);
     static const char* const xyz[] = {"x", "y", "z"};
     static const char* const stu[] = {"s", "t", "u"};
-    std::vector<double> points = per_axis(m, axes, dim, xyz);
-    std::vector<double> targets;
+    HostPoints<T> pts, tgs;
+    pts.count = m;
+    pts.names = xyz;
+    for (int a = 0; a < dim; ++a) pts.axes[a] = axes[a];
     if (kind == 3) {
       if (n < 0) invalid("N must not be negative");
-      targets = per_axis(n, target_axes, dim, stu);
+      tgs.count = n;
+      tgs.names = stu;
+      for (int a = 0; a < dim; ++a) tgs.axes[a] = target_axes[a];
     }
+    // The arrays are checked before a plan is made or taken from the cache.
+    validate_points(pts, dim);
+    if (kind == 3) validate_points(tgs, dim);
     std::lock_guard<std::mutex> lock(g_cache_mutex);
     auto found = std::find_if(g_cache.begin(), g_cache.end(),
                               [&](const std::unique_ptr<HostPlan>& p) { return p->spec == spec; });
@@ -676,15 +721,16 @@ int one_call(int kind, int dim, int64_t m, const T* const* axes, int32_t isign, 
     } else {
       plan = make_host_plan(spec);
     }
-    set_points(*plan, std::move(points), std::move(targets));
-    int64_t in_count, out_count;
-    lengths(*plan, in_count, out_count);
-    const std::vector<double> in = widened(input, 2 * in_count, kind == 2 ? "f" : "c");
-    std::vector<double> out(static_cast<size_t>(2 * out_count));
-    execute(*plan, in, out);
-    narrow_into(out, output, kind == 2 ? "c" : "f");
-    g_cache.push_front(std::move(plan));
-    while (g_cache.size() > kCacheSize) g_cache.pop_back();
+    // The plan stays kept whether or not the call succeeds.
+    struct Keep {
+      std::unique_ptr<HostPlan>& plan;
+      ~Keep() {
+        g_cache.push_front(std::move(plan));
+        while (g_cache.size() > kCacheSize) g_cache.pop_back();
+      }
+    } keep{plan};
+    set_points(*plan, pts, tgs);
+    execute(*plan, input, output, kind == 2 ? "f" : "c", kind == 2 ? "c" : "f");
   });
 }
 
@@ -736,17 +782,23 @@ int setpts_impl(void* handle, int64_t m, const T* x, const T* y, const T* z, int
   return call([&] {
     HostPlan& p = host<T>(handle);
     if (p.spec.dim > 3) invalid("plans of more than three dimensions take their points through setpts_nd");
-    const T* axes[3] = {x, y, z};
-    const T* targets[3] = {s, t, u};
     static const char* const xyz[] = {"x", "y", "z"};
     static const char* const stu[] = {"s", "t", "u"};
-    std::vector<double> points = per_axis(m, axes, p.spec.dim, xyz);
-    std::vector<double> tg;
+    HostPoints<T> pts, tgs;
+    pts.count = m;
+    pts.names = xyz;
+    pts.axes[0] = x;
+    pts.axes[1] = y;
+    pts.axes[2] = z;
     if (p.spec.kind == 3) {
       if (n < 0) invalid("N must not be negative");
-      tg = per_axis(n, targets, p.spec.dim, stu);
+      tgs.count = n;
+      tgs.names = stu;
+      tgs.axes[0] = s;
+      tgs.axes[1] = t;
+      tgs.axes[2] = u;
     }
-    set_points(p, std::move(points), std::move(tg));
+    set_points(p, pts, tgs);
   });
 }
 
@@ -754,14 +806,17 @@ template <typename T>
 int setpts_nd_impl(void* handle, int64_t m, const T* points, int64_t n, const T* targets) {
   return call([&] {
     HostPlan& p = host<T>(handle);
-    if (m < 0) invalid("M must not be negative");
-    std::vector<double> pts = widened(points, m * p.spec.dim, "points");
-    std::vector<double> tg;
+    HostPoints<T> pts, tgs;
+    pts.count = m;
+    pts.interleaved = points;
+    if (m > 0 && !points) invalid("points is null");
     if (p.spec.kind == 3) {
       if (n < 0) invalid("N must not be negative");
-      tg = widened(targets, n * p.spec.dim, "targets");
+      if (n > 0 && !targets) invalid("targets is null");
+      tgs.count = n;
+      tgs.interleaved = targets;
     }
-    set_points(p, std::move(pts), std::move(tg));
+    set_points(p, pts, tgs);
   });
 }
 
@@ -769,13 +824,11 @@ template <typename T>
 int execute_impl(void* handle, T* c, T* f) {
   return call([&] {
     HostPlan& p = host<T>(handle);
-    int64_t in_count, out_count;
-    lengths(p, in_count, out_count);
-    const bool type2 = p.spec.kind == 2;
-    const std::vector<double> in = widened(type2 ? f : c, 2 * in_count, type2 ? "f" : "c");
-    std::vector<double> out(static_cast<size_t>(2 * out_count));
-    execute(p, in, out);
-    narrow_into(out, type2 ? c : f, type2 ? "c" : "f");
+    if (p.spec.kind == 2) {
+      execute<T>(p, f, c, "f", "c");
+    } else {
+      execute<T>(p, c, f, "c", "f");
+    }
   });
 }
 

@@ -41,6 +41,21 @@ class DeviceBuffer {
 };
 
 // Fine-grid geometry and window of an F32 plan as the kernels see it.
+// The f32 window as per-tap polynomials (src/kernel.rs Horner panels, fitted
+// in f64 and rounded to f32): rows of highest degree first, w + 3 rows for a
+// w-point window with unused leading rows zero.
+constexpr int kHornerRows32 = 19;   // horner32_window (fold.cuh) assumes 19 x 16
+constexpr int kHornerWidth32 = 16;
+
+// Per slot of an f32 plan: the wrapped support start and the offset
+// (start - position, in [-w/2, 1 - w/2)) of every axis; start[0] < 0 marks a
+// point outside the fold reach, which the reference weighs zero.
+template <int D>
+struct alignas(D == 3 ? 32 : 16) PreparedWindow {
+  int32_t start[D == 3 ? 4 : 2];
+  float offset[D == 3 ? 4 : 2];
+};
+
 struct GridParams {
   int32_t dimensions;
   int32_t width;
@@ -54,7 +69,13 @@ struct GridParams {
   double half_width64;
   const double* horner;  // device, rows x width
   int32_t horner_rows;
+  float horner32[kHornerRows32][kHornerWidth32];
 };
+
+// Prepared windows of `count` f32 points in slot order (coordinates in slot order).
+void prepare_windows(const float* sorted_points, int64_t count, const GridParams& grid, void* windows,
+                     cudaStream_t stream);
+size_t prepared_window_bytes(int dimensions);
 
 // Stable sort of the points by bin key. Launches on `stream`; all pointers
 // are device pointers owned by the caller.

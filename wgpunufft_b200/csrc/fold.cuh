@@ -207,4 +207,19 @@ __device__ __forceinline__ void f32_window(float x, const FoldAxis& axis, float 
   }
 }
 
+// The W window weights of one axis from the f32 Horner panels: every tap j
+// evaluates its panel at local = 2 offset + W - 1 in [-1, 1].
+template <int W>
+__device__ __forceinline__ void horner32_window(float offset, const float (&table)[19][16], float* w) {
+  const float local = fmaf(2.0f, offset, static_cast<float>(W - 1));
+  const bool inside = fabsf(local) <= 1.0f;
+#pragma unroll
+  for (int j = 0; j < W; ++j) {
+    float v = 0.0f;
+#pragma unroll
+    for (int r = 19 - (W + 3); r < 19; ++r) v = fmaf(v, local, table[r][j]);
+    w[j] = inside ? v : 0.0f;
+  }
+}
+
 }  // namespace b200nufft

@@ -21,6 +21,7 @@ namespace b200nufft {
 namespace {
 
 struct F32Window {
+  static constexpr bool kPreparedWindows = true;
   using Real = float;
   using Complex = float2;
   static __device__ __forceinline__ bool in_reach(float x) { return in_fold_reach(x); }
@@ -42,6 +43,7 @@ struct F32Window {
 };
 
 struct F64Window {
+  static constexpr bool kPreparedWindows = false;
   using Real = double;
   using Complex = double2;
   static __device__ __forceinline__ bool in_reach(double x) { return in_fold_reach64(x); }
@@ -59,15 +61,16 @@ struct F64Window {
 };
 
 // Resident blocks per SM the register budget is tuned for: narrow 1D and 2D
-// f32 windows fit three 256-thread blocks without spilling, the others two.
+// f32 windows (w <= 4) fit three 256-thread blocks without spilling, the others two.
 template <int D, int W, typename T>
 struct InterpBlocks {
-  static constexpr int value = (D <= 2 && W <= 6 && sizeof(typename T::Real) == 4) ? 3 : 2;
+  static constexpr int value = (D <= 2 && W <= 4 && sizeof(typename T::Real) == 4) ? 3 : 2;
 };
 
 template <int D, int W, typename T>
 __global__ void __launch_bounds__(256, InterpBlocks<D, W, T>::value)
-    interpolate_kernel(GridParams g, const typename T::Real* __restrict__ points, int64_t count,
+    interpolate_kernel(GridParams g, const typename T::Real* __restrict__ points,
+                       const void* __restrict__ windows, int64_t count,
                        const uint32_t* __restrict__ perm,
                        const typename T::Complex* __restrict__ fine, int batch,
                        typename T::Complex* __restrict__ output) {
@@ -76,12 +79,31 @@ __global__ void __launch_bounds__(256, InterpBlocks<D, W, T>::value)
   const int64_t slot = static_cast<int64_t>(blockIdx.x) * blockDim.x + threadIdx.x;
   if (slot >= count) return;
   const uint32_t point = perm[slot];
-  Real p[D];
-#pragma unroll
-  for (int a = 0; a < D; ++a) p[a] = points[slot * D + a];
+  int first[D];
+  Real w[D][W];
   bool reach = true;
+  if constexpr (T::kPreparedWindows) {
+    // f32 plans: the window start and offset prepared at set_points.
+    const PreparedWindow<D> win = static_cast<const PreparedWindow<D>*>(windows)[slot];
+    reach = win.start[0] >= 0;
+    if (reach) {
 #pragma unroll
-  for (int a = 0; a < D; ++a) reach = reach && T::in_reach(p[a]);
+      for (int a = 0; a < D; ++a) {
+        first[a] = win.start[a];
+        horner32_window<W>(win.offset[a], g.horner32, w[a]);
+      }
+    }
+  } else {
+    Real p[D];
+#pragma unroll
+    for (int a = 0; a < D; ++a) p[a] = points[slot * D + a];
+#pragma unroll
+    for (int a = 0; a < D; ++a) reach = reach && T::in_reach(p[a]);
+    if (reach) {
+#pragma unroll
+      for (int a = 0; a < D; ++a) T::template window<W>(p[a], g, a, first[a], w[a]);
+    }
+  }
   if (!reach) {
     Complex zero;
     zero.x = 0;
@@ -89,10 +111,6 @@ __global__ void __launch_bounds__(256, InterpBlocks<D, W, T>::value)
     for (int b = 0; b < batch; ++b) output[static_cast<int64_t>(b) * count + point] = zero;
     return;
   }
-  int first[D];
-  Real w[D][W];
-#pragma unroll
-  for (int a = 0; a < D; ++a) T::template window<W>(p[a], g, a, first[a], w[a]);
   const int32_t n0 = g.axis[0].length;
   int x[W];
 #pragma unroll
@@ -164,6 +182,7 @@ __global__ void __launch_bounds__(256, InterpBlocks<D, W, T>::value)
 template <typename T>
 struct Launch {
   const typename T::Real* points;
+  const void* windows;
   int64_t point_count;
   const uint32_t* perm;
   const typename T::Complex* fine;
@@ -174,7 +193,7 @@ struct Launch {
 template <int D, int W, typename T>
 void launch_width(const GridParams& g, const Launch<T>& l, cudaStream_t stream) {
   const unsigned blocks = static_cast<unsigned>((l.point_count + 255) / 256);
-  interpolate_kernel<D, W, T><<<blocks, 256, 0, stream>>>(g, l.points, l.point_count, l.perm,
+  interpolate_kernel<D, W, T><<<blocks, 256, 0, stream>>>(g, l.points, l.windows, l.point_count, l.perm,
                                                            l.fine, l.batch, l.output);
   note_launch();
 }
@@ -213,12 +232,12 @@ void execute_impl(const GridParams& g, const Launch<T>& l, cudaStream_t stream) 
 }  // namespace
 
 void interpolate_execute(const GridParams& g, const InterpLaunch& l, cudaStream_t stream) {
-  execute_impl<F32Window>(g, Launch<F32Window>{l.points, l.point_count, l.perm, l.fine, l.batch, l.output},
+  execute_impl<F32Window>(g, Launch<F32Window>{l.points, l.windows, l.point_count, l.perm, l.fine, l.batch, l.output},
                           stream);
 }
 
 void interpolate_execute64(const GridParams& g, const InterpLaunch64& l, cudaStream_t stream) {
-  execute_impl<F64Window>(g, Launch<F64Window>{l.points, l.point_count, l.perm, l.fine, l.batch, l.output},
+  execute_impl<F64Window>(g, Launch<F64Window>{l.points, nullptr, l.point_count, l.perm, l.fine, l.batch, l.output},
                           stream);
 }
 

@@ -11,6 +11,7 @@ namespace b200nufft {
 
 struct InterpLaunch {
   const float* points;    // coordinates in bin (slot) order
+  const void* windows;    // PreparedWindow per slot
   int64_t point_count;
   const uint32_t* perm;   // slot -> original point, in bin order
   const float2* fine;     // batch * fine_count

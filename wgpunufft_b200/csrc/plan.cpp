@@ -114,8 +114,18 @@ NufftPlan::NufftPlan(const b200nufft_config& c, bool with_device) : has_device_(
     throw NufftFailure{B200NUFFT_INVALID_ARGUMENT, "precision must be F64 (1), DF64 (2) or F32 (3)"};
   }
   kernel_ = EsKernel::for_tolerance(eps_, sigma_);
-  tc_enabled_ = type_ == 1 && dim_ == 2 && precision_ == B200NUFFT_PRECISION_F32 &&
-                kernel_.width <= kTcMaxWidth && batch_ >= kTcMinBatch;
+  if (c.spread_method < B200NUFFT_SPREAD_AUTO || c.spread_method > B200NUFFT_SPREAD_TENSOR_CORES) {
+    throw NufftFailure{B200NUFFT_INVALID_ARGUMENT, "spread method must be 0 (auto), 1 (CUDA cores) or 2 (tensor cores)"};
+  }
+  const bool tc_qualifies = type_ == 1 && dim_ == 2 && precision_ == B200NUFFT_PRECISION_F32 &&
+                            kernel_.width <= kTcMaxWidth;
+  if (c.spread_method == B200NUFFT_SPREAD_TENSOR_CORES && !tc_qualifies) {
+    throw NufftFailure{B200NUFFT_INVALID_ARGUMENT,
+                       "tensor-core spreading needs a 2D f32 type-1 plan with a window of at most 8 points"};
+  }
+  tc_enabled_ = tc_qualifies && ((c.spread_method == B200NUFFT_SPREAD_AUTO && batch_ >= kTcMinBatch) ||
+                                 c.spread_method == B200NUFFT_SPREAD_TENSOR_CORES);
+  tc_min_batch_ = c.spread_method == B200NUFFT_SPREAD_TENSOR_CORES ? 1 : kTcMinBatch;
   fine_count_ = 1;
   for (int a = 0; a < dim_; ++a) {
     const uint64_t n = select_fine_grid_size(static_cast<uint64_t>(modes_[a]), sigma_, kernel_.width);
@@ -209,6 +219,17 @@ NufftPlan::NufftPlan(const b200nufft_config& c, bool with_device) : has_device_(
   grid_.half_width64 = kernel_.half_width();
   grid_.horner = horner ? static_cast<const double*>(horner_device_.get()) : nullptr;
   grid_.horner_rows = horner ? horner_.coefficient_count : 0;
+  if (!horner && kernel_.width + 3 <= kHornerRows32 && kernel_.width <= kHornerWidth32) {
+    // f32 plans: the same panels rounded to f32, bottom-aligned in w + 3 rows.
+    const EsHornerTable table = EsHornerTable::fit(kernel_);
+    const int rows = table.coefficient_count;
+    const int first = kHornerRows32 - rows;
+    for (int r = 0; r < rows; ++r) {
+      for (int j = 0; j < kernel_.width; ++j) {
+        grid_.horner32[first + r][j] = static_cast<float>(table.coefficients[r * kernel_.width + j]);
+      }
+    }
+  }
   for (int a = 0; a < dim_; ++a) {
     const double scale = static_cast<double>(fine_[a]) / kTwoPi;
     FoldAxis& axis = grid_.axis[a];
@@ -477,6 +498,11 @@ void NufftPlan::set_points(int64_t count, const void* points, cudaStream_t strea
     float* sorted = static_cast<float*>(sorted_points_.reserve(sorted_bytes, "sorted coordinates"));
     gather_sorted_points(static_cast<const float*>(points), perm_, count, dim_, sorted, stream,
                          &timer_);
+    // The spreader and interpolator read each point's window start and offset.
+    void* windows = windows_.reserve(static_cast<size_t>(std::max<int64_t>(count, 1)) * prepared_window_bytes(dim_),
+                                     "prepared windows");
+    StageScope scope(&timer_, kStageBinOffsets, stream);
+    prepare_windows(sorted, count, grid_, windows, stream);
   } else {
     const double* points64 = static_cast<const double*>(points);
     if (precision_ == B200NUFFT_PRECISION_DF64 && count > 0) {
@@ -595,7 +621,7 @@ void NufftPlan::execute_f32(int batch, const void* input, void* output, uint64_t
       check_cuda(cudaMemsetAsync(output, 0, out_bytes, stream), "zero type-1 output");
       return;
     }
-    if (tc_active_ && batch >= kTcMinBatch) {
+    if (tc_active_ && batch >= tc_min_batch_) {
       const int64_t groups = (batch + kTcVectors - 1) / kTcVectors;
       TcLaunch t;
       t.strengths = static_cast<const float2*>(input);
@@ -626,6 +652,7 @@ void NufftPlan::execute_f32(int batch, const void* input, void* output, uint64_t
                                  spread_.padded_cells * sizeof(float2);
     SpreadLaunch l;
     l.points = static_cast<const float*>(sorted_points_.get());
+    l.windows = windows_.get();
     l.strengths = static_cast<const float2*>(input);
     l.point_count = point_count_;
     l.batch = batch;
@@ -651,6 +678,7 @@ void NufftPlan::execute_f32(int batch, const void* input, void* output, uint64_t
     run_fft(fine, batch, direction, stream);
     InterpLaunch l;
     l.points = static_cast<const float*>(sorted_points_.get());
+    l.windows = windows_.get();
     l.point_count = point_count_;
     l.perm = perm_;
     l.fine = fine;
@@ -744,6 +772,7 @@ void NufftPlan::spread_to(int64_t active_batch, const void* strengths, void* gri
   if (precision_ == B200NUFFT_PRECISION_F32) {
     SpreadLaunch l;
     l.points = static_cast<const float*>(sorted_points_.get());
+    l.windows = windows_.get();
     l.strengths = static_cast<const float2*>(strengths);
     l.point_count = point_count_;
     l.batch = batch;

@@ -105,6 +105,7 @@ class NufftPlan {
   uint32_t* sorted_keys_ = nullptr;
   DeviceBuffer keys_a_, keys_b_, vals_a_, vals_b_, hist_, status_, counters_, offsets_;
   DeviceBuffer sorted_points_;
+  DeviceBuffer windows_;  // f32 plans: PreparedWindow per slot
 
   // Spreading state.
   DeviceBuffer parts_, part_start_, max_bits_, scratch_, candidates_;
@@ -116,6 +117,7 @@ class NufftPlan {
   // enabled by the configuration, active when the chosen bins allow it.
   bool tc_enabled_ = false;
   bool tc_active_ = false;
+  int64_t tc_min_batch_ = kTcMinBatch;  // smallest active batch run on the tensor cores
   DeviceBuffer tc_weights_, tc_inverse_, tc_tile_chunks_, tc_tile_chunk_start_, tc_chunks_;
   DeviceBuffer tc_parts_, tc_part_start_, tc_packed_;
   int64_t tc_part_upper_bound_ = 0;

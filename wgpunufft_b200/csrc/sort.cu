@@ -425,6 +425,67 @@ void gather_sorted_points(const float* points, const uint32_t* perm, int64_t cou
   note_launch();
 }
 
+namespace {
+
+template <int D>
+__global__ void prepare_windows_kernel(const float* __restrict__ sorted, int64_t count, GridParams g,
+                                       PreparedWindow<D>* __restrict__ windows) {
+  const int64_t slot = static_cast<int64_t>(blockIdx.x) * blockDim.x + threadIdx.x;
+  if (slot >= count) return;
+  float p[D];
+#pragma unroll
+  for (int a = 0; a < D; ++a) p[a] = sorted[slot * D + a];
+  bool reach = true;
+#pragma unroll
+  for (int a = 0; a < D; ++a) reach = reach && in_fold_reach(p[a]);
+  PreparedWindow<D> w;
+#pragma unroll
+  for (int a = 0; a < (D == 3 ? 4 : 2); ++a) {
+    w.start[a] = 0;
+    w.offset[a] = 0.0f;
+  }
+  if (reach) {
+#pragma unroll
+    for (int a = 0; a < D; ++a) {
+      int32_t start;
+      Df64 off;
+      support_of(p[a], g.axis[a], g.half_width, start, off);
+      w.start[a] = wrap_start(start, g.axis[a].length);
+      w.offset[a] = __fadd_rn(off.hi, off.lo);
+    }
+  } else {
+    w.start[0] = -1;
+  }
+  windows[slot] = w;
+}
+
+}  // namespace
+
+size_t prepared_window_bytes(int dimensions) {
+  return dimensions == 3 ? sizeof(PreparedWindow<3>) : sizeof(PreparedWindow<2>);
+}
+
+void prepare_windows(const float* sorted_points, int64_t count, const GridParams& grid, void* windows,
+                     cudaStream_t stream) {
+  if (count == 0) return;
+  const unsigned blocks = static_cast<unsigned>((count + 255) / 256);
+  switch (grid.dimensions) {
+    case 1:
+      prepare_windows_kernel<1><<<blocks, 256, 0, stream>>>(sorted_points, count, grid,
+                                                            static_cast<PreparedWindow<1>*>(windows));
+      break;
+    case 2:
+      prepare_windows_kernel<2><<<blocks, 256, 0, stream>>>(sorted_points, count, grid,
+                                                            static_cast<PreparedWindow<2>*>(windows));
+      break;
+    default:
+      prepare_windows_kernel<3><<<blocks, 256, 0, stream>>>(sorted_points, count, grid,
+                                                            static_cast<PreparedWindow<3>*>(windows));
+      break;
+  }
+  note_launch();
+}
+
 size_t sort_status_bytes(int64_t count) {
   const int64_t tiles = (count + kSortTile - 1) / kSortTile;
   return static_cast<size_t>(std::max<int64_t>(tiles, 1)) * kRadix * sizeof(uint32_t);

@@ -35,6 +35,7 @@ constexpr int kSpreadThreads = 256;
 // Precision traits: coordinates, window, fixed-point accumulator.
 
 struct F32Traits {
+  static constexpr bool kPreparedWindows = true;
   using Real = float;
   using Complex = float2;
   using Bits = uint32_t;
@@ -85,6 +86,7 @@ struct F32Traits {
 };
 
 struct F64Traits {
+  static constexpr bool kPreparedWindows = false;
   using Real = double;
   using Complex = double2;
   using Bits = unsigned long long;
@@ -124,6 +126,7 @@ struct F64Traits {
 template <typename T>
 struct SpreadLaunchT {
   const typename T::Real* points;
+  const void* windows;
   const typename T::Complex* strengths;
   int64_t point_count;
   int batch;
@@ -243,11 +246,11 @@ __host__ __device__ constexpr int spread_run() {
 // wider than the tile).
 template <int D, int W, typename T>
 __device__ __forceinline__ bool tile_record(const SpreadParams& sp, const typename T::Real* points,
-                                            const typename T::Complex* sv, const uint32_t* perm,
-                                            const uint32_t* row_begin, const uint32_t* row_prefix,
-                                            int rows, const int* origin, uint32_t r, int& row,
-                                            int* local_start, typename T::Real (*w)[W],
-                                            typename T::Complex& s) {
+                                            const void* windows, const typename T::Complex* sv,
+                                            const uint32_t* perm, const uint32_t* row_begin,
+                                            const uint32_t* row_prefix, int rows, const int* origin,
+                                            uint32_t r, int& row, int* local_start,
+                                            typename T::Real (*w)[W], typename T::Complex& s) {
   using Real = typename T::Real;
   // Advance to the row holding record r (rows are visited in order).
   if (r >= row_prefix[row + 1] || r < row_prefix[row]) {
@@ -259,6 +262,22 @@ __device__ __forceinline__ bool tile_record(const SpreadParams& sp, const typena
     row = low;
   }
   const uint32_t slot = row_begin[row] + (r - row_prefix[row]);
+  if constexpr (T::kPreparedWindows) {
+    // f32 plans: the window start and offset prepared at set_points.
+    const PreparedWindow<D> win = static_cast<const PreparedWindow<D>*>(windows)[slot];
+    if (win.start[0] < 0) return false;  // outside the fold reach: weighed zero
+    bool inside = true;
+#pragma unroll
+    for (int a = 0; a < D; ++a) {
+      local_start[a] = win.start[a] - origin[a];
+      inside = inside && local_start[a] >= 0 && local_start[a] < sp.tile[a];
+    }
+    if (!inside) return false;  // a bin wider than the tile: another tile owns it
+#pragma unroll
+    for (int a = 0; a < D; ++a) horner32_window<W>(win.offset[a], sp.grid.horner32, w[a]);
+    s = sv[perm[slot]];
+    return true;
+  }
   Real p[D];
 #pragma unroll
   for (int a = 0; a < D; ++a) p[a] = points[static_cast<int64_t>(slot) * D + a];
@@ -301,7 +320,7 @@ __device__ __forceinline__ void flush_run(typename T::Word* acc, int padded, int
 // of fixed-point sums and writes the tile out in floating point.
 template <int D, int W, typename T>
 __global__ void __launch_bounds__(kSpreadThreads, (spread_run<D, W, T>() > 1 || sizeof(typename T::Real) == 8 ? 2 : 3)) spread_tiles_kernel(
-    SpreadParams sp, const typename T::Real* __restrict__ points,
+    SpreadParams sp, const typename T::Real* __restrict__ points, const void* __restrict__ windows,
     const typename T::Complex* __restrict__ strengths, int64_t point_count, int batch,
     const uint32_t* __restrict__ perm, const uint32_t* __restrict__ offsets,
     const uint32_t* __restrict__ part_start, const typename T::Bits* __restrict__ max_bits,
@@ -416,7 +435,7 @@ __global__ void __launch_bounds__(kSpreadThreads, (spread_run<D, W, T>() > 1 || 
       int local_start[D];
       Real w[D][W];
       typename T::Complex s;
-      if (!tile_record<D, W, T>(sp, points, sv, perm, row_begin, row_prefix, rows, origin, r, row,
+      if (!tile_record<D, W, T>(sp, points, windows, sv, perm, row_begin, row_prefix, rows, origin, r, row,
                                 local_start, w, s)) {
         continue;
       }
@@ -482,8 +501,8 @@ __global__ void __launch_bounds__(kSpreadThreads, (spread_run<D, W, T>() > 1 || 
         int local_start[D];
         Real w[D][W];
         typename T::Complex s;
-        if (!tile_record<D, W, T>(sp, points, sv, perm, row_begin, row_prefix, rows, origin, r, row,
-                                  local_start, w, s)) {
+        if (!tile_record<D, W, T>(sp, points, windows, sv, perm, row_begin, row_prefix, rows, origin, r,
+                                  row, local_start, w, s)) {
           continue;
         }
         const int l1 = D == 2 ? local_start[D - 1] : 0;
@@ -635,7 +654,7 @@ void launch_spread_width(const SpreadParams& sp, const SpreadLaunchT<T>& l, cuda
                                   static_cast<int>(smem)),
              "spread shared memory");
   const dim3 grid(static_cast<unsigned>(l.part_upper_bound), static_cast<unsigned>(l.batch));
-  kernel<<<grid, kSpreadThreads, smem, stream>>>(sp, l.points, l.strengths, l.point_count, l.batch,
+  kernel<<<grid, kSpreadThreads, smem, stream>>>(sp, l.points, l.windows, l.strengths, l.point_count, l.batch,
                                                  l.perm, l.offsets, l.part_start, l.max_bits,
                                                  l.scratch);
   note_launch();
@@ -716,7 +735,7 @@ void spread_fold(const SpreadParams& sp, int batch, const float2* scratch, const
 
 void spread_execute(const SpreadParams& sp, const SpreadLaunch& l, cudaStream_t stream,
                     StageTimer* timer) {
-  SpreadLaunchT<F32Traits> t{l.points,   l.strengths,        l.point_count, l.batch,
+  SpreadLaunchT<F32Traits> t{l.points,   l.windows,  l.strengths,        l.point_count, l.batch,
                              l.perm,     l.offsets,          l.part_start,  l.part_upper_bound,
                              l.max_bits, l.scratch,          l.candidates,  l.fine};
   spread_execute_impl<F32Traits>(sp, t, stream, timer);
@@ -724,7 +743,7 @@ void spread_execute(const SpreadParams& sp, const SpreadLaunch& l, cudaStream_t 
 
 void spread_execute64(const SpreadParams& sp, const SpreadLaunch64& l, cudaStream_t stream,
                       StageTimer* timer) {
-  SpreadLaunchT<F64Traits> t{l.points,   l.strengths,        l.point_count, l.batch,
+  SpreadLaunchT<F64Traits> t{l.points,   nullptr,    l.strengths,        l.point_count, l.batch,
                              l.perm,     l.offsets,          l.part_start,  l.part_upper_bound,
                              l.max_bits, l.scratch,          l.candidates,  l.fine};
   spread_execute_impl<F64Traits>(sp, t, stream, timer);

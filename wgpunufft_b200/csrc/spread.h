@@ -33,6 +33,7 @@ struct SpreadParams {
 
 struct SpreadLaunch {
   const float* points;    // coordinates in bin (slot) order
+  const void* windows;    // PreparedWindow per slot
   const float2* strengths;
   int64_t point_count;
   int batch;

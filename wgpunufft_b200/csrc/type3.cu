@@ -279,6 +279,8 @@ Type3Plan::Type3Plan(const b200nufft_type3_config& c) {
   outer.sigma = sigma_;
   outer.precision = inner_precision;
   outer.device = c.device;
+  // The outer spread runs through spread_to, on the CUDA cores.
+  outer.spread_method = B200NUFFT_SPREAD_CUDA_CORES;
   b200nufft_config inner = outer;
   inner.type = 2;
   for (int a = 0; a < dim_; ++a) {

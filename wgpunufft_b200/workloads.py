@@ -1,0 +1,106 @@
+"""Seeded synthetic workloads with the shapes of the reference's benchmark
+configurations, generated on the GPU, and a runner for profiling them.
+
+    python -m wgpunufft_b200.workloads CASE [--batch B] [--executes N] [--kind 1|2|both]
+
+Cases:
+  small     2D 64^2 modes, 1e5 uniform points, eps 1e-6
+  uniform   2D 1024^2 modes, 1e7 uniform points, eps 1e-5
+  clustered 2D 1024^2 modes, 1e7 points around 8 centres (N(c, 0.01^2 I), wrapped), eps 1e-5
+  radial    3D 256^3 modes, 4096 spokes x 12207 samples (radius linear in [-pi, pi),
+            directions uniform on the sphere, +-1e-3 jitter), eps 1e-5
+  batched   2D 512^2 modes, 2e6 uniform points, eps 1e-6, --batch vectors (default 64)
+
+Points are f32 point-major in [-pi, pi); strengths and modes complex64 with
+N(0, 1) real and imaginary parts. No external dataset is involved.
+"""
+
+from __future__ import annotations
+
+import argparse
+import math
+
+CASES = {
+    "small": ((64, 64), 100_000, 1e-6, "uniform"),
+    "uniform": ((1024, 1024), 10_000_000, 1e-5, "uniform"),
+    "clustered": ((1024, 1024), 10_000_000, 1e-5, "clustered"),
+    "radial": ((256, 256, 256), 4096 * 12207, 1e-5, "radial"),
+    "batched": ((512, 512), 2_000_000, 1e-6, "uniform"),
+}
+
+
+def points(kind: str, count: int, dims: int, seed: int = 7, device: str = "cuda"):
+    """Seeded f32 points (count, dims) of the given distribution on `device`."""
+    import torch
+
+    g = torch.Generator(device=device)
+    g.manual_seed(seed)
+    two_pi = 2.0 * math.pi
+    if kind == "uniform":
+        p = torch.rand((count, dims), generator=g, device=device, dtype=torch.float64) * two_pi - math.pi
+    elif kind == "clustered":
+        centres = torch.rand((8, dims), generator=g, device=device, dtype=torch.float64) * two_pi - math.pi
+        which = torch.randint(0, 8, (count,), generator=g, device=device)
+        p = centres[which] + 0.01 * torch.randn((count, dims), generator=g, device=device, dtype=torch.float64)
+        p = torch.remainder(p + math.pi, two_pi) - math.pi
+    elif kind == "radial":
+        spokes, per = 4096, count // 4096
+        v = torch.randn((spokes, 3), generator=g, device=device, dtype=torch.float64)
+        v = v / v.norm(dim=1, keepdim=True)
+        r = torch.linspace(-math.pi, math.pi, per + 1, device=device, dtype=torch.float64)[:-1]
+        p = (v[:, None, :] * r[None, :, None]).reshape(-1, 3)
+        p = p + (torch.rand(p.shape, generator=g, device=device, dtype=torch.float64) * 2e-3 - 1e-3)
+        p = torch.clamp(p, -math.pi, math.pi - 1e-6)
+    else:
+        raise ValueError(f"unknown point distribution {kind!r}")
+    return p.to(torch.float32).contiguous()
+
+
+def values(batch: int, count: int, seed: int = 8, device: str = "cuda"):
+    """Seeded complex64 values (batch, count) with N(0, 1) parts."""
+    import torch
+
+    g = torch.Generator(device=device)
+    g.manual_seed(seed)
+    return torch.complex(torch.randn((batch, count), generator=g, device=device),
+                         torch.randn((batch, count), generator=g, device=device))
+
+
+def run(case: str, batch: int, executes: int, kinds) -> None:
+    import torch
+
+    import wgpunufft_b200 as w
+
+    modes, count, eps, dist = CASES[case]
+    p = points(dist, count, len(modes))
+    n = 1
+    for m in modes:
+        n *= m
+    for kind in kinds:
+        config = w.NufftConfig(modes, eps, batch=batch)
+        plan = (w.NufftPlan.type1_gpu if kind == 1 else w.NufftPlan.type2_gpu)(config)
+        plan.set_points_gpu(p)
+        inputs = values(batch, count if kind == 1 else n)
+        out = torch.empty((batch, n if kind == 1 else count), dtype=torch.complex64, device="cuda")
+        for _ in range(executes):
+            plan.execute_gpu_batch(batch, inputs, out)
+        plan.synchronize()
+        del plan, inputs, out
+    torch.cuda.synchronize()
+
+
+def main() -> None:
+    parser = argparse.ArgumentParser(description=__doc__, formatter_class=argparse.RawDescriptionHelpFormatter)
+    parser.add_argument("case", choices=sorted(CASES))
+    parser.add_argument("--batch", type=int, default=None)
+    parser.add_argument("--executes", type=int, default=2)
+    parser.add_argument("--kind", choices=["1", "2", "both"], default="both")
+    args = parser.parse_args()
+    batch = args.batch if args.batch is not None else (64 if args.case == "batched" else 1)
+    kinds = (1, 2) if args.kind == "both" else (int(args.kind),)
+    run(args.case, batch, args.executes, kinds)
+    print("ok")
+
+
+if __name__ == "__main__":
+    main()
