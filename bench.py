@@ -151,6 +151,24 @@ class ClockSampler:
                 "reasons": reasons, "samples": len(rows)}
 
 
+def max_over_ranks(values, device="cpu"):
+    """The maximum of each value over all ranks (the slowest replica's time);
+    the values themselves on a single process."""
+    import torch
+    import torch.distributed as dist
+
+    if not (dist.is_available() and dist.is_initialized()) or dist.get_world_size() == 1:
+        return list(values)
+    t = torch.tensor(list(values), dtype=torch.float64, device=device)
+    dist.all_reduce(t, op=dist.ReduceOp.MAX)
+    return t.tolist()
+
+
+def replica_throughput(world, units_per_replica, total_ms, steps):
+    """Whole-job units/s of `world` independent replicas timed at the slowest one."""
+    return world * units_per_replica / (total_ms / steps / 1e3)
+
+
 def c_interface_e2e(w, torch, points_h, strengths_h, timed, barrier, world, dev, args):
     """NU points/s of wgpu_nufftf_setpts + wgpu_nufftf_execute on pinned host arrays."""
     import ctypes
@@ -187,13 +205,8 @@ def c_interface_e2e(w, torch, points_h, strengths_h, timed, barrier, world, dev,
         lib.wgpu_nufftf_destroy(plan)
     if failures:
         return {"error": failures[0]}
-    if world > 1:
-        import torch.distributed as dist
-
-        t = torch.tensor([e2e_ms], device=dev)
-        dist.all_reduce(t, op=dist.ReduceOp.MAX)
-        e2e_ms = t.item()
-    return {"value": world * POINTS / (e2e_ms / args.steps / 1e3), "unit": UNIT,
+    (e2e_ms,) = max_over_ranks([e2e_ms], dev)
+    return {"value": replica_throughput(world, POINTS, e2e_ms, args.steps), "unit": UNIT,
             "ms_per_step": e2e_ms / args.steps,
             "h2d_bytes_per_step": POINTS * 4 * 2 + POINTS * 8, "d2h_bytes_per_step": MODES[0] * MODES[1] * 8,
             "path": "C interface wgpu_nufftf_setpts (per-axis f32, pinned host) + wgpu_nufftf_execute, "
@@ -234,14 +247,9 @@ def batched_comparison(w, torch, timed, barrier, world, dev, args, rank):
             total = timed(lambda: plan.execute_gpu_batch(batch, c, out), steps)
             stages = plan.stage_report()
             plan.stage_timing(False)
-            if world > 1:
-                import torch.distributed as dist
-
-                t = torch.tensor([total], device=dev)
-                dist.all_reduce(t, op=dist.ReduceOp.MAX)
-                total = t.item()
+            (total,) = max_over_ranks([total], dev)
             ms = total / steps
-            item = {"value": world * BATCH_POINTS * batch / (ms / 1e3), "ms_per_step": ms,
+            item = {"value": replica_throughput(world, BATCH_POINTS * batch, total, steps), "ms_per_step": ms,
                     "stages_ms_per_step": {k: v[0] / steps for k, v in stages.items()}}
             if rank == 0:
                 from oracle import native
@@ -342,13 +350,10 @@ def main():
         one_shot_ms = timed(lambda: plan.encode_type1_gpu(points, strengths, out), args.steps)
     barrier()
     clock_summary = clocks.summary()
-    if world > 1:
-        t = torch.tensor([total_ms, one_shot_ms], device=dev)
-        dist.all_reduce(t, op=dist.ReduceOp.MAX)
-        total_ms, one_shot_ms = t.tolist()
+    total_ms, one_shot_ms = max_over_ranks([total_ms, one_shot_ms], dev)
     ms = total_ms / args.steps
-    value = world * POINTS / (ms / 1e3)
-    one_shot = world * POINTS / (one_shot_ms / args.steps / 1e3)
+    value = replica_throughput(world, POINTS, total_ms, args.steps)
+    one_shot = replica_throughput(world, POINTS, one_shot_ms, args.steps)
 
     # Type 2 on the same points (reported beside the headline, same timing rules).
     plan2 = w.NufftPlan.type2_gpu(config, device=local)
@@ -365,13 +370,10 @@ def main():
     stages2 = plan2.stage_report()
     plan2.stage_timing(False)
     type2_one_shot_ms = timed(lambda: plan2.encode_type2_gpu(points, coefficients, values), args.steps)
-    if world > 1:
-        t = torch.tensor([type2_ms, type2_one_shot_ms], device=dev)
-        dist.all_reduce(t, op=dist.ReduceOp.MAX)
-        type2_ms, type2_one_shot_ms = t.tolist()
-    type2 = {"value": world * POINTS / (type2_ms / args.steps / 1e3), "unit": UNIT,
+    type2_ms, type2_one_shot_ms = max_over_ranks([type2_ms, type2_one_shot_ms], dev)
+    type2 = {"value": replica_throughput(world, POINTS, type2_ms, args.steps), "unit": UNIT,
              "ms_per_step": type2_ms / args.steps,
-             "one_shot_value": world * POINTS / (type2_one_shot_ms / args.steps / 1e3),
+             "one_shot_value": replica_throughput(world, POINTS, type2_one_shot_ms, args.steps),
              "stages_ms_per_step": {k: v[0] / args.steps for k, v in stages2.items()}}
 
     # Accuracy of this output against FP64 direct sums on 16 seeded modes.
