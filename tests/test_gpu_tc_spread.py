@@ -101,3 +101,26 @@ def test_empty_and_single_point_sets():
     got = _run(plan, points, c, 16)
     ref = native.direct_type1(points.astype(np.float64), c.astype(np.complex128), (32, 32), 1)
     assert rel_l2(got, ref) < 1e-5
+
+
+@pytest.mark.parametrize("eps", [1e-3, 1e-6])
+def test_batched_type2_bins_match_single_vectors_bit_for_bit(eps):
+    """Batched 2D f32 type-2 plans stage bin regions in shared memory; every
+    vector equals its single-vector execution bit for bit."""
+    rng = np.random.default_rng(int(-np.log10(eps)) + 40)
+    points = np.concatenate([uniform_points(rng, 6000, 2), clustered_points(rng, 3000, 2, centres=3, spread=0.02)])
+    batch, modes = 40, (48, 36)
+    f = _strengths(rng, batch, modes[0] * modes[1])
+    plan = w.NufftPlan.type2_gpu(w.NufftConfig(modes, eps, batch=batch))
+    p = torch.from_numpy(points).to(DEV)
+    plan.set_points_gpu(p)
+    fin = torch.from_numpy(f).to(DEV)
+    out = torch.empty((batch, len(points)), dtype=torch.complex64, device=DEV)
+    plan.execute_gpu_batch(batch, fin, out)
+    one = torch.empty((1, len(points)), dtype=torch.complex64, device=DEV)
+    for b in (0, 17, 39):
+        plan.execute_gpu_batch(1, fin[b:b + 1].contiguous(), one)
+        assert torch.equal(one[0].view(torch.int32), out[b].view(torch.int32)), b
+    torch.cuda.synchronize()
+    ref = native.direct_type2(points.astype(np.float64), f[:4].astype(np.complex128), modes, 1)
+    assert rel_l2(out[:4].cpu().numpy(), ref) < 20 * eps

@@ -76,6 +76,8 @@ struct GridParams {
 void prepare_windows(const float* sorted_points, int64_t count, const GridParams& grid, void* windows,
                      cudaStream_t stream);
 size_t prepared_window_bytes(int dimensions);
+// inverse[perm[s]] = s for s < count.
+void invert_permutation(const uint32_t* perm, int64_t count, uint32_t* inverse, cudaStream_t stream);
 
 // Stable sort of the points by bin key. Launches on `stream`; all pointers
 // are device pointers owned by the caller.

@@ -179,6 +179,171 @@ __global__ void __launch_bounds__(256, InterpBlocks<D, W, T>::value)
   }
 }
 
+// Batched 2D f32 interpolation: one CTA per (8 x 8-cell bin, 32 vectors).
+// The fine-grid region that the bin's windows can reach (8 + w + 3 cells per
+// axis; the bins come from f32 approximate cells, so the exact starts may lie
+// one cell beyond the bin) is staged in shared memory with the 32 vectors of a
+// cell contiguous, and a warp serves one point at a time with one vector per
+// lane, summing in the order of interpolate_kernel (bitwise the same values).
+constexpr int kBinVectors = 32;
+constexpr int kBinPitch = kBinVectors + 1;  // float2 per staged cell, padded against bank conflicts
+
+template <int W>
+__host__ __device__ constexpr int bin_region_side() { return 8 + W + 3; }
+
+template <int W>
+__global__ void __launch_bounds__(256) interpolate_bins_kernel(GridParams g, const void* __restrict__ windows,
+                                                               int64_t count, const uint32_t* __restrict__ perm,
+                                                               const uint32_t* __restrict__ offsets,
+                                                               const float2* __restrict__ fine, int batch,
+                                                               float2* __restrict__ staged, int64_t staged_stride) {
+  constexpr int S = bin_region_side<W>();
+  extern __shared__ float2 region[];  // S * S cells x kBinPitch
+  const int64_t bin = blockIdx.x;
+  const uint32_t first = offsets[bin], last = offsets[bin + 1];
+  if (first == last) return;
+  const int vb = blockIdx.y * kBinVectors;
+  const int nv = min(kBinVectors, batch - vb);
+  const int bins0 = static_cast<int>(g.axis[0].bins);
+  const int n0 = g.axis[0].length, n1 = g.axis[1].length;
+  const int ox = static_cast<int>(bin % bins0) * 8 - W / 2 - 2;
+  const int oy = static_cast<int>(bin / bins0) * 8 - W / 2 - 2;
+  // Eight independent loads in flight per thread before their stores.
+  constexpr int kLoads = 8;
+  constexpr int kTotal = S * S * kBinVectors;
+  for (int base = threadIdx.x; base < kTotal; base += kLoads * 256) {
+    float2 value[kLoads];
+#pragma unroll
+    for (int q = 0; q < kLoads; ++q) {
+      const int e = base + q * 256;
+      value[q] = make_float2(0.0f, 0.0f);
+      const int v = e / (S * S), cell = e - v * (S * S);
+      if (e < kTotal && v < nv) {
+        const int r = cell / S, c = cell - r * S;
+        int y = (oy + r) % n1;
+        y = y < 0 ? y + n1 : y;
+        int x = (ox + c) % n0;
+        x = x < 0 ? x + n0 : x;
+        value[q] = __ldg(&fine[static_cast<int64_t>(vb + v) * g.fine_count + static_cast<int64_t>(y) * n0 + x]);
+      }
+    }
+#pragma unroll
+    for (int q = 0; q < kLoads; ++q) {
+      const int e = base + q * 256;
+      if (e < kTotal) {
+        const int v = e / (S * S), cell = e - v * (S * S);
+        region[cell * kBinPitch + v] = value[q];
+      }
+    }
+  }
+  __syncthreads();
+  const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
+  const float2* grid = fine + static_cast<int64_t>(vb + min(lane, nv - 1)) * g.fine_count;
+  // The bin's windows and point indices, 256 at a time, staged by one load per thread.
+  __shared__ PreparedWindow<2> s_win[256];
+  __shared__ uint32_t s_point[256];
+  for (uint32_t batch_first = first; batch_first < last; batch_first += 256) {
+  const uint32_t batch_last = min(last, batch_first + 256);
+  __syncthreads();
+  if (batch_first + threadIdx.x < batch_last) {
+    s_win[threadIdx.x] = static_cast<const PreparedWindow<2>*>(windows)[batch_first + threadIdx.x];
+    s_point[threadIdx.x] = perm[batch_first + threadIdx.x];
+  }
+  __syncthreads();
+  for (uint32_t slot = batch_first + warp; slot < batch_last; slot += blockDim.x >> 5) {
+    const PreparedWindow<2> win = s_win[slot - batch_first];
+    const uint32_t point = s_point[slot - batch_first];
+    float re = 0.0f, im = 0.0f;
+    if (win.start[0] >= 0) {
+      float wx[W], wy[W];
+      horner32_window<W>(win.offset[0], g.horner32, wx);
+      horner32_window<W>(win.offset[1], g.horner32, wy);
+      int dx = (win.start[0] - ox) % n0;
+      dx = dx < 0 ? dx + n0 : dx;
+      int dy = (win.start[1] - oy) % n1;
+      dy = dy < 0 ? dy + n1 : dy;
+      if (dx + W <= S && dy + W <= S) {
+#pragma unroll
+        for (int j = 0; j < W; ++j) {
+          const float2* row = region + ((dy + j) * S + dx) * kBinPitch + lane;
+          float rr = 0.0f, ri = 0.0f;
+#pragma unroll
+          for (int i = 0; i < W; ++i) {
+            const float2 v = row[i * kBinPitch];
+            rr = fmaf(v.x, wx[i], rr);
+            ri = fmaf(v.y, wx[i], ri);
+          }
+          re = fmaf(rr, wy[j], re);
+          im = fmaf(ri, wy[j], im);
+        }
+      } else {
+        // A window beyond the staged region: read the grid directly.
+#pragma unroll 1
+        for (int j = 0; j < W; ++j) {
+          int y = win.start[1] + j;
+          y = y >= n1 ? y - n1 : y;
+          float rr = 0.0f, ri = 0.0f;
+          for (int i = 0; i < W; ++i) {
+            int x = win.start[0] + i;
+            x = x >= n0 ? x - n0 : x;
+            const float2 v = __ldg(&grid[static_cast<int64_t>(y) * n0 + x]);
+            rr = fmaf(v.x, wx[i], rr);
+            ri = fmaf(v.y, wx[i], ri);
+          }
+          re = fmaf(rr, wy[j], re);
+          im = fmaf(ri, wy[j], im);
+        }
+      }
+    }
+    if (lane < nv) staged[static_cast<int64_t>(slot) * staged_stride + vb + lane] = make_float2(re, im);
+    (void)point;
+  }
+  }
+}
+
+// output[b][i] = staged[slot of i][b]: 32 points x 64 vectors per CTA through
+// shared memory, so both the staged rows and the output rows move in whole
+// sectors.
+__global__ void __launch_bounds__(256) unpermute_kernel(const float2* __restrict__ staged, int64_t staged_stride,
+                                                        const uint32_t* __restrict__ inverse, int64_t count,
+                                                        int batch, float2* __restrict__ output) {
+  __shared__ float2 tile[32][65];
+  __shared__ uint32_t rows[32];
+  const int64_t i0 = static_cast<int64_t>(blockIdx.x) * 32;
+  const int b0 = blockIdx.y * 64;
+  if (threadIdx.x < 32) rows[threadIdx.x] = i0 + threadIdx.x < count ? inverse[i0 + threadIdx.x] : 0u;
+  __syncthreads();
+#pragma unroll
+  for (int q = 0; q < 8; ++q) {
+    const int e = threadIdx.x + q * 256;
+    const int k = e >> 6, v = e & 63;
+    if (i0 + k < count && b0 + v < batch) tile[k][v] = staged[static_cast<int64_t>(rows[k]) * staged_stride + b0 + v];
+  }
+  __syncthreads();
+#pragma unroll
+  for (int q = 0; q < 8; ++q) {
+    const int e = threadIdx.x + q * 256;
+    const int v = e >> 5, k = e & 31;
+    if (i0 + k < count && b0 + v < batch) output[static_cast<int64_t>(b0 + v) * count + i0 + k] = tile[k][v];
+  }
+}
+
+template <int W>
+void launch_bins_width(const GridParams& g, const InterpBinsLaunch& l, cudaStream_t stream) {
+  constexpr int S = bin_region_side<W>();
+  const size_t smem = static_cast<size_t>(S) * S * kBinPitch * sizeof(float2);
+  auto kernel = interpolate_bins_kernel<W>;
+  check_cuda(cudaFuncSetAttribute(kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, static_cast<int>(smem)),
+             "interpolation region shared memory");
+  const dim3 grid(static_cast<unsigned>(l.bins), static_cast<unsigned>((l.batch + kBinVectors - 1) / kBinVectors));
+  const int64_t stride = (l.batch + kBinVectors - 1) / kBinVectors * kBinVectors;
+  kernel<<<grid, 256, smem, stream>>>(g, l.windows, l.point_count, l.perm, l.offsets, l.fine, l.batch, l.staged,
+                                      stride);
+  const dim3 grid2(static_cast<unsigned>((l.point_count + 31) / 32), static_cast<unsigned>((l.batch + 63) / 64));
+  unpermute_kernel<<<grid2, 256, 0, stream>>>(l.staged, stride, l.inverse, l.point_count, l.batch, l.output);
+  note_launch(2);
+}
+
 template <typename T>
 struct Launch {
   const typename T::Real* points;
@@ -234,6 +399,23 @@ void execute_impl(const GridParams& g, const Launch<T>& l, cudaStream_t stream) 
 void interpolate_execute(const GridParams& g, const InterpLaunch& l, cudaStream_t stream) {
   execute_impl<F32Window>(g, Launch<F32Window>{l.points, l.windows, l.point_count, l.perm, l.fine, l.batch, l.output},
                           stream);
+}
+
+bool interpolate_bins_supported(const GridParams& g) {
+  return g.dimensions == 2 && g.width <= 8 && g.axis[0].shift == 3 && g.axis[1].shift == 3;
+}
+
+void interpolate_bins_execute(const GridParams& g, const InterpBinsLaunch& l, cudaStream_t stream) {
+  if (l.point_count == 0) return;
+  switch (g.width) {
+    case 2: launch_bins_width<2>(g, l, stream); break;
+    case 3: launch_bins_width<3>(g, l, stream); break;
+    case 4: launch_bins_width<4>(g, l, stream); break;
+    case 5: launch_bins_width<5>(g, l, stream); break;
+    case 6: launch_bins_width<6>(g, l, stream); break;
+    case 7: launch_bins_width<7>(g, l, stream); break;
+    default: launch_bins_width<8>(g, l, stream); break;
+  }
 }
 
 void interpolate_execute64(const GridParams& g, const InterpLaunch64& l, cudaStream_t stream) {

@@ -29,6 +29,24 @@ struct InterpLaunch64 {
 };
 
 void interpolate_execute(const GridParams& g, const InterpLaunch& launch, cudaStream_t stream);
+
+// Batched 2D f32 interpolation over the type-2 bins (8 x 8 cells): the
+// reachable fine-grid region of a bin is staged in shared memory for 32
+// vectors at a time. Same values, bit for bit, as interpolate_execute.
+struct InterpBinsLaunch {
+  const void* windows;      // PreparedWindow per slot
+  int64_t point_count;
+  const uint32_t* perm;
+  const uint32_t* offsets;  // bins + 1 slot offsets
+  uint64_t bins;
+  const float2* fine;
+  int batch;
+  float2* output;
+  const uint32_t* inverse;  // slot of every point
+  float2* staged;           // point_count x round_up(batch, 32), slot order
+};
+bool interpolate_bins_supported(const GridParams& g);
+void interpolate_bins_execute(const GridParams& g, const InterpBinsLaunch& launch, cudaStream_t stream);
 void interpolate_execute64(const GridParams& g, const InterpLaunch64& launch, cudaStream_t stream);
 
 }  // namespace b200nufft

@@ -20,6 +20,8 @@ constexpr int32_t kPartCap = 4096;
 constexpr int64_t kTileBytesTarget = 100 * 1024;
 // Points one plan can bin: look-back words hold 30-bit counts.
 constexpr int64_t kMaxPoints = (int64_t(1) << 30) - 1;
+// Active batches from which 2D f32 type-2 plans stage bin regions in shared memory.
+constexpr int kInterpBinsMinBatch = 8;
 
 int64_t mode_for_storage_index(int order, int64_t index, int64_t length) {
   // src/direct.rs:120-131
@@ -503,6 +505,11 @@ void NufftPlan::set_points(int64_t count, const void* points, cudaStream_t strea
                                      "prepared windows");
     StageScope scope(&timer_, kStageBinOffsets, stream);
     prepare_windows(sorted, count, grid_, windows, stream);
+    if (type_ == 2 && dim_ == 2 && batch_ >= kInterpBinsMinBatch) {
+      void* inverse = inverse_.reserve(static_cast<size_t>(std::max<int64_t>(count, 1)) * sizeof(uint32_t),
+                                       "point slots");
+      invert_permutation(perm_, count, static_cast<uint32_t*>(inverse), stream);
+    }
   } else {
     const double* points64 = static_cast<const double*>(points);
     if (precision_ == B200NUFFT_PRECISION_DF64 && count > 0) {
@@ -676,6 +683,24 @@ void NufftPlan::execute_f32(int batch, const void* input, void* output, uint64_t
                         static_cast<const float*>(amplitudes_.get()), fine, stream);
     }
     run_fft(fine, batch, direction, stream);
+    if (dim_ == 2 && batch >= kInterpBinsMinBatch && interpolate_bins_supported(grid_)) {
+      InterpBinsLaunch b;
+      b.windows = windows_.get();
+      b.point_count = point_count_;
+      b.perm = perm_;
+      b.offsets = static_cast<const uint32_t*>(offsets_.get());
+      b.bins = bins_;
+      b.fine = fine;
+      b.batch = batch;
+      b.output = static_cast<float2*>(output);
+      b.inverse = static_cast<const uint32_t*>(inverse_.get());
+      b.staged = static_cast<float2*>(staged_.reserve(
+          static_cast<size_t>(std::max<int64_t>(point_count_, 1)) * ((batch + 31) / 32 * 32) * sizeof(float2),
+          "staged type-2 values"));
+      StageScope scope(&timer_, kStageInterpolation, stream);
+      interpolate_bins_execute(grid_, b, stream);
+      return;
+    }
     InterpLaunch l;
     l.points = static_cast<const float*>(sorted_points_.get());
     l.windows = windows_.get();

@@ -106,6 +106,8 @@ class NufftPlan {
   DeviceBuffer keys_a_, keys_b_, vals_a_, vals_b_, hist_, status_, counters_, offsets_;
   DeviceBuffer sorted_points_;
   DeviceBuffer windows_;  // f32 plans: PreparedWindow per slot
+  DeviceBuffer inverse_;  // batched 2D f32 type-2 plans: slot of every point
+  DeviceBuffer staged_;   // batched 2D f32 type-2 plans: values in slot order
 
   // Spreading state.
   DeviceBuffer parts_, part_start_, max_bits_, scratch_, candidates_;

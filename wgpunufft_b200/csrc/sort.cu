@@ -461,6 +461,20 @@ __global__ void prepare_windows_kernel(const float* __restrict__ sorted, int64_t
 
 }  // namespace
 
+namespace {
+__global__ void invert_permutation_kernel(const uint32_t* __restrict__ perm, int64_t count,
+                                          uint32_t* __restrict__ inverse) {
+  const int64_t s = static_cast<int64_t>(blockIdx.x) * blockDim.x + threadIdx.x;
+  if (s < count) inverse[perm[s]] = static_cast<uint32_t>(s);
+}
+}  // namespace
+
+void invert_permutation(const uint32_t* perm, int64_t count, uint32_t* inverse, cudaStream_t stream) {
+  if (count == 0) return;
+  invert_permutation_kernel<<<static_cast<unsigned>((count + 255) / 256), 256, 0, stream>>>(perm, count, inverse);
+  note_launch();
+}
+
 size_t prepared_window_bytes(int dimensions) {
   return dimensions == 3 ? sizeof(PreparedWindow<3>) : sizeof(PreparedWindow<2>);
 }
