@@ -3,9 +3,10 @@
 // Per point set (set_points): the window of every point in slot order
 // (support start and w weights per axis), the slot of every original index,
 // and a table of chunks: up to eight consecutive slots of one bin row of a
-// tile. Tiles are 8 cells wide and 33 - w rows high, so that a padded tile
-// ((8 + w - 1) x 32 cells at a row pitch of 16 columns) fits the 512
-// tensor-memory columns of one SM.
+// tile. Tiles are 8 cells wide and 17 - w rows high, so that a padded tile
+// ((8 + w - 1) x 16 cells at a row pitch of 16 columns) fits 256
+// tensor-memory columns: two CTAs share an SM, so one CTA's setup and
+// read-out overlap the other's MMAs.
 //
 // Per execution: the strengths of 64 vectors are packed point-major in slot
 // order (128 floats per point: real and imaginary parts interleaved), so a
@@ -35,10 +36,10 @@ namespace {
 constexpr int kTcTeams = 4;          // converter teams, each converting every fourth chunk
 constexpr int kTcTeamThreads = 64;
 constexpr int kTcThreads = 64 + kTcTeams * kTcTeamThreads;  // producer warp, MMA warp, converters
-constexpr int kTcCopyStages = 20;    // chunks whose copies are in flight or unread
-constexpr int kTcOperandStages = 6;  // chunks whose MMAs may still read their operands
+constexpr int kTcCopyStages = 8;     // chunks whose copies are in flight or unread
+constexpr int kTcOperandStages = 4;  // chunks whose MMAs may still read their operands
 constexpr uint32_t kSpinLimit = 1u << 22;
-constexpr size_t kTcSharedBytes = 200 * 1024;  // one CTA per SM: it holds all 512 columns
+constexpr size_t kTcSharedBytes = 108 * 1024;  // two CTAs per SM, 256 tensor-memory columns each
 
 __device__ __forceinline__ uint32_t smem_u32(const void* p) {
   return static_cast<uint32_t>(__cvta_generic_to_shared(p));
@@ -331,7 +332,7 @@ __device__ __forceinline__ void tc_convert(const TcChunk& ch, const unsigned cha
 // c = t (mod 4). Barriers: full (copy landed), copy_free (copy read),
 // op_full (operands written), op_empty (MMAs done with the operands).
 template <int W>
-__global__ void __launch_bounds__(kTcThreads, 1) tc_spread_kernel(
+__global__ void __launch_bounds__(kTcThreads, 2) tc_spread_kernel(
     SpreadParams sp, const float* __restrict__ packed, int64_t count, const TcWeights* __restrict__ weights,
     const TcChunk* __restrict__ chunks, const uint32_t* __restrict__ tile_chunk_start,
     const uint32_t* __restrict__ part_start, int groups, float* __restrict__ scratch,
@@ -387,11 +388,12 @@ __global__ void __launch_bounds__(kTcThreads, 1) tc_spread_kernel(
   for (int c = tid; c < n; c += kTcThreads) s_chunks[c] = chunks[first + c];
 
   // Zero the accumulator: the eight converter warps, two per lane quadrant,
-  // clear 256 columns each.
+  // clear half of the columns each.
   if (warp >= 2) {
     const int cw = warp - 2;
-    const uint32_t base = tm + (static_cast<uint32_t>((warp & 3) * 32) << 16) + static_cast<uint32_t>((cw >> 2) * 256);
-    for (int c = 0; c < 256; c += 8) tmem_zero8(base + c);
+    constexpr int kHalf = kTcColumns / 2;
+    const uint32_t base = tm + (static_cast<uint32_t>((warp & 3) * 32) << 16) + static_cast<uint32_t>((cw >> 2) * kHalf);
+    for (int c = 0; c < kHalf; c += 8) tmem_zero8(base + c);
     asm volatile("tcgen05.wait::st.sync.aligned;" ::: "memory");
   }
   tc_fence_before();

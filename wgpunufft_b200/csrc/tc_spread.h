@@ -30,7 +30,7 @@ constexpr int kTcPitch = 16;          // tensor-memory columns per padded tile r
 constexpr int kTcTileX = 8;           // tile width in cells (one column group)
 constexpr int kTcMaxWidth = 8;        // widest window (weights stored per point)
 constexpr int kTcMinBatch = 16;       // active batches below this use the CUDA-core spreader
-constexpr int kTcColumns = 512;       // tensor-memory columns a CTA allocates
+constexpr int kTcColumns = 256;       // tensor-memory columns a CTA allocates (two CTAs per SM)
 
 // One chunk: up to eight consecutive slots of one bin row of a tile.
 struct TcChunk {
