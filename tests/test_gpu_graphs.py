@@ -1,0 +1,74 @@
+"""Executions on prepared points can be captured in a CUDA graph (after one
+warm-up execution has sized the plan's buffers) and replayed with the same
+bits as eager executions: type 1 (CUDA cores and tensor cores), type 2, and
+type 3."""
+
+from __future__ import annotations
+
+import numpy as np
+import pytest
+
+from tests.conftest import uniform_points
+
+pytestmark = pytest.mark.gpu
+
+torch = pytest.importorskip("torch")
+if not torch.cuda.is_available():  # pragma: no cover - CPU containers
+    pytest.skip("needs a CUDA device", allow_module_level=True)
+
+import wgpunufft_b200 as w  # noqa: E402
+
+DEV = "cuda:0"
+
+
+@pytest.mark.parametrize("kind,modes,batch", [(1, (64, 48), 1), (1, (64, 48), 32), (2, (64, 48), 1),
+                                               (2, (64, 48), 16), (1, (24, 20, 16), 2)])
+def test_captured_execution_replays_bit_for_bit(kind, modes, batch):
+    rng = np.random.default_rng(kind * 100 + batch)
+    m = 20000
+    points = torch.from_numpy(uniform_points(rng, m, len(modes))).to(DEV)
+    n = int(np.prod(modes))
+    plan = (w.NufftPlan.type1_gpu if kind == 1 else w.NufftPlan.type2_gpu)(w.NufftConfig(modes, 1e-6, batch=batch))
+    stream = torch.cuda.Stream()
+    in_len, out_len = (m, n) if kind == 1 else (n, m)
+    inputs = torch.complex(torch.randn((batch, in_len), device=DEV), torch.randn((batch, in_len), device=DEV))
+    out = torch.empty((batch, out_len), dtype=torch.complex64, device=DEV)
+    with torch.cuda.stream(stream):
+        plan.set_points_gpu(points, stream=stream)
+        plan.execute_gpu_batch(batch, inputs, out, stream=stream)
+        stream.synchronize()
+        eager = out.clone()
+        graph = torch.cuda.CUDAGraph()
+        with torch.cuda.graph(graph, stream=stream):
+            plan.execute_gpu_batch(batch, inputs, out, stream=stream)
+    for _ in range(3):
+        out.zero_()
+        graph.replay()
+        torch.cuda.synchronize()
+        assert torch.equal(out.view(torch.int32), eager.view(torch.int32))
+    plan.synchronize()
+    del graph
+
+
+def test_captured_type3_replays_bit_for_bit():
+    rng = np.random.default_rng(9)
+    src = torch.from_numpy(rng.uniform(-1, 1, (3000, 2))).to(DEV)
+    tgt = torch.from_numpy(rng.uniform(-30, 30, (2000, 2))).to(DEV)
+    c = torch.complex(torch.randn((1, 3000), device=DEV, dtype=torch.float64),
+                      torch.randn((1, 3000), device=DEV, dtype=torch.float64))
+    plan = w.NufftType3Plan(w.NufftType3Config(((-1.0, 1.0),) * 2, ((-30.0, 30.0),) * 2, eps=1e-9))
+    out = torch.empty((1, 2000), dtype=torch.complex128, device=DEV)
+    stream = torch.cuda.Stream()
+    with torch.cuda.stream(stream):
+        plan.set_points_gpu(src, tgt, stream=stream)
+        plan.execute_gpu_batch(1, c, out, stream=stream)
+        stream.synchronize()
+        eager = out.clone()
+        graph = torch.cuda.CUDAGraph()
+        with torch.cuda.graph(graph, stream=stream):
+            plan.execute_gpu_batch(1, c, out, stream=stream)
+    out.zero_()
+    graph.replay()
+    torch.cuda.synchronize()
+    assert torch.equal(out.view(torch.int64), eager.view(torch.int64))
+    del graph
