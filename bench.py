@@ -49,6 +49,7 @@ def parse():
     p.add_argument("--no-e2e", action="store_true")
     p.add_argument("--no-cpu", action="store_true")
     p.add_argument("--no-batched", action="store_true")
+    p.add_argument("--no-uneven", action="store_true")
     return p.parse_args()
 
 
@@ -260,6 +261,28 @@ def batched_comparison(w, torch, timed, barrier, world, dev, args, rank):
                 item["rel_l2"] = float(np.linalg.norm(got - ref) / np.linalg.norm(ref))
             entry[name] = item
             del plan
+        # Type 2 on the same points: modes of every vector to the points.
+        plan2 = w.NufftPlan.type2_gpu(w.NufftConfig(BATCH_MODES, BATCH_EPS, batch=batch))
+        plan2.set_points_gpu(pts)
+        f = torch.complex(torch.randn((batch, BATCH_MODES[0] * BATCH_MODES[1]), generator=g, device=dev),
+                          torch.randn((batch, BATCH_MODES[0] * BATCH_MODES[1]), generator=g, device=dev))
+        vals = torch.empty((batch, BATCH_POINTS), dtype=torch.complex64, device=dev)
+        for _ in range(max(1, args.warmup)):
+            plan2.execute_gpu_batch(batch, f, vals)
+        barrier()
+        total2 = timed(lambda: plan2.execute_gpu_batch(batch, f, vals), steps)
+        (total2,) = max_over_ranks([total2], dev)
+        item2 = {"value": replica_throughput(world, BATCH_POINTS * batch, total2, steps), "ms_per_step": total2 / steps,
+                 "engine": "CUDA cores, bin regions staged in shared memory"}
+        if rank == 0:
+            from oracle import native
+
+            pick = np.random.default_rng(4).choice(BATCH_POINTS, 64, replace=False)
+            ref2 = native.direct_type2(pts_h[pick], f[:4].cpu().numpy().astype(np.complex128), BATCH_MODES)
+            got2 = vals[:4].cpu().numpy()[:, pick]
+            item2["rel_l2"] = float(np.linalg.norm(got2 - ref2) / np.linalg.norm(ref2))
+        entry["type2"] = item2
+        del plan2, f, vals
         entry["speedup_tensor_over_cuda_cores"] = entry["tensor_cores"]["value"] / entry["cuda_cores"]["value"]
         spread_ms = entry["tensor_cores"]["stages_ms_per_step"].get("spread", 0.0)
         useful = 4.0 * batch * BATCH_POINTS * 7 * 7
@@ -268,6 +291,64 @@ def batched_comparison(w, torch, timed, barrier, world, dev, args, rank):
         del c, out
         torch.cuda.empty_cache()
     return result
+
+
+def uneven_problems_line(w, torch, barrier, world, dev, args, rank):
+    """256 independent type-1 problems of uneven sizes (2D/3D, 64^2..256^2 and
+    32^3..64^3 modes, 1e3..1e6 points, uniform or clustered, eps 1e-6), one
+    plan each with its points set: all executions issued one after another
+    (eager) and replayed from one captured CUDA graph."""
+    from wgpunufft_b200 import workloads
+
+    problems = workloads.uneven_problems(256, seed=SEED % 1000)
+    stream = torch.cuda.Stream()
+    plans, outs = [], []
+    with torch.cuda.stream(stream):
+        for modes, p, c in problems:
+            plan = w.NufftPlan.type1_gpu(w.NufftConfig(modes, 1e-6))
+            plan.set_points_gpu(p, stream=stream)
+            out = torch.empty((1, int(np.prod(modes))), dtype=torch.complex64, device=dev)
+            plan.execute_gpu_batch(1, c, out, stream=stream)
+            plans.append(plan)
+            outs.append(out)
+        stream.synchronize()
+
+        def run_all():
+            for plan, (modes, p, c), out in zip(plans, problems, outs):
+                plan.execute_gpu_batch(1, c, out, stream=stream)
+
+        graph = torch.cuda.CUDAGraph()
+        with torch.cuda.graph(graph, stream=stream):
+            run_all()
+        stream.synchronize()
+
+        def timed_on(fn, steps):
+            total = 0.0
+            for _ in range(steps):
+                start, end = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+                start.record(stream)
+                fn()
+                end.record(stream)
+                end.synchronize()
+                total += start.elapsed_time(end)
+            return total
+
+        steps = max(1, min(args.steps, 5))
+        for _ in range(2):
+            run_all()
+            graph.replay()
+        barrier()
+        eager_ms = timed_on(run_all, steps)
+        graph_ms = timed_on(graph.replay, steps)
+    del graph
+    eager_ms, graph_ms = max_over_ranks([eager_ms, graph_ms], dev)
+    total_points = sum(int(p.shape[0]) for _, p, _ in problems)
+    return {"problems": len(problems), "points": total_points, "eps": 1e-6,
+            "graph": {"value": replica_throughput(world, total_points, graph_ms, steps), "unit": UNIT,
+                      "ms_per_step": graph_ms / steps},
+            "eager": {"value": replica_throughput(world, total_points, eager_ms, steps), "unit": UNIT,
+                      "ms_per_step": eager_ms / steps},
+            "note": "one plan per problem (prepared points); a step executes all 256"}
 
 
 def profile_traffic():
@@ -401,6 +482,9 @@ def main():
     batched = None
     if not args.no_batched:
         batched = batched_comparison(w, torch, timed, barrier, world, dev, args, rank)
+    uneven = None
+    if not args.no_uneven:
+        uneven = uneven_problems_line(w, torch, barrier, world, dev, args, rank)
 
     if rank == 0:
         peaks = json.loads((ROOT / "MEASURED_PEAKS.json").read_text()) if (ROOT / "MEASURED_PEAKS.json").exists() else {}
@@ -435,6 +519,7 @@ def main():
             "stages_ms_per_step": {k: v[0] / args.steps for k, v in stages.items()},
             "type2": type2,
             "batched": batched,
+            "uneven_problems": uneven,
             "roofline": roofline,
             "cpu_baseline": cpu,
             "e2e": e2e,

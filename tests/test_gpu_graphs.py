@@ -72,3 +72,41 @@ def test_captured_type3_replays_bit_for_bit():
     torch.cuda.synchronize()
     assert torch.equal(out.view(torch.int64), eager.view(torch.int64))
     del graph
+
+
+def test_uneven_problems_in_one_graph_match_direct_sums():
+    """Independent problems of uneven sizes (2D and 3D), one plan each,
+    executed from one CUDA graph: a seeded sample against direct sums."""
+    from oracle import native
+    from tests.conftest import rel_l2
+    from wgpunufft_b200 import workloads
+
+    problems = workloads.uneven_problems(24, seed=77)
+    stream = torch.cuda.Stream()
+    plans, outs = [], []
+    with torch.cuda.stream(stream):
+        for modes, p, c in problems:
+            plan = w.NufftPlan.type1_gpu(w.NufftConfig(modes, 1e-6))
+            plan.set_points_gpu(p, stream=stream)
+            out = torch.empty((1, int(np.prod(modes))), dtype=torch.complex64, device=DEV)
+            plan.execute_gpu_batch(1, c, out, stream=stream)
+            plans.append(plan)
+            outs.append(out)
+        stream.synchronize()
+        graph = torch.cuda.CUDAGraph()
+        with torch.cuda.graph(graph, stream=stream):
+            for plan, (modes, p, c), out in zip(plans, problems, outs):
+                plan.execute_gpu_batch(1, c, out, stream=stream)
+    for out in outs:
+        out.zero_()
+    graph.replay()
+    torch.cuda.synchronize()
+    rng = np.random.default_rng(1)
+    for k in rng.choice(len(problems), 6, replace=False):
+        modes, p, c = problems[k]
+        select = rng.choice(int(np.prod(modes)), 64, replace=False)
+        ref = native.direct_type1(p.cpu().numpy().astype(np.float64), c.cpu().numpy().astype(np.complex128),
+                                  modes, select=select)
+        bound = 20e-6 if len(modes) == 2 else 32e-6
+        assert rel_l2(outs[k].cpu().numpy()[:, select], ref) < bound, (k, modes, p.shape[0])
+    del graph

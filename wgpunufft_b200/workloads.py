@@ -11,6 +11,10 @@ Cases:
             directions uniform on the sphere, +-1e-3 jitter), eps 1e-5
   batched   2D 512^2 modes, 2e6 uniform points, eps 1e-6, --batch vectors (default 64)
 
+uneven_problems() gives 256 independent problems of uneven sizes (2D or 3D,
+modes from 64^2, 128^2, 256^2, 32^3, 64^3, M log-uniform in [1e3, 1e6],
+uniform or clustered points, eps 1e-6).
+
 Points are f32 point-major in [-pi, pi); strengths and modes complex64 with
 N(0, 1) real and imaginary parts. No external dataset is involved.
 """
@@ -66,6 +70,30 @@ def values(batch: int, count: int, seed: int = 8, device: str = "cuda"):
                          torch.randn((batch, count), generator=g, device=device))
 
 
+UNEVEN_MODES = ((64, 64), (128, 128), (256, 256), (32, 32, 32), (64, 64, 64))
+
+
+def uneven_problems(count: int = 256, seed: int = 5, device: str = "cuda"):
+    """Independent type-1 problems of uneven sizes: dimensions 2D or 3D with
+    equal odds, modes from UNEVEN_MODES of that dimension, M log-uniform in
+    [1e3, 1e6], uniform or clustered points with equal odds, eps 1e-6.
+    Returns a list of (modes, points, strengths) on `device`."""
+    import numpy as np
+
+    rng = np.random.default_rng(seed)
+    problems = []
+    for k in range(count):
+        dims = 2 if rng.random() < 0.5 else 3
+        choices = [m for m in UNEVEN_MODES if len(m) == dims]
+        modes = choices[int(rng.integers(len(choices)))]
+        m = int(round(10 ** rng.uniform(3.0, 6.0)))
+        dist = "uniform" if rng.random() < 0.5 else "clustered"
+        p = points(dist, m, dims, seed=seed * 1000 + 2 * k)
+        c = values(1, m, seed=seed * 1000 + 2 * k + 1)
+        problems.append((modes, p, c))
+    return problems
+
+
 def run(case: str, batch: int, executes: int, kinds) -> None:
     import torch
 
@@ -104,3 +132,4 @@ def main() -> None:
 
 if __name__ == "__main__":
     main()
+
