@@ -283,6 +283,26 @@ def test_clustered_and_heavy_tiles_match_direct():
     assert rel_l2(got[0, select], ref[0]) < tolerance(2, 1e-5)
 
 
+@pytest.mark.parametrize("eps", [1e-4, 1e-5, 1e-6, 1e-7])
+def test_crowded_3d_tiles_match_direct_and_repeat(eps):
+    """3D tiles holding far more points than start cells (tight clusters over
+    uniform background; windows 5 to 8 wide): accurate against direct sums
+    and bitwise repeatable, including after a fresh sort of the points."""
+    rng = np.random.default_rng(41)
+    n_modes = (24, 20, 16)
+    points = np.concatenate([clustered_points(rng, 150_000, 3, centres=2, spread=0.05),
+                             uniform_points(rng, 50_000, 3)])
+    strengths = complex_normal(rng, points.shape[0])
+    got, plan = run_type1(n_modes, eps, points, strengths)
+    assert 5 <= plan.kernel_width() <= 8
+    again, _ = run_type1(n_modes, eps, points, strengths, plan=plan)
+    assert np.array_equal(got.view(np.int32), again.view(np.int32))
+    n = n_modes[0] * n_modes[1] * n_modes[2]
+    select = rng.choice(n, 200, replace=False)
+    ref = native.direct_type1(points.astype(np.float64), strengths, n_modes, select=select)
+    assert rel_l2(got[0, select], ref[0]) < tolerance(3, eps)
+
+
 def test_2d_1024_ten_million_points_against_direct_subsets():
     """The 2D 1024^2, 10^7-point workload: a seeded subset of modes (type 1)
     and of points (type 2) against FP64 direct sums over all inputs."""

@@ -402,11 +402,32 @@ void NufftPlan::configure_tiles() {
   if (rows > kMaxTileRows) {
     throw NufftFailure{B200NUFFT_INTERNAL, "spreading tile spans too many bin rows"};
   }
+  // 3D f32 tiles of widths 5 to 8: the shared-memory pitches and the segment
+  // table of the warp spreader (uploaded when the tile shape changes).
+  if (dim_ == 3 && precision_ == B200NUFFT_PRECISION_F32 && w >= kWarpMinWidth && w <= kWarpMaxWidth) {
+    uint32_t table[32 * warp_max_rounds()];
+    int32_t pitch0 = 0, pitch01 = 0;
+    if (spread_warp_layout(w, sp.pad, pitch0, pitch01, table)) {
+      const int32_t key[4] = {w, sp.pad[0], sp.pad[1], sp.pad[2]};
+      const size_t bytes = sizeof(uint32_t) * 32 * warp_rounds(w);
+      if (std::memcmp(key, warp_layout_key_, sizeof(key)) != 0) {
+        void* dst = warp_segments_.reserve(bytes, "warp segment table");
+        check_cuda(cudaMemcpy(dst, table, bytes, cudaMemcpyHostToDevice), "upload warp segment table");
+        std::memcpy(warp_layout_key_, key, sizeof(key));
+      }
+      sp.pitch0 = pitch0;
+      sp.pitch01 = pitch01;
+      sp.span = pitch01 * sp.pad[2];
+      sp.warp_segments = static_cast<const uint32_t*>(warp_segments_.get());
+    }
+  }
   // Parts of at most kPartCap records, fewer for small point sets so that
   // about four CTAs per SM have work.
   const int64_t spread_ctas = 4 * 148;
   int64_t cap = (std::max<int64_t>(point_count_, 1) + spread_ctas - 1) / spread_ctas;
-  cap = std::min<int64_t>(kPartCap, std::max<int64_t>(256, (cap + 255) / 256 * 256));
+  // 3D parts stay within the 2048 records that crowded tiles bucket in shared memory.
+  const int64_t part_cap = dim_ == 3 ? 2048 : kPartCap;
+  cap = std::min<int64_t>(part_cap, std::max<int64_t>(256, (cap + 255) / 256 * 256));
   sp.part_cap = static_cast<int32_t>(cap);
   sp.headroom = ilog2(static_cast<int64_t>(kPartCap) + 1);
   // Candidate (tile, local) pairs of every coordinate of every axis: tile t

@@ -111,6 +111,8 @@ class NufftPlan {
 
   // Spreading state.
   DeviceBuffer parts_, part_start_, max_bits_, scratch_, candidates_;
+  DeviceBuffer warp_segments_;     // 3D f32: segment table of the warp spreader
+  int32_t warp_layout_key_[4] = {};  // width and padded tile of that table
   int64_t part_upper_bound_ = 0;
   std::vector<int2> host_candidates_;
   int64_t candidate_tile_[3] = {0, 0, 0};

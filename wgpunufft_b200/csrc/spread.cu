@@ -316,10 +316,266 @@ __device__ __forceinline__ void flush_run(typename T::Word* acc, int padded, int
   }
 }
 
+// 3D f32 tiles of widths 5 to 8 are spread by whole warps, one record at a
+// time. The padded tile lives in shared memory with pitches chosen so that
+// the window's segments (L consecutive cells of one x row) start in
+// distinct banks, and lane l owns the segments that start in bank l: every
+// add instruction of the warp touches 32 different banks, whatever the
+// record. Lanes sum the records of a run with one support start in float
+// registers (a fixed order: the record order) and add the run to the
+// fixed-point tile once, rounded, when the start changes or after
+// 2^kWarpRunBits records.
+//
+// In crowded tiles (at least one record per start cell) each part's records
+// are first bucketed by their start in shared memory by a stable counting
+// sort, so that runs are as long as the data allows; otherwise the records
+// are taken in bin order. Points outside the fold reach or starting in
+// another tile are skipped.
+constexpr int kWarpRunBits = 5;
+constexpr int kWarpMaxRecords = 2048;  // the 3D part cap
+constexpr int kWarpGroup = 8;          // records staged per warp at a time
+constexpr int kStageStride = 28;       // wx[8] wy[8] wz[8] re im base -
+constexpr int kSpreadWarps = kSpreadThreads / 32;
+
+template <int D, int W, typename T>
+__host__ __device__ constexpr bool warp_capable() {
+  return D == 3 && T::kPreparedWindows && W >= kWarpMinWidth && W <= kWarpMaxWidth;
+}
+
+template <int W>
+__device__ void spread_warp3(const SpreadParams& sp, const PreparedWindow<3>* win3, const float2* sv,
+                             const uint32_t* perm, const uint32_t* row_begin, const uint32_t* row_prefix,
+                             int rows, const int* origin, uint32_t record_begin, uint32_t record_end,
+                             bool bucket, uint32_t* acc, int span, uint32_t* sorted,
+                             float (*stage)[kWarpGroup][kStageStride], int exponent, int& S) {
+  const int tid = threadIdx.x, lane = tid & 31, warp = tid >> 5;
+  const int t0 = sp.tile[0], t1 = sp.tile[1];
+  const int cells = t0 * t1 * sp.tile[2];
+  const int pitch0 = sp.pitch0, pitch01 = sp.pitch01;
+  auto slot_of = [&](uint32_t r, int& row) {
+    if (r >= row_prefix[row + 1] || r < row_prefix[row]) {
+      int low = 0, high = rows - 1;
+      while (low < high) {
+        const int mid = (low + high + 1) >> 1;
+        if (row_prefix[mid] <= r) low = mid; else high = mid - 1;
+      }
+      row = low;
+    }
+    return row_begin[row] + (r - row_prefix[row]);
+  };
+  // Local start of a record; false when it is skipped.
+  auto local_of = [&](const PreparedWindow<3>& win, int& x, int& y, int& z) {
+    if (win.start[0] < 0) return false;
+    x = win.start[0] - origin[0];
+    y = win.start[1] - origin[1];
+    z = win.start[2] - origin[2];
+    return x >= 0 && x < t0 && y >= 0 && y < t1 && z >= 0 && z < sp.tile[2];
+  };
+  const uint32_t n = record_end - record_begin;
+  uint32_t spread_count = n;
+  if (bucket) {
+    // count[key * warps + warp]: each warp's records per start (the last key
+    // collects the skipped records), in the tile region, cleared below.
+    uint32_t* count = acc;
+    const int entries = (cells + 1) * kSpreadWarps;
+    for (int c = tid; c < entries; c += kSpreadThreads) count[c] = 0u;
+    __syncthreads();
+    auto key_of = [&](const PreparedWindow<3>& win) {
+      int x, y, z;
+      return local_of(win, x, y, z) ? x + t0 * (y + t1 * z) : cells;
+    };
+    // Warp w sorts the consecutive records [warp_begin, warp_end).
+    const uint32_t per_warp = (n + kSpreadWarps - 1) / kSpreadWarps;
+    const uint32_t warp_begin = record_begin + min(n, per_warp * warp);
+    const uint32_t warp_end = record_begin + min(n, per_warp * (warp + 1));
+    int row = 0;
+    for (uint32_t r = warp_begin + lane; r < warp_end; r += 32) {
+      atomicAdd(&count[key_of(win3[slot_of(r, row)]) * kSpreadWarps + warp], 1u);
+    }
+    __syncthreads();
+    // Exclusive scan of the entries, key-major: a contiguous block per
+    // thread, the block sums in the front of `sorted`, filled afterwards.
+    uint32_t* block_sums = sorted;
+    const int per = (entries + kSpreadThreads - 1) / kSpreadThreads;
+    const int c0 = min(entries, tid * per), c1 = min(entries, c0 + per);
+    uint32_t sum = 0;
+    for (int c = c0; c < c1; ++c) sum += count[c];
+    block_sums[tid] = sum;
+    __syncthreads();
+    if (warp == 0) {
+      constexpr int kPer = kSpreadThreads / 32;
+      uint32_t v[kPer];
+      uint32_t mine = 0;
+#pragma unroll
+      for (int k = 0; k < kPer; ++k) {
+        v[k] = block_sums[lane * kPer + k];
+        mine += v[k];
+      }
+      uint32_t x = mine;
+#pragma unroll
+      for (int offset = 1; offset < 32; offset <<= 1) {
+        const uint32_t y = __shfl_up_sync(0xFFFFFFFFu, x, offset);
+        if (lane >= offset) x += y;
+      }
+      uint32_t running = x - mine;
+#pragma unroll
+      for (int k = 0; k < kPer; ++k) {
+        block_sums[lane * kPer + k] = running;
+        running += v[k];
+      }
+    }
+    __syncthreads();
+    uint32_t running = block_sums[tid];
+    for (int c = c0; c < c1; ++c) {
+      const uint32_t v = count[c];
+      count[c] = running;
+      running += v;
+    }
+    __syncthreads();
+    spread_count = count[cells * kSpreadWarps];
+    __syncthreads();  // every thread has read the count before the scatter moves the counters
+    // Stable scatter: each warp walks its records in order, 32 at a time;
+    // equal keys in one step take consecutive places in lane order.
+    row = 0;
+    const unsigned lower = (1u << lane) - 1u;
+    for (uint32_t first = warp_begin; first < warp_end; first += 32) {
+      const uint32_t r = first + lane;
+      int key = -1;
+      uint32_t slot = 0;
+      if (r < warp_end) {
+        slot = slot_of(r, row);
+        key = key_of(win3[slot]);
+      }
+      const unsigned same = __match_any_sync(0xFFFFFFFFu, key);
+      uint32_t* counter = &count[(key < 0 ? 0 : key) * kSpreadWarps + warp];
+      const uint32_t place = key < 0 ? 0u : *counter + __popc(same & lower);
+      __syncwarp();
+      if (key >= 0) {
+        sorted[place] = slot;
+        if ((same & lower) == 0u) *counter += __popc(same);
+      }
+      __syncwarp();
+    }
+    __syncthreads();
+    for (int c = tid; c < 4 * span; c += kSpreadThreads) acc[c] = 0u;
+    __syncthreads();
+  }
+  S = exponent - kWarpRunBits;
+  const float scale_lo = ldexpf(1.0f, S / 2);
+  const float scale_hi = ldexpf(1.0f, S - S / 2);
+
+  constexpr int L = warp_segment_cells(W);
+  constexpr int R = warp_rounds(W);
+  uint32_t desc[R];
+#pragma unroll
+  for (int r = 0; r < R; ++r) desc[r] = sp.warp_segments[r * 32 + lane];
+  float ar[R][L], ai[R][L];
+#pragma unroll
+  for (int r = 0; r < R; ++r) {
+#pragma unroll
+    for (int t = 0; t < L; ++t) ar[r][t] = ai[r][t] = 0.0f;
+  }
+  int run = -1, run_length = 0;
+  auto flush = [&]() {
+#pragma unroll
+    for (int r = 0; r < R; ++r) {
+      if (desc[r] & kSegmentValid) {
+        const int c = run + static_cast<int>(desc[r] & 0xFFFFu);
+#pragma unroll
+        for (int t = 0; t < L; ++t) {
+          F32Traits::add(acc, span, 0, c + t, ar[r][t]);
+          F32Traits::add(acc, span, 1, c + t, ai[r][t]);
+        }
+      }
+#pragma unroll
+      for (int t = 0; t < L; ++t) ar[r][t] = ai[r][t] = 0.0f;
+    }
+  };
+  float (*my_stage)[kStageStride] = stage[warp];
+  // Warp w spreads the consecutive records [spread_begin, spread_end) of the
+  // bucketed order (or of the bin order), so runs continue across groups.
+  const uint32_t per_warp = (spread_count + kSpreadWarps - 1) / kSpreadWarps;
+  const uint32_t spread_begin = min(spread_count, per_warp * warp);
+  const uint32_t spread_end = min(spread_count, per_warp * (warp + 1));
+  int row = 0;
+  for (uint32_t first = spread_begin; first < spread_end; first += kWarpGroup) {
+    // Stage the group: lane 3 g + a evaluates axis a of record g; lane 3 g
+    // also stages the scaled strength and the start's tile offset (-1: skip).
+    if (lane < 3 * kWarpGroup) {
+      const int g = lane / 3, a = lane - 3 * g;
+      const uint32_t r = first + g;
+      int base = -1;
+      float w[W];
+#pragma unroll
+      for (int j = 0; j < W; ++j) w[j] = 0.0f;
+      if (r < spread_end) {
+        const uint32_t slot = bucket ? sorted[r] : slot_of(record_begin + r, row);
+        const PreparedWindow<3> win = win3[slot];
+        int x, y, z;
+        if (local_of(win, x, y, z)) {
+          base = x + y * pitch0 + z * pitch01;
+          const float offset = a == 0 ? win.offset[0] : (a == 1 ? win.offset[1] : win.offset[2]);
+          horner32_window<W>(offset, sp.grid.horner32, w);
+          if (a == 0) {
+            const float2 c = sv[perm[slot]];
+            my_stage[g][24] = (c.x * scale_lo) * scale_hi;
+            my_stage[g][25] = (c.y * scale_lo) * scale_hi;
+          }
+        }
+      }
+#pragma unroll
+      for (int j = 0; j < 8; ++j) my_stage[g][a * 8 + j] = j < W ? w[j] : 0.0f;
+      if (a == 0) my_stage[g][26] = __int_as_float(base);
+    }
+    __syncwarp();
+#pragma unroll 1
+    for (int g = 0; g < kWarpGroup; ++g) {
+      const float* st = my_stage[g];
+      const int base = __float_as_int(st[26]);
+      if (base < 0) continue;
+      if (base != run || run_length == (1 << kWarpRunBits)) {
+        if (run >= 0) flush();
+        run = base;
+        run_length = 0;
+      }
+      ++run_length;
+      const float4 x_lo = *reinterpret_cast<const float4*>(st);
+      const float4 x_hi = *reinterpret_cast<const float4*>(st + 4);
+      const float wx[8] = {x_lo.x, x_lo.y, x_lo.z, x_lo.w, x_hi.x, x_hi.y, x_hi.z, x_hi.w};
+      const float2 c = *reinterpret_cast<const float2*>(st + 24);
+#pragma unroll
+      for (int r = 0; r < R; ++r) {
+        const uint32_t d = desc[r];
+        const int s = (d >> 16) & 15, j = (d >> 20) & 15, k = (d >> 24) & 15;
+        const float wyz = st[8 + j] * st[16 + k];
+        const float wr = c.x * wyz, wi = c.y * wyz;
+        float wxs[L];
+#pragma unroll
+        for (int t = 0; t < L; ++t) wxs[t] = wx[t];
+#pragma unroll
+        for (int q = 1; q < W / L; ++q) {
+          if (s == q) {
+#pragma unroll
+            for (int t = 0; t < L; ++t) wxs[t] = wx[q * L + t];
+          }
+        }
+#pragma unroll
+        for (int t = 0; t < L; ++t) {
+          ar[r][t] = fmaf(wr, wxs[t], ar[r][t]);
+          ai[r][t] = fmaf(wi, wxs[t], ai[r][t]);
+        }
+      }
+    }
+    __syncwarp();
+  }
+  if (run >= 0) flush();
+}
+
 // One CTA per (part, vector): spreads the part's records into a padded tile
 // of fixed-point sums and writes the tile out in floating point.
 template <int D, int W, typename T>
-__global__ void __launch_bounds__(kSpreadThreads, (spread_run<D, W, T>() > 1 || sizeof(typename T::Real) == 8 ? 2 : 3)) spread_tiles_kernel(
+__global__ void __launch_bounds__(kSpreadThreads, (spread_run<D, W, T>() > 1 || sizeof(typename T::Real) == 8 ||
+                                                    warp_capable<D, W, T>() ? 2 : 3)) spread_tiles_kernel(
     SpreadParams sp, const typename T::Real* __restrict__ points, const void* __restrict__ windows,
     const typename T::Complex* __restrict__ strengths, int64_t point_count, int batch,
     const uint32_t* __restrict__ perm, const uint32_t* __restrict__ offsets,
@@ -349,7 +605,11 @@ __global__ void __launch_bounds__(kSpreadThreads, (spread_run<D, W, T>() > 1 || 
     s_tile = low;
   }
   const int padded = sp.padded_cells;
-  for (int c = tid; c < T::kWordsPerCell * padded; c += kSpreadThreads) acc[c] = Word(0);
+  // The shared tile: dense (span = padded) or with the warp path's pitches.
+  constexpr bool kWarpCapable = warp_capable<D, W, T>();
+  const bool warp_path = kWarpCapable && sp.span > 0;
+  const int span = warp_path ? sp.span : padded;
+  for (int c = tid; c < T::kWordsPerCell * span; c += kSpreadThreads) acc[c] = Word(0);
   __syncthreads();
   const int64_t tile = s_tile;
   const uint32_t part_in_tile = part - part_start[tile];
@@ -424,14 +684,27 @@ __global__ void __launch_bounds__(kSpreadThreads, (spread_run<D, W, T>() > 1 || 
   // fixed order within the run) and reach the fixed-point tile once per run,
   // which leaves that much headroom in the scale.
   constexpr int kRun = spread_run<D, W, T>();
-  const int S = T::exponent(max_bits[b]) - (kRun > 1 ? kRunBits : 0);
+  __shared__ uint32_t sorted[kWarpCapable ? kWarpMaxRecords : 1];
+  __shared__ __align__(16) float stage[kWarpCapable ? kSpreadWarps : 1][kWarpGroup][kStageStride];
+  const int tile_cells = sp.tile[0] * sp.tile[1] * sp.tile[2];
+  const bool bucket = warp_path && record_end - record_begin <= static_cast<uint32_t>(kWarpMaxRecords) &&
+                      (tile_cells + 1) * kSpreadWarps <= T::kWordsPerCell * span &&
+                      tile_total >= static_cast<uint32_t>(tile_cells);
+  int S = T::exponent(max_bits[b]) - (kRun > 1 ? kRunBits : 0);
   const Real scale_lo = T::power_of_two(S / 2);
   const Real scale_hi = T::power_of_two(S - S / 2);
   const typename T::Complex* sv = strengths + static_cast<int64_t>(b) * point_count;
 
   int row = 0;
+  if constexpr (kWarpCapable) {
+    if (warp_path) {
+      spread_warp3<W>(sp, static_cast<const PreparedWindow<3>*>(windows), sv, perm, row_begin, row_prefix, rows,
+                      origin, record_begin, record_end, bucket, acc, span, sorted, stage,
+                      T::exponent(max_bits[b]), S);
+    }
+  }
   if constexpr (kRun == 1) {
-    for (uint32_t r = record_begin + tid; r < record_end; r += kSpreadThreads) {
+    for (uint32_t r = record_begin + tid; !warp_path && r < record_end; r += kSpreadThreads) {
       int local_start[D];
       Real w[D][W];
       typename T::Complex s;
@@ -527,6 +800,19 @@ __global__ void __launch_bounds__(kSpreadThreads, (spread_run<D, W, T>() > 1 || 
   }
   __syncthreads();
   typename T::Complex* out = scratch + (static_cast<int64_t>(part) * batch + b) * padded;
+  if (warp_path) {
+    const int pad0 = sp.pad[0], pad01 = sp.pad[0] * sp.pad[1];
+    for (int c = tid; c < padded; c += kSpreadThreads) {
+      const int z = c / pad01, rest = c - z * pad01;
+      const int y = rest / pad0, x = rest - y * pad0;
+      const int at = x + y * sp.pitch0 + z * sp.pitch01;
+      typename T::Complex v;
+      v.x = T::value(acc, span, 0, at, S);
+      v.y = T::value(acc, span, 1, at, S);
+      out[c] = v;
+    }
+    return;
+  }
   for (int c = tid; c < padded; c += kSpreadThreads) {
     typename T::Complex v;
     v.x = T::value(acc, padded, 0, c, S);
@@ -647,8 +933,8 @@ void fold_any(const SpreadParams& sp, int batch, const Complex* scratch, const u
 
 template <int D, int W, typename T>
 void launch_spread_width(const SpreadParams& sp, const SpreadLaunchT<T>& l, cudaStream_t stream) {
-  const size_t smem =
-      static_cast<size_t>(T::kWordsPerCell) * sp.padded_cells * sizeof(typename T::Word);
+  const int span = warp_capable<D, W, T>() && sp.span > 0 ? sp.span : sp.padded_cells;
+  const size_t smem = static_cast<size_t>(T::kWordsPerCell) * span * sizeof(typename T::Word);
   auto kernel = spread_tiles_kernel<D, W, T>;
   check_cuda(cudaFuncSetAttribute(kernel, cudaFuncAttributeMaxDynamicSharedMemorySize,
                                   static_cast<int>(smem)),
@@ -739,6 +1025,55 @@ void spread_execute(const SpreadParams& sp, const SpreadLaunch& l, cudaStream_t 
                              l.perm,     l.offsets,          l.part_start,  l.part_upper_bound,
                              l.max_bits, l.scratch,          l.candidates,  l.fine};
   spread_execute_impl<F32Traits>(sp, t, stream, timer);
+}
+
+bool spread_warp_layout(int width, const int32_t pad[3], int32_t& pitch0, int32_t& pitch01,
+                        uint32_t* table) {
+  if (width < kWarpMinWidth || width > kWarpMaxWidth) return false;
+  const int L = warp_segment_cells(width);
+  const int R = warp_rounds(width);
+  const int per_row = width / L;
+  int best_banks = 1 << 30;
+  int64_t best_cells = 0;
+  for (int d0 = 0; d0 < 16; ++d0) {
+    for (int d1 = 0; d1 < 32; ++d1) {
+      const int p0 = pad[0] + d0;
+      const int p01 = p0 * pad[1] + d1;
+      int banks[32] = {};
+      for (int k = 0; k < width; ++k) {
+        for (int j = 0; j < width; ++j) {
+          for (int s = 0; s < per_row; ++s) ++banks[(s * L + j * p0 + k * p01) & 31];
+        }
+      }
+      int most = 0;
+      for (int v : banks) most = std::max(most, v);
+      const int64_t cells = static_cast<int64_t>(p01) * pad[2];
+      if (most < best_banks || (most == best_banks && cells < best_cells)) {
+        best_banks = most;
+        best_cells = cells;
+        pitch0 = p0;
+        pitch01 = p01;
+      }
+    }
+  }
+  if (best_banks > R) return false;
+  const int last = (width - 1) * (1 + pitch0 + pitch01);
+  if (last > 0xFFFF) return false;
+  for (int i = 0; i < R * 32; ++i) table[i] = 0u;
+  int filled[32] = {};
+  for (int k = 0; k < width; ++k) {
+    for (int j = 0; j < width; ++j) {
+      for (int s = 0; s < per_row; ++s) {
+        const int offset = s * L + j * pitch0 + k * pitch01;
+        const int lane = offset & 31;
+        table[filled[lane] * 32 + lane] = kSegmentValid | static_cast<uint32_t>(offset) |
+                                          (static_cast<uint32_t>(s) << 16) | (static_cast<uint32_t>(j) << 20) |
+                                          (static_cast<uint32_t>(k) << 24);
+        ++filled[lane];
+      }
+    }
+  }
+  return true;
 }
 
 void spread_execute64(const SpreadParams& sp, const SpreadLaunch64& l, cudaStream_t stream,

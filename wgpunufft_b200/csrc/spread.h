@@ -9,7 +9,8 @@
 
 namespace b200nufft {
 
-constexpr int kMaxTileRows = 1024;
+// At most 16 x 16 bin rows: 3D tiles are at most 16 cells per axis.
+constexpr int kMaxTileRows = 256;
 
 // Tiling of the fine grid into spreading subproblems. A tile holds the
 // support starts tile[a] cells wide per axis; its padded copy is
@@ -29,7 +30,43 @@ struct SpreadParams {
   // by a negative tile when fewer.
   int64_t candidate_base[3];
   int32_t candidate_count[3];
+  // 3D f32 plans of widths kWarpMinWidth..kWarpMaxWidth: the shared-memory
+  // layout of the padded tile (row pitch, plane pitch, cells per word array)
+  // and, per round and lane, the window segment the lane accumulates
+  // (spread_warp_layout). span 0: the tile is kept dense and records are
+  // spread one per thread.
+  int32_t pitch0;
+  int32_t pitch01;
+  int32_t span;
+  const uint32_t* warp_segments;
 };
+
+// Window widths spread by whole warps, one record at a time (3D f32).
+constexpr int kWarpMinWidth = 5;
+constexpr int kWarpMaxWidth = 8;
+// Cells per window segment (consecutive cells of one x row) and the rounds
+// of 32 segments that cover a w^3 window.
+__host__ __device__ constexpr int warp_segment_cells(int w) { return w == 6 ? 3 : w; }
+__host__ __device__ constexpr int warp_rounds(int w) {
+  return (w * w * (w / warp_segment_cells(w)) + 31) / 32;
+}
+__host__ __device__ constexpr int warp_max_rounds() {
+  int most = 0;
+  for (int w = kWarpMinWidth; w <= kWarpMaxWidth; ++w) most = warp_rounds(w) > most ? warp_rounds(w) : most;
+  return most;
+}
+// Descriptor bits of a segment: its first cell's offset from the window
+// origin in the shared tile, its index within the x row, j, k, and a valid bit.
+constexpr uint32_t kSegmentValid = 0x80000000u;
+
+// Chooses the shared-memory pitches of a padded tile (pad[a] cells per axis,
+// a few cells of slack per row and plane allowed) so that the window
+// segments spread evenly over the 32 banks, and assigns every segment to the
+// lane of its bank: in each round the lanes then add to 32 different banks.
+// Fills table[round * 32 + lane] (32 * warp_max_rounds() entries at most);
+// false when no pitch reaches the warp_rounds(width) rounds.
+bool spread_warp_layout(int width, const int32_t pad[3], int32_t& pitch0, int32_t& pitch01,
+                        uint32_t* table);
 
 struct SpreadLaunch {
   const float* points;    // coordinates in bin (slot) order

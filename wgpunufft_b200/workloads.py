@@ -10,6 +10,9 @@ Cases:
   radial    3D 256^3 modes, 4096 spokes x 12207 samples (radius linear in [-pi, pi),
             directions uniform on the sphere, +-1e-3 jitter), eps 1e-5
   batched   2D 512^2 modes, 2e6 uniform points, eps 1e-6, --batch vectors (default 64)
+  radial128 the radial case at 128^3 modes, 4096 spokes x 1526 samples (profiling size)
+  uniform3d 3D 256^3 modes, 4096 x 12207 uniform points, eps 1e-5
+  uniform128 3D 128^3 modes, 4096 x 1526 uniform points, eps 1e-5 (profiling size)
 
 uneven_problems() gives 256 independent problems of uneven sizes (2D or 3D,
 modes from 64^2, 128^2, 256^2, 32^3, 64^3, M log-uniform in [1e3, 1e6],
@@ -30,6 +33,9 @@ CASES = {
     "clustered": ((1024, 1024), 10_000_000, 1e-5, "clustered"),
     "radial": ((256, 256, 256), 4096 * 12207, 1e-5, "radial"),
     "batched": ((512, 512), 2_000_000, 1e-6, "uniform"),
+    "radial128": ((128, 128, 128), 4096 * 1526, 1e-5, "radial"),
+    "uniform3d": ((256, 256, 256), 4096 * 12207, 1e-5, "uniform"),
+    "uniform128": ((128, 128, 128), 4096 * 1526, 1e-5, "uniform"),
 }
 
 
