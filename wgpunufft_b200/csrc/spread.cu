@@ -821,6 +821,8 @@ __global__ void __launch_bounds__(kSpreadThreads, (spread_run<D, W, T>() > 1 || 
   }
 }
 
+constexpr int kFoldThreads = 256;
+
 // Every fine-grid cell as the sum, in a fixed order, of the padded tiles and
 // parts that cover it.
 template <int D, int BB, typename Complex>
@@ -829,18 +831,21 @@ __global__ void fold_tiles_kernel(SpreadParams sp, int batch, const Complex* __r
                                   const int2* __restrict__ candidates,
                                   Complex* __restrict__ fine) {
   // Each thread sums one cell of BB consecutive vectors, so the candidate
-  // lookups are shared and the vectors' loads are independent.
-  const int64_t cell = static_cast<int64_t>(blockIdx.x) * blockDim.x + threadIdx.x;
-  if (cell >= sp.grid.fine_count) return;
+  // lookups are shared and the vectors' loads are independent. A CTA covers
+  // kFoldThreads consecutive cells of one x row: the row and its (y, z) are
+  // found once per CTA with 32-bit arithmetic.
+  const uint32_t chunks = (static_cast<uint32_t>(sp.grid.fine[0]) + kFoldThreads - 1) / kFoldThreads;
+  const uint32_t row = blockIdx.x / chunks;
+  const int x = static_cast<int>((blockIdx.x - row * chunks) * kFoldThreads + threadIdx.x);
+  if (x >= sp.grid.fine[0]) return;
+  const int64_t cell = x + sp.grid.fine[0] * static_cast<int64_t>(row);
   const int b0 = blockIdx.y * BB;
-  int coord[3] = {0, 0, 0};
-  {
-    int64_t rest = cell;
-#pragma unroll
-    for (int a = 0; a < D; ++a) {
-      coord[a] = static_cast<int>(rest % sp.grid.fine[a]);
-      rest /= sp.grid.fine[a];
-    }
+  int coord[3] = {x, 0, 0};
+  if (D == 2) coord[1] = static_cast<int>(row);
+  if (D == 3) {
+    const uint32_t f1 = static_cast<uint32_t>(sp.grid.fine[1]);
+    coord[2] = static_cast<int>(row / f1);
+    coord[1] = static_cast<int>(row - static_cast<uint32_t>(coord[2]) * f1);
   }
   const int2* c0 = candidates + sp.candidate_base[0] + coord[0] * sp.candidate_count[0];
   const int2* c1 = D > 1 ? candidates + sp.candidate_base[1] + coord[1] * sp.candidate_count[1] : nullptr;
@@ -901,20 +906,23 @@ __global__ void fold_tiles_kernel(SpreadParams sp, int batch, const Complex* __r
 template <int BB, typename Complex>
 void launch_fold(const SpreadParams& sp, int batch, const Complex* scratch, const uint32_t* part_start,
                  int64_t part_limit, const int2* candidates, Complex* fine, cudaStream_t stream) {
-  const dim3 grid(static_cast<unsigned>((sp.grid.fine_count + 255) / 256),
-                  static_cast<unsigned>((batch + BB - 1) / BB));
+  // One CTA per kFoldThreads cells of an x row.
+  int64_t rows = 1;
+  for (int a = 1; a < sp.grid.dimensions; ++a) rows *= sp.grid.fine[a];
+  const int64_t chunks = (sp.grid.fine[0] + kFoldThreads - 1) / kFoldThreads;
+  const dim3 grid(static_cast<unsigned>(rows * chunks), static_cast<unsigned>((batch + BB - 1) / BB));
   switch (sp.grid.dimensions) {
     case 1:
-      fold_tiles_kernel<1, BB, Complex><<<grid, 256, 0, stream>>>(sp, batch, scratch, part_start, part_limit,
-                                                                  candidates, fine);
+      fold_tiles_kernel<1, BB, Complex><<<grid, kFoldThreads, 0, stream>>>(sp, batch, scratch, part_start,
+                                                                           part_limit, candidates, fine);
       break;
     case 2:
-      fold_tiles_kernel<2, BB, Complex><<<grid, 256, 0, stream>>>(sp, batch, scratch, part_start, part_limit,
-                                                                  candidates, fine);
+      fold_tiles_kernel<2, BB, Complex><<<grid, kFoldThreads, 0, stream>>>(sp, batch, scratch, part_start,
+                                                                           part_limit, candidates, fine);
       break;
     default:
-      fold_tiles_kernel<3, BB, Complex><<<grid, 256, 0, stream>>>(sp, batch, scratch, part_start, part_limit,
-                                                                  candidates, fine);
+      fold_tiles_kernel<3, BB, Complex><<<grid, kFoldThreads, 0, stream>>>(sp, batch, scratch, part_start,
+                                                                           part_limit, candidates, fine);
       break;
   }
   note_launch();
