@@ -50,6 +50,7 @@ def parse():
     p.add_argument("--no-cpu", action="store_true")
     p.add_argument("--no-batched", action="store_true")
     p.add_argument("--no-uneven", action="store_true")
+    p.add_argument("--no-radial", action="store_true")
     return p.parse_args()
 
 
@@ -293,6 +294,69 @@ def batched_comparison(w, torch, timed, barrier, world, dev, args, rank):
     return result
 
 
+def radial_3d_line(w, torch, timed, barrier, world, dev, args, rank):
+    """The 3D configuration: 256^3 modes, 4096 radial spokes x 12207 samples
+    (49,999,872 points), eps 1e-5. Type-1 and type-2 NU points/s on prepared
+    points with stage times, and rel-l2 against FP64 direct sums on 4 modes
+    (type 1) and 64 points (type 2)."""
+    from wgpunufft_b200 import workloads
+
+    modes, count, eps, dist = workloads.CASES["radial"]
+    pts = workloads.points(dist, count, 3, seed=SEED % 1000 + 31, device=dev)
+    c = workloads.values(1, count, seed=SEED % 1000 + 32, device=dev)
+    n = modes[0] * modes[1] * modes[2]
+    result = {"workload": "3d_type1_type2_modes256^3_M49999872_radial_eps1e-5", "modes": list(modes),
+              "points": count, "eps": eps, "unit": UNIT}
+    steps = max(1, min(args.steps, 5))
+    pts_h = pts.cpu().numpy().astype(np.float64) if rank == 0 else None
+    plan = w.NufftPlan.type1_gpu(w.NufftConfig(modes, eps))
+    plan.set_points_gpu(pts)
+    out = torch.empty((1, n), dtype=torch.complex64, device=dev)
+    for _ in range(max(1, args.warmup)):
+        plan.execute_gpu_batch(1, c, out)
+    barrier()
+    plan.stage_timing(True)
+    plan.stage_report()
+    total = timed(lambda: plan.execute_gpu_batch(1, c, out), steps)
+    stages = plan.stage_report()
+    plan.stage_timing(False)
+    (total,) = max_over_ranks([total], dev)
+    item = {"value": replica_throughput(world, count, total, steps), "ms_per_step": total / steps,
+            "stages_ms_per_step": {k: v[0] / steps for k, v in stages.items()}}
+    if rank == 0:
+        from oracle import native
+
+        select = np.random.default_rng(9).choice(n, 4, replace=False)
+        ref = native.direct_type1(pts_h, c.cpu().numpy().astype(np.complex128), modes, select=select)
+        got = out.cpu().numpy()[:, select]
+        item["rel_l2"] = float(np.linalg.norm(got - ref) / np.linalg.norm(ref))
+    result["type1"] = item
+    del plan, out
+    plan2 = w.NufftPlan.type2_gpu(w.NufftConfig(modes, eps))
+    plan2.set_points_gpu(pts)
+    g = torch.Generator(device=dev)
+    g.manual_seed(SEED + 33)
+    f = torch.complex(torch.randn((1, n), generator=g, device=dev), torch.randn((1, n), generator=g, device=dev))
+    vals = torch.empty((1, count), dtype=torch.complex64, device=dev)
+    for _ in range(max(1, args.warmup)):
+        plan2.execute_gpu_batch(1, f, vals)
+    barrier()
+    total2 = timed(lambda: plan2.execute_gpu_batch(1, f, vals), steps)
+    (total2,) = max_over_ranks([total2], dev)
+    item2 = {"value": replica_throughput(world, count, total2, steps), "ms_per_step": total2 / steps}
+    if rank == 0:
+        from oracle import native
+
+        pick = np.random.default_rng(10).choice(count, 64, replace=False)
+        ref2 = native.direct_type2(pts_h[pick], f.cpu().numpy().astype(np.complex128), modes)
+        got2 = vals.cpu().numpy()[:, pick]
+        item2["rel_l2"] = float(np.linalg.norm(got2 - ref2) / np.linalg.norm(ref2))
+    result["type2"] = item2
+    del plan2, f, vals, pts, c
+    torch.cuda.empty_cache()
+    return result
+
+
 def uneven_problems_line(w, torch, barrier, world, dev, args, rank):
     """256 independent type-1 problems of uneven sizes (2D/3D, 64^2..256^2 and
     32^3..64^3 modes, 1e3..1e6 points, uniform or clustered, eps 1e-6), one
@@ -485,6 +549,10 @@ def main():
     uneven = None
     if not args.no_uneven:
         uneven = uneven_problems_line(w, torch, barrier, world, dev, args, rank)
+    # The 3D radial configuration (256^3 modes, 5e7 points, eps 1e-5).
+    radial = None
+    if not args.no_radial:
+        radial = radial_3d_line(w, torch, timed, barrier, world, dev, args, rank)
 
     if rank == 0:
         peaks = json.loads((ROOT / "MEASURED_PEAKS.json").read_text()) if (ROOT / "MEASURED_PEAKS.json").exists() else {}
@@ -520,6 +588,7 @@ def main():
             "type2": type2,
             "batched": batched,
             "uneven_problems": uneven,
+            "radial_3d": radial,
             "roofline": roofline,
             "cpu_baseline": cpu,
             "e2e": e2e,
