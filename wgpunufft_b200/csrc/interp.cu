@@ -301,6 +301,89 @@ __global__ void __launch_bounds__(256) interpolate_bins_kernel(GridParams g, con
   }
 }
 
+// 2D f32 interpolation of fewer than kBinVectors/4 vectors: one CTA of
+// kRegionThreads per 8 x 8-cell bin. The region the bin's windows reach is
+// staged in shared memory one vector at a time (coalesced row loads, mostly
+// L2 hits shared with the neighbouring bins), and a thread serves one point
+// from it, summing in the order of interpolate_kernel (bitwise the same
+// values); windows beyond the region read the grid directly.
+constexpr int kRegionThreads = 128;
+
+template <int W>
+__global__ void __launch_bounds__(kRegionThreads) interpolate_region_kernel(
+    GridParams g, const void* __restrict__ windows, int64_t count, const uint32_t* __restrict__ perm,
+    const uint32_t* __restrict__ offsets, const float2* __restrict__ fine, int batch,
+    float2* __restrict__ output) {
+  constexpr int S = bin_region_side<W>();
+  __shared__ float2 region[S * S];
+  const int64_t bin = blockIdx.x;
+  const uint32_t first = offsets[bin], last = offsets[bin + 1];
+  if (first == last) return;
+  const int bins0 = static_cast<int>(g.axis[0].bins);
+  const int n0 = g.axis[0].length, n1 = g.axis[1].length;
+  const int ox = static_cast<int>(bin % bins0) * 8 - W / 2 - 2;
+  const int oy = static_cast<int>(bin / bins0) * 8 - W / 2 - 2;
+  for (int b = 0; b < batch; ++b) {
+    const float2* grid = fine + static_cast<int64_t>(b) * g.fine_count;
+    __syncthreads();  // the previous vector's reads are done
+    for (int e = threadIdx.x; e < S * S; e += kRegionThreads) {
+      const int r = e / S, c = e - r * S;
+      int y = (oy + r) % n1;
+      y = y < 0 ? y + n1 : y;
+      int x = (ox + c) % n0;
+      x = x < 0 ? x + n0 : x;
+      region[e] = __ldg(&grid[static_cast<int64_t>(y) * n0 + x]);
+    }
+    __syncthreads();
+    for (uint32_t slot = first + threadIdx.x; slot < last; slot += kRegionThreads) {
+      const PreparedWindow<2> win = static_cast<const PreparedWindow<2>*>(windows)[slot];
+      const uint32_t point = perm[slot];
+      float re = 0.0f, im = 0.0f;
+      if (win.start[0] >= 0) {
+        float wx[W], wy[W];
+        horner32_window<W>(win.offset[0], g.horner32, wx);
+        horner32_window<W>(win.offset[1], g.horner32, wy);
+        int dx = (win.start[0] - ox) % n0;
+        dx = dx < 0 ? dx + n0 : dx;
+        int dy = (win.start[1] - oy) % n1;
+        dy = dy < 0 ? dy + n1 : dy;
+        if (dx + W <= S && dy + W <= S) {
+#pragma unroll
+          for (int j = 0; j < W; ++j) {
+            const float2* row = region + (dy + j) * S + dx;
+            float rr = 0.0f, ri = 0.0f;
+#pragma unroll
+            for (int i = 0; i < W; ++i) {
+              const float2 v = row[i];
+              rr = fmaf(v.x, wx[i], rr);
+              ri = fmaf(v.y, wx[i], ri);
+            }
+            re = fmaf(rr, wy[j], re);
+            im = fmaf(ri, wy[j], im);
+          }
+        } else {
+#pragma unroll 1
+          for (int j = 0; j < W; ++j) {
+            int y = win.start[1] + j;
+            y = y >= n1 ? y - n1 : y;
+            float rr = 0.0f, ri = 0.0f;
+            for (int i = 0; i < W; ++i) {
+              int x = win.start[0] + i;
+              x = x >= n0 ? x - n0 : x;
+              const float2 v = __ldg(&grid[static_cast<int64_t>(y) * n0 + x]);
+              rr = fmaf(v.x, wx[i], rr);
+              ri = fmaf(v.y, wx[i], ri);
+            }
+            re = fmaf(rr, wy[j], re);
+            im = fmaf(ri, wy[j], im);
+          }
+        }
+      }
+      output[static_cast<int64_t>(b) * count + point] = make_float2(re, im);
+    }
+  }
+}
+
 // output[b][i] = staged[slot of i][b]: 32 points x 64 vectors per CTA through
 // shared memory, so both the staged rows and the output rows move in whole
 // sectors.
@@ -399,6 +482,28 @@ void execute_impl(const GridParams& g, const Launch<T>& l, cudaStream_t stream) 
 void interpolate_execute(const GridParams& g, const InterpLaunch& l, cudaStream_t stream) {
   execute_impl<F32Window>(g, Launch<F32Window>{l.points, l.windows, l.point_count, l.perm, l.fine, l.batch, l.output},
                           stream);
+}
+
+void interpolate_region_execute(const GridParams& g, const InterpBinsLaunch& l, cudaStream_t stream) {
+  if (l.point_count == 0) return;
+  const dim3 grid(static_cast<unsigned>(l.bins));
+  switch (g.width) {
+#define B200NUFFT_REGION_CASE(WIDTH)                                                                   \
+  case WIDTH:                                                                                          \
+    interpolate_region_kernel<WIDTH><<<grid, kRegionThreads, 0, stream>>>(                              \
+        g, l.windows, l.point_count, l.perm, l.offsets, l.fine, l.batch, l.output);                     \
+    break;
+    B200NUFFT_REGION_CASE(2)
+    B200NUFFT_REGION_CASE(3)
+    B200NUFFT_REGION_CASE(4)
+    B200NUFFT_REGION_CASE(5)
+    B200NUFFT_REGION_CASE(6)
+    B200NUFFT_REGION_CASE(7)
+    default:
+    B200NUFFT_REGION_CASE(8)
+#undef B200NUFFT_REGION_CASE
+  }
+  note_launch();
 }
 
 bool interpolate_bins_supported(const GridParams& g) {

@@ -47,6 +47,9 @@ struct InterpBinsLaunch {
 };
 bool interpolate_bins_supported(const GridParams& g);
 void interpolate_bins_execute(const GridParams& g, const InterpBinsLaunch& launch, cudaStream_t stream);
+// Small batches: one CTA per bin, the bin's grid region staged in shared
+// memory, outputs written in point order (inverse and staged unused).
+void interpolate_region_execute(const GridParams& g, const InterpBinsLaunch& launch, cudaStream_t stream);
 void interpolate_execute64(const GridParams& g, const InterpLaunch64& launch, cudaStream_t stream);
 
 }  // namespace b200nufft

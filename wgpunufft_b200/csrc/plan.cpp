@@ -722,6 +722,20 @@ void NufftPlan::execute_f32(int batch, const void* input, void* output, uint64_t
       interpolate_bins_execute(grid_, b, stream);
       return;
     }
+    if (dim_ == 2 && interpolate_bins_supported(grid_)) {
+      InterpBinsLaunch b{};
+      b.windows = windows_.get();
+      b.point_count = point_count_;
+      b.perm = perm_;
+      b.offsets = static_cast<const uint32_t*>(offsets_.get());
+      b.bins = bins_;
+      b.fine = fine;
+      b.batch = batch;
+      b.output = static_cast<float2*>(output);
+      StageScope scope(&timer_, kStageInterpolation, stream);
+      interpolate_region_execute(grid_, b, stream);
+      return;
+    }
     InterpLaunch l;
     l.points = static_cast<const float*>(sorted_points_.get());
     l.windows = windows_.get();
