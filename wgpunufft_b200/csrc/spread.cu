@@ -298,19 +298,19 @@ __device__ __forceinline__ bool tile_record(const SpreadParams& sp, const typena
   return true;
 }
 
-// Adds a run's register sums to the fixed-point tile and clears them.
+// Adds a run's register sums (already in the fixed-point scale) to the tile
+// and clears them.
 template <int D, int W, typename T>
 __device__ __forceinline__ void flush_run(typename T::Word* acc, int padded, int pad0, int x, int y,
-                                          typename T::Real (*ar)[W], typename T::Real (*ai)[W],
-                                          typename T::Real scale_lo, typename T::Real scale_hi) {
+                                          typename T::Real (*ar)[W], typename T::Real (*ai)[W]) {
   constexpr int R = D == 2 ? W : 1;
 #pragma unroll
   for (int j = 0; j < R; ++j) {
     const int base = (y + j) * pad0 + x;
 #pragma unroll
     for (int i = 0; i < W; ++i) {
-      T::add(acc, padded, 0, base + i, (ar[j][i] * scale_lo) * scale_hi);
-      T::add(acc, padded, 1, base + i, (ai[j][i] * scale_lo) * scale_hi);
+      T::add(acc, padded, 0, base + i, ar[j][i]);
+      T::add(acc, padded, 1, base + i, ai[j][i]);
       ar[j][i] = ai[j][i] = typename T::Real(0);
     }
   }
@@ -778,9 +778,13 @@ __global__ void __launch_bounds__(kSpreadThreads, (spread_run<D, W, T>() > 1 || 
                                   row, local_start, w, s)) {
           continue;
         }
+        // The strength in the fixed-point scale (a power of two: exact), so
+        // the run sums reach the tile without another product.
+        s.x = (s.x * scale_lo) * scale_hi;
+        s.y = (s.y * scale_lo) * scale_hi;
         const int l1 = D == 2 ? local_start[D - 1] : 0;
         if (local_start[0] != run0 || l1 != run1) {
-          if (run0 >= 0) flush_run<D, W, T>(acc, padded, sp.pad[0], run0, run1, ar, ai, scale_lo, scale_hi);
+          if (run0 >= 0) flush_run<D, W, T>(acc, padded, sp.pad[0], run0, run1, ar, ai);
           run0 = local_start[0];
           run1 = l1;
         }
@@ -795,7 +799,7 @@ __global__ void __launch_bounds__(kSpreadThreads, (spread_run<D, W, T>() > 1 || 
           }
         }
       }
-      if (run0 >= 0) flush_run<D, W, T>(acc, padded, sp.pad[0], run0, run1, ar, ai, scale_lo, scale_hi);
+      if (run0 >= 0) flush_run<D, W, T>(acc, padded, sp.pad[0], run0, run1, ar, ai);
     }
   }
   __syncthreads();
