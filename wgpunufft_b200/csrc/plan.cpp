@@ -425,8 +425,10 @@ void NufftPlan::configure_tiles() {
   // about four CTAs per SM have work.
   const int64_t spread_ctas = 4 * 148;
   int64_t cap = (std::max<int64_t>(point_count_, 1) + spread_ctas - 1) / spread_ctas;
-  // 3D parts stay within the 2048 records that crowded tiles bucket in shared memory.
-  const int64_t part_cap = dim_ == 3 ? 2048 : kPartCap;
+  // 3D parts stay within the 2048 records that crowded tiles bucket in shared
+  // memory; 1D and 2D f32 parts take up to 16384 records, so that a thread's
+  // register runs can reach 64 records in crowded tiles.
+  const int64_t part_cap = dim_ == 3 ? 2048 : (precision_ == B200NUFFT_PRECISION_F32 ? 16384 : kPartCap);
   cap = std::min<int64_t>(part_cap, std::max<int64_t>(256, (cap + 255) / 256 * 256));
   sp.part_cap = static_cast<int32_t>(cap);
   sp.headroom = ilog2(static_cast<int64_t>(kPartCap) + 1);

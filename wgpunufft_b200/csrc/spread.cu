@@ -234,7 +234,7 @@ __global__ void __launch_bounds__(1024) part_scan_kernel(const uint32_t* __restr
 
 // Records per register run of a thread: one for 3D and for windows whose
 // w^2 complex accumulators would not fit in registers.
-constexpr int kRunBits = 3;
+constexpr int kRunBits = 6;
 template <int D, int W, typename T>
 __host__ __device__ constexpr int spread_run() {
   return (D == 1 || (D == 2 && 2 * W * W * sizeof(typename T::Real) < 400)) ? (1 << kRunBits) : 1;
