@@ -395,6 +395,33 @@ int select_device(const AdapterSelection& sel) {
 
 // ---------------------------------------------------------------------------
 
+// A non-blocking stream for the input upload of execute, so that the copy
+// overlaps the bin sort that set_points left running on the default stream;
+// the plan's kernels wait for it through `uploaded`.
+struct UploadStream {
+  cudaStream_t stream = nullptr;
+  cudaEvent_t uploaded = nullptr;
+  int device = -1;
+  void ensure(int dev) {
+    if (stream) return;
+    b200nufft::check_cuda(cudaStreamCreateWithFlags(&stream, cudaStreamNonBlocking), "create upload stream");
+    b200nufft::check_cuda(cudaEventCreateWithFlags(&uploaded, cudaEventDisableTiming), "create upload event");
+    device = dev;
+  }
+  UploadStream() = default;
+  UploadStream(const UploadStream&) = delete;
+  UploadStream& operator=(const UploadStream&) = delete;
+  ~UploadStream() {
+    if (!stream) return;
+    int current = 0;
+    cudaGetDevice(&current);
+    cudaSetDevice(device);
+    cudaEventDestroy(uploaded);
+    cudaStreamDestroy(stream);
+    cudaSetDevice(current);
+  }
+};
+
 struct HostPlan {
   Spec spec;
   int precision = B200NUFFT_PRECISION_F64;
@@ -404,6 +431,7 @@ struct HostPlan {
   std::unique_ptr<b200nufft::Type3Plan> plan3;
   std::vector<double> source_lo, source_hi, target_lo, target_hi;
   DeviceBuffer points, targets, input, output, staging, checks;
+  UploadStream upload;
   int64_t point_count = -1;
   int64_t target_count = 0;
 };
@@ -653,14 +681,21 @@ void execute(HostPlan& p, const T* in, T* out, const char* in_name, const char* 
                       "host copies");
   }
   unsigned long long* checks = static_cast<unsigned long long*>(p.checks.reserve(16 * sizeof(unsigned long long), "checks"));
-  b200nufft::check_cuda(cudaMemsetAsync(checks, 0xFF, sizeof(unsigned long long), nullptr), "reset checks");
+  // The upload and its checks run beside the sort of set_points (the previous
+  // execute ended with a synchronous read, and set_points' own copies were
+  // read back, so nothing in flight uses these buffers).
+  p.upload.ensure(p.device);
+  cudaStream_t upload = p.upload.stream;
+  b200nufft::check_cuda(cudaMemsetAsync(checks, 0xFF, sizeof(unsigned long long), upload), "reset checks");
   if (in_scalars > 0) {
     void* landing = direct ? d_in : p.staging.get();
     b200nufft::check_cuda(cudaMemcpyAsync(landing, in, static_cast<size_t>(in_scalars) * sizeof(T),
-                                          cudaMemcpyHostToDevice, nullptr),
+                                          cudaMemcpyHostToDevice, upload),
                           "copy input");
-    capi_convert_values(scalar, landing, in_scalars, p.precision, direct ? nullptr : d_in, checks, nullptr);
+    capi_convert_values(scalar, landing, in_scalars, p.precision, direct ? nullptr : d_in, checks, upload);
   }
+  b200nufft::check_cuda(cudaEventRecord(p.upload.uploaded, upload), "record upload");
+  b200nufft::check_cuda(cudaStreamWaitEvent(nullptr, p.upload.uploaded, 0), "wait for upload");
   if (p.spec.kind != 3) {
     p.plan12->execute(p.spec.ntrans, d_in, d_out, nullptr);
   } else {
