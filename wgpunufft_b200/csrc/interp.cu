@@ -323,6 +323,14 @@ __global__ void __launch_bounds__(kRegionThreads) interpolate_region_kernel(
   const int n0 = g.axis[0].length, n1 = g.axis[1].length;
   const int ox = static_cast<int>(bin % bins0) * 8 - W / 2 - 2;
   const int oy = static_cast<int>(bin / bins0) * 8 - W / 2 - 2;
+  // The first point's window and index are loaded before the region, so
+  // their latency overlaps the staging.
+  PreparedWindow<2> next_win{};
+  uint32_t next_point = 0;
+  if (first + threadIdx.x < last) {
+    next_win = static_cast<const PreparedWindow<2>*>(windows)[first + threadIdx.x];
+    next_point = perm[first + threadIdx.x];
+  }
   for (int b = 0; b < batch; ++b) {
     const float2* grid = fine + static_cast<int64_t>(b) * g.fine_count;
     __syncthreads();  // the previous vector's reads are done
@@ -336,8 +344,10 @@ __global__ void __launch_bounds__(kRegionThreads) interpolate_region_kernel(
     }
     __syncthreads();
     for (uint32_t slot = first + threadIdx.x; slot < last; slot += kRegionThreads) {
-      const PreparedWindow<2> win = static_cast<const PreparedWindow<2>*>(windows)[slot];
-      const uint32_t point = perm[slot];
+      const PreparedWindow<2> win = slot == first + threadIdx.x
+                                        ? next_win
+                                        : static_cast<const PreparedWindow<2>*>(windows)[slot];
+      const uint32_t point = slot == first + threadIdx.x ? next_point : perm[slot];
       float re = 0.0f, im = 0.0f;
       if (win.start[0] >= 0) {
         float wx[W], wy[W];
