@@ -298,6 +298,38 @@ __device__ __forceinline__ bool tile_record(const SpreadParams& sp, const typena
   return true;
 }
 
+// Slot of record r of the tile's bin rows (rows are visited in order).
+__device__ __forceinline__ uint32_t record_slot(uint32_t r, int& row, const uint32_t* row_begin,
+                                                const uint32_t* row_prefix, int rows) {
+  if (r >= row_prefix[row + 1] || r < row_prefix[row]) {
+    int low = 0, high = rows - 1;
+    while (low < high) {
+      const int mid = (low + high + 1) >> 1;
+      if (row_prefix[mid] <= r) low = mid; else high = mid - 1;
+    }
+    row = low;
+  }
+  return row_begin[row] + (r - row_prefix[row]);
+}
+
+// A prepared f32 record: its start relative to the tile and its window
+// weights; false when it lies outside the fold reach or starts in another tile.
+template <int D, int W>
+__device__ __forceinline__ bool prepared_record(const SpreadParams& sp, const PreparedWindow<D>& win,
+                                                const int* origin, int* local_start, float (*w)[W]) {
+  if (win.start[0] < 0) return false;
+  bool inside = true;
+#pragma unroll
+  for (int a = 0; a < D; ++a) {
+    local_start[a] = win.start[a] - origin[a];
+    inside = inside && local_start[a] >= 0 && local_start[a] < sp.tile[a];
+  }
+  if (!inside) return false;
+#pragma unroll
+  for (int a = 0; a < D; ++a) horner32_window<W>(win.offset[a], sp.grid.horner32, w[a]);
+  return true;
+}
+
 // Adds a run's register sums (already in the fixed-point scale) to the tile
 // and clears them.
 template <int D, int W, typename T>
@@ -770,13 +802,36 @@ __global__ void __launch_bounds__(kSpreadThreads, (spread_run<D, W, T>() > 1 || 
         for (int i = 0; i < W; ++i) ar[j][i] = ai[j][i] = Real(0);
       }
       int run0 = -1, run1 = 0;
+      // f32: the next record's window and point index are loaded one record
+      // ahead, so their latency overlaps the current record's work.
+      PreparedWindow<D> next_win{};
+      uint32_t next_point = 0;
+      if constexpr (T::kPreparedWindows) {
+        if (first < stop) {
+          const uint32_t slot = record_slot(first, row, row_begin, row_prefix, rows);
+          next_win = static_cast<const PreparedWindow<D>*>(windows)[slot];
+          next_point = perm[slot];
+        }
+      }
       for (uint32_t r = first; r < stop; ++r) {
         int local_start[D];
         Real w[D][W];
         typename T::Complex s;
-        if (!tile_record<D, W, T>(sp, points, windows, sv, perm, row_begin, row_prefix, rows, origin, r,
-                                  row, local_start, w, s)) {
-          continue;
+        if constexpr (T::kPreparedWindows) {
+          const PreparedWindow<D> win = next_win;
+          const uint32_t point = next_point;
+          if (r + 1 < stop) {
+            const uint32_t slot = record_slot(r + 1, row, row_begin, row_prefix, rows);
+            next_win = static_cast<const PreparedWindow<D>*>(windows)[slot];
+            next_point = perm[slot];
+          }
+          s = sv[point];
+          if (!prepared_record<D, W>(sp, win, origin, local_start, w)) continue;
+        } else {
+          if (!tile_record<D, W, T>(sp, points, windows, sv, perm, row_begin, row_prefix, rows, origin, r,
+                                    row, local_start, w, s)) {
+            continue;
+          }
         }
         // The strength in the fixed-point scale (a power of two: exact), so
         // the run sums reach the tile without another product.
