@@ -802,15 +802,25 @@ __global__ void __launch_bounds__(kSpreadThreads, (spread_run<D, W, T>() > 1 || 
         for (int i = 0; i < W; ++i) ar[j][i] = ai[j][i] = Real(0);
       }
       int run0 = -1, run1 = 0;
-      // f32: the next record's window and point index are loaded one record
-      // ahead, so their latency overlaps the current record's work.
-      PreparedWindow<D> next_win{};
-      uint32_t next_point = 0;
+      // f32: records are loaded ahead of their use, so the load latency
+      // overlaps the work on earlier records: the window and point index two
+      // records ahead and the strength one ahead (one and zero ahead for
+      // windows wider than 6, whose accumulators leave no registers for it).
+      constexpr bool kTwoAhead = 2 * W * W * sizeof(Real) < 392;
+      PreparedWindow<D> win0{}, win1{};
+      uint32_t point0 = 0, point1 = 0;
+      typename T::Complex s0{};
       if constexpr (T::kPreparedWindows) {
         if (first < stop) {
           const uint32_t slot = record_slot(first, row, row_begin, row_prefix, rows);
-          next_win = static_cast<const PreparedWindow<D>*>(windows)[slot];
-          next_point = perm[slot];
+          win0 = static_cast<const PreparedWindow<D>*>(windows)[slot];
+          point0 = perm[slot];
+          if (kTwoAhead) s0 = sv[point0];
+        }
+        if (kTwoAhead && first + 1 < stop) {
+          const uint32_t slot = record_slot(first + 1, row, row_begin, row_prefix, rows);
+          win1 = static_cast<const PreparedWindow<D>*>(windows)[slot];
+          point1 = perm[slot];
         }
       }
       for (uint32_t r = first; r < stop; ++r) {
@@ -818,14 +828,25 @@ __global__ void __launch_bounds__(kSpreadThreads, (spread_run<D, W, T>() > 1 || 
         Real w[D][W];
         typename T::Complex s;
         if constexpr (T::kPreparedWindows) {
-          const PreparedWindow<D> win = next_win;
-          const uint32_t point = next_point;
-          if (r + 1 < stop) {
-            const uint32_t slot = record_slot(r + 1, row, row_begin, row_prefix, rows);
-            next_win = static_cast<const PreparedWindow<D>*>(windows)[slot];
-            next_point = perm[slot];
+          const PreparedWindow<D> win = win0;
+          if constexpr (kTwoAhead) {
+            s = s0;
+            if (r + 1 < stop) s0 = sv[point1];
+            win0 = win1;
+            if (r + 2 < stop) {
+              const uint32_t slot = record_slot(r + 2, row, row_begin, row_prefix, rows);
+              win1 = static_cast<const PreparedWindow<D>*>(windows)[slot];
+              point1 = perm[slot];
+            }
+          } else {
+            const uint32_t point = point0;
+            if (r + 1 < stop) {
+              const uint32_t slot = record_slot(r + 1, row, row_begin, row_prefix, rows);
+              win0 = static_cast<const PreparedWindow<D>*>(windows)[slot];
+              point0 = perm[slot];
+            }
+            s = sv[point];
           }
-          s = sv[point];
           if (!prepared_record<D, W>(sp, win, origin, local_start, w)) continue;
         } else {
           if (!tile_record<D, W, T>(sp, points, windows, sv, perm, row_begin, row_prefix, rows, origin, r,
