@@ -530,26 +530,51 @@ __device__ void spread_warp3(const SpreadParams& sp, const PreparedWindow<3>* wi
   const uint32_t spread_begin = min(spread_count, per_warp * warp);
   const uint32_t spread_end = min(spread_count, per_warp * (warp + 1));
   int row = 0;
+  // Lane 3 g + a stages axis a of record g of each group; its record's
+  // window and point index are loaded two groups ahead and the strength one
+  // group ahead, so the loads overlap the spreading of earlier groups.
+  const int stage_g = lane / 3, stage_a = lane - 3 * stage_g;
+  const bool stager = lane < 3 * kWarpGroup;
+  PreparedWindow<3> win0{}, win1{};
+  win0.start[0] = win1.start[0] = -1;
+  uint32_t point1 = 0;
+  float2 c0 = make_float2(0.0f, 0.0f);
+  auto fetch = [&](uint32_t r, PreparedWindow<3>& win, uint32_t& point) {
+    win.start[0] = -1;
+    if (stager && r < spread_end) {
+      const uint32_t slot = bucket ? sorted[r] : slot_of(record_begin + r, row);
+      win = win3[slot];
+      if (stage_a == 0) point = perm[slot];
+    }
+  };
+  {
+    uint32_t point0 = 0;
+    fetch(spread_begin + stage_g, win0, point0);
+    if (stager && stage_a == 0 && spread_begin + stage_g < spread_end) c0 = sv[point0];
+    fetch(spread_begin + kWarpGroup + stage_g, win1, point1);
+  }
   for (uint32_t first = spread_begin; first < spread_end; first += kWarpGroup) {
+    const PreparedWindow<3> win = win0;
+    const float2 c = c0;
+    if (stager && stage_a == 0 && first + kWarpGroup + stage_g < spread_end) c0 = sv[point1];
+    win0 = win1;
+    fetch(first + 2 * kWarpGroup + stage_g, win1, point1);
     // Stage the group: lane 3 g + a evaluates axis a of record g; lane 3 g
     // also stages the scaled strength and the start's tile offset (-1: skip).
-    if (lane < 3 * kWarpGroup) {
-      const int g = lane / 3, a = lane - 3 * g;
+    if (stager) {
+      const int g = stage_g, a = stage_a;
       const uint32_t r = first + g;
       int base = -1;
       float w[W];
 #pragma unroll
       for (int j = 0; j < W; ++j) w[j] = 0.0f;
       if (r < spread_end) {
-        const uint32_t slot = bucket ? sorted[r] : slot_of(record_begin + r, row);
-        const PreparedWindow<3> win = win3[slot];
         int x, y, z;
         if (local_of(win, x, y, z)) {
           base = x + y * pitch0 + z * pitch01;
           const float offset = a == 0 ? win.offset[0] : (a == 1 ? win.offset[1] : win.offset[2]);
           horner32_window<W>(offset, sp.grid.horner32, w);
           if (a == 0) {
-            const float2 c = sv[perm[slot]];
             my_stage[g][24] = (c.x * scale_lo) * scale_hi;
             my_stage[g][25] = (c.y * scale_lo) * scale_hi;
           }
