@@ -87,7 +87,10 @@ typedef enum b200nufft_status {
 #define B200NUFFT_MODE_ORDER_CENTERED 0
 #define B200NUFFT_MODE_ORDER_FFT 1
 
-#define B200NUFFT_MAX_DIMENSIONS 3
+/* Type-1 and type-2 plans take 1 to 8 dimensions (4 to 8 run a generic
+ * path without bins); type-3 plans 1 to 3. */
+#define B200NUFFT_MAX_DIMENSIONS 8
+#define B200NUFFT_MAX_TYPE3_DIMENSIONS 3
 
 /* Type-1 spreading engines. AUTO runs 2D f32 type-1 plans of batch >= 16 on
  * the tensor cores (3xTF32 tcgen05 MMAs) when their active batch is at least

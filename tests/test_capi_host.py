@@ -57,7 +57,9 @@ def test_validation_errors_follow_the_reference():
     assert status_of(1, (8, 0), 1e-6) == "ZeroMode"
     assert status_of(1, (8,), 1e-6, batch=0) == "InvalidBatch"
     assert status_of(1, (), 1e-6) == "InvalidDimensions"
-    assert status_of(1, (4,) * 4, 1e-6) == "GpuDimensionsUnsupported"
+    assert status_of(1, (2,) * 9, 1e-6) == "InvalidDimensions"
+    assert status_of(1, (4,) * 4, 1e-6) == "Success"
+    assert status_of(2, (3,) * 8, 1e-2) == "Success"
     assert status_of(1, (1000,), 1e-6, sigma=1.0e15) == "FineGridTooLarge"
     # src/config.rs:310-318: sigma 1.25 at 1e-6 misses f32 by far in 2D and 3D.
     assert status_of(1, (256, 256), 1e-6, sigma=1.25) == "F32ToleranceUnreachable"

@@ -354,8 +354,8 @@ def test_gpu_errors_are_reported_with_messages():
         assert lib.wgpu_nufft_execute(plan, ptr(good), ptr(f)) == 0, last_error()
         ref = native.direct_type1(ok[:, None], np.array([[1.0 + 0j]]), [8], 1)[0]
         assert rel_l2(complex_of(f), ref) < 1e-5
-        # Dimensions beyond the GPU's three are a plan error.
-        assert makeplan(1, [4, 4, 4, 4])[0] == 2
+        # More than eight dimensions are an argument error.
+        assert makeplan(1, [2] * 9)[0] == 1 and "between 1 and 8" in last_error()
     finally:
         lib.wgpu_nufft_destroy(plan)
 
@@ -438,3 +438,33 @@ def test_gpu_adapters_are_listed_and_selected():
     if len(adapters) > 1:
         assert type1_with(opts(index=2)) == 1 and "wgpu_nufft_shutdown" in last_error()
     lib.wgpu_nufft_shutdown()
+
+
+@pytest.mark.gpu
+def test_gpu_four_dimensional_plans_through_setpts_nd():
+    """Plans of more than three dimensions take point-major coordinates
+    through setpts_nd and match FP64 direct sums (type 1 and type 2)."""
+    rng = np.random.default_rng(44)
+    n_modes = [4, 3, 5, 2]
+    m = 300
+    pts = rng.uniform(-np.pi, np.pi, (m, 4))
+    for kind in (1, 2):
+        code, plan = makeplan(kind, n_modes, eps=1e-6)
+        assert code == 0, last_error()
+        try:
+            assert lib.wgpu_nufft_setpts_nd(plan, m, ptr(pts), 0, None) == 0, last_error()
+            if kind == 1:
+                c = rng.standard_normal(2 * m)
+                f = np.zeros(2 * int(np.prod(n_modes)))
+                assert lib.wgpu_nufft_execute(plan, ptr(c), ptr(f)) == 0, last_error()
+                ref = native.direct_type1(pts, complex_of(c)[None, :], n_modes, 1)[0]
+                assert rel_l2(complex_of(f), ref) < 1e-5
+            else:
+                f = rng.standard_normal(2 * int(np.prod(n_modes)))
+                c = np.zeros(2 * m)
+                # execute(plan, c, f): values at the points, then modes.
+                assert lib.wgpu_nufft_execute(plan, ptr(c), ptr(f)) == 0, last_error()
+                ref = native.direct_type2(pts, complex_of(f)[None, :], n_modes, 1)[0]
+                assert rel_l2(complex_of(c), ref) < 1e-5
+        finally:
+            lib.wgpu_nufft_destroy(plan)

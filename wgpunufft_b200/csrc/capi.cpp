@@ -471,7 +471,7 @@ std::unique_ptr<HostPlan> make_host_plan(const Spec& spec) {
   b200nufft::check_cuda(cudaSetDevice(plan->device), "select device");
   if (spec.kind != 3) {
     if (spec.dim > B200NUFFT_MAX_DIMENSIONS) {
-      throw NufftFailure{B200NUFFT_GPU_DIMENSIONS_UNSUPPORTED, "GPU plans support 1 to 3 dimensions"};
+      throw NufftFailure{B200NUFFT_GPU_DIMENSIONS_UNSUPPORTED, "GPU plans support 1 to 8 dimensions"};
     }
     b200nufft_config c;
     b200nufft_default_config(&c);
@@ -490,7 +490,7 @@ std::unique_ptr<HostPlan> make_host_plan(const Spec& spec) {
     c.device = plan->device;
     plan->plan12 = std::make_unique<b200nufft::NufftPlan>(c, true);
   } else {
-    if (spec.dim > B200NUFFT_MAX_DIMENSIONS) {
+    if (spec.dim > B200NUFFT_MAX_TYPE3_DIMENSIONS) {
       throw NufftFailure{B200NUFFT_GPU_DIMENSIONS_UNSUPPORTED, "GPU type-3 plans support 1 to 3 dimensions"};
     }
     // The parts of the configuration that do not depend on the points are
@@ -591,7 +591,7 @@ void set_points(HostPlan& p, const HostPoints<T>& pts, const HostPoints<T>& tgs)
   p.staging.reserve(std::max<size_t>(target_offset + target_bytes, 16), "host copies");
   // checks: [0] first bad point element, [1] first bad target element,
   // [2 .. 2 + 2 dim) point bounds, [2 + 2 dim .. 2 + 4 dim) target bounds.
-  unsigned long long init[16];
+  unsigned long long init[2 + 4 * 8];
   init[0] = init[1] = ~0ull;
   for (int a = 0; a < dim; ++a) {
     init[2 + 2 * a] = init[2 + 2 * dim + 2 * a] = ~0ull;
@@ -601,7 +601,7 @@ void set_points(HostPlan& p, const HostPoints<T>& pts, const HostPoints<T>& tgs)
   b200nufft::check_cuda(cudaMemcpyAsync(checks, init, sizeof(init), cudaMemcpyHostToDevice, nullptr), "reset checks");
   upload_points(p, pts, p.points, type3 ? 1 : 0, checks, type3 ? checks + 2 : nullptr, 0);
   if (type3) upload_points(p, tgs, p.targets, 1, checks + 1, checks + 2 + 2 * dim, target_offset);
-  unsigned long long result[16];
+  unsigned long long result[2 + 4 * 8];
   b200nufft::check_cuda(cudaMemcpy(result, checks, sizeof(result), cudaMemcpyDeviceToHost), "read checks");
   if (type3 && result[1] != ~0ull) {
     const int64_t i = static_cast<int64_t>(result[1] / dim);

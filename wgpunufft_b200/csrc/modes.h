@@ -10,8 +10,8 @@ namespace b200nufft {
 struct ModeParams {
   int32_t dimensions;
   int32_t centered;  // centered mode order, else FFT order
-  int64_t modes[3];
-  int64_t fine[3];
+  int64_t modes[8];
+  int64_t fine[8];
   int64_t mode_count;
   int64_t fine_count;
 };

@@ -85,7 +85,7 @@ NufftPlan::NufftPlan(const b200nufft_config& c, bool with_device) : has_device_(
   }
   if (c.dimensions > B200NUFFT_MAX_DIMENSIONS) {
     throw NufftFailure{B200NUFFT_GPU_DIMENSIONS_UNSUPPORTED,
-                       "GPU plans support 1 to 3 dimensions"};
+                       "GPU plans support 1 to 8 dimensions"};
   }
   dim_ = c.dimensions;
   batch_ = c.batch;
@@ -157,7 +157,7 @@ NufftPlan::NufftPlan(const b200nufft_config& c, bool with_device) : has_device_(
     }
     fine_count_ *= fine_[a];
   }
-  layout_ = SpreadLayout::for_grid(kernel_.width, fine_,
+  if (dim_ <= 3) layout_ = SpreadLayout::for_grid(kernel_.width, fine_,
                                    precision_ == B200NUFFT_PRECISION_F32 ? LayoutPrecision::F32
                                    : precision_ == B200NUFFT_PRECISION_F64 ? LayoutPrecision::F64
                                                                            : LayoutPrecision::Df64);
@@ -232,7 +232,32 @@ NufftPlan::NufftPlan(const b200nufft_config& c, bool with_device) : has_device_(
       }
     }
   }
-  for (int a = 0; a < dim_; ++a) {
+  if (dim_ > 3) {
+    // Plans of 4 to 8 dimensions: fold constants for every axis, no bins.
+    nd_.dimensions = dim_;
+    nd_.width = kernel_.width;
+    nd_.f32 = precision_ == B200NUFFT_PRECISION_F32 ? 1 : 0;
+    nd_.half_width = static_cast<float>(kernel_.half_width());
+    nd_.beta = static_cast<float>(kernel_.beta);
+    nd_.half_width64 = kernel_.half_width();
+    nd_.fine_count = fine_count_;
+    nd_.horner = grid_.horner;
+    nd_.horner_rows = grid_.horner_rows;
+    for (int a = 0; a < dim_; ++a) {
+      const double scale = static_cast<double>(fine_[a]) / kTwoPi;
+      FoldAxis& axis = nd_.axis[a];
+      axis.scale_hi = static_cast<float>(scale);
+      axis.scale_lo = static_cast<float>(scale - static_cast<double>(axis.scale_hi));
+      axis.origin = static_cast<float>(fine_[a] / 2);
+      axis.length_f = static_cast<float>(fine_[a]);
+      axis.length = static_cast<int32_t>(fine_[a]);
+      nd_.axis64[a].scale = scale;
+      nd_.axis64[a].origin = static_cast<double>(fine_[a] / 2);
+      nd_.axis64[a].length = static_cast<double>(fine_[a]);
+      nd_.fine[a] = fine_[a];
+    }
+  }
+  for (int a = 0; a < std::min(dim_, 3); ++a) {
     const double scale = static_cast<double>(fine_[a]) / kTwoPi;
     FoldAxis& axis = grid_.axis[a];
     axis.scale_hi = static_cast<float>(scale);
@@ -266,6 +291,7 @@ NufftPlan::~NufftPlan() {
   cudaSetDevice(device_);
   cudaDeviceSynchronize();
   for (auto& entry : ffts_) cufftDestroy(entry.second);
+  for (auto& entry : nd_ffts_) cufftDestroy(entry.second);
 }
 
 void NufftPlan::make_current() const { check_cuda(cudaSetDevice(device_), "select plan device"); }
@@ -479,6 +505,7 @@ void NufftPlan::configure_tiles() {
 int NufftPlan::choose_geometry(int64_t point_count) const {
   if (type_ != 1) throw NufftFailure{B200NUFFT_INVALID_ARGUMENT, "type-2 plans bin in one geometry"};
   if (point_count < 0) throw NufftFailure{B200NUFFT_INVALID_ARGUMENT, "negative point count"};
+  if (dim_ > 3) throw NufftFailure{B200NUFFT_INVALID_ARGUMENT, "plans of more than three dimensions do not bin"};
   return layout_.choose_geometry(point_count);
 }
 
@@ -497,6 +524,29 @@ void NufftPlan::set_points(int64_t count, const void* points, cudaStream_t strea
   }
   point_count_ = count;
   points_ = points;
+  if (dim_ > 3) {
+    // No bins: the coordinates are kept (in f64 for Df64 plans) as given.
+    const size_t coords = static_cast<size_t>(std::max<int64_t>(count, 1)) * dim_;
+    if (precision_ == B200NUFFT_PRECISION_F32) {
+      void* kept = sorted_points_.reserve(coords * sizeof(float), "coordinates");
+      if (count > 0) {
+        check_cuda(cudaMemcpyAsync(kept, points, static_cast<size_t>(count) * dim_ * sizeof(float),
+                                   cudaMemcpyDeviceToDevice, stream),
+                   "keep coordinates");
+      }
+    } else {
+      void* kept = sorted_points_.reserve(coords * sizeof(double), "coordinates");
+      if (count > 0 && precision_ == B200NUFFT_PRECISION_DF64) {
+        df64_to_f64(static_cast<const float*>(points), count * dim_, static_cast<double*>(kept), stream);
+      } else if (count > 0) {
+        check_cuda(cudaMemcpyAsync(kept, points, static_cast<size_t>(count) * dim_ * sizeof(double),
+                                   cudaMemcpyDeviceToDevice, stream),
+                   "keep coordinates");
+      }
+    }
+    check_cuda(cudaGetLastError(), "set points launch");
+    return;
+  }
   if (type_ == 1) {
     geometry_ = layout_.choose_geometry(count);
     configure_bins(geometry_);
@@ -646,6 +696,10 @@ void NufftPlan::execute_f32(int batch, const void* input, void* output, uint64_t
                             cudaStream_t stream) {
   float2* fine = static_cast<float2*>(fine_grid_.get());
   const int direction = isign_ >= 0 ? CUFFT_INVERSE : CUFFT_FORWARD;
+  if (dim_ > 3) {
+    execute_nd(batch, input, output, fine, direction, stream);
+    return;
+  }
   if (type_ == 1) {
     if (point_count_ == 0) {
       check_cuda(cudaMemsetAsync(output, 0, out_bytes, stream), "zero type-1 output");
@@ -766,7 +820,9 @@ void NufftPlan::execute_f64(int batch, const void* input, void* output, uint64_t
     in = reinterpret_cast<const double2*>(converted);
     out = static_cast<double2*>(output64_.reserve(std::max<uint64_t>(out_bytes, 16), "f64 output"));
   }
-  if (type_ == 1) {
+  if (dim_ > 3) {
+    execute_nd(batch, in, out, fine, direction, stream);
+  } else if (type_ == 1) {
     if (point_count_ == 0) {
       check_cuda(cudaMemsetAsync(output, 0, out_bytes, stream), "zero type-1 output");
       return;
@@ -814,6 +870,103 @@ void NufftPlan::execute_f64(int batch, const void* input, void* output, uint64_t
   }
 }
 
+void NufftPlan::spread_nd(int batch, const void* strengths, void* grid, cudaStream_t stream) {
+  StageScope scope(&timer_, kStageSpread, stream);
+  auto* acc = static_cast<unsigned long long*>(
+      nd_acc_.reserve(static_cast<size_t>(batch) * fine_count_ * 2 * sizeof(unsigned long long), "integer fine grid"));
+  nd_spread(nd_, sorted_points_.get(), strengths, point_count_, batch, acc,
+            static_cast<unsigned long long*>(max_bits_.get()), grid, stream);
+}
+
+void NufftPlan::execute_nd(int batch, const void* input, void* output, void* fine, int direction,
+                           cudaStream_t stream) {
+  const bool f32 = precision_ == B200NUFFT_PRECISION_F32;
+  if (type_ == 1) {
+    spread_nd(batch, input, fine, stream);
+    run_fft_nd(fine, batch, direction, stream);
+    StageScope scope(&timer_, kStageDeconvolution, stream);
+    if (f32) {
+      deconvolve_f32(modes_params_, batch, static_cast<const float2*>(fine),
+                     static_cast<const float*>(amplitudes_.get()), static_cast<float2*>(output), stream);
+    } else {
+      deconvolve_f64(modes_params_, batch, static_cast<const double2*>(fine),
+                     static_cast<const double*>(amplitudes_.get()), static_cast<double2*>(output), stream);
+    }
+    return;
+  }
+  {
+    StageScope scope(&timer_, kStagePredeconvolution, stream);
+    if (f32) {
+      predeconvolve_f32(modes_params_, batch, static_cast<const float2*>(input),
+                        static_cast<const float*>(amplitudes_.get()), static_cast<float2*>(fine), stream);
+    } else {
+      predeconvolve_f64(modes_params_, batch, static_cast<const double2*>(input),
+                        static_cast<const double*>(amplitudes_.get()), static_cast<double2*>(fine), stream);
+    }
+  }
+  run_fft_nd(fine, batch, direction, stream);
+  StageScope scope(&timer_, kStageInterpolation, stream);
+  nd_interpolate(nd_, sorted_points_.get(), fine, point_count_, batch, output, stream);
+}
+
+// The d-dimensional transform as transforms over groups of up to three
+// consecutive axes: the first group batched over everything else, each later
+// group batched over the cells of the axes before it (element stride
+// `inner`) and run once per block of the axes after it.
+void NufftPlan::run_fft_nd(void* fine, int batch, int direction, cudaStream_t stream) {
+  StageScope scope(&timer_, kStageFft, stream);
+  const bool f32 = precision_ == B200NUFFT_PRECISION_F32;
+  const size_t element = 2 * scalar_bytes();
+  int64_t inner = 1;
+  for (int a0 = 0; a0 < dim_; a0 += 3) {
+    const int a1 = std::min(dim_, a0 + 3);
+    const int rank = a1 - a0;
+    int64_t span = 1, outer = batch;
+    for (int a = a0; a < a1; ++a) span *= fine_[a];
+    for (int a = a1; a < dim_; ++a) outer *= fine_[a];
+    const int64_t key = static_cast<int64_t>(a0) * (int64_t(1) << 32) + batch;
+    auto found = nd_ffts_.find(key);
+    cufftHandle h;
+    if (found != nd_ffts_.end()) {
+      h = found->second;
+    } else {
+      if (inner * span > std::numeric_limits<int32_t>::max() || outer > std::numeric_limits<int32_t>::max()) {
+        throw NufftFailure{B200NUFFT_FFT_SHAPE_UNSUPPORTED, "fine grid too large for the grouped FFT"};
+      }
+      int n[3];
+      for (int r = 0; r < rank; ++r) n[r] = static_cast<int>(fine_[a1 - 1 - r]);
+      const cufftType kind = f32 ? CUFFT_C2C : CUFFT_Z2Z;
+      cufftResult r;
+      if (a0 == 0) {
+        r = cufftPlanMany(&h, rank, n, nullptr, 1, static_cast<int>(span), nullptr, 1, static_cast<int>(span), kind,
+                          static_cast<int>(outer));
+      } else {
+        r = cufftPlanMany(&h, rank, n, n, static_cast<int>(inner), 1, n, static_cast<int>(inner), 1, kind,
+                          static_cast<int>(inner));
+      }
+      if (r != CUFFT_SUCCESS) {
+        throw NufftFailure{B200NUFFT_FFT_SHAPE_UNSUPPORTED,
+                           "cuFFT plan creation failed with code " + std::to_string(static_cast<int>(r))};
+      }
+      nd_ffts_[key] = h;
+    }
+    cufftSetStream(h, stream);
+    const int64_t blocks = a0 == 0 ? 1 : outer;
+    for (int64_t o = 0; o < blocks; ++o) {
+      char* base = static_cast<char*>(fine) + static_cast<size_t>(o * inner * span) * element;
+      const cufftResult r =
+          f32 ? cufftExecC2C(h, reinterpret_cast<cufftComplex*>(base), reinterpret_cast<cufftComplex*>(base), direction)
+              : cufftExecZ2Z(h, reinterpret_cast<cufftDoubleComplex*>(base),
+                             reinterpret_cast<cufftDoubleComplex*>(base), direction);
+      if (r != CUFFT_SUCCESS) {
+        throw NufftFailure{B200NUFFT_FFT_EXECUTION_FAILED,
+                           "cuFFT execution failed with code " + std::to_string(static_cast<int>(r))};
+      }
+    }
+    inner *= span;
+  }
+}
+
 void NufftPlan::spread_to(int64_t active_batch, const void* strengths, void* grid,
                           cudaStream_t stream) {
   if (!has_device_ || type_ != 1) {
@@ -829,6 +982,11 @@ void NufftPlan::spread_to(int64_t active_batch, const void* strengths, void* gri
     check_cuda(cudaMemsetAsync(grid, 0, static_cast<size_t>(batch) * fine_count_ * 2 * scalar_bytes(),
                                stream),
                "zero spread grid");
+    return;
+  }
+  if (dim_ > 3) {
+    spread_nd(batch, strengths, grid, stream);
+    check_cuda(cudaGetLastError(), "spread launch");
     return;
   }
   if (precision_ == B200NUFFT_PRECISION_F32) {
@@ -872,6 +1030,7 @@ void NufftPlan::spread_to(int64_t active_batch, const void* strengths, void* gri
 
 void NufftPlan::copy_bin_order(uint32_t* permutation, uint32_t* bin_offsets, cudaStream_t stream) {
   make_current();
+  if (dim_ > 3) throw NufftFailure{B200NUFFT_INVALID_ARGUMENT, "plans of more than three dimensions do not bin"};
   if (point_count_ < 0) {
     throw NufftFailure{B200NUFFT_GPU_EXECUTION_UNAVAILABLE, "no point set"};
   }
@@ -888,6 +1047,7 @@ void NufftPlan::copy_bin_order(uint32_t* permutation, uint32_t* bin_offsets, cud
 }
 
 void NufftPlan::copy_prepared_slots(int32_t* starts, float* offsets, cudaStream_t stream) {
+  if (dim_ > 3) throw NufftFailure{B200NUFFT_INVALID_ARGUMENT, "plans of more than three dimensions do not bin"};
   make_current();
   if (point_count_ < 0 || type_ != 1) {
     throw NufftFailure{B200NUFFT_GPU_EXECUTION_UNAVAILABLE, "no type-1 point set"};

@@ -12,6 +12,7 @@
 #include "interp.h"
 #include "layout.h"
 #include "modes.h"
+#include "nd.h"
 #include "spread.h"
 #include "tc_spread.h"
 
@@ -64,11 +65,16 @@ class NufftPlan {
                    cudaStream_t stream);
   void execute_f64(int batch, const void* input, void* output, uint64_t in_bytes,
                    uint64_t out_bytes, cudaStream_t stream);
+  // Plans of 4 to 8 dimensions: generic spreading / interpolation and an FFT
+  // over groups of up to three axes.
+  void execute_nd(int batch, const void* input, void* output, void* fine, int direction, cudaStream_t stream);
+  void spread_nd(int batch, const void* strengths, void* grid, cudaStream_t stream);
+  void run_fft_nd(void* fine, int batch, int direction, cudaStream_t stream);
   size_t scalar_bytes() const;
 
   int type_ = 1;
   int dim_ = 1;
-  int64_t modes_[3] = {1, 1, 1};
+  int64_t modes_[8] = {1, 1, 1, 1, 1, 1, 1, 1};
   int64_t batch_ = 1;
   double eps_ = 1e-6;
   int isign_ = 1;
@@ -95,6 +101,10 @@ class NufftPlan {
   DeviceBuffer points64_, input64_, output64_;
   DeviceBuffer fine_grid_;
   std::map<int, cufftHandle> ffts_;
+  // Plans of 4 to 8 dimensions.
+  NdParams nd_{};
+  DeviceBuffer nd_acc_;                       // 64-bit integer fine grids of type 1
+  std::map<int64_t, cufftHandle> nd_ffts_;    // by first axis of the group and batch
 
   // Remembered points and their bin order.
   int64_t point_count_ = -1;

@@ -213,7 +213,7 @@ Type3Plan::Type3Plan(const b200nufft_type3_config& c) {
   if (c.dimensions < 1 || c.dimensions > 8) {
     throw NufftFailure{B200NUFFT_INVALID_DIMENSIONS, "dimensions must lie in 1..8"};
   }
-  if (c.dimensions > B200NUFFT_MAX_DIMENSIONS) {
+  if (c.dimensions > B200NUFFT_MAX_TYPE3_DIMENSIONS) {
     throw NufftFailure{B200NUFFT_GPU_DIMENSIONS_UNSUPPORTED, "GPU type-3 plans support 1 to 3 dimensions"};
   }
   if (c.batch <= 0) throw NufftFailure{B200NUFFT_INVALID_BATCH, "batch must be at least one"};

@@ -12,9 +12,9 @@ C-contiguity, finite values, coordinates within [-3 pi, 3 pi] or the type-3
 bounds, batch capacity) before anything runs. Calls on one plan are
 serialized, as the reference's plans lock their state.
 
-Differences: plans of 4 to 8 dimensions raise (the GPU plans here cover 1 to
-3 dimensions), and the reference's CPU plans (`CpuType1Plan` and friends) are
-not provided: this package has no CPU engine.
+Differences: the reference's CPU plans (`CpuType1Plan` and friends) are not
+provided: this package has no CPU engine. Type-1 and type-2 plans take 1 to 8
+dimensions, type-3 plans 1 to 3.
 """
 
 from __future__ import annotations
