@@ -51,6 +51,7 @@ def parse():
     p.add_argument("--no-batched", action="store_true")
     p.add_argument("--no-uneven", action="store_true")
     p.add_argument("--no-radial", action="store_true")
+    p.add_argument("--no-f64", action="store_true")
     return p.parse_args()
 
 
@@ -357,6 +358,56 @@ def radial_3d_line(w, torch, timed, barrier, world, dev, args, rank):
     return result
 
 
+def f64_line(w, torch, timed, barrier, world, dev, args, rank):
+    """f64 plans of the batched configuration: 2D 512^2 modes, 2e6 uniform
+    points, eps 1e-9 (w = 10) and 1e-12 (w = 13), one vector; type-1 and
+    type-2 NU points/s with rel-l2 against FP64 direct sums (8 modes, 64
+    points)."""
+    g = torch.Generator(device=dev)
+    g.manual_seed(SEED + 41)
+    pts = (torch.rand((BATCH_POINTS, 2), generator=g, device=dev, dtype=torch.float64) * (2 * np.pi) - np.pi).contiguous()
+    n = BATCH_MODES[0] * BATCH_MODES[1]
+    steps = max(1, min(args.steps, 5))
+    pts_h = pts.cpu().numpy() if rank == 0 else None
+    result = {"workload": "2d_modes512x512_M2e6_uniform_f64", "modes": list(BATCH_MODES), "points": BATCH_POINTS,
+              "unit": UNIT}
+    for eps in (1e-9, 1e-12):
+        entry = {}
+        c = torch.complex(torch.randn((1, BATCH_POINTS), generator=g, device=dev, dtype=torch.float64),
+                          torch.randn((1, BATCH_POINTS), generator=g, device=dev, dtype=torch.float64))
+        f = torch.complex(torch.randn((1, n), generator=g, device=dev, dtype=torch.float64),
+                          torch.randn((1, n), generator=g, device=dev, dtype=torch.float64))
+        for kind in (1, 2):
+            config = w.NufftConfig(BATCH_MODES, eps, precision=w.Precision.F64)
+            plan = (w.NufftPlan.type1_gpu if kind == 1 else w.NufftPlan.type2_gpu)(config)
+            plan.set_points_gpu(pts)
+            inputs = c if kind == 1 else f
+            out = torch.empty((1, n if kind == 1 else BATCH_POINTS), dtype=torch.complex128, device=dev)
+            for _ in range(max(1, args.warmup)):
+                plan.execute_gpu_batch(1, inputs, out)
+            barrier()
+            total = timed(lambda: plan.execute_gpu_batch(1, inputs, out), steps)
+            (total,) = max_over_ranks([total], dev)
+            item = {"value": replica_throughput(world, BATCH_POINTS, total, steps), "ms_per_step": total / steps,
+                    "kernel_width": plan.kernel_width()}
+            if rank == 0:
+                from oracle import native
+
+                if kind == 1:
+                    select = np.random.default_rng(12).choice(n, 8, replace=False)
+                    ref = native.direct_type1(pts_h, c.cpu().numpy(), BATCH_MODES, select=select)
+                    got = out.cpu().numpy()[:, select]
+                else:
+                    pick = np.random.default_rng(13).choice(BATCH_POINTS, 64, replace=False)
+                    ref = native.direct_type2(pts_h[pick], f.cpu().numpy(), BATCH_MODES)
+                    got = out.cpu().numpy()[:, pick]
+                item["rel_l2"] = float(np.linalg.norm(got - ref) / np.linalg.norm(ref))
+            entry[f"type{kind}"] = item
+            del plan, out
+        result[f"eps{eps:g}"] = entry
+    return result
+
+
 def uneven_problems_line(w, torch, barrier, world, dev, args, rank):
     """256 independent type-1 problems of uneven sizes (2D/3D, 64^2..256^2 and
     32^3..64^3 modes, 1e3..1e6 points, uniform or clustered, eps 1e-6), one
@@ -553,6 +604,10 @@ def main():
     radial = None
     if not args.no_radial:
         radial = radial_3d_line(w, torch, timed, barrier, world, dev, args, rank)
+    # f64 plans (2D 512^2 modes, 2e6 points, eps 1e-9 and 1e-12).
+    f64 = None
+    if not args.no_f64:
+        f64 = f64_line(w, torch, timed, barrier, world, dev, args, rank)
 
     if rank == 0:
         peaks = json.loads((ROOT / "MEASURED_PEAKS.json").read_text()) if (ROOT / "MEASURED_PEAKS.json").exists() else {}
@@ -589,6 +644,7 @@ def main():
             "batched": batched,
             "uneven_problems": uneven,
             "radial_3d": radial,
+            "f64": f64,
             "roofline": roofline,
             "cpu_baseline": cpu,
             "e2e": e2e,
