@@ -628,6 +628,98 @@ __device__ void spread_warp3(const SpreadParams& sp, const PreparedWindow<3>* wi
   if (run >= 0) flush();
 }
 
+// 2D f64 tiles (windows of 5 taps or more, too wide for a thread's register
+// run) are spread by whole warps, one record at a time: lanes 0 .. 2w-1
+// evaluate one window tap each (axis a = lane / w), and lane l owns the
+// window cells u = l + 32 q (x = u mod w, y = u / w), summing a run of
+// records with one support start in f64 registers in record order. A run
+// reaches the 64-bit fixed-point tile once, when its start changes; the tile
+// of a part of at most 4096 records stays below 2^62 in every cell whatever
+// the runs, so the scale is the record-by-record one.
+template <int W>
+__device__ void spread_warp2_f64(const SpreadParams& sp, const double* points, const double2* sv,
+                                 const uint32_t* perm, const uint32_t* row_begin, const uint32_t* row_prefix,
+                                 int rows, const int* origin, uint32_t record_begin, uint32_t record_end,
+                                 unsigned long long* acc, int padded, double (*stage)[2][W], double scale_lo,
+                                 double scale_hi) {
+  const int tid = threadIdx.x, lane = tid & 31, warp = tid >> 5;
+  constexpr int R = (W * W + 31) / 32;
+  double ar[R], ai[R];
+#pragma unroll
+  for (int q = 0; q < R; ++q) ar[q] = ai[q] = 0.0;
+  int run_x = -1, run_y = 0;
+  const int pad0 = sp.pad[0];
+  auto flush = [&]() {
+#pragma unroll
+    for (int q = 0; q < R; ++q) {
+      const int u = lane + 32 * q;
+      if (u < W * W) {
+        const int c = (run_y + u / W) * pad0 + run_x + u % W;
+        F64Traits::add(acc, padded, 0, c, ar[q]);
+        F64Traits::add(acc, padded, 1, c, ai[q]);
+      }
+      ar[q] = ai[q] = 0.0;
+    }
+  };
+  // Warp w spreads the consecutive records [warp_begin, warp_end).
+  const uint32_t n = record_end - record_begin;
+  const uint32_t per_warp = (n + kSpreadWarps - 1) / kSpreadWarps;
+  const uint32_t warp_begin = record_begin + min(n, per_warp * warp);
+  const uint32_t warp_end = record_begin + min(n, per_warp * (warp + 1));
+  const int axis = lane < W ? 0 : 1, tap = lane < W ? lane : lane - W;
+  double* my_tap = &stage[warp][axis][tap];
+  int row = 0;
+  // The next record's coordinates and point index are loaded one record
+  // ahead, and the strength as soon as its index is known.
+  double next_x = 0.0, next_y = 0.0;
+  uint32_t next_point = 0;
+  if (warp_begin < warp_end) {
+    const uint32_t slot = record_slot(warp_begin, row, row_begin, row_prefix, rows);
+    next_x = points[static_cast<int64_t>(slot) * 2];
+    next_y = points[static_cast<int64_t>(slot) * 2 + 1];
+    next_point = perm[slot];
+  }
+  for (uint32_t r = warp_begin; r < warp_end; ++r) {
+    const double x = next_x, y = next_y;
+    const double2 c = sv[next_point];
+    if (r + 1 < warp_end) {
+      const uint32_t slot = record_slot(r + 1, row, row_begin, row_prefix, rows);
+      next_x = points[static_cast<int64_t>(slot) * 2];
+      next_y = points[static_cast<int64_t>(slot) * 2 + 1];
+      next_point = perm[slot];
+    }
+    if (!F64Traits::in_reach(x) || !F64Traits::in_reach(y)) continue;
+    int32_t start[2];
+    double offset[2];
+    support_of64(x, sp.grid.axis64[0], sp.grid.half_width64, start[0], offset[0]);
+    support_of64(y, sp.grid.axis64[1], sp.grid.half_width64, start[1], offset[1]);
+    const int lx = wrap_start(start[0], sp.grid.axis[0].length) - origin[0];
+    const int ly = wrap_start(start[1], sp.grid.axis[1].length) - origin[1];
+    if (lx < 0 || lx >= sp.tile[0] || ly < 0 || ly >= sp.tile[1]) continue;  // another tile owns it
+    __syncwarp();  // the previous record's taps are read
+    if (lane < 2 * W) {
+      *my_tap = horner_weight(axis == 0 ? offset[0] : offset[1], tap, W, sp.grid.horner, sp.grid.horner_rows);
+    }
+    __syncwarp();
+    if (lx != run_x || ly != run_y) {
+      if (run_x >= 0) flush();
+      run_x = lx;
+      run_y = ly;
+    }
+    const double sr = (c.x * scale_lo) * scale_hi, si = (c.y * scale_lo) * scale_hi;
+#pragma unroll
+    for (int q = 0; q < R; ++q) {
+      const int u = lane + 32 * q;
+      if (u < W * W) {
+        const double weight = stage[warp][0][u % W] * stage[warp][1][u / W];
+        ar[q] = fma(sr, weight, ar[q]);
+        ai[q] = fma(si, weight, ai[q]);
+      }
+    }
+  }
+  if (run_x >= 0) flush();
+}
+
 // One CTA per (part, vector): spreads the part's records into a padded tile
 // of fixed-point sums and writes the tile out in floating point.
 template <int D, int W, typename T>
@@ -760,7 +852,14 @@ __global__ void __launch_bounds__(kSpreadThreads, (spread_run<D, W, T>() > 1 || 
                       T::exponent(max_bits[b]), S);
     }
   }
-  if constexpr (kRun == 1) {
+  constexpr bool kWarp64 = D == 2 && sizeof(Real) == 8 && kRun == 1 && W >= 5;
+  __shared__ double stage64[kWarp64 ? kSpreadWarps : 1][2][kWarp64 ? W : 1];
+  if constexpr (kWarp64) {
+    spread_warp2_f64<W>(sp, reinterpret_cast<const double*>(points), reinterpret_cast<const double2*>(sv), perm,
+                        row_begin, row_prefix, rows, origin, record_begin, record_end,
+                        reinterpret_cast<unsigned long long*>(acc), padded, stage64, scale_lo, scale_hi);
+  }
+  if constexpr (kRun == 1 && !kWarp64) {
     for (uint32_t r = record_begin + tid; !warp_path && r < record_end; r += kSpreadThreads) {
       int local_start[D];
       Real w[D][W];
@@ -809,7 +908,7 @@ __global__ void __launch_bounds__(kSpreadThreads, (spread_run<D, W, T>() > 1 || 
         }
       }
     }
-  } else {
+  } else if constexpr (kRun > 1) {
     // Each thread takes runs of up to kRun consecutive records (consecutive
     // slots of one bin row share starts when bins are one cell wide), sized so
     // that every pass gives every thread the same number of records.
