@@ -720,11 +720,19 @@ __device__ void spread_warp2_f64(const SpreadParams& sp, const double* points, c
   if (run_x >= 0) flush();
 }
 
+// Resident CTAs per SM that the register budget is sized for: three for the
+// 2D f64 warp spreader and for narrow windows without register runs, two for
+// register runs, other f64 windows and the 3D warp spreader.
+template <int D, int W, typename T>
+__host__ __device__ constexpr int spread_min_blocks() {
+  if (D == 2 && sizeof(typename T::Real) == 8 && spread_run<D, W, T>() == 1 && W >= 5) return 3;
+  return (spread_run<D, W, T>() > 1 || sizeof(typename T::Real) == 8 || warp_capable<D, W, T>()) ? 2 : 3;
+}
+
 // One CTA per (part, vector): spreads the part's records into a padded tile
 // of fixed-point sums and writes the tile out in floating point.
 template <int D, int W, typename T>
-__global__ void __launch_bounds__(kSpreadThreads, (spread_run<D, W, T>() > 1 || sizeof(typename T::Real) == 8 ||
-                                                    warp_capable<D, W, T>() ? 2 : 3)) spread_tiles_kernel(
+__global__ void __launch_bounds__(kSpreadThreads, spread_min_blocks<D, W, T>()) spread_tiles_kernel(
     SpreadParams sp, const typename T::Real* __restrict__ points, const void* __restrict__ windows,
     const typename T::Complex* __restrict__ strengths, int64_t point_count, int batch,
     const uint32_t* __restrict__ perm, const uint32_t* __restrict__ offsets,
