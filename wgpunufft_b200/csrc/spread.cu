@@ -720,12 +720,12 @@ __device__ void spread_warp2_f64(const SpreadParams& sp, const double* points, c
   if (run_x >= 0) flush();
 }
 
-// Resident CTAs per SM that the register budget is sized for: three for the
-// 2D f64 warp spreader and for narrow windows without register runs, two for
+// Resident CTAs per SM that the register budget is sized for: four for the
+// 2D f64 warp spreader, three for narrow windows without register runs, two for
 // register runs, other f64 windows and the 3D warp spreader.
 template <int D, int W, typename T>
 __host__ __device__ constexpr int spread_min_blocks() {
-  if (D == 2 && sizeof(typename T::Real) == 8 && spread_run<D, W, T>() == 1 && W >= 5) return 3;
+  if (D == 2 && sizeof(typename T::Real) == 8 && spread_run<D, W, T>() == 1 && W >= 5) return 4;
   return (spread_run<D, W, T>() > 1 || sizeof(typename T::Real) == 8 || warp_capable<D, W, T>()) ? 2 : 3;
 }
 
