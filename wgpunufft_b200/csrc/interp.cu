@@ -394,6 +394,85 @@ __global__ void __launch_bounds__(kRegionThreads) interpolate_region_kernel(
   }
 }
 
+// 2D f64 interpolation over the type-2 bins of 4 x 4 cells, which f64 plans
+// key by the exact support start: one CTA of kRegionThreads per bin stages
+// the (4 + w - 1)^2 cells the bin's windows cover in shared memory, one
+// vector at a time, and a thread serves one point from it, summing in the
+// order of interpolate_kernel (bitwise the same values). A window that the
+// region does not hold (not expected with start keys) reads the grid.
+template <int W>
+__global__ void __launch_bounds__(kRegionThreads) interpolate_region64_kernel(
+    GridParams g, const double* __restrict__ points, int64_t count, const uint32_t* __restrict__ perm,
+    const uint32_t* __restrict__ offsets, const double2* __restrict__ fine, int batch,
+    double2* __restrict__ output) {
+  constexpr int S = 4 + W - 1;
+  __shared__ double2 region[S * S];
+  const int64_t bin = blockIdx.x;
+  const uint32_t first = offsets[bin], last = offsets[bin + 1];
+  if (first == last) return;
+  const int bins0 = static_cast<int>(g.axis[0].bins);
+  const int n0 = g.axis[0].length, n1 = g.axis[1].length;
+  const int ox = static_cast<int>(bin % bins0) * 4;
+  const int oy = static_cast<int>(bin / bins0) * 4;
+  for (int b = 0; b < batch; ++b) {
+    const double2* grid = fine + static_cast<int64_t>(b) * g.fine_count;
+    __syncthreads();  // the previous vector's reads are done
+    for (int e = threadIdx.x; e < S * S; e += kRegionThreads) {
+      const int r = e / S, c = e - r * S;
+      const int y = (oy + r) % n1, x = (ox + c) % n0;
+      region[e] = __ldg(&grid[static_cast<int64_t>(y) * n0 + x]);
+    }
+    __syncthreads();
+    for (uint32_t slot = first + threadIdx.x; slot < last; slot += kRegionThreads) {
+      const uint32_t point = perm[slot];
+      const double px = points[static_cast<int64_t>(slot) * 2], py = points[static_cast<int64_t>(slot) * 2 + 1];
+      double re = 0.0, im = 0.0;
+      if (F64Window::in_reach(px) && F64Window::in_reach(py)) {
+        int first_x, first_y;
+        double wx[W], wy[W];
+        F64Window::window<W>(px, g, 0, first_x, wx);
+        F64Window::window<W>(py, g, 1, first_y, wy);
+        int dx = (first_x - ox) % n0;
+        dx = dx < 0 ? dx + n0 : dx;
+        int dy = (first_y - oy) % n1;
+        dy = dy < 0 ? dy + n1 : dy;
+        if (dx + W <= S && dy + W <= S) {
+#pragma unroll
+          for (int j = 0; j < W; ++j) {
+            const double2* row = region + (dy + j) * S + dx;
+            double rr = 0.0, ri = 0.0;
+#pragma unroll
+            for (int i = 0; i < W; ++i) {
+              const double2 v = row[i];
+              rr = fma(v.x, wx[i], rr);
+              ri = fma(v.y, wx[i], ri);
+            }
+            re = fma(rr, wy[j], re);
+            im = fma(ri, wy[j], im);
+          }
+        } else {
+#pragma unroll 1
+          for (int j = 0; j < W; ++j) {
+            int y = first_y + j;
+            y = y >= n1 ? y - n1 : y;
+            double rr = 0.0, ri = 0.0;
+            for (int i = 0; i < W; ++i) {
+              int x = first_x + i;
+              x = x >= n0 ? x - n0 : x;
+              const double2 v = __ldg(&grid[static_cast<int64_t>(y) * n0 + x]);
+              rr = fma(v.x, wx[i], rr);
+              ri = fma(v.y, wx[i], ri);
+            }
+            re = fma(rr, wy[j], re);
+            im = fma(ri, wy[j], im);
+          }
+        }
+      }
+      output[static_cast<int64_t>(b) * count + point] = make_double2(re, im);
+    }
+  }
+}
+
 // output[b][i] = staged[slot of i][b]: 32 points x 64 vectors per CTA through
 // shared memory, so both the staged rows and the output rows move in whole
 // sectors.
@@ -531,6 +610,41 @@ void interpolate_bins_execute(const GridParams& g, const InterpBinsLaunch& l, cu
     case 7: launch_bins_width<7>(g, l, stream); break;
     default: launch_bins_width<8>(g, l, stream); break;
   }
+}
+
+bool interpolate_region64_supported(const GridParams& g) {
+  return g.dimensions == 2 && g.width >= 2 && g.width <= 16 && g.axis[0].shift == 2 && g.axis[1].shift == 2;
+}
+
+void interpolate_region64_execute(const GridParams& g, const InterpLaunch64& l, const uint32_t* offsets,
+                                  uint64_t bins, cudaStream_t stream) {
+  if (l.point_count == 0) return;
+  const dim3 grid(static_cast<unsigned>(bins));
+  switch (g.width) {
+#define B200NUFFT_REGION64_CASE(WIDTH)                                                                  \
+  case WIDTH:                                                                                          \
+    interpolate_region64_kernel<WIDTH><<<grid, kRegionThreads, 0, stream>>>(                            \
+        g, l.points, l.point_count, l.perm, offsets, l.fine, l.batch, l.output);                        \
+    break;
+    B200NUFFT_REGION64_CASE(2)
+    B200NUFFT_REGION64_CASE(3)
+    B200NUFFT_REGION64_CASE(4)
+    B200NUFFT_REGION64_CASE(5)
+    B200NUFFT_REGION64_CASE(6)
+    B200NUFFT_REGION64_CASE(7)
+    B200NUFFT_REGION64_CASE(8)
+    B200NUFFT_REGION64_CASE(9)
+    B200NUFFT_REGION64_CASE(10)
+    B200NUFFT_REGION64_CASE(11)
+    B200NUFFT_REGION64_CASE(12)
+    B200NUFFT_REGION64_CASE(13)
+    B200NUFFT_REGION64_CASE(14)
+    B200NUFFT_REGION64_CASE(15)
+    default:
+    B200NUFFT_REGION64_CASE(16)
+#undef B200NUFFT_REGION64_CASE
+  }
+  note_launch();
 }
 
 void interpolate_execute64(const GridParams& g, const InterpLaunch64& l, cudaStream_t stream) {

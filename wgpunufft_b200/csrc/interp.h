@@ -51,5 +51,10 @@ void interpolate_bins_execute(const GridParams& g, const InterpBinsLaunch& launc
 // memory, outputs written in point order (inverse and staged unused).
 void interpolate_region_execute(const GridParams& g, const InterpBinsLaunch& launch, cudaStream_t stream);
 void interpolate_execute64(const GridParams& g, const InterpLaunch64& launch, cudaStream_t stream);
+// 2D f64 plans on 4 x 4-cell bins: each bin's grid region staged in shared
+// memory (same sums, bit for bit, as interpolate_execute64).
+bool interpolate_region64_supported(const GridParams& g);
+void interpolate_region64_execute(const GridParams& g, const InterpLaunch64& launch, const uint32_t* offsets,
+                                  uint64_t bins, cudaStream_t stream);
 
 }  // namespace b200nufft
