@@ -52,6 +52,7 @@ def parse():
     p.add_argument("--no-uneven", action="store_true")
     p.add_argument("--no-radial", action="store_true")
     p.add_argument("--no-f64", action="store_true")
+    p.add_argument("--no-type3", action="store_true")
     return p.parse_args()
 
 
@@ -408,6 +409,46 @@ def f64_line(w, torch, timed, barrier, world, dev, args, rank):
     return result
 
 
+def type3_line(w, torch, timed, barrier, world, dev, args, rank):
+    """The 3D type-3 configuration: f64, 10^6 sources uniform in [-1, 1]^3 to
+    10^6 targets uniform in [-200, 200]^3, eps 1e-9. Execution on set points
+    (pre-phase, outer spread, inner type 2, post-phase) and set_points +
+    execution, with rel-l2 against FP64 direct sums on 64 targets."""
+    count = 1_000_000
+    g = torch.Generator(device=dev)
+    g.manual_seed(SEED + 51)
+    src = (torch.rand((count, 3), generator=g, device=dev, dtype=torch.float64) * 2 - 1).contiguous()
+    tgt = (torch.rand((count, 3), generator=g, device=dev, dtype=torch.float64) * 400 - 200).contiguous()
+    c = torch.complex(torch.randn((1, count), generator=g, device=dev, dtype=torch.float64),
+                      torch.randn((1, count), generator=g, device=dev, dtype=torch.float64))
+    config = w.NufftType3Config(((-1.0, 1.0),) * 3, ((-200.0, 200.0),) * 3, eps=1e-9)
+    plan = w.NufftType3Plan(config)
+    out = torch.empty((1, count), dtype=torch.complex128, device=dev)
+    steps = max(1, min(args.steps, 3))
+    plan.set_points_gpu(src, tgt)
+    for _ in range(max(1, args.warmup)):
+        plan.execute_gpu_batch(1, c, out)
+    barrier()
+    total = timed(lambda: plan.execute_gpu_batch(1, c, out), steps)
+    total_all = timed(lambda: plan.encode_gpu_batch(1, src, c, tgt, out), steps)
+    (total, total_all) = max_over_ranks([total, total_all], dev)
+    result = {"workload": "3d_type3_f64_src1e6_in[-1,1]^3_tgt1e6_in[-200,200]^3_eps1e-9", "unit": UNIT,
+              "value": replica_throughput(world, count, total, steps), "ms_per_step": total / steps,
+              "with_set_points": {"value": replica_throughput(world, count, total_all, steps),
+                                  "ms_per_step": total_all / steps},
+              "note": "points/s counts sources (= targets)"}
+    if rank == 0:
+        from oracle import native
+
+        pick = np.random.default_rng(14).choice(count, 64, replace=False)
+        ref = native.direct_type3(src.cpu().numpy(), c.cpu().numpy(), tgt.cpu().numpy()[pick], 1)
+        got = out.cpu().numpy()[:, pick]
+        result["rel_l2"] = float(np.linalg.norm(got - ref) / np.linalg.norm(ref))
+    del plan, out, src, tgt, c
+    torch.cuda.empty_cache()
+    return result
+
+
 def uneven_problems_line(w, torch, barrier, world, dev, args, rank):
     """256 independent type-1 problems of uneven sizes (2D/3D, 64^2..256^2 and
     32^3..64^3 modes, 1e3..1e6 points, uniform or clustered, eps 1e-6), one
@@ -608,6 +649,10 @@ def main():
     f64 = None
     if not args.no_f64:
         f64 = f64_line(w, torch, timed, barrier, world, dev, args, rank)
+    # The 3D type-3 f64 configuration (10^6 sources to 10^6 targets).
+    type3 = None
+    if not args.no_type3:
+        type3 = type3_line(w, torch, timed, barrier, world, dev, args, rank)
 
     if rank == 0:
         peaks = json.loads((ROOT / "MEASURED_PEAKS.json").read_text()) if (ROOT / "MEASURED_PEAKS.json").exists() else {}
@@ -645,6 +690,7 @@ def main():
             "uneven_problems": uneven,
             "radial_3d": radial,
             "f64": f64,
+            "type3": type3,
             "roofline": roofline,
             "cpu_baseline": cpu,
             "e2e": e2e,
