@@ -447,7 +447,7 @@ void NufftPlan::configure_tiles() {
       sp.warp_segments = static_cast<const uint32_t*>(warp_segments_.get());
     }
   }
-  // Parts of at most kPartCap records, fewer for small point sets so that
+  // Parts of at most kPartCap records (f64), fewer for small point sets so that
   // about four CTAs per SM have work.
   const int64_t spread_ctas = 4 * 148;
   int64_t cap = (std::max<int64_t>(point_count_, 1) + spread_ctas - 1) / spread_ctas;
@@ -457,7 +457,6 @@ void NufftPlan::configure_tiles() {
   const int64_t part_cap = dim_ == 3 ? 2048 : (precision_ == B200NUFFT_PRECISION_F32 ? 16384 : kPartCap);
   cap = std::min<int64_t>(part_cap, std::max<int64_t>(256, (cap + 255) / 256 * 256));
   sp.part_cap = static_cast<int32_t>(cap);
-  sp.headroom = ilog2(static_cast<int64_t>(kPartCap) + 1);
   // Candidate (tile, local) pairs of every coordinate of every axis: tile t
   // covers cells (t * tile + l) mod n for l < pad. They depend on the grid
   // and tile shape only, so later point sets reuse them.

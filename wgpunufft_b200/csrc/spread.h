@@ -24,7 +24,6 @@ struct SpreadParams {
   int64_t tile_count;
   int32_t padded_cells;
   int32_t part_cap;     // records per part, at most
-  int32_t headroom;     // ceil(log2(part_cap + 1))
   // For each axis, candidate (tile, local) pairs of every coordinate:
   // candidate_count[a] entries per coordinate from candidate_base[a], ended
   // by a negative tile when fewer.
