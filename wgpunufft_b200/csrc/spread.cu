@@ -720,6 +720,78 @@ __device__ void spread_warp2_f64(const SpreadParams& sp, const double* points, c
   if (run_x >= 0) flush();
 }
 
+// 3D f64 tiles (windows of 5 taps or more) are spread by whole warps, one
+// record at a time: the lanes evaluate the 3w window taps (tap t on axis
+// t / w), and lane l adds the contributions of window cells
+// u = l + 32 q (x = u mod w, y = (u / w) mod w, z = u / w^2) straight to the
+// 64-bit fixed-point tile; the 32 lanes of an add touch 32 different cells.
+template <int W>
+__device__ void spread_warp3_f64(const SpreadParams& sp, const double* points, const double2* sv,
+                                 const uint32_t* perm, const uint32_t* row_begin, const uint32_t* row_prefix,
+                                 int rows, const int* origin, uint32_t record_begin, uint32_t record_end,
+                                 unsigned long long* acc, int padded, double (*stage)[3][W], double scale_lo,
+                                 double scale_hi) {
+  const int tid = threadIdx.x, lane = tid & 31, warp = tid >> 5;
+  constexpr int kCells = W * W * W;
+  constexpr int R = (kCells + 31) / 32;
+  const int pad0 = sp.pad[0], pad01 = sp.pad[0] * sp.pad[1];
+  const uint32_t n = record_end - record_begin;
+  const uint32_t per_warp = (n + kSpreadWarps - 1) / kSpreadWarps;
+  const uint32_t warp_begin = record_begin + min(n, per_warp * warp);
+  const uint32_t warp_end = record_begin + min(n, per_warp * (warp + 1));
+  int row = 0;
+  double next[3] = {0.0, 0.0, 0.0};
+  uint32_t next_point = 0;
+  if (warp_begin < warp_end) {
+    const uint32_t slot = record_slot(warp_begin, row, row_begin, row_prefix, rows);
+#pragma unroll
+    for (int a = 0; a < 3; ++a) next[a] = points[static_cast<int64_t>(slot) * 3 + a];
+    next_point = perm[slot];
+  }
+  for (uint32_t r = warp_begin; r < warp_end; ++r) {
+    const double p[3] = {next[0], next[1], next[2]};
+    const double2 c = sv[next_point];
+    if (r + 1 < warp_end) {
+      const uint32_t slot = record_slot(r + 1, row, row_begin, row_prefix, rows);
+#pragma unroll
+      for (int a = 0; a < 3; ++a) next[a] = points[static_cast<int64_t>(slot) * 3 + a];
+      next_point = perm[slot];
+    }
+    if (!F64Traits::in_reach(p[0]) || !F64Traits::in_reach(p[1]) || !F64Traits::in_reach(p[2])) continue;
+    int local[3];
+    double offset[3];
+    bool inside = true;
+#pragma unroll
+    for (int a = 0; a < 3; ++a) {
+      int32_t start;
+      support_of64(p[a], sp.grid.axis64[a], sp.grid.half_width64, start, offset[a]);
+      local[a] = wrap_start(start, sp.grid.axis[a].length) - origin[a];
+      inside = inside && local[a] >= 0 && local[a] < sp.tile[a];
+    }
+    if (!inside) continue;  // another tile owns it
+    __syncwarp();  // the previous record's taps are read
+    for (int t = lane; t < 3 * W; t += 32) {
+      const int a = t / W, j = t - a * W;
+      const double o = a == 0 ? offset[0] : (a == 1 ? offset[1] : offset[2]);
+      stage[warp][a][j] = horner_weight(o, j, W, sp.grid.horner, sp.grid.horner_rows);
+    }
+    __syncwarp();
+    const double sr = (c.x * scale_lo) * scale_hi, si = (c.y * scale_lo) * scale_hi;
+    const int base = local[2] * pad01 + local[1] * pad0 + local[0];
+#pragma unroll 4
+    for (int q = 0; q < R; ++q) {
+      const int u = lane + 32 * q;
+      if (u < kCells) {
+        const int i = u % W, j = (u / W) % W, k = u / (W * W);
+        const double weight = stage[warp][0][i] * stage[warp][1][j] * stage[warp][2][k];
+        const int cell = base + k * pad01 + j * pad0 + i;
+        F64Traits::add(acc, padded, 0, cell, sr * weight);
+        F64Traits::add(acc, padded, 1, cell, si * weight);
+      }
+    }
+  }
+}
+
 // Resident CTAs per SM that the register budget is sized for: four for the
 // 2D f64 warp spreader, three for narrow windows without register runs, two for
 // register runs, other f64 windows and the 3D warp spreader.
@@ -860,10 +932,15 @@ __global__ void __launch_bounds__(kSpreadThreads, spread_min_blocks<D, W, T>()) 
                       T::exponent(max_bits[b]), S);
     }
   }
-  constexpr bool kWarp64 = D == 2 && sizeof(Real) == 8 && kRun == 1 && W >= 5;
-  __shared__ double stage64[kWarp64 ? kSpreadWarps : 1][2][kWarp64 ? W : 1];
-  if constexpr (kWarp64) {
+  constexpr bool kWarp64 = D >= 2 && sizeof(Real) == 8 && kRun == 1 && W >= 5;
+  __shared__ double stage64[kWarp64 ? kSpreadWarps : 1][kWarp64 ? D : 1][kWarp64 ? W : 1];
+  if constexpr (kWarp64 && D == 2) {
     spread_warp2_f64<W>(sp, reinterpret_cast<const double*>(points), reinterpret_cast<const double2*>(sv), perm,
+                        row_begin, row_prefix, rows, origin, record_begin, record_end,
+                        reinterpret_cast<unsigned long long*>(acc), padded, stage64, scale_lo, scale_hi);
+  }
+  if constexpr (kWarp64 && D == 3) {
+    spread_warp3_f64<W>(sp, reinterpret_cast<const double*>(points), reinterpret_cast<const double2*>(sv), perm,
                         row_begin, row_prefix, rows, origin, record_begin, record_end,
                         reinterpret_cast<unsigned long long*>(acc), padded, stage64, scale_lo, scale_hi);
   }

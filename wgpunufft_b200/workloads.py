@@ -13,6 +13,8 @@ Cases:
   radial128 the radial case at 128^3 modes, 4096 spokes x 1526 samples (profiling size)
   uniform3d 3D 256^3 modes, 4096 x 12207 uniform points, eps 1e-5
   uniform128 3D 128^3 modes, 4096 x 1526 uniform points, eps 1e-5 (profiling size)
+  type3     3D type 3 in f64: 1e6 sources uniform in [-1, 1]^3 to 1e6 targets
+            uniform in [-200, 200]^3, eps 1e-9 (--kind and --batch ignored)
 
 uneven_problems() gives 256 independent problems of uneven sizes (2D or 3D,
 modes from 64^2, 128^2, 256^2, 32^3, 64^3, M log-uniform in [1e3, 1e6],
@@ -36,6 +38,7 @@ CASES = {
     "radial128": ((128, 128, 128), 4096 * 1526, 1e-5, "radial"),
     "uniform3d": ((256, 256, 256), 4096 * 12207, 1e-5, "uniform"),
     "uniform128": ((128, 128, 128), 4096 * 1526, 1e-5, "uniform"),
+    "type3": ((270, 270, 270), 1_000_000, 1e-9, "uniform"),
 }
 
 
@@ -100,10 +103,33 @@ def uneven_problems(count: int = 256, seed: int = 5, device: str = "cuda"):
     return problems
 
 
+def run_type3(executes: int) -> None:
+    import torch
+
+    import wgpunufft_b200 as w
+
+    g = torch.Generator(device="cuda")
+    g.manual_seed(51)
+    src = (torch.rand((1_000_000, 3), generator=g, device="cuda", dtype=torch.float64) * 2 - 1).contiguous()
+    tgt = (torch.rand((1_000_000, 3), generator=g, device="cuda", dtype=torch.float64) * 400 - 200).contiguous()
+    c = torch.complex(torch.randn((1, 1_000_000), generator=g, device="cuda", dtype=torch.float64),
+                      torch.randn((1, 1_000_000), generator=g, device="cuda", dtype=torch.float64))
+    plan = w.NufftType3Plan(w.NufftType3Config(((-1.0, 1.0),) * 3, ((-200.0, 200.0),) * 3, eps=1e-9))
+    out = torch.empty((1, 1_000_000), dtype=torch.complex128, device="cuda")
+    plan.set_points_gpu(src, tgt)
+    for _ in range(executes):
+        plan.execute_gpu_batch(1, c, out)
+    torch.cuda.synchronize()
+
+
 def run(case: str, batch: int, executes: int, kinds) -> None:
     import torch
 
     import wgpunufft_b200 as w
+
+    if case == "type3":
+        run_type3(executes)
+        return
 
     modes, count, eps, dist = CASES[case]
     p = points(dist, count, len(modes))
