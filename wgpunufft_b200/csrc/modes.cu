@@ -40,16 +40,20 @@ __device__ __forceinline__ int64_t mode_index(int64_t c, int64_t N, int64_t n, b
   return -1;
 }
 
-template <typename Real, typename Complex>
+// Index: uint32_t when every mode and cell index fits (32-bit divisions are
+// far cheaper than 64-bit ones), else int64_t.
+template <typename Real, typename Complex, typename Index>
 __global__ void deconvolve_kernel(ModeParams mp, int batch, const Complex* __restrict__ fine,
                                   const Real* __restrict__ amplitudes,
                                   Complex* __restrict__ output) {
   const int64_t k = static_cast<int64_t>(blockIdx.x) * blockDim.x + threadIdx.x;
   if (k >= mp.mode_count) return;
-  int64_t rest = k, flat = 0, stride = 1;
+  Index rest = static_cast<Index>(k);
+  int64_t flat = 0, stride = 1;
   for (int a = 0; a < mp.dimensions; ++a) {
-    const int64_t index = rest % mp.modes[a];
-    rest /= mp.modes[a];
+    const Index n = static_cast<Index>(mp.modes[a]);
+    const int64_t index = rest % n;
+    rest /= n;
     flat += fine_index(index, mp.modes[a], mp.fine[a], mp.centered) * stride;
     stride *= mp.fine[a];
   }
@@ -63,17 +67,19 @@ __global__ void deconvolve_kernel(ModeParams mp, int batch, const Complex* __res
   }
 }
 
-template <typename Real, typename Complex>
+template <typename Real, typename Complex, typename Index>
 __global__ void predeconvolve_kernel(ModeParams mp, int batch, const Complex* __restrict__ input,
                                      const Real* __restrict__ amplitudes,
                                      Complex* __restrict__ fine) {
   const int64_t c = static_cast<int64_t>(blockIdx.x) * blockDim.x + threadIdx.x;
   if (c >= mp.fine_count) return;
-  int64_t rest = c, flat = 0, stride = 1;
+  Index rest = static_cast<Index>(c);
+  int64_t flat = 0, stride = 1;
   bool mapped = true;
   for (int a = 0; a < mp.dimensions; ++a) {
-    const int64_t cell = rest % mp.fine[a];
-    rest /= mp.fine[a];
+    const Index n = static_cast<Index>(mp.fine[a]);
+    const int64_t cell = rest % n;
+    rest /= n;
     const int64_t index = mode_index(cell, mp.modes[a], mp.fine[a], mp.centered);
     mapped = mapped && index >= 0;
     flat += index * stride;
@@ -93,35 +99,54 @@ __global__ void predeconvolve_kernel(ModeParams mp, int batch, const Complex* __
   }
 }
 
+bool narrow(const ModeParams& mp) {
+  return mp.fine_count < (int64_t(1) << 31) && mp.mode_count < (int64_t(1) << 31);
+}
+
+template <typename Real, typename Complex>
+void deconvolve_any(const ModeParams& mp, int batch, const Complex* fine, const Real* amplitudes, Complex* output,
+                    cudaStream_t stream) {
+  const unsigned blocks = static_cast<unsigned>((mp.mode_count + 255) / 256);
+  if (narrow(mp)) {
+    deconvolve_kernel<Real, Complex, uint32_t><<<blocks, 256, 0, stream>>>(mp, batch, fine, amplitudes, output);
+  } else {
+    deconvolve_kernel<Real, Complex, int64_t><<<blocks, 256, 0, stream>>>(mp, batch, fine, amplitudes, output);
+  }
+  note_launch();
+}
+
+template <typename Real, typename Complex>
+void predeconvolve_any(const ModeParams& mp, int batch, const Complex* input, const Real* amplitudes,
+                       Complex* fine, cudaStream_t stream) {
+  const unsigned blocks = static_cast<unsigned>((mp.fine_count + 255) / 256);
+  if (narrow(mp)) {
+    predeconvolve_kernel<Real, Complex, uint32_t><<<blocks, 256, 0, stream>>>(mp, batch, input, amplitudes, fine);
+  } else {
+    predeconvolve_kernel<Real, Complex, int64_t><<<blocks, 256, 0, stream>>>(mp, batch, input, amplitudes, fine);
+  }
+  note_launch();
+}
+
 }  // namespace
 
 void deconvolve_f32(const ModeParams& mp, int batch, const float2* fine, const float* amplitudes,
                     float2* output, cudaStream_t stream) {
-  const unsigned blocks = static_cast<unsigned>((mp.mode_count + 255) / 256);
-  deconvolve_kernel<float, float2><<<blocks, 256, 0, stream>>>(mp, batch, fine, amplitudes, output);
-  note_launch();
+  deconvolve_any<float, float2>(mp, batch, fine, amplitudes, output, stream);
 }
 
 void predeconvolve_f32(const ModeParams& mp, int batch, const float2* input,
                        const float* amplitudes, float2* fine, cudaStream_t stream) {
-  const unsigned blocks = static_cast<unsigned>((mp.fine_count + 255) / 256);
-  predeconvolve_kernel<float, float2><<<blocks, 256, 0, stream>>>(mp, batch, input, amplitudes, fine);
-  note_launch();
+  predeconvolve_any<float, float2>(mp, batch, input, amplitudes, fine, stream);
 }
 
 void deconvolve_f64(const ModeParams& mp, int batch, const double2* fine,
                     const double* amplitudes, double2* output, cudaStream_t stream) {
-  const unsigned blocks = static_cast<unsigned>((mp.mode_count + 255) / 256);
-  deconvolve_kernel<double, double2><<<blocks, 256, 0, stream>>>(mp, batch, fine, amplitudes, output);
-  note_launch();
+  deconvolve_any<double, double2>(mp, batch, fine, amplitudes, output, stream);
 }
 
 void predeconvolve_f64(const ModeParams& mp, int batch, const double2* input,
                        const double* amplitudes, double2* fine, cudaStream_t stream) {
-  const unsigned blocks = static_cast<unsigned>((mp.fine_count + 255) / 256);
-  predeconvolve_kernel<double, double2><<<blocks, 256, 0, stream>>>(mp, batch, input, amplitudes,
-                                                                   fine);
-  note_launch();
+  predeconvolve_any<double, double2>(mp, batch, input, amplitudes, fine, stream);
 }
 
 }  // namespace b200nufft
