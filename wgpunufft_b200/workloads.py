@@ -15,6 +15,8 @@ Cases:
   uniform128 3D 128^3 modes, 4096 x 1526 uniform points, eps 1e-5 (profiling size)
   type3     3D type 3 in f64: 1e6 sources uniform in [-1, 1]^3 to 1e6 targets
             uniform in [-200, 200]^3, eps 1e-9 (--kind and --batch ignored)
+  uneven    the 256 problems of uneven_problems(), type 1, one plan each
+            (--kind and --batch ignored)
 
 uneven_problems() gives 256 independent problems of uneven sizes (2D or 3D,
 modes from 64^2, 128^2, 256^2, 32^3, 64^3, M log-uniform in [1e3, 1e6],
@@ -39,6 +41,7 @@ CASES = {
     "uniform3d": ((256, 256, 256), 4096 * 12207, 1e-5, "uniform"),
     "uniform128": ((128, 128, 128), 4096 * 1526, 1e-5, "uniform"),
     "type3": ((270, 270, 270), 1_000_000, 1e-9, "uniform"),
+    "uneven": ((64, 64), 0, 1e-6, "uniform"),
 }
 
 
@@ -129,6 +132,20 @@ def run(case: str, batch: int, executes: int, kinds) -> None:
 
     if case == "type3":
         run_type3(executes)
+        return
+    if case == "uneven":
+        plans = []
+        for modes, p, c in uneven_problems():
+            plan = w.NufftPlan.type1_gpu(w.NufftConfig(modes, 1e-6))
+            plan.set_points_gpu(p)
+            n = 1
+            for m in modes:
+                n *= m
+            plans.append((plan, c, torch.empty((1, n), dtype=torch.complex64, device="cuda")))
+        for _ in range(executes):
+            for plan, c, out in plans:
+                plan.execute_gpu_batch(1, c, out)
+        torch.cuda.synchronize()
         return
 
     modes, count, eps, dist = CASES[case]
