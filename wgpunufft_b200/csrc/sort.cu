@@ -326,6 +326,21 @@ __global__ void bin_offsets_kernel(const uint32_t* __restrict__ keys, int64_t co
   for (uint64_t b = low; b <= high && b <= bins; ++b) offsets[b] = static_cast<uint32_t>(i);
 }
 
+// The same offsets a bin at a time, for bins far outnumbering the points:
+// offsets[b] = the number of keys below b, by binary search, so that no
+// thread walks a long run of empty bins.
+__global__ void bin_offsets_search_kernel(const uint32_t* __restrict__ keys, int64_t count, uint64_t bins,
+                                          uint32_t* __restrict__ offsets) {
+  const uint64_t b = static_cast<uint64_t>(blockIdx.x) * blockDim.x + threadIdx.x;
+  if (b > bins) return;
+  int64_t low = 0, high = count;
+  while (low < high) {
+    const int64_t mid = (low + high) >> 1;
+    if (static_cast<uint64_t>(keys[mid]) < b) low = mid + 1; else high = mid;
+  }
+  offsets[b] = static_cast<uint32_t>(low);
+}
+
 // Coordinates in bin order: sorted[slot] = points[perm[slot]], so that the
 // spreading and interpolation kernels read them contiguously.
 template <int D, typename T>
@@ -612,8 +627,13 @@ void sort_from_keys(int64_t count, uint64_t bins, int passes, SortBuffers buf, u
     *sorted_keys = keys_in;
   }
   StageScope scope(timer, kStageBinOffsets, stream);
-  bin_offsets_kernel<<<static_cast<unsigned>((count + 1 + 255) / 256), 256, 0, stream>>>(
-      *sorted_keys, count, bins, offsets);
+  if (bins > 2 * static_cast<uint64_t>(count)) {
+    bin_offsets_search_kernel<<<static_cast<unsigned>((bins + 1 + 255) / 256), 256, 0, stream>>>(
+        *sorted_keys, count, bins, offsets);
+  } else {
+    bin_offsets_kernel<<<static_cast<unsigned>((count + 1 + 255) / 256), 256, 0, stream>>>(
+        *sorted_keys, count, bins, offsets);
+  }
   note_launch();
 }
 
