@@ -446,7 +446,51 @@ def type3_line(w, torch, timed, barrier, world, dev, args, rank):
         result["rel_l2"] = float(np.linalg.norm(got - ref) / np.linalg.norm(ref))
     del plan, out, src, tgt, c
     torch.cuda.empty_cache()
+    result["small_outer_grids_f32"] = type3_small_grid_lines(w, torch, timed, barrier, world, dev, args, rank)
     return result
+
+
+def type3_small_grid_lines(w, torch, timed, barrier, world, dev, args, rank):
+    """Type 3 in f32 on small outer grids, the regime the reference serves with
+    its dense small-grid spreader (src/gpu_dense_spread.rs:68-78: one or two
+    axes, at most 2^16 cells): 10^6 sources uniform in [-1, 1]^d to 10^6
+    targets uniform in [-30, 30]^d, eps 1e-6, d = 1 and 2. Here the binned
+    spreader serves it, its parts sized so that every SM has work."""
+    lines = {}
+    count = 1_000_000
+    steps = max(1, min(args.steps, 3))
+    for d in (1, 2):
+        g = torch.Generator(device=dev)
+        g.manual_seed(SEED + 60 + d)
+        src = (torch.rand((count, d), generator=g, device=dev) * 2 - 1).contiguous()
+        tgt = (torch.rand((count, d), generator=g, device=dev) * 60 - 30).contiguous()
+        c = torch.complex(torch.randn((1, count), generator=g, device=dev),
+                          torch.randn((1, count), generator=g, device=dev))
+        config = w.NufftType3Config(((-1.0, 1.0),) * d, ((-30.0, 30.0),) * d, eps=1e-6,
+                                    precision=w.Precision.F32)
+        plan = w.NufftType3Plan(config)
+        out = torch.empty((1, count), dtype=torch.complex64, device=dev)
+        plan.set_points_gpu(src, tgt)
+        for _ in range(max(1, args.warmup)):
+            plan.execute_gpu_batch(1, c, out)
+        barrier()
+        total = timed(lambda: plan.execute_gpu_batch(1, c, out), steps)
+        (total,) = max_over_ranks([total], dev)
+        line = {"workload": f"{d}d_type3_f32_src1e6_in[-1,1]^{d}_tgt1e6_in[-30,30]^{d}_eps1e-6", "unit": UNIT,
+                "value": replica_throughput(world, count, total, steps), "ms_per_step": total / steps,
+                "outer_grid": list(plan.info().outer_shape[:d])}
+        if rank == 0:
+            from oracle import native
+
+            pick = np.random.default_rng(15 + d).choice(count, 64, replace=False)
+            ref = native.direct_type3(src.double().cpu().numpy(), c.cpu().numpy().astype(np.complex128),
+                                      tgt.double().cpu().numpy()[pick], 1)
+            got = out.cpu().numpy()[:, pick]
+            line["rel_l2"] = float(np.linalg.norm(got - ref) / np.linalg.norm(ref))
+        lines[f"{d}d"] = line
+        del plan, out, src, tgt, c
+    torch.cuda.empty_cache()
+    return lines
 
 
 def uneven_problems_line(w, torch, barrier, world, dev, args, rank):

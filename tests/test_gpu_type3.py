@@ -98,3 +98,24 @@ def test_type3_f32_and_df64():
     assert rel_l2(got32, ref32) < 100 * 1e-5
     got64, _ = run_type3(sources, targets, strengths, sb, tb, 1e-11)
     assert rel_l2(got64, ref) < 100 * 1e-11
+
+
+@pytest.mark.parametrize("d", [1, 2])
+def test_type3_f32_small_outer_grids(d):
+    """The regime of the reference's dense small-grid spreader
+    (src/gpu_dense_spread.rs:68-78: F32, one or two axes, at most 2^16 outer
+    cells): tens of thousands of sources on a few dozen cells per axis."""
+    rng = np.random.default_rng(40 + d)
+    sb = np.array([[-1.0, 1.0], [-0.5, 1.5]][:d])
+    tb = np.array([[-30.0, 30.0], [-20.0, 25.0]][:d])
+    sources = rng.uniform(sb[:, 0], sb[:, 1], (60_000, d)).astype(np.float32)
+    targets = rng.uniform(tb[:, 0], tb[:, 1], (700, d)).astype(np.float32)
+    strengths = (rng.standard_normal((2, 60_000)) + 1j * rng.standard_normal((2, 60_000))).astype(np.complex64)
+    got, plan = run_type3(sources, targets, strengths, sb, tb, 1e-5, precision=w.Precision.F32)
+    outer = list(plan.info().outer_shape[:d])
+    assert int(np.prod(outer)) <= 1 << 16 and max(outer) < 100, outer
+    ref = native.direct_type3(sources.astype(np.float64), strengths.astype(np.complex128),
+                              targets.astype(np.float64), 1)
+    assert rel_l2(got, ref) < 100 * 1e-5
+    again, _ = run_type3(sources, targets, strengths, sb, tb, 1e-5, precision=w.Precision.F32)
+    assert np.array_equal(got, again)

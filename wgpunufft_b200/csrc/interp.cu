@@ -13,6 +13,8 @@
 // (src/gpu_nd_wgsl.rs:373-481).
 #include <cuda_runtime.h>
 
+#include <algorithm>
+
 #include "device.h"
 #include "interp.h"
 
@@ -309,6 +311,25 @@ __global__ void __launch_bounds__(256) interpolate_bins_kernel(GridParams g, con
 // values); windows beyond the region read the grid directly.
 constexpr int kRegionThreads = 128;
 
+// CTAs per bin of the region kernels: a bin holding many points (a small
+// grid under a large point set) splits its slots over gridDim.y CTAs that
+// each stage the same region, so that the launch still fills every SM. Each
+// point's sum is the same whichever CTA serves it.
+inline unsigned region_splits(int64_t points, uint64_t bins) {
+  const int64_t per_bin = points / static_cast<int64_t>(bins > 0 ? bins : 1);
+  return static_cast<unsigned>(std::min<int64_t>(64, std::max<int64_t>(1, per_bin / (4 * kRegionThreads))));
+}
+
+// The slots [first, last) of this CTA's share of its bin.
+__device__ __forceinline__ void region_share(const uint32_t* __restrict__ offsets, int64_t bin, uint32_t& first,
+                                             uint32_t& last) {
+  const uint64_t begin = offsets[bin], end = offsets[bin + 1];
+  const uint64_t share = (end - begin + gridDim.y - 1) / gridDim.y;
+  const uint64_t lo = begin + share * blockIdx.y, hi = lo + share;
+  first = static_cast<uint32_t>(lo < end ? lo : end);
+  last = static_cast<uint32_t>(hi < end ? hi : end);
+}
+
 template <int W>
 __global__ void __launch_bounds__(kRegionThreads) interpolate_region_kernel(
     GridParams g, const void* __restrict__ windows, int64_t count, const uint32_t* __restrict__ perm,
@@ -317,8 +338,9 @@ __global__ void __launch_bounds__(kRegionThreads) interpolate_region_kernel(
   constexpr int S = bin_region_side<W>();
   __shared__ float2 region[S * S];
   const int64_t bin = blockIdx.x;
-  const uint32_t first = offsets[bin], last = offsets[bin + 1];
-  if (first == last) return;
+  uint32_t first, last;
+  region_share(offsets, bin, first, last);
+  if (first >= last) return;
   const int bins0 = static_cast<int>(g.axis[0].bins);
   const int n0 = g.axis[0].length, n1 = g.axis[1].length;
   const int ox = static_cast<int>(bin % bins0) * 8 - W / 2 - 2;
@@ -408,8 +430,9 @@ __global__ void __launch_bounds__(kRegionThreads) interpolate_region64_kernel(
   constexpr int S = 4 + W - 1;
   __shared__ double2 region[S * S];
   const int64_t bin = blockIdx.x;
-  const uint32_t first = offsets[bin], last = offsets[bin + 1];
-  if (first == last) return;
+  uint32_t first, last;
+  region_share(offsets, bin, first, last);
+  if (first >= last) return;
   const int bins0 = static_cast<int>(g.axis[0].bins);
   const int n0 = g.axis[0].length, n1 = g.axis[1].length;
   const int ox = static_cast<int>(bin % bins0) * 4;
@@ -575,7 +598,7 @@ void interpolate_execute(const GridParams& g, const InterpLaunch& l, cudaStream_
 
 void interpolate_region_execute(const GridParams& g, const InterpBinsLaunch& l, cudaStream_t stream) {
   if (l.point_count == 0) return;
-  const dim3 grid(static_cast<unsigned>(l.bins));
+  const dim3 grid(static_cast<unsigned>(l.bins), region_splits(l.point_count, l.bins));
   switch (g.width) {
 #define B200NUFFT_REGION_CASE(WIDTH)                                                                   \
   case WIDTH:                                                                                          \
@@ -619,7 +642,7 @@ bool interpolate_region64_supported(const GridParams& g) {
 void interpolate_region64_execute(const GridParams& g, const InterpLaunch64& l, const uint32_t* offsets,
                                   uint64_t bins, cudaStream_t stream) {
   if (l.point_count == 0) return;
-  const dim3 grid(static_cast<unsigned>(bins));
+  const dim3 grid(static_cast<unsigned>(bins), region_splits(l.point_count, bins));
   switch (g.width) {
 #define B200NUFFT_REGION64_CASE(WIDTH)                                                                  \
   case WIDTH:                                                                                          \

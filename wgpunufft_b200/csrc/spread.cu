@@ -1192,6 +1192,101 @@ __global__ void fold_tiles_kernel(SpreadParams sp, int batch, const Complex* __r
   }
 }
 
+// Grids of at most kWarpFoldCells cells fold a cell per warp. Small grids
+// holding many points have hundreds of parts per tile, and a thread walking
+// them one after another would leave the GPU idle: here the lanes take every
+// 32nd part of each covering tile, in order, and a fixed butterfly adds the
+// 32 lane sums (every lane ends with the same bits). The order depends on the
+// grid alone, so single vectors and batches agree bit for bit.
+constexpr int64_t kWarpFoldCells = int64_t{1} << 16;
+constexpr int kWarpFoldThreads = 256;
+
+template <int D, typename Complex>
+__global__ void __launch_bounds__(kWarpFoldThreads) fold_cells_warp_kernel(
+    SpreadParams sp, int batch, const Complex* __restrict__ scratch, const uint32_t* __restrict__ part_start,
+    int64_t part_limit, const int2* __restrict__ candidates, Complex* __restrict__ fine) {
+  const int lane = threadIdx.x & 31;
+  const int64_t cell = (static_cast<int64_t>(blockIdx.x) * kWarpFoldThreads + threadIdx.x) >> 5;
+  if (cell >= sp.grid.fine_count) return;  // the whole warp leaves together
+  int coord[3] = {0, 0, 0};
+  int64_t rest = cell;
+  for (int a = 0; a < D; ++a) {
+    coord[a] = static_cast<int>(rest % sp.grid.fine[a]);
+    rest /= sp.grid.fine[a];
+  }
+  const int2* c0 = candidates + sp.candidate_base[0] + coord[0] * sp.candidate_count[0];
+  const int2* c1 = D > 1 ? candidates + sp.candidate_base[1] + coord[1] * sp.candidate_count[1] : nullptr;
+  const int2* c2 = D > 2 ? candidates + sp.candidate_base[2] + coord[2] * sp.candidate_count[2] : nullptr;
+  const int k2n = D > 2 ? sp.candidate_count[2] : 1;
+  const int k1n = D > 1 ? sp.candidate_count[1] : 1;
+  for (int b = blockIdx.y; b < batch; b += gridDim.y) {
+    Complex sum;
+    sum.x = 0;
+    sum.y = 0;
+    for (int k2 = 0; k2 < k2n; ++k2) {
+      int t2 = 0, l2 = 0;
+      if (D > 2) {
+        const int2 e = c2[k2];
+        if (e.x < 0) break;
+        t2 = e.x;
+        l2 = e.y;
+      }
+      for (int k1 = 0; k1 < k1n; ++k1) {
+        int t1 = 0, l1 = 0;
+        if (D > 1) {
+          const int2 e = c1[k1];
+          if (e.x < 0) break;
+          t1 = e.x;
+          l1 = e.y;
+        }
+        for (int k0 = 0; k0 < sp.candidate_count[0]; ++k0) {
+          const int2 e = c0[k0];
+          if (e.x < 0) break;
+          const int64_t tile =
+              e.x + static_cast<int64_t>(sp.ntiles[0]) * (t1 + static_cast<int64_t>(sp.ntiles[1]) * t2);
+          const int local = e.y + sp.pad[0] * (l1 + sp.pad[1] * l2);
+          const uint32_t first = part_start[tile];
+          const uint32_t last = min(part_start[tile + 1], static_cast<uint32_t>(part_limit));
+          for (uint32_t p = first + lane; p < last; p += 32) {
+            const Complex v = scratch[(static_cast<int64_t>(p) * batch + b) * sp.padded_cells + local];
+            sum.x += v.x;
+            sum.y += v.y;
+          }
+        }
+      }
+    }
+#pragma unroll
+    for (int o = 16; o > 0; o >>= 1) {
+      sum.x += __shfl_xor_sync(0xffffffffu, sum.x, o);
+      sum.y += __shfl_xor_sync(0xffffffffu, sum.y, o);
+    }
+    if (lane == 0) fine[static_cast<int64_t>(b) * sp.grid.fine_count + cell] = sum;
+  }
+}
+
+template <typename Complex>
+void launch_warp_fold(const SpreadParams& sp, int batch, const Complex* scratch, const uint32_t* part_start,
+                      int64_t part_limit, const int2* candidates, Complex* fine, cudaStream_t stream) {
+  constexpr int kCellsPerCta = kWarpFoldThreads / 32;
+  const dim3 grid(static_cast<unsigned>((sp.grid.fine_count + kCellsPerCta - 1) / kCellsPerCta),
+                  static_cast<unsigned>(std::min(batch, 65535)));
+  switch (sp.grid.dimensions) {
+    case 1:
+      fold_cells_warp_kernel<1, Complex><<<grid, kWarpFoldThreads, 0, stream>>>(sp, batch, scratch, part_start,
+                                                                                part_limit, candidates, fine);
+      break;
+    case 2:
+      fold_cells_warp_kernel<2, Complex><<<grid, kWarpFoldThreads, 0, stream>>>(sp, batch, scratch, part_start,
+                                                                                part_limit, candidates, fine);
+      break;
+    default:
+      fold_cells_warp_kernel<3, Complex><<<grid, kWarpFoldThreads, 0, stream>>>(sp, batch, scratch, part_start,
+                                                                                part_limit, candidates, fine);
+      break;
+  }
+  note_launch();
+}
+
 template <int BB, typename Complex>
 void launch_fold(const SpreadParams& sp, int batch, const Complex* scratch, const uint32_t* part_start,
                  int64_t part_limit, const int2* candidates, Complex* fine, cudaStream_t stream) {
@@ -1221,7 +1316,9 @@ void launch_fold(const SpreadParams& sp, int batch, const Complex* scratch, cons
 template <typename Complex>
 void fold_any(const SpreadParams& sp, int batch, const Complex* scratch, const uint32_t* part_start,
               int64_t part_limit, const int2* candidates, Complex* fine, cudaStream_t stream) {
-  if (batch >= 8) {
+  if (sp.grid.fine_count <= kWarpFoldCells) {
+    launch_warp_fold(sp, batch, scratch, part_start, part_limit, candidates, fine, stream);
+  } else if (batch >= 8) {
     launch_fold<8>(sp, batch, scratch, part_start, part_limit, candidates, fine, stream);
   } else {
     launch_fold<1>(sp, batch, scratch, part_start, part_limit, candidates, fine, stream);

@@ -15,6 +15,9 @@ Cases:
   uniform128 3D 128^3 modes, 4096 x 1526 uniform points, eps 1e-5 (profiling size)
   type3     3D type 3 in f64: 1e6 sources uniform in [-1, 1]^3 to 1e6 targets
             uniform in [-200, 200]^3, eps 1e-9 (--kind and --batch ignored)
+  type3small2d, type3small1d
+            type 3 in f32 on small outer grids: 1e6 sources uniform in
+            [-1, 1]^d to 1e6 targets uniform in [-30, 30]^d, eps 1e-6
   uneven    the 256 problems of uneven_problems(), type 1, one plan each
             (--kind and --batch ignored)
 
@@ -41,6 +44,8 @@ CASES = {
     "uniform3d": ((256, 256, 256), 4096 * 12207, 1e-5, "uniform"),
     "uniform128": ((128, 128, 128), 4096 * 1526, 1e-5, "uniform"),
     "type3": ((270, 270, 270), 1_000_000, 1e-9, "uniform"),
+    "type3small1d": ((40,), 1_000_000, 1e-6, "uniform"),
+    "type3small2d": ((40, 40), 1_000_000, 1e-6, "uniform"),
     "uneven": ((64, 64), 0, 1e-6, "uniform"),
 }
 
@@ -125,6 +130,26 @@ def run_type3(executes: int) -> None:
     torch.cuda.synchronize()
 
 
+def run_type3_small(d: int, executes: int) -> None:
+    import torch
+
+    import wgpunufft_b200 as w
+
+    g = torch.Generator(device="cuda")
+    g.manual_seed(60 + d)
+    src = (torch.rand((1_000_000, d), generator=g, device="cuda") * 2 - 1).contiguous()
+    tgt = (torch.rand((1_000_000, d), generator=g, device="cuda") * 60 - 30).contiguous()
+    c = torch.complex(torch.randn((1, 1_000_000), generator=g, device="cuda"),
+                      torch.randn((1, 1_000_000), generator=g, device="cuda"))
+    config = w.NufftType3Config(((-1.0, 1.0),) * d, ((-30.0, 30.0),) * d, eps=1e-6, precision=w.Precision.F32)
+    plan = w.NufftType3Plan(config)
+    out = torch.empty((1, 1_000_000), dtype=torch.complex64, device="cuda")
+    plan.set_points_gpu(src, tgt)
+    for _ in range(executes):
+        plan.execute_gpu_batch(1, c, out)
+    torch.cuda.synchronize()
+
+
 def run(case: str, batch: int, executes: int, kinds) -> None:
     import torch
 
@@ -132,6 +157,9 @@ def run(case: str, batch: int, executes: int, kinds) -> None:
 
     if case == "type3":
         run_type3(executes)
+        return
+    if case.startswith("type3small"):
+        run_type3_small(int(case[-2]), executes)
         return
     if case == "uneven":
         plans = []
