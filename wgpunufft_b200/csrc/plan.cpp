@@ -448,8 +448,19 @@ void NufftPlan::configure_tiles() {
     }
   }
   // Parts of at most kPartCap records (f64), fewer for small point sets so that
-  // about four CTAs per SM have work.
-  const int64_t spread_ctas = 4 * 148;
+  // about four CTAs per SM have work. On one-cell bins holding eight or more
+  // points per cell, consecutive records share their start: parts sized for
+  // one CTA per SM give every thread runs several times longer, and the
+  // warps' flushes, which would otherwise all land on the same few windows,
+  // fall on more cells and come less often.
+  // (Register runs are taken in 1D, and in 2D while the 2 w^2 accumulators
+  // fit: spread_run in spread.cu.)
+  const int64_t real_bytes = precision_ == B200NUFFT_PRECISION_F32 ? 4 : 8;
+  const bool runs = dim_ == 1 || (dim_ == 2 && 2 * w * w * real_bytes < 400);
+  bool one_cell_bins = true;
+  for (int a = 0; a < dim_; ++a) one_cell_bins = one_cell_bins && grid_.axis[a].shift == 0;
+  const bool crowded = runs && one_cell_bins && point_count_ >= 8 * grid_.fine_count;
+  const int64_t spread_ctas = (crowded ? 1 : 4) * 148;
   int64_t cap = (std::max<int64_t>(point_count_, 1) + spread_ctas - 1) / spread_ctas;
   // 3D parts stay within the 2048 records that crowded tiles bucket in shared
   // memory; 1D and 2D f32 parts take up to 16384 records, so that a thread's
