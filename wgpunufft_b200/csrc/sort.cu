@@ -316,14 +316,34 @@ __global__ void __launch_bounds__(kSortThreads) onesweep_pass_kernel(
 }
 
 // First slot of every bin from the sorted keys: bins (key[i-1], key[i]]
-// start at slot i, and bins past the last key start at `count`.
+// start at slot i, and bins past the last key start at `count`. A thread
+// writes its own short range; ranges of 32 bins or more (the empty stretches
+// between clusters) are written by the whole warp, one range after another,
+// so that no lane walks a long stretch while the others wait. Launched with
+// whole warps (blockDim a multiple of 32): every lane takes the ballot.
 __global__ void bin_offsets_kernel(const uint32_t* __restrict__ keys, int64_t count,
                                    uint64_t bins, uint32_t* __restrict__ offsets) {
   const int64_t i = static_cast<int64_t>(blockIdx.x) * blockDim.x + threadIdx.x;
-  if (i > count) return;
-  const uint64_t low = i == 0 ? 0ull : static_cast<uint64_t>(keys[i - 1]) + 1ull;
-  const uint64_t high = i == count ? bins : static_cast<uint64_t>(keys[i]);
-  for (uint64_t b = low; b <= high && b <= bins; ++b) offsets[b] = static_cast<uint32_t>(i);
+  const int lane = static_cast<int>(threadIdx.x & 31u);
+  uint64_t low = 1, high = 0;  // empty unless this thread owns a slot
+  if (i <= count) {
+    low = i == 0 ? 0ull : static_cast<uint64_t>(keys[i - 1]) + 1ull;
+    high = i == count ? bins : static_cast<uint64_t>(keys[i]);
+    high = high < bins ? high : bins;
+  }
+  const bool wide = low <= high && high - low >= 32;
+  if (!wide) {
+    for (uint64_t b = low; b <= high; ++b) offsets[b] = static_cast<uint32_t>(i);
+  }
+  unsigned pending = __ballot_sync(0xffffffffu, wide);
+  while (pending != 0) {
+    const int source = __ffs(pending) - 1;
+    pending &= pending - 1;
+    const uint64_t first = __shfl_sync(0xffffffffu, static_cast<unsigned long long>(low), source);
+    const uint64_t last = __shfl_sync(0xffffffffu, static_cast<unsigned long long>(high), source);
+    const uint32_t slot = static_cast<uint32_t>(__shfl_sync(0xffffffffu, static_cast<long long>(i), source));
+    for (uint64_t b = first + static_cast<uint64_t>(lane); b <= last; b += 32) offsets[b] = slot;
+  }
 }
 
 // The same offsets a bin at a time, for bins far outnumbering the points:
