@@ -34,6 +34,8 @@ from __future__ import annotations
 import argparse
 import math
 
+# (modes, points, eps, distribution); the type-3 entries list their outer
+# grid, and "uneven" stands for its 256 problems.
 CASES = {
     "small": ((64, 64), 100_000, 1e-6, "uniform"),
     "uniform": ((1024, 1024), 10_000_000, 1e-5, "uniform"),
@@ -44,8 +46,8 @@ CASES = {
     "uniform3d": ((256, 256, 256), 4096 * 12207, 1e-5, "uniform"),
     "uniform128": ((128, 128, 128), 4096 * 1526, 1e-5, "uniform"),
     "type3": ((270, 270, 270), 1_000_000, 1e-9, "uniform"),
-    "type3small1d": ((40,), 1_000_000, 1e-6, "uniform"),
-    "type3small2d": ((40, 40), 1_000_000, 1e-6, "uniform"),
+    "type3small1d": ((48,), 1_000_000, 1e-6, "uniform"),
+    "type3small2d": ((48, 48), 1_000_000, 1e-6, "uniform"),
     "uneven": ((64, 64), 0, 1e-6, "uniform"),
 }
 
