@@ -1406,13 +1406,6 @@ void exclusive_scan_u32(const uint32_t* in, int64_t n, uint32_t* out, cudaStream
   note_launch();
 }
 
-void spread_fold(const SpreadParams& sp, int batch, const float2* scratch, const uint32_t* part_start,
-                 int64_t part_limit, const int2* candidates, float2* fine, cudaStream_t stream,
-                 StageTimer* timer) {
-  StageScope scope(timer, kStageFold, stream);
-  fold_any(sp, batch, scratch, part_start, part_limit, candidates, fine, stream);
-}
-
 void spread_execute(const SpreadParams& sp, const SpreadLaunch& l, cudaStream_t stream,
                     StageTimer* timer) {
   SpreadLaunchT<F32Traits> t{l.points,   l.windows,  l.strengths,        l.point_count, l.batch,

@@ -106,12 +106,6 @@ void spread_count_parts(const SpreadParams& sp, const uint32_t* offsets, uint32_
 // Exclusive scan of n words into out[0, n); out[n] receives the total.
 void exclusive_scan_u32(const uint32_t* in, int64_t n, uint32_t* out, cudaStream_t stream);
 
-// Every fine-grid cell of `batch` grids as the fixed-order sum of the padded
-// tiles in `scratch` ((part * batch + b) * padded_cells) that cover it.
-void spread_fold(const SpreadParams& sp, int batch, const float2* scratch, const uint32_t* part_start,
-                 int64_t part_limit, const int2* candidates, float2* fine, cudaStream_t stream,
-                 StageTimer* timer = nullptr);
-
 // Spreads `batch` strength vectors onto `fine`, overwriting every cell.
 void spread_execute(const SpreadParams& sp, const SpreadLaunch& launch, cudaStream_t stream,
                     StageTimer* timer = nullptr);
