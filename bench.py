@@ -4,13 +4,32 @@
 A step is one type-1 execution on prepared points (sort done once by
 set_points), the reference's execute_type1_gpu; `one_shot` adds the sort
 (encode_type1_gpu). Inputs are resident in HBM; L2 is flushed with a 256 MiB
-write between steps, outside the timed events. `e2e` runs the public API with
-host buffers: pinned host -> device copies of points and strengths, one-shot
-execution, device -> host copy of the modes, every step. `--impl reference`
-times the reference's CPU plan (its restatement under oracle/; the reference
-itself needs Rust and wgpu, absent here) on the host cores. With torchrun,
-every rank runs the same workload on its own GPU (independent replicas: weak
-scaling) and the slowest rank's time counts.
+write between steps, outside the timed events. `e2e` runs the reference's C
+interface with host buffers: pinned host -> device copies of points and
+strengths, one-shot execution, device -> host copy of the modes, every step.
+
+Every line reports its relative l2 error against FP64 direct sums over all
+of its inputs, on >= 1,024 modes (type 1) or >= 10,000 points (type 2), or
+every output where the workload is small, with `meets_eps` (rel-l2 <= eps)
+and the reference's own test bound for that kind and dimension. The sums
+come from the oracle's GPU checker (oracle/gpu_direct.py), which only
+checks: nothing measured runs through it.
+
+Secondary lines: the clustered variant of the headline workload; the small
+2D configuration (64^2 modes, 10^5 points, eps 1e-6) with every output
+checked and the CPU plan timed beside it; the batched sweep on one point set
+(2D 512^2 modes, 2e6 points, B in {1, 16, 64, 256}, eps 1e-3 and 1e-6 on
+CUDA cores and tensor cores; f64 and Df64 at eps 1e-9 and 1e-12); the 3D
+radial configuration (256^3 modes, 49,999,872 points, eps 1e-5); 256 uneven
+problems; 3D type-3 in f64; type-3 on small f32 grids.
+
+`--impl reference` times the reference's CPU implementation of the path (its
+CpuNufftPlan, restated under oracle/; the reference itself needs Rust and
+wgpu, absent here) on the host cores, on all 10^7 points of the same plan:
+its value is the execution on prepared points, the metric of the GPU arm's
+value; the one-shot execution (with the sort) is reported beside it. With
+torchrun, every rank runs the same workload on its own GPU (independent
+replicas: weak scaling) and the slowest rank's time counts.
 """
 
 from __future__ import annotations
@@ -37,7 +56,12 @@ SEED = 20240601
 WORKLOAD = "2d_type1_modes1024x1024_M1e7_uniform_eps1e-5"
 METRIC = "NU points/s (type-1 2D, 1024^2 modes, 1e7 uniform points, eps 1e-5, rel-l2 vs FP64 direct reported)"
 UNIT = "points/s"
-CPU_SAMPLE = 1_000_000
+CHECK_MODES = 1024      # type-1 outputs checked against direct sums
+CHECK_POINTS = 10_000   # type-2 outputs checked against direct sums
+# The reference's relative-l2 test bounds (tests/gpu_nufft.rs:14-18,
+# gpu_nufft_2d.rs:15-16, gpu_nufft_3d.rs:14-15, gpu_nufft_batch.rs:13-16,
+# gpu_nufft_precision.rs:16-20, gpu_nufft_df64.rs:16-20, gpu_nufft_type3.rs:13-14).
+REFERENCE_BOUND = {"1d": 4.0, "2d": 20.0, "3d": 32.0, "batch": 80.0, "f64": 20.0, "df64": 24.0, "type3": 100.0}
 
 
 def parse():
@@ -46,13 +70,8 @@ def parse():
     p.add_argument("--steps", type=int, default=10)
     p.add_argument("--warmup", type=int, default=3)
     p.add_argument("--impl", default="b200", choices=["b200", "reference"])
-    p.add_argument("--no-e2e", action="store_true")
-    p.add_argument("--no-cpu", action="store_true")
-    p.add_argument("--no-batched", action="store_true")
-    p.add_argument("--no-uneven", action="store_true")
-    p.add_argument("--no-radial", action="store_true")
-    p.add_argument("--no-f64", action="store_true")
-    p.add_argument("--no-type3", action="store_true")
+    for name in ("e2e", "cpu", "clustered", "small", "batched", "uneven", "radial", "f64", "type3"):
+        p.add_argument(f"--no-{name}", action="store_true")
     return p.parse_args()
 
 
@@ -63,47 +82,66 @@ def make_inputs(rng_seed=SEED, count=POINTS):
     return points, strengths
 
 
-def cpu_plan_throughput(points, strengths, repeats=3):
-    """Median NU points/s of the restated CPU plan (one-shot execution) over `repeats` runs."""
+def cpu_nproc():
+    threads = os.cpu_count() or 1
+    try:
+        threads = len(os.sched_getaffinity(0))
+    except AttributeError:
+        pass
+    return threads
+
+
+def cpu_model():
+    try:
+        for line in Path("/proc/cpuinfo").read_text().splitlines():
+            if line.startswith("model name"):
+                return line.split(":", 1)[1].strip()
+    except OSError:
+        pass
+    return "unknown"
+
+
+def cpu_plan_timings(points, strengths, modes, eps, steps, warmup, kind=1):
+    """Medians of the restated CPU plan over `steps` one-shot executions (after
+    `warmup`): one-shot, point preparation, execution on prepared points; the
+    same medians nufft_cpu_bench.rs:121-131 reports."""
     from oracle import native
 
-    plan = native.CpuPlan(1, MODES, EPS, precision="f32")
-    threads = os.cpu_count() or 1
-    times = []
-    for _ in range(repeats):
-        t0 = time.perf_counter()
+    plan = native.CpuPlan(kind, modes, eps, precision="f32")
+    threads = cpu_nproc()
+    for _ in range(warmup):
         plan.execute(points, strengths, threads=threads)
-        times.append(time.perf_counter() - t0)
-    return len(points) / statistics.median(times), threads, statistics.median(times)
+    totals, stages = [], []
+    for _ in range(steps):
+        t0 = time.perf_counter()
+        plan.execute(points, strengths, threads=threads, stage_seconds=stages)
+        totals.append(time.perf_counter() - t0)
+    return {"one_shot_s": statistics.median(totals), "prepare_s": statistics.median(s[0] for s in stages),
+            "prepared_s": statistics.median(s[1] for s in stages), "threads": threads,
+            "one_shot_total_s": sum(totals), "prepared_total_s": sum(s[1] for s in stages)}
 
 
 def reference_arm(args):
-    """The reference's CPU implementation (restated) on a bounded sample per step."""
+    """The reference's CPU implementation (restated) on all points of the workload."""
     rank = int(os.environ.get("RANK", "0"))
     if rank != 0:
         return
-    from oracle import native
-
-    points, strengths = make_inputs(count=CPU_SAMPLE)
-    plan = native.CpuPlan(1, MODES, EPS, precision="f32")
-    threads = os.cpu_count() or 1
-    for _ in range(args.warmup):
-        plan.execute(points, strengths, threads=threads)
-    times = []
-    for _ in range(args.steps):
-        t0 = time.perf_counter()
-        plan.execute(points, strengths, threads=threads)
-        times.append(time.perf_counter() - t0)
-    ms = 1e3 * sum(times) / len(times)
-    value = CPU_SAMPLE / (ms / 1e3)
-    sample = (f"{CPU_SAMPLE:,} of the {POINTS:,} uniform points per step on the same 1024^2-mode "
-              f"(2048^2 fine grid) eps 1e-5 plan; one-shot execution incl. sort")
+    points, strengths = make_inputs()
+    t = cpu_plan_timings(points, strengths, MODES, EPS, args.steps, args.warmup)
+    ms = 1e3 * t["prepared_total_s"] / args.steps
+    value = POINTS / (ms / 1e3)
+    sample = (f"all {POINTS:,} uniform points of the 1024^2-mode (2048^2 fine grid) eps 1e-5 plan per step; "
+              f"value = execution on prepared points (median {1e3 * t['prepared_s']:.0f} ms), "
+              f"one-shot with the sort {1e3 * t['one_shot_s']:.0f} ms; {t['threads']} threads of {cpu_model()}")
     line = {
         "impl": "reference", "metric": METRIC, "value": value, "unit": UNIT, "n_gpus": args.gpus,
         "steps": args.steps, "warmup": args.warmup, "ms_per_step": ms, "higher_is_better": True,
         "scaling": "weak", "vs_baseline": None, "dtype": "c64", "data": "synthetic (seeded uniform)",
-        "config": {"workload": WORKLOAD, "modes": list(MODES), "points_per_step": CPU_SAMPLE, "eps": EPS},
-        "cpu_baseline": {"value": value, "unit": UNIT, "cores": threads, "kind": "port", "sample": sample},
+        "config": {"workload": WORKLOAD, "modes": list(MODES), "points": POINTS, "points_per_step": POINTS,
+                   "eps": EPS},
+        "one_shot": {"value": POINTS / t["one_shot_s"], "unit": UNIT, "ms_per_step": 1e3 * t["one_shot_s"]},
+        "prepare_ms": 1e3 * t["prepare_s"],
+        "cpu_baseline": {"value": value, "unit": UNIT, "cores": t["threads"], "kind": "port", "sample": sample},
         "e2e": {"value": value, "unit": UNIT, "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0},
     }
     print(json.dumps(line), flush=True)
@@ -173,12 +211,92 @@ def replica_throughput(world, units_per_replica, total_ms, steps):
     return world * units_per_replica / (total_ms / steps / 1e3)
 
 
-def c_interface_e2e(w, torch, points_h, strengths_h, timed, barrier, world, dev, args):
+class Runner:
+    """Timing and accuracy helpers shared by every line."""
+
+    def __init__(self, torch, w, args, world, rank, local):
+        self.torch, self.w, self.args = torch, w, args
+        self.world, self.rank, self.local = world, rank, local
+        self.dev = f"cuda:{local}"
+        self.flush = torch.empty(256 * 1024 * 1024 // 4, dtype=torch.float32, device=self.dev)
+        self.stream = torch.cuda.current_stream()
+
+    def barrier(self):
+        import torch.distributed as dist
+
+        if self.world > 1:
+            dist.barrier()
+        self.torch.cuda.synchronize()
+
+    def timed(self, step_fn, steps, stream=None):
+        """Total ms of `steps` calls, each bracketed by CUDA events on the
+        launching stream after an L2 flush outside the events."""
+        torch = self.torch
+        stream = stream or self.stream
+        starts = [torch.cuda.Event(enable_timing=True) for _ in range(steps)]
+        ends = [torch.cuda.Event(enable_timing=True) for _ in range(steps)]
+        for i in range(steps):
+            with torch.cuda.stream(stream):
+                self.flush.fill_(float(i))
+            starts[i].record(stream)
+            step_fn()
+            ends[i].record(stream)
+        torch.cuda.synchronize()
+        return sum(s.elapsed_time(e) for s, e in zip(starts, ends))
+
+    def measure(self, step_fn, units, steps, warmup):
+        for _ in range(max(warmup, 1)):
+            step_fn()
+        self.barrier()
+        total = self.timed(step_fn, steps)
+        (total,) = max_over_ranks([total], self.dev)
+        return {"value": replica_throughput(self.world, units, total, steps), "ms_per_step": total / steps}
+
+    # Accuracy against FP64 direct sums (rank 0 only; None elsewhere).
+    def check_type1(self, points, strengths, out, modes, eps, bound_key, vectors=4, count=CHECK_MODES, seed=1,
+                    isign=1):
+        if self.rank != 0:
+            return None
+        from oracle import gpu_direct
+
+        n = int(np.prod(modes))
+        select = np.sort(np.random.default_rng(seed).choice(n, min(count, n), replace=False))
+        nb = min(vectors, strengths.shape[0] if strengths.dim() > 1 else 1)
+        s = strengths.reshape(-1, points.shape[0])[:nb]
+        ref = gpu_direct.direct_type1(points, s, modes, isign, select=select, device=self.dev)
+        got = out.reshape(-1, n)[:nb][:, self.torch.as_tensor(select, device=self.dev)].cpu().numpy()
+        return accuracy(got, ref, eps, bound_key, f"{len(select)} modes x {nb} vectors")
+
+    def check_type2(self, points, coefficients, out, modes, eps, bound_key, vectors=4, count=CHECK_POINTS, seed=2,
+                    isign=1):
+        if self.rank != 0:
+            return None
+        from oracle import gpu_direct
+
+        m = points.shape[0]
+        n = int(np.prod(modes))
+        pick = np.sort(np.random.default_rng(seed).choice(m, min(count, m), replace=False))
+        nb = min(vectors, coefficients.reshape(-1, n).shape[0])
+        ref = gpu_direct.direct_type2(points, coefficients.reshape(-1, n)[:nb], modes, isign, select=pick,
+                                      device=self.dev)
+        got = out.reshape(-1, m)[:nb][:, self.torch.as_tensor(pick, device=self.dev)].cpu().numpy()
+        return accuracy(got, ref, eps, bound_key, f"{len(pick)} points x {nb} vectors")
+
+
+def accuracy(got, ref, eps, bound_key, subset):
+    rel = float(np.linalg.norm(got.astype(np.complex128) - ref) / np.linalg.norm(ref))
+    bound = REFERENCE_BOUND[bound_key] * eps
+    return {"rel_l2": rel, "eps": eps, "meets_eps": rel <= eps, "reference_bound": bound,
+            "within_reference_bound": rel <= bound, "checked": subset}
+
+
+def c_interface_e2e(r, points_h, strengths_h):
     """NU points/s of wgpu_nufftf_setpts + wgpu_nufftf_execute on pinned host arrays."""
     import ctypes
 
     from wgpunufft_b200 import _native
 
+    torch = r.torch
     lib = _native.library()
     x = torch.from_numpy(np.ascontiguousarray(points_h[:, 0])).pin_memory()
     y = torch.from_numpy(np.ascontiguousarray(points_h[:, 1])).pin_memory()
@@ -201,305 +319,297 @@ def c_interface_e2e(w, torch, points_h, strengths_h, timed, barrier, world, dev,
             failures.append(lib.wgpu_nufft_last_error().decode())
 
     try:
-        for _ in range(2):
+        for _ in range(max(2, r.args.warmup)):
             step()
-        barrier()
-        e2e_ms = timed(step, args.steps)
+        r.barrier()
+        e2e_ms = r.timed(step, r.args.steps)
     finally:
         lib.wgpu_nufftf_destroy(plan)
     if failures:
         return {"error": failures[0]}
-    (e2e_ms,) = max_over_ranks([e2e_ms], dev)
-    return {"value": replica_throughput(world, POINTS, e2e_ms, args.steps), "unit": UNIT,
-            "ms_per_step": e2e_ms / args.steps,
+    (e2e_ms,) = max_over_ranks([e2e_ms], r.dev)
+    return {"value": replica_throughput(r.world, POINTS, e2e_ms, r.args.steps), "unit": UNIT,
+            "ms_per_step": e2e_ms / r.args.steps,
             "h2d_bytes_per_step": POINTS * 4 * 2 + POINTS * 8, "d2h_bytes_per_step": MODES[0] * MODES[1] * 8,
             "path": "C interface wgpu_nufftf_setpts (per-axis f32, pinned host) + wgpu_nufftf_execute, "
                     "plan made once; host-to-device copies, stable bin sort, spread, FFT, deconvolution "
                     "and device-to-host copy inside every step"}
 
 
+def stage_ms(stages, steps):
+    return {k: round(v[0] / steps, 4) for k, v in stages.items()}
+
+
+def clustered_line(r):
+    """The clustered variant of the headline workload (8 centres, N(c, 0.01^2 I)
+    wrapped), type 1 and type 2 on prepared points."""
+    from wgpunufft_b200 import workloads
+
+    torch, w = r.torch, r.w
+    steps = max(1, min(r.args.steps, 5))
+    pts = workloads.points("clustered", POINTS, 2, seed=SEED % 1000 + 21, device=r.dev)
+    c = workloads.values(1, POINTS, seed=SEED % 1000 + 22, device=r.dev)
+    n = MODES[0] * MODES[1]
+    out = {"workload": "2d_modes1024x1024_M1e7_clustered_eps1e-5", "unit": UNIT}
+    plan = w.NufftPlan.type1_gpu(w.NufftConfig(MODES, EPS))
+    plan.set_points_gpu(pts)
+    modes = torch.empty((1, n), dtype=torch.complex64, device=r.dev)
+    out["type1"] = r.measure(lambda: plan.execute_gpu_batch(1, c, modes), POINTS, steps, r.args.warmup)
+    out["type1"].update(r.check_type1(pts, c, modes, MODES, EPS, "2d") or {})
+    del plan
+    plan2 = w.NufftPlan.type2_gpu(w.NufftConfig(MODES, EPS))
+    plan2.set_points_gpu(pts)
+    f = workloads.values(1, n, seed=SEED % 1000 + 23, device=r.dev)
+    vals = torch.empty((1, POINTS), dtype=torch.complex64, device=r.dev)
+    out["type2"] = r.measure(lambda: plan2.execute_gpu_batch(1, f, vals), POINTS, steps, r.args.warmup)
+    out["type2"].update(r.check_type2(pts, f, vals, MODES, EPS, "2d") or {})
+    del plan2, pts, c, f, vals, modes
+    torch.cuda.empty_cache()
+    return out
+
+
+def small_line(r):
+    """The small 2D configuration: 64^2 modes, 10^5 uniform points, eps 1e-6,
+    type 1 and type 2 with every output checked against FP64 direct sums over
+    all points and modes, and the restated CPU plan timed on the same inputs."""
+    torch, w = r.torch, r.w
+    modes, count, eps = (64, 64), 100_000, 1e-6
+    rng = np.random.default_rng(SEED + 11)
+    pts_h = rng.uniform(-np.pi, np.pi, (count, 2)).astype(np.float32)
+    c_h = (rng.standard_normal(count) + 1j * rng.standard_normal(count)).astype(np.complex64)
+    f_h = (rng.standard_normal(64 * 64) + 1j * rng.standard_normal(64 * 64)).astype(np.complex64)
+    pts = torch.from_numpy(pts_h).to(r.dev)
+    c = torch.from_numpy(c_h).to(r.dev).reshape(1, -1)
+    f = torch.from_numpy(f_h).to(r.dev).reshape(1, -1)
+    steps = max(3, min(r.args.steps, 20))
+    out = {"workload": "2d_modes64x64_M1e5_uniform_eps1e-6", "unit": UNIT}
+    plan = w.NufftPlan.type1_gpu(w.NufftConfig(modes, eps))
+    plan.set_points_gpu(pts)
+    m1 = torch.empty((1, 4096), dtype=torch.complex64, device=r.dev)
+    out["type1"] = r.measure(lambda: plan.execute_gpu_batch(1, c, m1), count, steps, r.args.warmup)
+    out["type1"]["one_shot"] = r.measure(lambda: plan.encode_gpu_batch(1, pts, c, m1), count, steps, 1)["value"]
+    out["type1"].update(r.check_type1(pts, c, m1, modes, eps, "2d", count=4096) or {})
+    plan2 = w.NufftPlan.type2_gpu(w.NufftConfig(modes, eps))
+    plan2.set_points_gpu(pts)
+    v2 = torch.empty((1, count), dtype=torch.complex64, device=r.dev)
+    out["type2"] = r.measure(lambda: plan2.execute_gpu_batch(1, f, v2), count, steps, r.args.warmup)
+    out["type2"].update(r.check_type2(pts, f, v2, modes, eps, "2d", count=count) or {})
+    if r.rank == 0 and not r.args.no_cpu:
+        t1 = cpu_plan_timings(pts_h, c_h, modes, eps, 5, 1, kind=1)
+        t2 = cpu_plan_timings(pts_h, f_h, modes, eps, 5, 1, kind=2)
+        out["cpu_plan"] = {"type1_prepared": count / t1["prepared_s"], "type1_one_shot": count / t1["one_shot_s"],
+                           "type2_prepared": count / t2["prepared_s"], "type2_one_shot": count / t2["one_shot_s"],
+                           "threads": t1["threads"], "unit": UNIT}
+    del plan, plan2
+    return out
+
+
 BATCH_MODES = (512, 512)
 BATCH_POINTS = 2_000_000
-BATCH_EPS = 1e-6
 
 
-def batched_comparison(w, torch, timed, barrier, world, dev, args, rank):
-    """Type-1 NU points/s (points x vectors) of 64 and 256 vectors sharing one
-    point set, tensor cores (3xTF32) against CUDA cores, plus rel-l2 against
-    FP64 direct sums on 8 modes x 4 vectors."""
-    g = torch.Generator(device=dev)
-    g.manual_seed(SEED + 4)
-    pts = (torch.rand((BATCH_POINTS, 2), generator=g, device=dev) * (2 * np.pi) - np.pi).float().contiguous()
-    result = {"workload": "2d_type1_modes512x512_M2e6_uniform_eps1e-6", "modes": list(BATCH_MODES),
-              "points": BATCH_POINTS, "eps": BATCH_EPS, "unit": "NU points/s (points x vectors)"}
-    steps = max(1, min(args.steps, 5))
-    select = np.random.default_rng(3).choice(BATCH_MODES[0] * BATCH_MODES[1], 8, replace=False)
-    pts_h = pts.cpu().numpy().astype(np.float64) if rank == 0 else None
-    for batch in (64, 256):
-        c = torch.complex(torch.randn((batch, BATCH_POINTS), generator=g, device=dev),
-                          torch.randn((batch, BATCH_POINTS), generator=g, device=dev))
-        out = torch.empty((batch, BATCH_MODES[0] * BATCH_MODES[1]), dtype=torch.complex64, device=dev)
-        entry = {}
-        for name, method in (("tensor_cores", w.SpreadMethod.TENSOR_CORES), ("cuda_cores", w.SpreadMethod.CUDA_CORES)):
-            plan = w.NufftPlan.type1_gpu(w.NufftConfig(BATCH_MODES, BATCH_EPS, batch=batch, spread_method=method))
-            plan.set_points_gpu(pts)
-            for _ in range(max(1, args.warmup)):
-                plan.execute_gpu_batch(batch, c, out)
-            barrier()
-            plan.stage_timing(True)
-            plan.stage_report()
-            total = timed(lambda: plan.execute_gpu_batch(batch, c, out), steps)
-            stages = plan.stage_report()
-            plan.stage_timing(False)
-            (total,) = max_over_ranks([total], dev)
-            ms = total / steps
-            item = {"value": replica_throughput(world, BATCH_POINTS * batch, total, steps), "ms_per_step": ms,
-                    "stages_ms_per_step": {k: v[0] / steps for k, v in stages.items()}}
-            if rank == 0:
-                from oracle import native
+def batched_sweep(r):
+    """One point set (2D 512^2 modes, 2e6 uniform points), B vectors: f32 type 1
+    on CUDA cores and on tensor cores (3xTF32) and type 2, eps 1e-3 and 1e-6,
+    B in {1, 16, 64, 256}; f64 and Df64 at eps 1e-9 and 1e-12 for B in {1, 16}.
+    NU points/s counts points x vectors."""
+    from wgpunufft_b200 import workloads
 
-                got = out[:4].cpu().numpy()[:, select]
-                ref = native.direct_type1(pts_h, c[:4].cpu().numpy().astype(np.complex128), BATCH_MODES,
-                                          select=select)
-                item["rel_l2"] = float(np.linalg.norm(got - ref) / np.linalg.norm(ref))
-            entry[name] = item
-            del plan
-        # Type 2 on the same points: modes of every vector to the points.
-        plan2 = w.NufftPlan.type2_gpu(w.NufftConfig(BATCH_MODES, BATCH_EPS, batch=batch))
-        plan2.set_points_gpu(pts)
-        f = torch.complex(torch.randn((batch, BATCH_MODES[0] * BATCH_MODES[1]), generator=g, device=dev),
-                          torch.randn((batch, BATCH_MODES[0] * BATCH_MODES[1]), generator=g, device=dev))
-        vals = torch.empty((batch, BATCH_POINTS), dtype=torch.complex64, device=dev)
-        for _ in range(max(1, args.warmup)):
-            plan2.execute_gpu_batch(batch, f, vals)
-        barrier()
-        total2 = timed(lambda: plan2.execute_gpu_batch(batch, f, vals), steps)
-        (total2,) = max_over_ranks([total2], dev)
-        item2 = {"value": replica_throughput(world, BATCH_POINTS * batch, total2, steps), "ms_per_step": total2 / steps,
-                 "engine": "CUDA cores, bin regions staged in shared memory"}
-        if rank == 0:
-            from oracle import native
-
-            pick = np.random.default_rng(4).choice(BATCH_POINTS, 64, replace=False)
-            ref2 = native.direct_type2(pts_h[pick], f[:4].cpu().numpy().astype(np.complex128), BATCH_MODES)
-            got2 = vals[:4].cpu().numpy()[:, pick]
-            item2["rel_l2"] = float(np.linalg.norm(got2 - ref2) / np.linalg.norm(ref2))
-        entry["type2"] = item2
-        del plan2, f, vals
-        entry["speedup_tensor_over_cuda_cores"] = entry["tensor_cores"]["value"] / entry["cuda_cores"]["value"]
-        spread_ms = entry["tensor_cores"]["stages_ms_per_step"].get("spread", 0.0)
-        useful = 4.0 * batch * BATCH_POINTS * 7 * 7
-        entry["tensor_core_spread_useful_tflops"] = useful / (spread_ms / 1e3) / 1e12 if spread_ms else None
-        result[f"B{batch}"] = entry
-        del c, out
-        torch.cuda.empty_cache()
+    torch, w = r.torch, r.w
+    steps = max(1, min(r.args.steps, 5))
+    pts = workloads.points("uniform", BATCH_POINTS, 2, seed=SEED % 1000 + 4, device=r.dev)
+    n = BATCH_MODES[0] * BATCH_MODES[1]
+    result = {"workload": "2d_modes512x512_M2e6_uniform", "unit": "NU points/s (points x vectors)"}
+    for eps in (1e-3, 1e-6):
+        for batch in (1, 16, 64, 256):
+            c = workloads.values(batch, BATCH_POINTS, seed=batch, device=r.dev)
+            modes = torch.empty((batch, n), dtype=torch.complex64, device=r.dev)
+            entry = {}
+            for name, method in (("tensor_cores", w.SpreadMethod.TENSOR_CORES),
+                                 ("cuda_cores", w.SpreadMethod.CUDA_CORES)):
+                plan = w.NufftPlan.type1_gpu(w.NufftConfig(BATCH_MODES, eps, batch=batch, spread_method=method))
+                plan.set_points_gpu(pts)
+                plan.stage_timing(True)
+                item = r.measure(lambda: plan.execute_gpu_batch(batch, c, modes), BATCH_POINTS * batch, steps,
+                                 r.args.warmup)
+                stages = plan.stage_report()
+                plan.stage_timing(False)
+                item["spread_ms"] = round(stages.get("spread", (0.0, 1))[0] / (steps + max(r.args.warmup, 1)), 4)
+                item.update(r.check_type1(pts, c, modes, BATCH_MODES, eps, "batch", seed=batch) or {})
+                entry[f"type1_{name}"] = item
+                del plan
+            entry["tensor_over_cuda_cores"] = entry["type1_tensor_cores"]["value"] / entry["type1_cuda_cores"]["value"]
+            del c, modes
+            f = workloads.values(batch, n, seed=1000 + batch, device=r.dev)
+            vals = torch.empty((batch, BATCH_POINTS), dtype=torch.complex64, device=r.dev)
+            plan2 = w.NufftPlan.type2_gpu(w.NufftConfig(BATCH_MODES, eps, batch=batch))
+            plan2.set_points_gpu(pts)
+            item2 = r.measure(lambda: plan2.execute_gpu_batch(batch, f, vals), BATCH_POINTS * batch, steps,
+                              r.args.warmup)
+            item2.update(r.check_type2(pts, f, vals, BATCH_MODES, eps, "batch", seed=batch) or {})
+            entry["type2_cuda_cores"] = item2
+            del plan2, f, vals
+            torch.cuda.empty_cache()
+            result[f"eps{eps:g}_B{batch}"] = entry
+    pts64 = pts.double()
+    for precision, tag in ((w.Precision.F64, "f64"), (w.Precision.DF64, "df64")):
+        for eps in (1e-9, 1e-12):
+            for batch in (1, 16):
+                c = workloads.values(batch, BATCH_POINTS, seed=batch + 7, device=r.dev).to(torch.complex128)
+                f = workloads.values(batch, n, seed=batch + 8, device=r.dev).to(torch.complex128)
+                entry = {}
+                if precision == w.Precision.DF64:
+                    p_in, c_in, f_in = to_df64(torch, pts64), to_df64(torch, c), to_df64(torch, f)
+                else:
+                    p_in, c_in, f_in = pts64, c, f
+                for kind in (1, 2):
+                    config = w.NufftConfig(BATCH_MODES, eps, batch=batch, precision=precision)
+                    plan = (w.NufftPlan.type1_gpu if kind == 1 else w.NufftPlan.type2_gpu)(config)
+                    outputs = n if kind == 1 else BATCH_POINTS
+                    if precision == w.Precision.DF64:
+                        # (hi, lo) float pairs of the real and imaginary parts.
+                        out = torch.empty((batch, 4 * outputs), dtype=torch.float32, device=r.dev)
+                    else:
+                        out = torch.empty((batch, outputs), dtype=torch.complex128, device=r.dev)
+                    plan.set_points_gpu(p_in)
+                    inputs = c_in if kind == 1 else f_in
+                    item = r.measure(lambda: plan.execute_gpu_batch(batch, inputs, out), BATCH_POINTS * batch,
+                                     steps, r.args.warmup)
+                    item["kernel_width"] = plan.kernel_width()
+                    got = from_df64(torch, out) if precision == w.Precision.DF64 else out
+                    if kind == 1:
+                        item.update(r.check_type1(pts64, c, got, BATCH_MODES, eps, tag, seed=batch) or {})
+                    else:
+                        item.update(r.check_type2(pts64, f, got, BATCH_MODES, eps, tag, seed=batch) or {})
+                    entry[f"type{kind}"] = item
+                    del plan, out
+                result[f"{tag}_eps{eps:g}_B{batch}"] = entry
+                del c, f, p_in, c_in, f_in
+                torch.cuda.empty_cache()
+    del pts, pts64
+    torch.cuda.empty_cache()
     return result
 
 
-def radial_3d_line(w, torch, timed, barrier, world, dev, args, rank):
+def to_df64(torch, x):
+    """Double-float storage of an f64 (or c128) tensor: (hi, lo) f32 pairs per scalar."""
+    real = torch.view_as_real(x) if x.is_complex() else x
+    hi = real.to(torch.float32)
+    lo = (real - hi.to(torch.float64)).to(torch.float32)
+    return torch.stack([hi, lo], dim=-1).contiguous()
+
+
+def from_df64(torch, pairs):
+    """The complex128 values of Df64 output storage (hi, lo pairs of re and im)."""
+    p = torch.view_as_real(pairs) if pairs.is_complex() else pairs
+    p = p.reshape(p.shape[0], -1, 2, 2).to(torch.float64)
+    v = p[..., 0] + p[..., 1]
+    return torch.complex(v[..., 0], v[..., 1])
+
+
+def radial_3d_line(r):
     """The 3D configuration: 256^3 modes, 4096 radial spokes x 12207 samples
-    (49,999,872 points), eps 1e-5. Type-1 and type-2 NU points/s on prepared
-    points with stage times, and rel-l2 against FP64 direct sums on 4 modes
-    (type 1) and 64 points (type 2)."""
+    (49,999,872 points), eps 1e-5; type 1 and type 2 on prepared points."""
     from wgpunufft_b200 import workloads
 
+    torch, w = r.torch, r.w
     modes, count, eps, dist = workloads.CASES["radial"]
-    pts = workloads.points(dist, count, 3, seed=SEED % 1000 + 31, device=dev)
-    c = workloads.values(1, count, seed=SEED % 1000 + 32, device=dev)
+    pts = workloads.points(dist, count, 3, seed=SEED % 1000 + 31, device=r.dev)
+    c = workloads.values(1, count, seed=SEED % 1000 + 32, device=r.dev)
     n = modes[0] * modes[1] * modes[2]
-    result = {"workload": "3d_type1_type2_modes256^3_M49999872_radial_eps1e-5", "modes": list(modes),
-              "points": count, "eps": eps, "unit": UNIT}
-    steps = max(1, min(args.steps, 5))
-    pts_h = pts.cpu().numpy().astype(np.float64) if rank == 0 else None
+    result = {"workload": "3d_modes256^3_M49999872_radial_eps1e-5", "unit": UNIT}
+    steps = max(1, min(r.args.steps, 5))
     plan = w.NufftPlan.type1_gpu(w.NufftConfig(modes, eps))
     plan.set_points_gpu(pts)
-    out = torch.empty((1, n), dtype=torch.complex64, device=dev)
-    for _ in range(max(1, args.warmup)):
-        plan.execute_gpu_batch(1, c, out)
-    barrier()
+    out = torch.empty((1, n), dtype=torch.complex64, device=r.dev)
     plan.stage_timing(True)
-    plan.stage_report()
-    total = timed(lambda: plan.execute_gpu_batch(1, c, out), steps)
-    stages = plan.stage_report()
+    item = r.measure(lambda: plan.execute_gpu_batch(1, c, out), count, steps, r.args.warmup)
+    item["stages_ms_per_step"] = stage_ms(plan.stage_report(), steps + max(r.args.warmup, 1))
     plan.stage_timing(False)
-    (total,) = max_over_ranks([total], dev)
-    item = {"value": replica_throughput(world, count, total, steps), "ms_per_step": total / steps,
-            "stages_ms_per_step": {k: v[0] / steps for k, v in stages.items()}}
-    if rank == 0:
-        from oracle import native
-
-        select = np.random.default_rng(9).choice(n, 4, replace=False)
-        ref = native.direct_type1(pts_h, c.cpu().numpy().astype(np.complex128), modes, select=select)
-        got = out.cpu().numpy()[:, select]
-        item["rel_l2"] = float(np.linalg.norm(got - ref) / np.linalg.norm(ref))
+    item.update(r.check_type1(pts, c, out, modes, eps, "3d") or {})
     result["type1"] = item
     del plan, out
+    torch.cuda.empty_cache()
     plan2 = w.NufftPlan.type2_gpu(w.NufftConfig(modes, eps))
     plan2.set_points_gpu(pts)
-    g = torch.Generator(device=dev)
-    g.manual_seed(SEED + 33)
-    f = torch.complex(torch.randn((1, n), generator=g, device=dev), torch.randn((1, n), generator=g, device=dev))
-    vals = torch.empty((1, count), dtype=torch.complex64, device=dev)
-    for _ in range(max(1, args.warmup)):
-        plan2.execute_gpu_batch(1, f, vals)
-    barrier()
-    total2 = timed(lambda: plan2.execute_gpu_batch(1, f, vals), steps)
-    (total2,) = max_over_ranks([total2], dev)
-    item2 = {"value": replica_throughput(world, count, total2, steps), "ms_per_step": total2 / steps}
-    if rank == 0:
-        from oracle import native
-
-        pick = np.random.default_rng(10).choice(count, 64, replace=False)
-        ref2 = native.direct_type2(pts_h[pick], f.cpu().numpy().astype(np.complex128), modes)
-        got2 = vals.cpu().numpy()[:, pick]
-        item2["rel_l2"] = float(np.linalg.norm(got2 - ref2) / np.linalg.norm(ref2))
+    f = workloads.values(1, n, seed=SEED % 1000 + 33, device=r.dev)
+    vals = torch.empty((1, count), dtype=torch.complex64, device=r.dev)
+    item2 = r.measure(lambda: plan2.execute_gpu_batch(1, f, vals), count, steps, r.args.warmup)
+    item2.update(r.check_type2(pts, f, vals, modes, eps, "3d") or {})
     result["type2"] = item2
     del plan2, f, vals, pts, c
     torch.cuda.empty_cache()
     return result
 
 
-def f64_line(w, torch, timed, barrier, world, dev, args, rank):
-    """f64 plans of the batched configuration: 2D 512^2 modes, 2e6 uniform
-    points, eps 1e-9 (w = 10) and 1e-12 (w = 13), one vector; type-1 and
-    type-2 NU points/s with rel-l2 against FP64 direct sums (8 modes, 64
-    points)."""
-    g = torch.Generator(device=dev)
-    g.manual_seed(SEED + 41)
-    pts = (torch.rand((BATCH_POINTS, 2), generator=g, device=dev, dtype=torch.float64) * (2 * np.pi) - np.pi).contiguous()
-    n = BATCH_MODES[0] * BATCH_MODES[1]
-    steps = max(1, min(args.steps, 5))
-    pts_h = pts.cpu().numpy() if rank == 0 else None
-    result = {"workload": "2d_modes512x512_M2e6_uniform_f64", "modes": list(BATCH_MODES), "points": BATCH_POINTS,
-              "unit": UNIT}
-    for eps in (1e-9, 1e-12):
-        entry = {}
-        c = torch.complex(torch.randn((1, BATCH_POINTS), generator=g, device=dev, dtype=torch.float64),
-                          torch.randn((1, BATCH_POINTS), generator=g, device=dev, dtype=torch.float64))
-        f = torch.complex(torch.randn((1, n), generator=g, device=dev, dtype=torch.float64),
-                          torch.randn((1, n), generator=g, device=dev, dtype=torch.float64))
-        for kind in (1, 2):
-            config = w.NufftConfig(BATCH_MODES, eps, precision=w.Precision.F64)
-            plan = (w.NufftPlan.type1_gpu if kind == 1 else w.NufftPlan.type2_gpu)(config)
-            plan.set_points_gpu(pts)
-            inputs = c if kind == 1 else f
-            out = torch.empty((1, n if kind == 1 else BATCH_POINTS), dtype=torch.complex128, device=dev)
-            for _ in range(max(1, args.warmup)):
-                plan.execute_gpu_batch(1, inputs, out)
-            barrier()
-            total = timed(lambda: plan.execute_gpu_batch(1, inputs, out), steps)
-            (total,) = max_over_ranks([total], dev)
-            item = {"value": replica_throughput(world, BATCH_POINTS, total, steps), "ms_per_step": total / steps,
-                    "kernel_width": plan.kernel_width()}
-            if rank == 0:
-                from oracle import native
-
-                if kind == 1:
-                    select = np.random.default_rng(12).choice(n, 8, replace=False)
-                    ref = native.direct_type1(pts_h, c.cpu().numpy(), BATCH_MODES, select=select)
-                    got = out.cpu().numpy()[:, select]
-                else:
-                    pick = np.random.default_rng(13).choice(BATCH_POINTS, 64, replace=False)
-                    ref = native.direct_type2(pts_h[pick], f.cpu().numpy(), BATCH_MODES)
-                    got = out.cpu().numpy()[:, pick]
-                item["rel_l2"] = float(np.linalg.norm(got - ref) / np.linalg.norm(ref))
-            entry[f"type{kind}"] = item
-            del plan, out
-        result[f"eps{eps:g}"] = entry
-    return result
-
-
-def type3_line(w, torch, timed, barrier, world, dev, args, rank):
-    """The 3D type-3 configuration: f64, 10^6 sources uniform in [-1, 1]^3 to
-    10^6 targets uniform in [-200, 200]^3, eps 1e-9. Execution on set points
-    (pre-phase, outer spread, inner type 2, post-phase) and set_points +
-    execution, with rel-l2 against FP64 direct sums on 64 targets."""
+def type3_line(r):
+    """3D type 3 in f64: 10^6 sources uniform in [-1, 1]^3 to 10^6 targets
+    uniform in [-200, 200]^3, eps 1e-9, checked on 1,000 targets; and f32 type
+    3 on small outer grids (10^6 sources in [-1, 1]^d to 10^6 targets in
+    [-30, 30]^d, eps 1e-6, d = 1 and 2), the regime of the reference's dense
+    small-grid spreader (src/gpu_dense_spread.rs:68-78)."""
+    torch, w = r.torch, r.w
     count = 1_000_000
-    g = torch.Generator(device=dev)
+    g = torch.Generator(device=r.dev)
     g.manual_seed(SEED + 51)
-    src = (torch.rand((count, 3), generator=g, device=dev, dtype=torch.float64) * 2 - 1).contiguous()
-    tgt = (torch.rand((count, 3), generator=g, device=dev, dtype=torch.float64) * 400 - 200).contiguous()
-    c = torch.complex(torch.randn((1, count), generator=g, device=dev, dtype=torch.float64),
-                      torch.randn((1, count), generator=g, device=dev, dtype=torch.float64))
-    config = w.NufftType3Config(((-1.0, 1.0),) * 3, ((-200.0, 200.0),) * 3, eps=1e-9)
-    plan = w.NufftType3Plan(config)
-    out = torch.empty((1, count), dtype=torch.complex128, device=dev)
-    steps = max(1, min(args.steps, 3))
+    src = (torch.rand((count, 3), generator=g, device=r.dev, dtype=torch.float64) * 2 - 1).contiguous()
+    tgt = (torch.rand((count, 3), generator=g, device=r.dev, dtype=torch.float64) * 400 - 200).contiguous()
+    c = torch.complex(torch.randn((1, count), generator=g, device=r.dev, dtype=torch.float64),
+                      torch.randn((1, count), generator=g, device=r.dev, dtype=torch.float64))
+    plan = w.NufftType3Plan(w.NufftType3Config(((-1.0, 1.0),) * 3, ((-200.0, 200.0),) * 3, eps=1e-9))
+    out = torch.empty((1, count), dtype=torch.complex128, device=r.dev)
+    steps = max(1, min(r.args.steps, 3))
     plan.set_points_gpu(src, tgt)
-    for _ in range(max(1, args.warmup)):
-        plan.execute_gpu_batch(1, c, out)
-    barrier()
-    total = timed(lambda: plan.execute_gpu_batch(1, c, out), steps)
-    total_all = timed(lambda: plan.encode_gpu_batch(1, src, c, tgt, out), steps)
-    (total, total_all) = max_over_ranks([total, total_all], dev)
     result = {"workload": "3d_type3_f64_src1e6_in[-1,1]^3_tgt1e6_in[-200,200]^3_eps1e-9", "unit": UNIT,
-              "value": replica_throughput(world, count, total, steps), "ms_per_step": total / steps,
-              "with_set_points": {"value": replica_throughput(world, count, total_all, steps),
-                                  "ms_per_step": total_all / steps},
               "note": "points/s counts sources (= targets)"}
-    if rank == 0:
-        from oracle import native
+    result.update(r.measure(lambda: plan.execute_gpu_batch(1, c, out), count, steps, r.args.warmup))
+    result["with_set_points"] = r.measure(lambda: plan.encode_gpu_batch(1, src, c, tgt, out), count, steps, 1)
+    if r.rank == 0:
+        from oracle import gpu_direct
 
-        pick = np.random.default_rng(14).choice(count, 64, replace=False)
-        ref = native.direct_type3(src.cpu().numpy(), c.cpu().numpy(), tgt.cpu().numpy()[pick], 1)
-        got = out.cpu().numpy()[:, pick]
-        result["rel_l2"] = float(np.linalg.norm(got - ref) / np.linalg.norm(ref))
+        pick = np.sort(np.random.default_rng(14).choice(count, 1000, replace=False))
+        ref = gpu_direct.direct_type3(src, c, tgt, 1, select=pick, device=r.dev)
+        got = out[:, torch.as_tensor(pick, device=r.dev)].cpu().numpy()
+        result.update(accuracy(got, ref, 1e-9, "type3", "1000 targets"))
     del plan, out, src, tgt, c
     torch.cuda.empty_cache()
-    result["small_outer_grids_f32"] = type3_small_grid_lines(w, torch, timed, barrier, world, dev, args, rank)
+    lines = {}
+    for d in (1, 2):
+        g = torch.Generator(device=r.dev)
+        g.manual_seed(SEED + 60 + d)
+        src = (torch.rand((count, d), generator=g, device=r.dev) * 2 - 1).contiguous()
+        tgt = (torch.rand((count, d), generator=g, device=r.dev) * 60 - 30).contiguous()
+        c = torch.complex(torch.randn((1, count), generator=g, device=r.dev),
+                          torch.randn((1, count), generator=g, device=r.dev))
+        config = w.NufftType3Config(((-1.0, 1.0),) * d, ((-30.0, 30.0),) * d, eps=1e-6, precision=w.Precision.F32)
+        plan = w.NufftType3Plan(config)
+        out = torch.empty((1, count), dtype=torch.complex64, device=r.dev)
+        plan.set_points_gpu(src, tgt)
+        line = {"workload": f"{d}d_type3_f32_src1e6_in[-1,1]^{d}_tgt1e6_in[-30,30]^{d}_eps1e-6", "unit": UNIT,
+                "outer_grid": list(plan.info().outer_shape[:d])}
+        line.update(r.measure(lambda: plan.execute_gpu_batch(1, c, out), count, steps, r.args.warmup))
+        if r.rank == 0:
+            from oracle import gpu_direct
+
+            pick = np.sort(np.random.default_rng(15 + d).choice(count, 1000, replace=False))
+            ref = gpu_direct.direct_type3(src, c, tgt, 1, select=pick, device=r.dev)
+            got = out[:, torch.as_tensor(pick, device=r.dev)].cpu().numpy()
+            line.update(accuracy(got, ref, 1e-6, "type3", "1000 targets"))
+        lines[f"{d}d"] = line
+        del plan, out, src, tgt, c
+    result["small_outer_grids_f32"] = lines
+    torch.cuda.empty_cache()
     return result
 
 
-def type3_small_grid_lines(w, torch, timed, barrier, world, dev, args, rank):
-    """Type 3 in f32 on small outer grids, the regime the reference serves with
-    its dense small-grid spreader (src/gpu_dense_spread.rs:68-78: one or two
-    axes, at most 2^16 cells): 10^6 sources uniform in [-1, 1]^d to 10^6
-    targets uniform in [-30, 30]^d, eps 1e-6, d = 1 and 2. Here the binned
-    spreader serves it, its parts sized so that every SM has work."""
-    lines = {}
-    count = 1_000_000
-    steps = max(1, min(args.steps, 3))
-    for d in (1, 2):
-        g = torch.Generator(device=dev)
-        g.manual_seed(SEED + 60 + d)
-        src = (torch.rand((count, d), generator=g, device=dev) * 2 - 1).contiguous()
-        tgt = (torch.rand((count, d), generator=g, device=dev) * 60 - 30).contiguous()
-        c = torch.complex(torch.randn((1, count), generator=g, device=dev),
-                          torch.randn((1, count), generator=g, device=dev))
-        config = w.NufftType3Config(((-1.0, 1.0),) * d, ((-30.0, 30.0),) * d, eps=1e-6,
-                                    precision=w.Precision.F32)
-        plan = w.NufftType3Plan(config)
-        out = torch.empty((1, count), dtype=torch.complex64, device=dev)
-        plan.set_points_gpu(src, tgt)
-        for _ in range(max(1, args.warmup)):
-            plan.execute_gpu_batch(1, c, out)
-        barrier()
-        total = timed(lambda: plan.execute_gpu_batch(1, c, out), steps)
-        (total,) = max_over_ranks([total], dev)
-        line = {"workload": f"{d}d_type3_f32_src1e6_in[-1,1]^{d}_tgt1e6_in[-30,30]^{d}_eps1e-6", "unit": UNIT,
-                "value": replica_throughput(world, count, total, steps), "ms_per_step": total / steps,
-                "outer_grid": list(plan.info().outer_shape[:d])}
-        if rank == 0:
-            from oracle import native
-
-            pick = np.random.default_rng(15 + d).choice(count, 64, replace=False)
-            ref = native.direct_type3(src.double().cpu().numpy(), c.cpu().numpy().astype(np.complex128),
-                                      tgt.double().cpu().numpy()[pick], 1)
-            got = out.cpu().numpy()[:, pick]
-            line["rel_l2"] = float(np.linalg.norm(got - ref) / np.linalg.norm(ref))
-        lines[f"{d}d"] = line
-        del plan, out, src, tgt, c
-    torch.cuda.empty_cache()
-    return lines
-
-
-def uneven_problems_line(w, torch, barrier, world, dev, args, rank):
+def uneven_problems_line(r):
     """256 independent type-1 problems of uneven sizes (2D/3D, 64^2..256^2 and
     32^3..64^3 modes, 1e3..1e6 points, uniform or clustered, eps 1e-6), one
     plan each with its points set: all executions issued one after another
     (eager) and replayed from one captured CUDA graph."""
     from wgpunufft_b200 import workloads
 
+    torch, w = r.torch, r.w
     problems = workloads.uneven_problems(256, seed=SEED % 1000)
     stream = torch.cuda.Stream()
     plans, outs = [], []
@@ -507,7 +617,7 @@ def uneven_problems_line(w, torch, barrier, world, dev, args, rank):
         for modes, p, c in problems:
             plan = w.NufftPlan.type1_gpu(w.NufftConfig(modes, 1e-6))
             plan.set_points_gpu(p, stream=stream)
-            out = torch.empty((1, int(np.prod(modes))), dtype=torch.complex64, device=dev)
+            out = torch.empty((1, int(np.prod(modes))), dtype=torch.complex64, device=r.dev)
             plan.execute_gpu_batch(1, c, out, stream=stream)
             plans.append(plan)
             outs.append(out)
@@ -521,38 +631,27 @@ def uneven_problems_line(w, torch, barrier, world, dev, args, rank):
         with torch.cuda.graph(graph, stream=stream):
             run_all()
         stream.synchronize()
-
-        def timed_on(fn, steps):
-            total = 0.0
-            for _ in range(steps):
-                start, end = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
-                start.record(stream)
-                fn()
-                end.record(stream)
-                end.synchronize()
-                total += start.elapsed_time(end)
-            return total
-
-        steps = max(1, min(args.steps, 5))
-        for _ in range(2):
+        steps = max(1, min(r.args.steps, 5))
+        for _ in range(max(2, r.args.warmup)):
             run_all()
             graph.replay()
-        barrier()
-        eager_ms = timed_on(run_all, steps)
-        graph_ms = timed_on(graph.replay, steps)
+        r.barrier()
+        eager_ms = r.timed(run_all, steps, stream)
+        graph_ms = r.timed(graph.replay, steps, stream)
     del graph
-    eager_ms, graph_ms = max_over_ranks([eager_ms, graph_ms], dev)
+    eager_ms, graph_ms = max_over_ranks([eager_ms, graph_ms], r.dev)
     total_points = sum(int(p.shape[0]) for _, p, _ in problems)
-    return {"problems": len(problems), "points": total_points, "eps": 1e-6,
-            "graph": {"value": replica_throughput(world, total_points, graph_ms, steps), "unit": UNIT,
+    return {"problems": len(problems), "points": total_points, "eps": 1e-6, "unit": UNIT,
+            "graph": {"value": replica_throughput(r.world, total_points, graph_ms, steps),
                       "ms_per_step": graph_ms / steps},
-            "eager": {"value": replica_throughput(world, total_points, eager_ms, steps), "unit": UNIT,
+            "eager": {"value": replica_throughput(r.world, total_points, eager_ms, steps),
                       "ms_per_step": eager_ms / steps},
             "note": "one plan per problem (prepared points); a step executes all 256"}
 
 
 def profile_traffic():
-    """DRAM bytes per spread launch from the committed ncu summary, if present."""
+    """DRAM bytes per spread launch from the committed ncu capture of the same
+    launch (profiles/spread_tiles_2d_1024_M1e7.md), if present."""
     path = ROOT / "profiles" / "spread_tiles_2d_1024_M1e7.md"
     if not path.exists():
         return None
@@ -563,6 +662,49 @@ def profile_traffic():
             except ValueError:
                 return None
     return None
+
+
+def compact(value, digits=4):
+    if isinstance(value, float):
+        return float(f"{value:.{digits}g}")
+    if isinstance(value, dict):
+        return {k: compact(v, digits) for k, v in value.items()}
+    if isinstance(value, list):
+        return [compact(v, digits) for v in value]
+    return value
+
+
+def summary_of(line):
+    """The figures a reader needs first, kept short (the end of the line)."""
+    s = {}
+    if line.get("type2"):
+        s["type2"] = {k: line["type2"].get(k) for k in ("value", "rel_l2", "meets_eps")}
+    if line.get("one_shot"):
+        s["one_shot"] = line["one_shot"].get("value")
+    c = line.get("clustered")
+    if c:
+        s["clustered"] = {k: {q: c[k].get(q) for q in ("value", "rel_l2", "meets_eps")} for k in ("type1", "type2")}
+    sm = line.get("small_2d")
+    if sm:
+        s["small_2d"] = {k: {q: sm[k].get(q) for q in ("value", "rel_l2", "meets_eps")} for k in ("type1", "type2")}
+    b = line.get("batched")
+    if b:
+        s["batched"] = {}
+        for key, entry in b.items():
+            if not isinstance(entry, dict):
+                continue
+            s["batched"][key] = {k: [entry[k].get("value"), entry[k].get("rel_l2")] for k in entry
+                                 if isinstance(entry[k], dict)}
+    rad = line.get("radial_3d")
+    if rad:
+        s["radial_3d"] = {k: {q: rad[k].get(q) for q in ("value", "rel_l2", "meets_eps")} for k in ("type1", "type2")}
+    u = line.get("uneven_problems")
+    if u:
+        s["uneven_graph_ms"] = u["graph"]["ms_per_step"]
+    t3 = line.get("type3")
+    if t3:
+        s["type3_f64"] = {q: t3.get(q) for q in ("value", "rel_l2")}
+    return compact(s, 3)
 
 
 def main():
@@ -583,31 +725,14 @@ def main():
         dist.init_process_group("nccl", timeout=timedelta(seconds=300))
     import wgpunufft_b200 as w
 
-    dev = f"cuda:{local}"
+    r = Runner(torch, w, args, world, rank, local)
+    dev = r.dev
     points_h, strengths_h = make_inputs()
     points = torch.from_numpy(points_h).to(dev)
     strengths = torch.from_numpy(strengths_h.view(np.float32)).to(dev).view(torch.complex64)
     config = w.NufftConfig(MODES, EPS)
     plan = w.NufftPlan.type1_gpu(config, device=local)
     out = torch.empty(config.mode_count(), dtype=torch.complex64, device=dev)
-    flush = torch.empty(256 * 1024 * 1024 // 4, dtype=torch.float32, device=dev)
-    stream = torch.cuda.current_stream()
-
-    def barrier():
-        if world > 1:
-            dist.barrier()
-        torch.cuda.synchronize()
-
-    def timed(step_fn, steps):
-        starts = [torch.cuda.Event(enable_timing=True) for _ in range(steps)]
-        ends = [torch.cuda.Event(enable_timing=True) for _ in range(steps)]
-        for i in range(steps):
-            flush.fill_(float(i))
-            starts[i].record(stream)
-            step_fn()
-            ends[i].record(stream)
-        torch.cuda.synchronize()
-        return sum(s.elapsed_time(e) for s, e in zip(starts, ends))
 
     # Warm-up: plan scratch, cuFFT plan, the sort.
     plan.set_points_gpu(points)
@@ -622,19 +747,23 @@ def main():
     plan.stage_timing(True)
     plan.stage_report()
     launches0 = w.launch_count()
-    barrier()
+    r.barrier()
     with ClockSampler(local) as clocks:
-        total_ms = timed(lambda: plan.execute_type1_gpu(strengths, out), args.steps)
+        total_ms = r.timed(lambda: plan.execute_type1_gpu(strengths, out), args.steps)
         launches = w.launch_count() - launches0
         stages = plan.stage_report()
         plan.stage_timing(False)
-        one_shot_ms = timed(lambda: plan.encode_type1_gpu(points, strengths, out), args.steps)
-    barrier()
+        one_shot_ms = r.timed(lambda: plan.encode_type1_gpu(points, strengths, out), args.steps)
+    r.barrier()
     clock_summary = clocks.summary()
     total_ms, one_shot_ms = max_over_ranks([total_ms, one_shot_ms], dev)
     ms = total_ms / args.steps
     value = replica_throughput(world, POINTS, total_ms, args.steps)
     one_shot = replica_throughput(world, POINTS, one_shot_ms, args.steps)
+    plan.set_points_gpu(points)
+    plan.execute_type1_gpu(strengths, out)
+    plan.synchronize()
+    headline_accuracy = r.check_type1(points, strengths, out, MODES, EPS, "2d")
 
     # Type 2 on the same points (reported beside the headline, same timing rules).
     plan2 = w.NufftPlan.type2_gpu(config, device=local)
@@ -647,56 +776,28 @@ def main():
     plan2.synchronize()
     plan2.stage_timing(True)
     plan2.stage_report()
-    type2_ms = timed(lambda: plan2.execute_type2_gpu(coefficients, values), args.steps)
+    type2_ms = r.timed(lambda: plan2.execute_type2_gpu(coefficients, values), args.steps)
     stages2 = plan2.stage_report()
     plan2.stage_timing(False)
-    type2_one_shot_ms = timed(lambda: plan2.encode_type2_gpu(points, coefficients, values), args.steps)
+    type2_one_shot_ms = r.timed(lambda: plan2.encode_type2_gpu(points, coefficients, values), args.steps)
     type2_ms, type2_one_shot_ms = max_over_ranks([type2_ms, type2_one_shot_ms], dev)
+    plan2.set_points_gpu(points)
+    plan2.execute_type2_gpu(coefficients, values)
+    plan2.synchronize()
     type2 = {"value": replica_throughput(world, POINTS, type2_ms, args.steps), "unit": UNIT,
              "ms_per_step": type2_ms / args.steps,
              "one_shot_value": replica_throughput(world, POINTS, type2_one_shot_ms, args.steps),
-             "stages_ms_per_step": {k: v[0] / args.steps for k, v in stages2.items()}}
+             "stages_ms_per_step": stage_ms(stages2, args.steps)}
+    type2.update(r.check_type2(points, coefficients, values, MODES, EPS, "2d") or {})
+    del plan2, coefficients, values
 
-    # Accuracy of this output against FP64 direct sums on 16 seeded modes.
-    rel = None
-    if rank == 0:
-        from oracle import native
-
-        plan.execute_type1_gpu(strengths, out)
-        plan.synchronize()
-        got = out.cpu().numpy()
-        select = np.random.default_rng(1).choice(config.mode_count(), 16, replace=False)
-        ref = native.direct_type1(points_h.astype(np.float64), strengths_h, MODES, select=select)[0]
-        rel = float(np.linalg.norm(got[select] - ref) / np.linalg.norm(ref))
-
-    # End to end through the reference-facing C interface with host buffers:
-    # wgpu_nufftf_setpts (per-axis f32 coordinates) + wgpu_nufftf_execute
-    # every step, as a Fortran/MATLAB/Julia caller of the reference would.
-    e2e = None
-    if not args.no_e2e:
-        e2e = c_interface_e2e(w, torch, points_h, strengths_h, timed, barrier, world, dev, args)
-
-    # Batched vectors on one point set (2D 512^2 modes, 2e6 points, eps 1e-6):
-    # the tensor-core spreader against the CUDA-core spreader on the same plan
-    # shape and inputs.
-    batched = None
-    if not args.no_batched:
-        batched = batched_comparison(w, torch, timed, barrier, world, dev, args, rank)
-    uneven = None
-    if not args.no_uneven:
-        uneven = uneven_problems_line(w, torch, barrier, world, dev, args, rank)
-    # The 3D radial configuration (256^3 modes, 5e7 points, eps 1e-5).
-    radial = None
-    if not args.no_radial:
-        radial = radial_3d_line(w, torch, timed, barrier, world, dev, args, rank)
-    # f64 plans (2D 512^2 modes, 2e6 points, eps 1e-9 and 1e-12).
-    f64 = None
-    if not args.no_f64:
-        f64 = f64_line(w, torch, timed, barrier, world, dev, args, rank)
-    # The 3D type-3 f64 configuration (10^6 sources to 10^6 targets).
-    type3 = None
-    if not args.no_type3:
-        type3 = type3_line(w, torch, timed, barrier, world, dev, args, rank)
+    e2e = None if args.no_e2e else c_interface_e2e(r, points_h, strengths_h)
+    clustered = None if args.no_clustered else clustered_line(r)
+    small = None if args.no_small else small_line(r)
+    batched = None if args.no_batched else batched_sweep(r)
+    uneven = None if args.no_uneven else uneven_problems_line(r)
+    radial = None if args.no_radial else radial_3d_line(r)
+    type3 = None if args.no_type3 else type3_line(r)
 
     if rank == 0:
         peaks = json.loads((ROOT / "MEASURED_PEAKS.json").read_text()) if (ROOT / "MEASURED_PEAKS.json").exists() else {}
@@ -704,19 +805,25 @@ def main():
         spread_ms, spread_launches = stages.get("spread", (0.0, 0))
         per_launch_ms = spread_ms / max(spread_launches, 1)
         fine = plan.fine_grid_shape()
+        # Type-1 spread bytes (coordinates as the 16-byte prepared windows, the
+        # permutation word, the strength, and the padded tiles written).
         algorithmic = POINTS * (4 * 2 + 8 + 4) + fine[0] * fine[1] * 8
         achieved = algorithmic / (per_launch_ms / 1e3) / 1e9 if per_launch_ms > 0 else None
         roofline = {"bound": "hbm", "kernel": "spread_tiles_kernel<2,6>", "achieved": achieved, "peak": hbm,
                     "unit": "GB/s", "frac": achieved / hbm if achieved else None,
                     "traffic": profile_traffic(),
+                    "traffic_source": "dram__bytes_read.sum + dram__bytes_write.sum of one ncu capture of this "
+                                      "launch at this workload (profiles/spread_tiles_2d_1024_M1e7.md), not this run",
                     "peak_source": "MEASURED_PEAKS.json hbm_gbs (measured)" if peaks else "fallback 6650 GB/s",
-                    "algorithmic_bytes_per_launch": algorithmic}
+                    "algorithmic_bytes_per_launch": algorithmic, "launch_ms": per_launch_ms}
         cpu = None
         if not args.no_cpu:
-            sample_pts, sample_str = points_h[:CPU_SAMPLE], strengths_h[:CPU_SAMPLE]
-            cpu_value, threads, cpu_s = cpu_plan_throughput(sample_pts, sample_str)
-            cpu = {"value": cpu_value, "unit": UNIT, "cores": threads, "kind": "port",
-                   "sample": f"first {CPU_SAMPLE:,} of the {POINTS:,} points, same plan; restated CpuNufftPlan one-shot execute, median of 3 ({cpu_s:.2f} s each)"}
+            t = cpu_plan_timings(points_h, strengths_h, MODES, EPS, 3, 1)
+            cpu = {"value": POINTS / t["prepared_s"], "unit": UNIT, "cores": t["threads"], "kind": "port",
+                   "sample": f"all {POINTS:,} points, same plan; restated CpuNufftPlan, execution on prepared "
+                             f"points (median of 3: {1e3 * t['prepared_s']:.0f} ms; one-shot with the sort "
+                             f"{1e3 * t['one_shot_s']:.0f} ms) on {t['threads']} threads of {cpu_model()}",
+                   "one_shot_value": POINTS / t["one_shot_s"]}
         line = {
             "metric": METRIC, "value": value, "unit": UNIT, "n_gpus": world, "steps": args.steps,
             "warmup": args.warmup, "ms_per_step": ms, "higher_is_better": True, "scaling": "weak",
@@ -725,23 +832,26 @@ def main():
                        "fine_grid": list(fine), "kernel_width": plan.kernel_width(),
                        "l2": "flushed between steps by a 256 MiB write outside the timed events",
                        "parallelism": f"replicas x{world}"},
+            "batched": compact(batched) if batched else None,
+            "clustered": compact(clustered) if clustered else None,
+            "small_2d": compact(small) if small else None,
+            "radial_3d": compact(radial) if radial else None,
+            "uneven_problems": compact(uneven) if uneven else None,
+            "type3": compact(type3) if type3 else None,
+            "stages_ms_per_step": stage_ms(stages, args.steps),
+            "type2": compact(type2),
             "one_shot": {"value": one_shot, "unit": UNIT, "ms_per_step": one_shot_ms / args.steps,
                          "note": "set_points (stable bin sort) + execute per step"},
-            "rel_l2": rel,
-            "stages_ms_per_step": {k: v[0] / args.steps for k, v in stages.items()},
-            "type2": type2,
-            "batched": batched,
-            "uneven_problems": uneven,
-            "radial_3d": radial,
-            "f64": f64,
-            "type3": type3,
+            "accuracy": headline_accuracy,
+            "rel_l2": headline_accuracy["rel_l2"] if headline_accuracy else None,
             "roofline": roofline,
             "cpu_baseline": cpu,
             "e2e": e2e,
             "gpu_launches": launches,
             "clocks": clock_summary,
         }
-        print(json.dumps(line), flush=True)
+        line["summary"] = summary_of(line)
+        print(json.dumps(line, separators=(",", ":")), flush=True)
     if world > 1:
         dist.barrier()
         dist.destroy_process_group()

@@ -257,16 +257,24 @@ int b200nufft_copy_prepared_slots(b200nufft_plan plan, int32_t *starts, float *o
  * b200nufft_copy_bin_order on an F32 type-1 plan whose chosen bin geometry
  * has the sides `bin_sides` (b200nufft_plan_info.geometry_sides[chosen_geometry]);
  * `points` are point-major float coordinates. All scratch lives in a fixed
- * array of about 4.3 MB in the library's device image, which every GPU that
- * loads the library holds until the process exits; point counts above
+ * array of about 4.3 MB in the library's device image; point counts above
  * B200NUFFT_NOALLOC_MAX_POINTS are rejected with B200NUFFT_LENGTH_OVERFLOW.
  * The call allocates nothing: no cudaMalloc, no cudaFree, no library that
- * allocates. Its first call on a device looks up the array's device address
- * (cudaGetSymbolAddress, with that device current); make that first call
- * before any stream capture. Every call shares the one array and starts by
- * clearing what must start at zero, so calls that overlap on the GPU (on
- * different streams, or from different threads) race and must be ordered by
- * the caller. */
+ * allocates. The CUDA driver places the array on a GPU when it loads the
+ * library's module there: under lazy module loading (CUDA 12's default) at
+ * this entry point's first call on that GPU, which looks up the array's
+ * device address (cudaGetSymbolAddress, with that device current); with
+ * CUDA_MODULE_LOADING=EAGER at the library's first use of the GPU. So make
+ * that first call (a call with point_count 0 does this set-up and
+ * only writes zero bin offsets) before
+ * another framework takes the GPU's memory, and before any stream capture.
+ * From then on the GPU holds the array until the process exits. Every call
+ * shares the one array and starts by clearing what must start at zero, so
+ * calls that overlap on the GPU (on different streams, or from different
+ * threads) race and must be ordered by the caller. A sort whose look-back
+ * wait gave up (bounded at about a second) writes 0xFFFFFFFF to
+ * bin_offsets[bins], which otherwise equals point_count: check it after
+ * synchronizing the stream. */
 #define B200NUFFT_NOALLOC_MAX_POINTS 262144
 int b200nufft_bin_order_noalloc(int32_t dimensions, const int64_t *fine_shape,
                                 int32_t kernel_width, const int32_t *bin_sides,

@@ -13,14 +13,18 @@ file and lines it restates:
   offsets and prepared slots (src/gpu_nd_wgsl.rs:198-298,
   src/gpu_nd_bins.rs:474-709), and the type-2 grouped bins
   (src/gpu_point_bins.rs:422-465), all in numpy float32 arithmetic.
-- oracle.c (built as liboracle.so, wrapped by native.py): FP64 direct type-1,
+- oracle.cpp (built as liboracle.so, wrapped by native.py): FP64 direct type-1,
   type-2 and type-3 sums (src/direct.rs:9-118, src/type3.rs:609-673) and a
   restatement of the CPU plan CpuNufftPlan (src/cpu.rs, src/cpu/*.rs) with its
   own FFT, timed as the CPU baseline.
+- gpu_direct.cu (built as libgpu_direct.so, wrapped by gpu_direct.py): the
+  same FP64 direct sums evaluated on the GPU, term by term, so that the
+  full-size workloads can be checked on thousands of outputs; validated
+  against oracle.cpp's sums.
 
 Parity pins: the ES known answers, fine-grid sizes, layout values and the
 reference's own Python direct sums (python/tests/direct_sums.py) are committed
 as fixtures under tests/golden/. The df64 words of the absent wgpu-fft library
 are not available, so the fold restates published double-float algorithms;
-the sort permutation is pinned against this restatement (see DESIGN.md).
+the sort permutation is pinned against this restatement.
 """

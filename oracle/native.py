@@ -117,8 +117,10 @@ class CpuPlan:
         self.order = order
         self.precision = precision
 
-    def execute(self, points, values, batch: int = 1, threads: int = 0):
-        """Type 1: values (batch, M) -> modes (batch, N); type 2: (batch, N) -> (batch, M)."""
+    def execute(self, points, values, batch: int = 1, threads: int = 0, stage_seconds=None):
+        """Type 1: values (batch, M) -> modes (batch, N); type 2: (batch, N) -> (batch, M).
+        An f32 plan given a list `stage_seconds` appends (prepare, execute on
+        prepared points) wall times of this execution to it."""
         d = len(self.n_modes)
         real = np.float32 if self.precision == "f32" else np.float64
         ctype = np.complex64 if self.precision == "f32" else np.complex128
@@ -130,9 +132,15 @@ class CpuPlan:
         horner = np.ascontiguousarray(self.table, dtype=np.float64)
         phis = [np.ascontiguousarray(p, dtype=np.float64) for p in self.phi]
         phi_ptrs = (ctypes.c_void_p * 3)(*[_p(p) for p in phis] + [None] * (3 - d))
+        args = [ctypes.c_int(self.kind), ctypes.c_int(d), _p(_i64(self.n_modes)), _p(_i64(self.fine)),
+                ctypes.c_int(self.order), ctypes.c_int(self.isign), ctypes.c_int(self.width),
+                ctypes.c_int(self.rows), _p(horner), phi_ptrs, ctypes.c_int(batch), ctypes.c_int64(m),
+                _p(pts), _p(vin), _p(out), ctypes.c_int(threads)]
+        if stage_seconds is not None and self.precision == "f32":
+            seconds = np.zeros(2, dtype=np.float64)
+            library().oracle_cpu_nufft_f32_timed(*args, _p(seconds))
+            stage_seconds.append((float(seconds[0]), float(seconds[1])))
+            return out
         fn = library().oracle_cpu_nufft_f32 if self.precision == "f32" else library().oracle_cpu_nufft_f64
-        fn(ctypes.c_int(self.kind), ctypes.c_int(d), _p(_i64(self.n_modes)), _p(_i64(self.fine)),
-           ctypes.c_int(self.order), ctypes.c_int(self.isign), ctypes.c_int(self.width),
-           ctypes.c_int(self.rows), _p(horner), phi_ptrs, ctypes.c_int(batch), ctypes.c_int64(m),
-           _p(pts), _p(vin), _p(out), ctypes.c_int(threads))
+        fn(*args)
         return out

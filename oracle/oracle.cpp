@@ -510,9 +510,14 @@ void axis_modes(const CpuPlanParams& p, int a, std::vector<int64_t>& fine_index,
   }
 }
 
+// One execution including the point sort; when `seconds` is given it
+// receives the wall time of the point preparation (the reference's
+// CpuNufftPlan::prepare, src/cpu.rs:448-536) and of the rest of the
+// execution (its execution on prepared points).
 template <typename T, typename P>
 int run_cpu_plan(const CpuPlanParams& p, int batch, int64_t M, const P* points, const T* input_raw,
-                 T* output_raw) {
+                 T* output_raw, double* seconds = nullptr) {
+  const double t0 = omp_get_wtime();
   const int d = p.dim;
   int64_t cells = 1, N = 1;
   for (int a = 0; a < d; ++a) {
@@ -521,6 +526,7 @@ int run_cpu_plan(const CpuPlanParams& p, int batch, int64_t M, const P* points, 
   }
   Prepared<T> pr;
   prepare_points<T, P>(p, M, points, pr);
+  const double t1 = omp_get_wtime();
   std::vector<cplx<T>> fine(static_cast<size_t>(cells * batch));
   std::vector<int64_t> idx[3];
   std::vector<T> amp[3];
@@ -566,6 +572,10 @@ int run_cpu_plan(const CpuPlanParams& p, int batch, int64_t M, const P* points, 
     fft_nd<T>(fine.data(), d, p.fine, batch, sign);
     interpolate_all<T>(p, pr, batch, M, fine.data(), cells, reinterpret_cast<cplx<T>*>(output_raw));
   }
+  if (seconds != nullptr) {
+    seconds[0] = t1 - t0;
+    seconds[1] = omp_get_wtime() - t1;
+  }
   return 0;
 }
 
@@ -609,6 +619,17 @@ int oracle_cpu_nufft_f64(int type, int dim, const int64_t* modes, const int64_t*
   if (threads > 0) omp_set_num_threads(threads);
   const CpuPlanParams p = make_params(type, dim, modes, fine, order, isign, width, rows, horner, phi);
   return run_cpu_plan<double, double>(p, batch, M, points, input, output);
+}
+
+// The same f32 execution with its stage times: seconds[0] the point
+// preparation, seconds[1] the execution on the prepared points.
+int oracle_cpu_nufft_f32_timed(int type, int dim, const int64_t* modes, const int64_t* fine, int order,
+                               int isign, int width, int rows, const double* horner,
+                               const double* const* phi, int batch, int64_t M, const float* points,
+                               const float* input, float* output, int threads, double* seconds) {
+  if (threads > 0) omp_set_num_threads(threads);
+  const CpuPlanParams p = make_params(type, dim, modes, fine, order, isign, width, rows, horner, phi);
+  return run_cpu_plan<float, float>(p, batch, M, points, input, output, seconds);
 }
 
 // Unnormalised multi-dimensional complex FFT of `batch` f64 grids in place.

@@ -2,7 +2,8 @@
 
 The reference ships FP64 direct type-1/2/3 sums in numpy
 (python/tests/direct_sums.py); this script imports that file from a checkout
-of the reference (default /root/reference, or the first argument), evaluates
+of the reference (the first argument, or the WGPU_NUFFT_REFERENCE environment
+variable), evaluates
 seeded small cases that follow the reference's tests (python/tests/test_cpu.py:
 60 points, modes (11,), (6, 5), (4, 3, 5), both signs, both mode orders;
 type 3 in 2D with bounds [[-1, 2], [0.5, 1.5]] -> [[-20, 10], [-8, 8]]), and
@@ -14,6 +15,7 @@ reference without the reference present.
 from __future__ import annotations
 
 import importlib.util
+import os
 import sys
 from pathlib import Path
 
@@ -79,4 +81,7 @@ def main(root: Path) -> None:
 
 
 if __name__ == "__main__":
-    main(Path(sys.argv[1]) if len(sys.argv) > 1 else Path("/root/reference"))
+    location = sys.argv[1] if len(sys.argv) > 1 else os.environ.get("WGPU_NUFFT_REFERENCE")
+    if not location:
+        sys.exit("usage: make_golden.py <reference checkout> (or set WGPU_NUFFT_REFERENCE)")
+    main(Path(location))

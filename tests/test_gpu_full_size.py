@@ -7,7 +7,7 @@ from __future__ import annotations
 import numpy as np
 import pytest
 
-from oracle import native
+from oracle import gpu_direct
 from tests.conftest import rel_l2
 
 pytestmark = pytest.mark.gpu
@@ -44,16 +44,15 @@ def test_2d_clustered_ten_million_points_repeatable_over_ten_runs():
     plan.set_points_gpu(p.clone())
     plan.execute_gpu_batch(1, c, out)
     assert torch.equal(out.view(torch.int32), first.view(torch.int32))
-    select = np.random.default_rng(5).choice(modes[0] * modes[1], 300, replace=False)
-    ref = native.direct_type1(p.cpu().numpy().astype(np.float64), c.cpu().numpy().astype(np.complex128),
-                              modes, select=select)
+    select = np.sort(np.random.default_rng(5).choice(modes[0] * modes[1], 1024, replace=False))
+    ref = gpu_direct.direct_type1(p, c, modes, select=select)
     assert rel_l2(first.cpu().numpy()[:, select], ref) < 20 * eps
 
 
 def test_3d_radial_fifty_million_points():
-    """3D 256^3 modes, 4096 x 12207 radial samples, eps 1e-5: type-1 on 200
-    modes and type-2 on 300 points against direct sums (3D bound 32 eps), and
-    type-1 linearity at full size."""
+    """3D 256^3 modes, 4096 x 12207 radial samples, eps 1e-5: type-1 on 1,024
+    modes and type-2 on 10,000 points against direct sums over all inputs (3D
+    bound 32 eps), and type-1 linearity at full size."""
     modes, count, eps, dist = workloads.CASES["radial"]
     p = workloads.points(dist, count, 3, seed=31)
     c = workloads.values(1, count, seed=32)
@@ -64,9 +63,8 @@ def test_3d_radial_fifty_million_points():
     plan1.execute_gpu_batch(1, c, out)
     got = out.cpu().numpy()
     rng = np.random.default_rng(6)
-    select = rng.choice(n, 200, replace=False)
-    pts = p.cpu().numpy().astype(np.float64)
-    ref = native.direct_type1(pts, c.cpu().numpy().astype(np.complex128), modes, select=select)
+    select = np.sort(rng.choice(n, 1024, replace=False))
+    ref = gpu_direct.direct_type1(p, c, modes, select=select)
     assert rel_l2(got[:, select], ref) < 32 * eps
     # Linearity: T(2 c + c') = 2 T(c) + T(c').
     c2 = workloads.values(1, count, seed=33)
@@ -81,8 +79,8 @@ def test_3d_radial_fifty_million_points():
     f = workloads.values(1, n, seed=34)
     values = torch.empty((1, count), dtype=torch.complex64, device=DEV)
     plan2.execute_gpu_batch(1, f, values)
-    pick = rng.choice(count, 300, replace=False)
-    ref2 = native.direct_type2(pts[pick], f.cpu().numpy().astype(np.complex128), modes)
+    pick = np.sort(rng.choice(count, 10_000, replace=False))
+    ref2 = gpu_direct.direct_type2(p, f, modes, select=pick)
     assert rel_l2(values.cpu().numpy()[:, pick], ref2) < 32 * eps
 
 
@@ -104,9 +102,8 @@ def test_batched_256_vectors_tensor_cores_match_cuda_cores():
         del plan, out
     tensor, cuda = outs
     assert rel_l2(tensor, cuda) < 5e-6
-    select = np.random.default_rng(7).choice(n, 64, replace=False)
-    ref = native.direct_type1(p.cpu().numpy().astype(np.float64), c[::64].cpu().numpy().astype(np.complex128),
-                              modes, select=select)
+    select = np.sort(np.random.default_rng(7).choice(n, 1024, replace=False))
+    ref = gpu_direct.direct_type1(p, c[::64], modes, select=select)
     assert rel_l2(tensor[::64][:, select], ref) < 1e-5
 
 
@@ -127,6 +124,6 @@ def test_type3_3d_f64_million_sources_to_million_targets():
     out = torch.empty((1, 1_000_000), dtype=torch.complex128, device=DEV)
     plan.encode_gpu_batch(1, src, c, tgt, out)
     torch.cuda.synchronize()
-    pick = np.random.default_rng(8).choice(1_000_000, 1000, replace=False)
-    ref = native.direct_type3(src.cpu().numpy(), c.cpu().numpy(), tgt.cpu().numpy()[pick], 1)
+    pick = np.sort(np.random.default_rng(8).choice(1_000_000, 1000, replace=False))
+    ref = gpu_direct.direct_type3(src, c, tgt, 1, select=pick)
     assert rel_l2(out.cpu().numpy()[:, pick], ref) < 100 * 1e-9

@@ -304,21 +304,24 @@ def test_crowded_3d_tiles_match_direct_and_repeat(eps):
 
 
 def test_2d_1024_ten_million_points_against_direct_subsets():
-    """The 2D 1024^2, 10^7-point workload: a seeded subset of modes (type 1)
-    and of points (type 2) against FP64 direct sums over all inputs."""
+    """The 2D 1024^2, 10^7-point workload, uniform and clustered: 1,024 seeded
+    modes (type 1) and 10,000 seeded points (type 2) against FP64 direct sums
+    over all inputs (the oracle's GPU checker)."""
+    from oracle import gpu_direct
+
     rng = np.random.default_rng(2024)
     n_modes = (1024, 1024)
     m = 10_000_000
     for points in (uniform_points(rng, m, 2), clustered_points(rng, m, 2)):
         strengths = complex_normal(rng, m)
         got, plan = run_type1(n_modes, 1e-5, points, strengths)
-        select = rng.choice(1024 * 1024, 48, replace=False)
-        ref = native.direct_type1(points.astype(np.float64), strengths, n_modes, select=select)
+        select = np.sort(rng.choice(1024 * 1024, 1024, replace=False))
+        ref = gpu_direct.direct_type1(points, strengths[None], n_modes, select=select)
         assert rel_l2(got[0, select], ref[0]) < tolerance(2, 1e-5)
         coefficients = complex_normal(rng, 1024 * 1024)
         got2, _ = run_type2(n_modes, 1e-5, points, coefficients)
-        pick = rng.choice(m, 48, replace=False)
-        ref2 = native.direct_type2(points.astype(np.float64), coefficients, n_modes, select=pick)
+        pick = np.sort(rng.choice(m, 10_000, replace=False))
+        ref2 = gpu_direct.direct_type2(points, coefficients[None], n_modes, select=pick)
         assert rel_l2(got2[0, pick], ref2[0]) < tolerance(2, 1e-5)
 
 

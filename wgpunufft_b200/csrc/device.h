@@ -120,6 +120,11 @@ void gather_sorted_points64(const double* points, const uint32_t* perm, int64_t 
 void df64_to_f64(const float* pairs, int64_t count, double* out, cudaStream_t stream);
 void f64_to_df64(const double* values, int64_t count, float* pairs, cudaStream_t stream);
 
+// Points per tile of the sort's radix passes; each tile publishes 256
+// look-back words (one per digit) per pass.
+constexpr int kSortTilePoints = 4096;
+constexpr int kSortDigits = 256;
+
 // Bytes of look-back status words a sort of `count` points needs.
 size_t sort_status_bytes(int64_t count);
 

@@ -8,8 +8,19 @@
 // b200nufft_copy_bin_order, but all of its scratch memory (keys, permutation
 // buffers, digit histograms and look-back words of the radix sort) lives in
 // one fixed array in this library's device image. The array is sized for at
-// most B200NUFFT_NOALLOC_MAX_POINTS points and every GPU that loads the
-// library holds it until the process exits.
+// most B200NUFFT_NOALLOC_MAX_POINTS points. The CUDA driver places it on a
+// GPU when it loads this file's module there: at the library's first kernel
+// launch on that GPU with CUDA_MODULE_LOADING=EAGER, otherwise (lazy
+// loading, CUDA 12's default) at this entry point's first call on that GPU,
+// which looks up the array's address. So that first call (a call with no
+// points does that set-up and writes zero bin offsets) must come before another framework takes
+// the GPU's memory. From then on the GPU holds the array until the process
+// exits.
+//
+// A look-back wait of the radix sort that gives up (bounded at about a
+// second) cannot be reported by the return code, which is known before the
+// GPU runs: the call then writes 0xFFFFFFFF to bin_offsets[bins], the
+// trailing total that otherwise equals point_count.
 #include <cuda_runtime.h>
 
 #include <cmath>
@@ -28,7 +39,8 @@ constexpr int64_t kMaxPoints = B200NUFFT_NOALLOC_MAX_POINTS;
 constexpr size_t kWordBytes = sizeof(uint32_t);
 constexpr size_t kBufferBytes = static_cast<size_t>(kMaxPoints) * kWordBytes;
 constexpr size_t kHistBytes = 4 * 256 * kWordBytes;
-constexpr size_t kStatusBytes = ((kMaxPoints + 4095) / 4096) * 256 * kWordBytes;
+constexpr size_t kStatusBytes =
+    ((kMaxPoints + kSortTilePoints - 1) / kSortTilePoints) * kSortDigits * kWordBytes;
 constexpr size_t kCounterBytes = 8 * kWordBytes;
 constexpr size_t kScratchBytes = 4 * kBufferBytes + kHistBytes + kStatusBytes + kCounterBytes;
 constexpr int kMaxDevices = 64;
@@ -38,6 +50,12 @@ constexpr double kTwoPi = 6.28318530717958647692;
 // stand-in for the symbol, not a device address: its address comes from
 // cudaGetSymbolAddress below.
 static __device__ __align__(256) unsigned char g_noalloc_scratch[kScratchBytes];
+
+// Marks a sort whose look-back gave up: the trailing total of the bin
+// offsets, which otherwise equals the point count, becomes 0xFFFFFFFF.
+__global__ void mark_gave_up_kernel(const uint32_t* __restrict__ error_flag, uint32_t* __restrict__ total) {
+  if (*error_flag != 0u) *total = 0xFFFFFFFFu;
+}
 
 std::mutex g_setup_mutex;
 void* g_scratch_address[kMaxDevices] = {};
@@ -124,6 +142,9 @@ void bin_order_noalloc(int32_t dimensions, const int64_t* fine_shape, int32_t ke
   }
   g.fine_count = 1;
   for (int a = 0; a < dimensions; ++a) g.fine_count *= g.fine[a];
+  if (sort_status_bytes(point_count) > kStatusBytes) {
+    throw NufftFailure{B200NUFFT_INTERNAL, "look-back words exceed the fixed scratch array"};
+  }
 
   unsigned char* base = scratch_on_current_device();
   SortBuffers buffers;
@@ -146,6 +167,8 @@ void bin_order_noalloc(int32_t dimensions, const int64_t* fine_shape, int32_t ke
     check_cuda(cudaMemcpyAsync(permutation, perm, static_cast<size_t>(point_count) * kWordBytes,
                                cudaMemcpyDeviceToDevice, stream),
                "copy permutation");
+    mark_gave_up_kernel<<<1, 1, 0, stream>>>(buffers.counters + 7, bin_offsets + bins);
+    note_launch();
   }
   check_cuda(cudaGetLastError(), "bin order launch");
 }

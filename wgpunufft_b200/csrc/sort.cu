@@ -26,6 +26,8 @@ constexpr int kSortWarps = kSortThreads / 32;
 constexpr int kItemsPerThread = 16;
 constexpr int kSortTile = kSortThreads * kItemsPerThread;
 constexpr int kRadix = 256;
+static_assert(kSortTile == kSortTilePoints && kRadix == kSortDigits,
+              "sort_status_bytes and fixed scratch sizes assume 4096-point tiles of 256 digits");
 constexpr uint32_t kFlagAggregate = 1u << 30;
 constexpr uint32_t kFlagInclusive = 2u << 30;
 constexpr uint32_t kValueMask = (1u << 30) - 1;
