@@ -410,7 +410,7 @@ BATCH_POINTS = 2_000_000
 
 def batched_sweep(r):
     """One point set (2D 512^2 modes, 2e6 uniform points), B vectors: f32 type 1
-    on CUDA cores and on tensor cores (3xTF32) and type 2, eps 1e-3 and 1e-6,
+    and type 2 on CUDA cores and on tensor cores (3xTF32), eps 1e-3 and 1e-6,
     B in {1, 16, 64, 256}; f64 and Df64 at eps 1e-9 and 1e-12 for B in {1, 16}.
     NU points/s counts points x vectors."""
     from wgpunufft_b200 import workloads
@@ -442,13 +442,23 @@ def batched_sweep(r):
             del c, modes
             f = workloads.values(batch, n, seed=1000 + batch, device=r.dev)
             vals = torch.empty((batch, BATCH_POINTS), dtype=torch.complex64, device=r.dev)
-            plan2 = w.NufftPlan.type2_gpu(w.NufftConfig(BATCH_MODES, eps, batch=batch))
-            plan2.set_points_gpu(pts)
-            item2 = r.measure(lambda: plan2.execute_gpu_batch(batch, f, vals), BATCH_POINTS * batch, steps,
-                              r.args.warmup)
-            item2.update(r.check_type2(pts, f, vals, BATCH_MODES, eps, "batch", seed=batch) or {})
-            entry["type2_cuda_cores"] = item2
-            del plan2, f, vals
+            for name, method in (("tensor_cores", w.SpreadMethod.TENSOR_CORES),
+                                 ("cuda_cores", w.SpreadMethod.CUDA_CORES)):
+                plan2 = w.NufftPlan.type2_gpu(w.NufftConfig(BATCH_MODES, eps, batch=batch, spread_method=method))
+                plan2.set_points_gpu(pts)
+                plan2.stage_timing(True)
+                item2 = r.measure(lambda: plan2.execute_gpu_batch(batch, f, vals), BATCH_POINTS * batch, steps,
+                                  r.args.warmup)
+                stages = plan2.stage_report()
+                plan2.stage_timing(False)
+                item2["interpolation_ms"] = round(
+                    stages.get("interpolation", (0.0, 1))[0] / (steps + max(r.args.warmup, 1)), 4)
+                item2.update(r.check_type2(pts, f, vals, BATCH_MODES, eps, "batch", seed=batch) or {})
+                entry[f"type2_{name}"] = item2
+                del plan2
+            entry["type2_tensor_over_cuda_cores"] = (entry["type2_tensor_cores"]["value"] /
+                                                     entry["type2_cuda_cores"]["value"])
+            del f, vals
             torch.cuda.empty_cache()
             result[f"eps{eps:g}_B{batch}"] = entry
     pts64 = pts.double()

@@ -7,8 +7,10 @@ exact size.
   (tests/gpu_nufft_2d.rs:15-16); the restated CPU plan on the same inputs
   meets the same bound.
 - Batched executions equal a loop of single-vector executions bit for bit
-  (tests/gpu_nufft_batch.rs:96-147), type 1 on the CUDA-core spreader and
-  type 2, in 1D, 2D and 3D.
+  (tests/gpu_nufft_batch.rs:96-147) on the CUDA-core spreader and
+  interpolation, in 1D, 2D and 3D. (The tensor-core paths, chosen by default
+  for 2D batches of 16 or more, are held to relative l2 instead:
+  tests/test_gpu_tc_spread.py, tests/test_gpu_tc_interp.py.)
 - Duplicate points give bit-equal type-2 values (tests/gpu_nufft_2d.rs:149-163).
 """
 
@@ -79,9 +81,10 @@ def test_batched_equals_loop_of_single_vectors_bitwise(n_modes, batch):
     coefficients = complex_normal(rng, (batch, int(np.prod(n_modes))))
     method = w.SpreadMethod.CUDA_CORES
     many1 = execute(1, w.NufftConfig(n_modes, 1e-5, batch=batch, spread_method=method), points, strengths, batch)
-    many2 = execute(2, w.NufftConfig(n_modes, 1e-5, batch=batch), points, coefficients, batch)
+    many2 = execute(2, w.NufftConfig(n_modes, 1e-5, batch=batch, spread_method=method), points, coefficients,
+                    batch)
     single1 = w.NufftConfig(n_modes, 1e-5, spread_method=method)
-    single2 = w.NufftConfig(n_modes, 1e-5)
+    single2 = w.NufftConfig(n_modes, 1e-5, spread_method=method)
     for b in range(batch):
         one1 = execute(1, single1, points, strengths[b], 1)
         one2 = execute(2, single2, points, coefficients[b], 1)

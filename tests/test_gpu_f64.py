@@ -140,3 +140,27 @@ def test_f64_bitwise_repeatable_and_batch():
     for b in range(3):
         one, _ = run(1, n_modes, 1e-12, points, strengths[b])
         assert rel_l2(first[b], one[0]) < 1e-14
+
+
+def test_df64_point_count_follows_the_tensor_bytes_and_sizes_are_checked():
+    """A Df64 coordinate tensor holds two floats per coordinate: the point
+    count the wrapper derives from it is bytes / (dimensions x 8), the same as
+    an explicit count; tensors smaller than the plan needs are rejected before
+    anything reaches the device."""
+    rng = np.random.default_rng(88)
+    n_modes = (20, 16)
+    points = uniform64(rng, 5000, 2)
+    strengths = cnormal(rng, (1, 5000))
+    explicit, _ = run(1, n_modes, 1e-9, points, strengths, precision=w.Precision.DF64)
+    config = w.NufftConfig(n_modes, 1e-9, precision=w.Precision.DF64)
+    plan = w.NufftPlan.type1_gpu(config)
+    plan.set_points_gpu(torch.from_numpy(to_df64(points)).to(DEV))
+    out = torch.empty(20 * 16 * 4, dtype=torch.float32, device=DEV)
+    plan.execute_gpu_batch(1, torch.from_numpy(to_df64(strengths)).to(DEV), out)
+    plan.synchronize()
+    derived = from_df64(out.cpu().numpy()).reshape(1, -1)
+    assert np.array_equal(derived.view(np.uint64), explicit.view(np.uint64))
+    with pytest.raises(w.NufftError, match="InvalidArgument"):
+        plan.execute_gpu_batch(1, torch.from_numpy(to_df64(strengths)).to(DEV), out[:100])
+    with pytest.raises(w.NufftError, match="InvalidArgument"):
+        plan.set_points_gpu(torch.from_numpy(to_df64(points)).to(DEV)[:10], point_count=5000)

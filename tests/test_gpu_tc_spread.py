@@ -105,13 +105,14 @@ def test_empty_and_single_point_sets():
 
 @pytest.mark.parametrize("eps", [1e-3, 1e-6])
 def test_batched_type2_bins_match_single_vectors_bit_for_bit(eps):
-    """Batched 2D f32 type-2 plans stage bin regions in shared memory; every
-    vector equals its single-vector execution bit for bit."""
+    """Batched 2D f32 type-2 plans on the CUDA cores stage bin regions in
+    shared memory; every vector equals its single-vector execution bit for
+    bit."""
     rng = np.random.default_rng(int(-np.log10(eps)) + 40)
     points = np.concatenate([uniform_points(rng, 6000, 2), clustered_points(rng, 3000, 2, centres=3, spread=0.02)])
     batch, modes = 40, (48, 36)
     f = _strengths(rng, batch, modes[0] * modes[1])
-    plan = w.NufftPlan.type2_gpu(w.NufftConfig(modes, eps, batch=batch))
+    plan = w.NufftPlan.type2_gpu(w.NufftConfig(modes, eps, batch=batch, spread_method=w.SpreadMethod.CUDA_CORES))
     p = torch.from_numpy(points).to(DEV)
     plan.set_points_gpu(p)
     fin = torch.from_numpy(f).to(DEV)

@@ -204,6 +204,20 @@ def _stream_handle(stream) -> int:
     return int(stream.cuda_stream)
 
 
+def _nbytes(tensor) -> int:
+    return int(tensor.numel()) * int(tensor.element_size())
+
+
+def _require_bytes(tensor, needed: int, what: str) -> None:
+    """The device-pointer interface cannot see buffer sizes; tensors can. A
+    tensor smaller than the plan needs is rejected here instead of being
+    read or written past its end (the reference validates its buffer sizes
+    the same way, src/plan.rs:1311-1387)."""
+    if needed > 0 and (tensor is None or _nbytes(tensor) < needed):
+        have = 0 if tensor is None else _nbytes(tensor)
+        raise NufftError(25, f"{what} holds {have} bytes; the plan needs {needed}")
+
+
 def _ptr(tensor) -> int:
     if tensor is None:
         return 0
@@ -291,12 +305,28 @@ class NufftPlan:
 
     # -- execution ----------------------------------------------------------
     def set_points_gpu(self, points, point_count: int | None = None, stream=None) -> None:
-        """Bins `points` (a CUDA tensor, point-major) for repeated executions."""
-        count = points.numel() // self.config.dimensions if point_count is None else point_count
+        """Bins `points` (a CUDA tensor, point-major; Df64 plans: (hi, lo)
+        float pairs per coordinate) for repeated executions. Without
+        `point_count` the count is the tensor's bytes over the bytes of one
+        point in the plan's storage."""
+        per_point = self.required_point_buffer_size_bytes(1)
+        count = _nbytes(points) // per_point if point_count is None else int(point_count)
+        _require_bytes(points, self.required_point_buffer_size_bytes(count), "the point buffer")
         _check(_native.library().b200nufft_set_points(self._handle, count, _ptr(points), _stream_handle(stream)))
         self._points = points
+        self._count = count
+        self._sizes = {}
 
     def execute_gpu_batch(self, active_batch: int, inputs, output, stream=None) -> None:
+        count = getattr(self, "_count", None)
+        if count is not None and 0 < active_batch <= self.config.batch:
+            sizes = self._sizes.get(active_batch)
+            if sizes is None:
+                sizes = (self.required_input_buffer_size_bytes(count, active_batch),
+                         self.required_output_buffer_size_bytes(count, active_batch))
+                self._sizes[active_batch] = sizes
+            _require_bytes(inputs, sizes[0], "the input buffer")
+            _require_bytes(output, sizes[1], "the output buffer")
         _check(_native.library().b200nufft_execute(self._handle, active_batch, _ptr(inputs), _ptr(output),
                                                    _stream_handle(stream)))
 
@@ -444,14 +474,25 @@ class NufftType3Plan:
         _check(_native.library().b200nufft_type3_get_info(self._handle, ctypes.byref(info)))
         return info
 
+    def _scalar_bytes(self) -> int:
+        return 4 if self.config.precision == Precision.F32 else 8
+
     def set_points_gpu(self, sources, targets, stream=None) -> None:
-        d = self.config.dimensions
+        """Sources and targets point-major in the plan's storage (Df64: (hi,
+        lo) float pairs per coordinate); the counts follow from their bytes."""
+        per_point = self.config.dimensions * self._scalar_bytes()
+        sources_count, targets_count = _nbytes(sources) // per_point, _nbytes(targets) // per_point
         _check(_native.library().b200nufft_type3_set_points(
-            self._handle, sources.numel() // d, _ptr(sources), targets.numel() // d, _ptr(targets),
-            _stream_handle(stream)))
+            self._handle, sources_count, _ptr(sources), targets_count, _ptr(targets), _stream_handle(stream)))
         self._points = (sources, targets)
+        self._counts = (sources_count, targets_count)
 
     def execute_gpu_batch(self, active_batch: int, strengths, output, stream=None) -> None:
+        counts = getattr(self, "_counts", None)
+        if counts is not None and 0 < active_batch <= self.config.batch:
+            value = 2 * self._scalar_bytes() * active_batch
+            _require_bytes(strengths, value * counts[0], "the strength buffer")
+            _require_bytes(output, value * counts[1], "the output buffer")
         _check(_native.library().b200nufft_type3_execute(self._handle, active_batch, _ptr(strengths), _ptr(output),
                                                          _stream_handle(stream)))
 

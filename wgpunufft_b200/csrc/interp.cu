@@ -622,6 +622,14 @@ bool interpolate_bins_supported(const GridParams& g) {
   return g.dimensions == 2 && g.width <= 8 && g.axis[0].shift == 3 && g.axis[1].shift == 3;
 }
 
+void unpermute_values(const float2* staged, int64_t stride, const uint32_t* inverse, int64_t count, int batch,
+                      float2* output, cudaStream_t stream) {
+  if (count <= 0) return;
+  const dim3 grid(static_cast<unsigned>((count + 31) / 32), static_cast<unsigned>((batch + 63) / 64));
+  unpermute_kernel<<<grid, 256, 0, stream>>>(staged, stride, inverse, count, batch, output);
+  note_launch();
+}
+
 void interpolate_bins_execute(const GridParams& g, const InterpBinsLaunch& l, cudaStream_t stream) {
   if (l.point_count == 0) return;
   switch (g.width) {

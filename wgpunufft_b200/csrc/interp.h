@@ -51,6 +51,9 @@ void interpolate_bins_execute(const GridParams& g, const InterpBinsLaunch& launc
 // memory, outputs written in point order (inverse and staged unused).
 void interpolate_region_execute(const GridParams& g, const InterpBinsLaunch& launch, cudaStream_t stream);
 void interpolate_execute64(const GridParams& g, const InterpLaunch64& launch, cudaStream_t stream);
+// output[b][i] = staged[inverse[i] * stride + b] for b < batch, i < count.
+void unpermute_values(const float2* staged, int64_t stride, const uint32_t* inverse, int64_t count, int batch,
+                      float2* output, cudaStream_t stream);
 // 2D f64 plans on 4 x 4-cell bins: each bin's grid region staged in shared
 // memory (same sums, bit for bit, as interpolate_execute64).
 bool interpolate_region64_supported(const GridParams& g);

@@ -119,14 +119,17 @@ NufftPlan::NufftPlan(const b200nufft_config& c, bool with_device) : has_device_(
   if (c.spread_method < B200NUFFT_SPREAD_AUTO || c.spread_method > B200NUFFT_SPREAD_TENSOR_CORES) {
     throw NufftFailure{B200NUFFT_INVALID_ARGUMENT, "spread method must be 0 (auto), 1 (CUDA cores) or 2 (tensor cores)"};
   }
-  const bool tc_qualifies = type_ == 1 && dim_ == 2 && precision_ == B200NUFFT_PRECISION_F32 &&
-                            kernel_.width <= kTcMaxWidth;
-  if (c.spread_method == B200NUFFT_SPREAD_TENSOR_CORES && !tc_qualifies) {
+  const bool f32 = precision_ == B200NUFFT_PRECISION_F32;
+  const bool tc1_qualifies = type_ == 1 && dim_ == 2 && f32 && kernel_.width <= kTcMaxWidth;
+  const bool tc2_qualifies = type_ == 2 && dim_ == 2 && f32 && kernel_.width <= kTi2MaxWidth;
+  if (c.spread_method == B200NUFFT_SPREAD_TENSOR_CORES && !tc1_qualifies && !tc2_qualifies) {
     throw NufftFailure{B200NUFFT_INVALID_ARGUMENT,
-                       "tensor-core spreading needs a 2D f32 type-1 plan with a window of at most 8 points"};
+                       "tensor cores need a 2D f32 plan with a window of at most 8 points (type 1) or 7 (type 2)"};
   }
-  tc_enabled_ = tc_qualifies && ((c.spread_method == B200NUFFT_SPREAD_AUTO && batch_ >= kTcMinBatch) ||
-                                 c.spread_method == B200NUFFT_SPREAD_TENSOR_CORES);
+  const bool tc_requested = (c.spread_method == B200NUFFT_SPREAD_AUTO && batch_ >= kTcMinBatch) ||
+                            c.spread_method == B200NUFFT_SPREAD_TENSOR_CORES;
+  tc_enabled_ = tc1_qualifies && tc_requested;
+  tc2_enabled_ = tc2_qualifies && tc_requested;
   tc_min_batch_ = c.spread_method == B200NUFFT_SPREAD_TENSOR_CORES ? 1 : kTcMinBatch;
   fine_count_ = 1;
   for (int a = 0; a < dim_; ++a) {
@@ -577,6 +580,41 @@ void NufftPlan::set_points(int64_t count, const void* points, cudaStream_t strea
       static_cast<uint32_t*>(offsets_.reserve((bins_ + 1) * sizeof(uint32_t), "bin offsets"));
   const size_t sorted_bytes = static_cast<size_t>(std::max<int64_t>(count, 1)) * dim_ * scalar_bytes();
   if (precision_ == B200NUFFT_PRECISION_F32) {
+    tc2_active_ = tc2_enabled_ && tc_interp_supported(grid_);
+    if (tc2_active_ && count > 0) {
+      // The tensor-core order first (its permutation is consumed at once),
+      // then the reference's type-2 bins in the same sort buffers.
+      uint64_t bins2 = 0;
+      tc2_grid_ = tc_interp_bins(grid_, &bins2);
+      uint32_t* offsets2 =
+          static_cast<uint32_t*>(tc2_offsets_.reserve((bins2 + 1) * sizeof(uint32_t), "tensor-core bin offsets"));
+      uint32_t* perm2 = nullptr;
+      uint32_t* keys2 = nullptr;
+      sort_points(static_cast<const float*>(points), count, tc2_grid_, KeyKind::SupportStart, bins2, buf, offsets2,
+                  &perm2, &keys2, stream, &timer_);
+      StageScope scope(&timer_, kStageTileParts, stream);
+      const int64_t tiles = tc_interp_tiles(grid_);
+      const int64_t chunk_bound = tc_interp_chunk_bound(grid_, count);
+      Ti2Prepare p;
+      p.points = static_cast<const float*>(points);
+      p.count = count;
+      p.perm = perm2;
+      p.offsets = offsets2;
+      p.weights = static_cast<TcWeights*>(tc2_weights_.reserve(static_cast<size_t>(count) * sizeof(TcWeights),
+                                                                "tensor-core window records"));
+      p.inverse = static_cast<uint32_t*>(tc2_inverse_.reserve(static_cast<size_t>(count) * sizeof(uint32_t),
+                                                               "tensor-core point slots"));
+      p.tile_count = tiles;
+      p.tile_chunks = static_cast<uint32_t*>(tc2_tile_chunks_.reserve(tiles * sizeof(uint32_t), "tile chunks"));
+      p.tile_chunk_start = static_cast<uint32_t*>(
+          tc2_tile_chunk_start_.reserve((tiles + 1) * sizeof(uint32_t), "tile chunk offsets"));
+      p.chunks = static_cast<Ti2Chunk*>(tc2_chunks_.reserve(chunk_bound * sizeof(Ti2Chunk), "chunk table"));
+      p.parts = static_cast<uint32_t*>(tc2_parts_.reserve(tiles * sizeof(uint32_t), "tensor-core parts"));
+      p.part_start = static_cast<uint32_t*>(
+          tc2_part_start_.reserve((tiles + 1) * sizeof(uint32_t), "tensor-core part offsets"));
+      tc_interp_prepare(tc2_grid_, p, stream);
+      tc2_part_upper_bound_ = tiles + chunk_bound / kTi2ChunksPerPart + 1;
+    }
     sort_points(static_cast<const float*>(points), count, grid_,
                 type_ == 1 ? KeyKind::SupportStart : KeyKind::ApproximateCell, bins_, buf, offsets,
                 &perm_, &sorted_keys_, stream, &timer_);
@@ -770,6 +808,26 @@ void NufftPlan::execute_f32(int batch, const void* input, void* output, uint64_t
                         static_cast<const float*>(amplitudes_.get()), fine, stream);
     }
     run_fft(fine, batch, direction, stream);
+    if (tc2_active_ && batch >= tc_min_batch_) {
+      const int64_t groups = (batch + kTi2Vectors - 1) / kTi2Vectors;
+      Ti2Launch t;
+      t.fine = fine;
+      t.batch = batch;
+      t.count = point_count_;
+      t.weights = static_cast<const TcWeights*>(tc2_weights_.get());
+      t.chunks = static_cast<const Ti2Chunk*>(tc2_chunks_.get());
+      t.tile_chunk_start = static_cast<const uint32_t*>(tc2_tile_chunk_start_.get());
+      t.part_start = static_cast<const uint32_t*>(tc2_part_start_.get());
+      t.part_upper_bound = tc2_part_upper_bound_;
+      t.inverse = static_cast<const uint32_t*>(tc2_inverse_.get());
+      t.staged = static_cast<float2*>(staged_.reserve(
+          static_cast<size_t>(point_count_) * groups * kTi2Vectors * sizeof(float2), "staged type-2 values"));
+      t.output = static_cast<float2*>(output);
+      t.error_flag = static_cast<uint32_t*>(counters_.get()) + 7;
+      StageScope scope(&timer_, kStageInterpolation, stream);
+      tc_interp_execute(tc2_grid_, t, stream);
+      return;
+    }
     if (dim_ == 2 && batch >= kInterpBinsMinBatch && interpolate_bins_supported(grid_)) {
       InterpBinsLaunch b;
       b.windows = windows_.get();
@@ -1084,7 +1142,7 @@ void NufftPlan::synchronize(cudaStream_t stream) {
   if (flag != 0) {
     cudaMemset(static_cast<uint32_t*>(counters_.get()) + 7, 0, sizeof(uint32_t));
     throw NufftFailure{B200NUFFT_DEVICE_TIMEOUT,
-                       "a bin-sort tile gave up waiting for its predecessor; results are invalid"};
+                       "a device wait (bin-sort look-back or tensor-core pipeline) gave up; results are invalid"};
   }
 }
 

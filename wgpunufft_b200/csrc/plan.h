@@ -14,6 +14,7 @@
 #include "modes.h"
 #include "nd.h"
 #include "spread.h"
+#include "tc_interp.h"
 #include "tc_spread.h"
 
 namespace b200nufft {
@@ -135,6 +136,16 @@ class NufftPlan {
   DeviceBuffer tc_weights_, tc_inverse_, tc_tile_chunks_, tc_tile_chunk_start_, tc_chunks_;
   DeviceBuffer tc_parts_, tc_part_start_, tc_packed_;
   int64_t tc_part_upper_bound_ = 0;
+
+  // Tensor-core interpolation (2D f32 type-2 plans of batch >= kTcMinBatch):
+  // the points ordered by exact support start in bins of 8 x 1 cells, their
+  // window records, the slot of every point and the chunk tables.
+  bool tc2_enabled_ = false;
+  bool tc2_active_ = false;
+  GridParams tc2_grid_{};
+  DeviceBuffer tc2_offsets_, tc2_weights_, tc2_inverse_, tc2_tile_chunks_, tc2_tile_chunk_start_, tc2_chunks_;
+  DeviceBuffer tc2_parts_, tc2_part_start_;
+  int64_t tc2_part_upper_bound_ = 0;
 };
 
 }  // namespace b200nufft

@@ -1,0 +1,512 @@
+// Batched 2D type-2 interpolation on the tcgen05 tensor cores.
+//
+// The reference interpolates every vector separately: a workgroup of lanes
+// per point sums its w x w cells in lane order (src/gpu_2d.rs:1022-1113,
+// workgroups over the batch at :566-575). With many vectors on one point set
+// the same sums are a dense contraction, which this file runs on the tensor
+// cores.
+//
+// Per point set (set_points): the points are ordered a second time, by the
+// exact support start in bins of 8 x 1 cells (a column group of 8 cells in
+// one grid row), and every point gets its window record (y weights, and x
+// weights placed at their column within the 16 columns the group's windows
+// reach). A tile is one column group over kTi2TileRows rows; its chunks are
+// the runs of at most 32 points of one (row, group) bin, in row order.
+//
+// Per execution, one CTA per (tile part, 64 vectors) walks its chunks in row
+// order. The fine-grid rows the chunks reach (16 columns x 64 vectors) are
+// brought into shared memory by bulk copies two rows ahead, converted into
+// tf32 high and low parts in the UMMA K-major layout (128 rows: real and
+// imaginary part of every vector) and kept in a ring of w + 1 rows. A chunk
+// at row y is 2 w MMA steps (window row j, column half h) of M = 128,
+// N = 16 or 32 points, K = 8 cells: A = ring row y + j, B = the points'
+// weights wy[j] wx over the same cells (zero outside their windows), each
+// split into three tf32 MMAs (A_hi B_hi + A_hi B_lo + A_lo B_hi) into one of
+// four tensor-memory accumulators. Two chunks later the accumulator is read
+// out to the values in tensor-core slot order, and a final pass writes them
+// in the caller's point order. Every output comes from the MMAs of one chunk
+// issued in a fixed order, so results are bitwise repeatable.
+//
+// Every wait is bounded: a wait that gives up stops the CTA's work, lets the
+// copies and MMAs in flight finish (again with a bound), frees the tensor
+// memory and increments the plan's error flag.
+#include "tc_interp.h"
+
+#include <algorithm>
+
+#include "interp.h"
+#include "spread.h"
+#include "tc_common.cuh"
+
+namespace b200nufft {
+
+namespace {
+
+using namespace tc;
+
+constexpr int kThreads = 256;
+constexpr int kBuffers = 4;            // tensor-memory accumulators of 32 columns
+constexpr int kTmemColumns = 128;
+constexpr int kRawSlots = 2;           // rows fetched ahead
+constexpr int kRawPitch = 144;         // bytes per vector of a fetched row (128 + 16 against bank conflicts)
+constexpr int kRawBytes = kTi2Vectors * kRawPitch;
+constexpr int kRowHalf = 8192;         // one tf32 part of a converted row: 128 rows x 16 columns
+constexpr int kRowBytes = 2 * kRowHalf;
+
+template <int W>
+struct Ti2Layout {
+  static constexpr int kRing = W + 1;
+  static constexpr int kBHalf = kTi2ChunkPoints * kTi2Pitch * W * 4;  // one tf32 part of B: 32 x 16 W
+  static constexpr int kBBase = kRing * kRowBytes;
+  static constexpr int kRawBase = kBBase + 2 * 2 * kBHalf;
+  static constexpr int kWeightsBase = kRawBase + kRawSlots * kRawBytes;
+  static constexpr int kBytes = kWeightsBase + kTi2ChunkPoints * static_cast<int>(sizeof(TcWeights));
+  static constexpr uint32_t kBStride = 512u * W;  // bytes between 8-point groups of B
+};
+
+// Window records in tensor-core slot order and the slot of every point:
+// the support start and offsets of the prepared windows (the fold of
+// src/gpu_nd_wgsl.rs:263-298) and the f32 Horner panels of the window.
+template <int W>
+__global__ void ti2_weights_kernel(GridParams g, const float* __restrict__ points, int64_t count,
+                                   const uint32_t* __restrict__ perm, TcWeights* __restrict__ out,
+                                   uint32_t* __restrict__ inverse) {
+  const int64_t s = static_cast<int64_t>(blockIdx.x) * blockDim.x + threadIdx.x;
+  if (s >= count) return;
+  const uint32_t p = perm[s];
+  TcWeights r;
+  r.sx = r.sy = 0;
+  r.unused[0] = r.unused[1] = 0;
+#pragma unroll
+  for (int j = 0; j < kTcMaxWidth; ++j) r.wy[j] = 0.0f;
+#pragma unroll
+  for (int c = 0; c < 2 * kTcTileX; ++c) r.wxs[c] = 0.0f;
+  const float x = points[2 * static_cast<int64_t>(p)], y = points[2 * static_cast<int64_t>(p) + 1];
+  if (in_fold_reach(x) && in_fold_reach(y)) {
+    int32_t start;
+    Df64 off;
+    float wx[W], wy[W];
+    support_of(x, g.axis[0], g.half_width, start, off);
+    r.sx = wrap_start(start, g.axis[0].length);
+    horner32_window<W>(__fadd_rn(off.hi, off.lo), g.horner32, wx);
+    support_of(y, g.axis[1], g.half_width, start, off);
+    r.sy = wrap_start(start, g.axis[1].length);
+    horner32_window<W>(__fadd_rn(off.hi, off.lo), g.horner32, wy);
+    const int dx = r.sx & (kTi2GroupX - 1);
+#pragma unroll
+    for (int j = 0; j < W; ++j) {
+      r.wy[j] = wy[j];
+#pragma unroll
+      for (int d = 0; d < kTi2GroupX; ++d) {
+        if (d == dx) r.wxs[d + j] = wx[j];
+      }
+    }
+  }
+  out[s] = r;
+  inverse[p] = static_cast<uint32_t>(s);
+}
+
+__device__ __forceinline__ void tile_origin(const GridParams& g, int64_t t, int& tx, int& ty) {
+  const int64_t groups = g.axis[0].bins;
+  tx = static_cast<int>(t % groups);
+  ty = static_cast<int>(t / groups);
+}
+
+// Chunks and parts of every tile.
+__global__ void ti2_tile_chunks_kernel(GridParams g, int64_t tiles, const uint32_t* __restrict__ offsets,
+                                       uint32_t* __restrict__ tile_chunks, uint32_t* __restrict__ parts) {
+  const int64_t t = static_cast<int64_t>(blockIdx.x) * blockDim.x + threadIdx.x;
+  if (t >= tiles) return;
+  int tx, ty;
+  tile_origin(g, t, tx, ty);
+  const int n1 = g.axis[1].length;
+  const int y_end = min((ty + 1) * kTi2TileRows, n1);
+  const uint64_t groups = g.axis[0].bins;
+  uint32_t chunks = 0;
+  for (int y = ty * kTi2TileRows; y < y_end; ++y) {
+    const uint64_t b = tx + groups * static_cast<uint64_t>(y);
+    const uint32_t n = offsets[b + 1] - offsets[b];
+    chunks += (n + kTi2ChunkPoints - 1) / kTi2ChunkPoints;
+  }
+  tile_chunks[t] = chunks;
+  parts[t] = (chunks + kTi2ChunksPerPart - 1) / kTi2ChunksPerPart;
+}
+
+__global__ void ti2_chunk_fill_kernel(GridParams g, int64_t tiles, const uint32_t* __restrict__ offsets,
+                                      const uint32_t* __restrict__ tile_chunk_start, Ti2Chunk* __restrict__ chunks) {
+  const int64_t t = static_cast<int64_t>(blockIdx.x) * blockDim.x + threadIdx.x;
+  if (t >= tiles) return;
+  int tx, ty;
+  tile_origin(g, t, tx, ty);
+  const int n1 = g.axis[1].length;
+  const int y0 = ty * kTi2TileRows;
+  const int y_end = min(y0 + kTi2TileRows, n1);
+  const uint64_t groups = g.axis[0].bins;
+  uint32_t next = tile_chunk_start[t];
+  for (int y = y0; y < y_end; ++y) {
+    const uint64_t b = tx + groups * static_cast<uint64_t>(y);
+    const uint32_t begin = offsets[b], end = offsets[b + 1];
+    for (uint32_t s = begin; s < end; s += kTi2ChunkPoints) {
+      Ti2Chunk c;
+      c.slot = s;
+      c.count = static_cast<uint16_t>(min(static_cast<uint32_t>(kTi2ChunkPoints), end - s));
+      c.row = static_cast<uint16_t>(y - y0);
+      chunks[next++] = c;
+    }
+  }
+}
+
+// Converts fetched row `raw` (64 vectors x 16 complex cells at kRawPitch)
+// into tf32 high and low parts at `ring` (K-major: 4 K blocks of 128 bytes,
+// 16 groups of 8 rows 512 bytes apart; row m = 2 v + part).
+__device__ __forceinline__ void ti2_convert_row(const unsigned char* raw, unsigned char* ring, int nv, int tid) {
+#pragma unroll
+  for (int i = 0; i < 2; ++i) {
+    const int u = tid + i * kThreads;
+    const int kb = u >> 7, m = u & 127, v = m >> 1, part = m & 1;
+    float4 value = make_float4(0.0f, 0.0f, 0.0f, 0.0f);
+    if (v < nv) {
+      const float4 a = *reinterpret_cast<const float4*>(raw + v * kRawPitch + kb * 32);
+      const float4 b = *reinterpret_cast<const float4*>(raw + v * kRawPitch + kb * 32 + 16);
+      value = part ? make_float4(a.y, a.w, b.y, b.w) : make_float4(a.x, a.z, b.x, b.z);
+    }
+    float4 hi, lo;
+    split_tf32(value.x, hi.x, lo.x);
+    split_tf32(value.y, hi.y, lo.y);
+    split_tf32(value.z, hi.z, lo.z);
+    split_tf32(value.w, hi.w, lo.w);
+    const int off = kb * 128 + (m >> 3) * 512 + (m & 7) * 16;
+    *reinterpret_cast<float4*>(ring + off) = hi;
+    *reinterpret_cast<float4*>(ring + kRowHalf + off) = lo;
+  }
+}
+
+template <int W>
+__global__ void __launch_bounds__(kThreads, 1) tc_interp_kernel(
+    GridParams g, const float2* __restrict__ fine, int batch, const TcWeights* __restrict__ weights,
+    const Ti2Chunk* __restrict__ chunks, const uint32_t* __restrict__ tile_chunk_start,
+    const uint32_t* __restrict__ part_start, int64_t tiles, float2* __restrict__ staged, int64_t staged_stride,
+    uint32_t* __restrict__ error_flag) {
+  using L = Ti2Layout<W>;
+  extern __shared__ __align__(1024) unsigned char smem[];
+  __shared__ __align__(8) uint64_t done_bar[kBuffers];
+  __shared__ __align__(8) uint64_t raw_bar[kRawSlots];
+  __shared__ uint32_t tmem_base;
+  __shared__ int64_t s_tile;
+  __shared__ int s_ok;
+  __shared__ Ti2Chunk s_chunks[kTi2ChunksPerPart];
+
+  const uint32_t part = blockIdx.x;
+  if (part >= part_start[tiles]) return;
+  const int group = blockIdx.y;
+  const int tid = threadIdx.x, warp = tid >> 5, lane = tid & 31;
+  if (tid == 0) {
+    int64_t low = 0, high = tiles - 1;
+    while (low < high) {
+      const int64_t mid = (low + high + 1) >> 1;
+      if (part_start[mid] <= part) low = mid; else high = mid - 1;
+    }
+    s_tile = low;
+    s_ok = 1;
+#pragma unroll
+    for (int b = 0; b < kBuffers; ++b) mbar_init(&done_bar[b], 1);
+#pragma unroll
+    for (int s = 0; s < kRawSlots; ++s) mbar_init(&raw_bar[s], 1);
+    asm volatile("fence.mbarrier_init.release.cluster;" ::: "memory");
+  }
+  if (warp == 0) {
+    asm volatile("tcgen05.alloc.cta_group::1.sync.aligned.shared::cta.b32 [%0], %1;" ::"r"(smem_u32(&tmem_base)),
+                 "r"(kTmemColumns));
+    asm volatile("tcgen05.relinquish_alloc_permit.cta_group::1.sync.aligned;");
+  }
+  tc_fence_before();
+  __syncthreads();
+  tc_fence_after();
+  const uint32_t tm = tmem_base;
+  const int64_t tile = s_tile;
+  const uint32_t first = tile_chunk_start[tile] + (part - part_start[tile]) * kTi2ChunksPerPart;
+  const uint32_t stop = min(first + static_cast<uint32_t>(kTi2ChunksPerPart), tile_chunk_start[tile + 1]);
+  const int n = stop > first ? static_cast<int>(stop - first) : 0;
+  for (int c = tid; c < n; c += kThreads) s_chunks[c] = chunks[first + c];
+  __syncthreads();
+
+  int tx, ty;
+  tile_origin(g, tile, tx, ty);
+  const int n0 = g.axis[0].length, n1 = g.axis[1].length;
+  const int x0 = tx * kTi2GroupX, y0 = ty * kTi2TileRows;
+  const int vb = group * kTi2Vectors;
+  const int nv = min(kTi2Vectors, batch - vb);
+  // Rows [r_begin, r_end) relative to y0 are fetched and converted in order.
+  const int r_begin = n > 0 ? s_chunks[0].row : 0;
+  const int r_end = n > 0 ? s_chunks[n - 1].row + W : 0;
+  unsigned char* ring = smem;
+  unsigned char* raw = smem + L::kRawBase;
+  const TcWeights* s_w = reinterpret_cast<const TcWeights*>(smem + L::kWeightsBase);
+
+  // Fetches relative row r (its k-th fetch, k = r - r_begin) into raw slot k % 2.
+  auto fetch = [&](int r) {
+    const int k = r - r_begin;
+    const uint32_t bar = smem_u32(&raw_bar[k % kRawSlots]);
+    unsigned char* dst = raw + (k % kRawSlots) * kRawBytes;
+    int y = (y0 + r) % n1;
+    const int64_t row = static_cast<int64_t>(y) * n0;
+    mbar_expect(bar, static_cast<uint32_t>(nv) * 128u);
+    for (int v = 0; v < nv; ++v) {
+      const float2* grid = fine + static_cast<int64_t>(vb + v) * g.fine_count + row;
+      const uint32_t d = smem_u32(dst + v * kRawPitch);
+      if (x0 + 2 * kTi2GroupX <= n0) {
+        bulk_load(d, grid + x0, 128, bar);
+      } else {
+        bulk_load(d, grid + x0, 64, bar);
+        bulk_load(d + 64, grid, 64, bar);
+      }
+    }
+  };
+  int fetched = r_begin;  // rows [r_begin, fetched) have been fetched
+  if (tid == 0) {
+    for (; fetched < min(r_end, r_begin + kRawSlots); ++fetched) fetch(fetched);
+  }
+
+  int ring_hi = r_begin;  // rows [.., ring_hi) are converted
+  int issued = 0;
+  bool aborted = false;
+  for (int c = 0; c < n + 2 && !aborted; ++c) {
+    const int r = c < n ? s_chunks[c].row : 0;
+    const int rows_now = c < n ? min(r + W, ring_hi + kRawSlots) - ring_hi : 0;
+    if (tid == 0) {
+      bool ok = true;
+      if (c >= 2) ok = mbar_wait(smem_u32(&done_bar[(c - 2) % kBuffers]), static_cast<uint32_t>((c - 2) / kBuffers) & 1u,
+                                 nullptr);
+      // New rows overwrite ring slots of rows that chunk c - 1 may still read
+      // when chunk c starts two or more rows below it.
+      if (ok && c >= 1 && c < n && r >= s_chunks[c - 1].row + 2) {
+        ok = mbar_wait(smem_u32(&done_bar[(c - 1) % kBuffers]), static_cast<uint32_t>((c - 1) / kBuffers) & 1u,
+                       nullptr);
+      }
+      for (int q = 0; ok && q < rows_now; ++q) {
+        const int k = ring_hi + q - r_begin;
+        ok = mbar_wait(smem_u32(&raw_bar[k % kRawSlots]), static_cast<uint32_t>(k / kRawSlots) & 1u, nullptr);
+      }
+      s_ok = ok ? 1 : 0;
+    }
+    __syncthreads();
+    if (!s_ok) {
+      aborted = true;
+      break;
+    }
+    tc_fence_after();
+    if (c >= 2) {
+      // Read out chunk c - 2: warp w holds rows 32 (w % 4) + lane (vector
+      // m / 2, real part when m is even) of columns 16 (w / 4) .. + 15.
+      const int cc = c - 2;
+      const Ti2Chunk ch = s_chunks[cc];
+      const int col0 = warp >= 4 ? 16 : 0;
+      if (col0 < ch.count) {
+        uint32_t v[16];
+        tmem_ld16(tm + (static_cast<uint32_t>((warp & 3) * 32) << 16) + static_cast<uint32_t>((cc % kBuffers) * 32 + col0),
+                  v);
+        tmem_wait_ld();
+        const int m = (warp & 3) * 32 + lane;
+        const int vec = m >> 1;
+#pragma unroll
+        for (int i = 0; i < 16; ++i) {
+          const float x = __uint_as_float(v[i]);
+          const float y = __shfl_xor_sync(0xFFFFFFFFu, x, 1);
+          const int p = col0 + i;
+          if ((m & 1) == 0 && p < ch.count && vec < nv) {
+            staged[(static_cast<int64_t>(ch.slot) + p) * staged_stride + vb + vec] = make_float2(x, y);
+          }
+        }
+      }
+    }
+    if (c >= n) continue;
+    const Ti2Chunk ch = s_chunks[c];
+    // Rows fetched ahead, converted into the ring; the chunk's window records.
+    for (int q = 0; q < rows_now; ++q) {
+      const int rr = ring_hi + q;
+      ti2_convert_row(raw + ((rr - r_begin) % kRawSlots) * kRawBytes, ring + (rr % L::kRing) * kRowBytes, nv, tid);
+    }
+    if (tid < 7 * ch.count) {
+      const float4* src = reinterpret_cast<const float4*>(weights + ch.slot);
+      reinterpret_cast<float4*>(smem + L::kWeightsBase)[tid] = src[tid];
+    }
+    __syncthreads();
+    ring_hi += rows_now;
+    if (tid == 0) {
+      for (; fetched < min(r_end, ring_hi + kRawSlots); ++fetched) fetch(fetched);
+    }
+    // A chunk far below the last one needs more rows than were fetched ahead.
+    while (ring_hi < r + W) {
+      if (tid == 0) {
+        const int k = ring_hi - r_begin;
+        s_ok = mbar_wait(smem_u32(&raw_bar[k % kRawSlots]), static_cast<uint32_t>(k / kRawSlots) & 1u, nullptr) ? 1 : 0;
+      }
+      __syncthreads();
+      if (!s_ok) {
+        aborted = true;
+        break;
+      }
+      ti2_convert_row(raw + ((ring_hi - r_begin) % kRawSlots) * kRawBytes, ring + (ring_hi % L::kRing) * kRowBytes, nv,
+                      tid);
+      __syncthreads();
+      ++ring_hi;
+      if (tid == 0) {
+        for (; fetched < min(r_end, ring_hi + kRawSlots); ++fetched) fetch(fetched);
+      }
+    }
+    if (aborted) break;
+    // B: point n, K unit kb (window row kb / 4, columns 4 (kb % 4) .. + 3).
+    const int cols = ch.count <= 16 ? 16 : 32;
+    unsigned char* b_hi = smem + L::kBBase + (c & 1) * 2 * L::kBHalf;
+    unsigned char* b_lo = b_hi + L::kBHalf;
+    for (int u = tid; u < cols * 4 * W; u += kThreads) {
+      const int kb = u / cols, pn = u - kb * cols;
+      float4 value = make_float4(0.0f, 0.0f, 0.0f, 0.0f);
+      if (pn < ch.count) {
+        const float wy = s_w[pn].wy[kb >> 2];
+        const float4 wx = *reinterpret_cast<const float4*>(&s_w[pn].wxs[4 * (kb & 3)]);
+        value = make_float4(wy * wx.x, wy * wx.y, wy * wx.z, wy * wx.w);
+      }
+      float4 hi, lo;
+      split_tf32(value.x, hi.x, lo.x);
+      split_tf32(value.y, hi.y, lo.y);
+      split_tf32(value.z, hi.z, lo.z);
+      split_tf32(value.w, hi.w, lo.w);
+      const int off = kb * 128 + (pn >> 3) * static_cast<int>(L::kBStride) + (pn & 7) * 16;
+      *reinterpret_cast<float4*>(b_hi + off) = hi;
+      *reinterpret_cast<float4*>(b_lo + off) = lo;
+    }
+    asm volatile("fence.proxy.async.shared::cta;" ::: "memory");
+    tc_fence_before();
+    __syncthreads();
+    if (tid == 0) {
+      tc_fence_after();
+      const uint32_t idesc = idesc_tf32(128, static_cast<uint32_t>(cols));
+      const uint32_t d = tm + static_cast<uint32_t>((c % kBuffers) * 32);
+      const uint32_t bh = smem_u32(b_hi), bl = smem_u32(b_lo);
+#pragma unroll 1
+      for (int j = 0; j < W; ++j) {
+        const uint32_t rb = smem_u32(ring + ((ch.row + j) % L::kRing) * kRowBytes);
+#pragma unroll
+        for (int h = 0; h < 2; ++h) {
+          const uint64_t ahi = kmajor_desc(rb + h * 256, 128, 512);
+          const uint64_t alo = kmajor_desc(rb + kRowHalf + h * 256, 128, 512);
+          const uint64_t bhi = kmajor_desc(bh + (4 * j + 2 * h) * 128, 128, L::kBStride);
+          const uint64_t blo = kmajor_desc(bl + (4 * j + 2 * h) * 128, 128, L::kBStride);
+          mma_tf32(d, ahi, bhi, idesc, j > 0 || h > 0);
+          mma_tf32(d, ahi, blo, idesc, true);
+          mma_tf32(d, alo, bhi, idesc, true);
+        }
+      }
+      mma_commit(smem_u32(&done_bar[c % kBuffers]));
+    }
+    issued = c + 1;
+  }
+
+  // Drain: the MMAs and the fetches in flight finish before the CTA leaves.
+  if (tid == 0) {
+    bool drained = true;
+    if (issued > 0) {
+      drained = mbar_wait(smem_u32(&done_bar[(issued - 1) % kBuffers]),
+                          static_cast<uint32_t>((issued - 1) / kBuffers) & 1u, nullptr);
+    }
+    for (int r = ring_hi; r < fetched; ++r) {
+      const int k = r - r_begin;
+      drained = mbar_wait(smem_u32(&raw_bar[k % kRawSlots]), static_cast<uint32_t>(k / kRawSlots) & 1u, nullptr) &&
+                drained;
+    }
+    if (aborted || !drained) atomicAdd(error_flag, 1u);
+  }
+  tc_fence_before();
+  __syncthreads();
+  if (warp == 0) {
+    asm volatile("tcgen05.dealloc.cta_group::1.sync.aligned.b32 %0, %1;" ::"r"(tm), "r"(kTmemColumns));
+  }
+}
+
+template <int W>
+void launch_weights(const GridParams& g, const Ti2Prepare& p, cudaStream_t stream) {
+  const unsigned blocks = static_cast<unsigned>((p.count + 255) / 256);
+  ti2_weights_kernel<W><<<blocks, 256, 0, stream>>>(g, p.points, p.count, p.perm, p.weights, p.inverse);
+  note_launch();
+}
+
+template <int W>
+void launch_interp(const GridParams& g, const Ti2Launch& l, int64_t tiles, int64_t stride, cudaStream_t stream) {
+  using L = Ti2Layout<W>;
+  static_assert(L::kBytes <= 227 * 1024, "tensor-core interpolation stages exceed shared memory");
+  auto kernel = tc_interp_kernel<W>;
+  check_cuda(cudaFuncSetAttribute(kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, L::kBytes),
+             "tensor-core interpolation shared memory");
+  const int groups = (l.batch + kTi2Vectors - 1) / kTi2Vectors;
+  const dim3 grid(static_cast<unsigned>(l.part_upper_bound), static_cast<unsigned>(groups));
+  kernel<<<grid, kThreads, L::kBytes, stream>>>(g, l.fine, l.batch, l.weights, l.chunks, l.tile_chunk_start,
+                                                l.part_start, tiles, l.staged, stride, l.error_flag);
+  note_launch();
+}
+
+}  // namespace
+
+bool tc_interp_supported(const GridParams& g) {
+  return g.dimensions == 2 && g.width >= 2 && g.width <= kTi2MaxWidth && g.fine[0] % kTi2GroupX == 0 &&
+         g.fine[0] >= 2 * kTi2GroupX && g.fine[1] >= g.width;
+}
+
+GridParams tc_interp_bins(const GridParams& g, uint64_t* bins) {
+  GridParams b = g;
+  const uint32_t groups = static_cast<uint32_t>(g.fine[0] / kTi2GroupX);
+  b.axis[0].shift = 3;
+  b.axis[0].bins = groups;
+  b.axis[0].stride = 1;
+  b.axis[1].shift = 0;
+  b.axis[1].bins = static_cast<uint32_t>(g.fine[1]);
+  b.axis[1].stride = groups;
+  *bins = static_cast<uint64_t>(groups) * static_cast<uint64_t>(g.fine[1]);
+  return b;
+}
+
+int64_t tc_interp_tiles(const GridParams& g) {
+  return (g.fine[0] / kTi2GroupX) * ((g.fine[1] + kTi2TileRows - 1) / kTi2TileRows);
+}
+
+int64_t tc_interp_chunk_bound(const GridParams& g, int64_t count) {
+  return count / kTi2ChunkPoints + 1 + (g.fine[0] / kTi2GroupX) * g.fine[1];
+}
+
+void tc_interp_prepare(const GridParams& g, const Ti2Prepare& p, cudaStream_t stream) {
+  if (p.count > 0) {
+    switch (g.width) {
+      case 2: launch_weights<2>(g, p, stream); break;
+      case 3: launch_weights<3>(g, p, stream); break;
+      case 4: launch_weights<4>(g, p, stream); break;
+      case 5: launch_weights<5>(g, p, stream); break;
+      case 6: launch_weights<6>(g, p, stream); break;
+      default: launch_weights<7>(g, p, stream); break;
+    }
+  }
+  const unsigned blocks = static_cast<unsigned>((p.tile_count + 255) / 256);
+  ti2_tile_chunks_kernel<<<blocks, 256, 0, stream>>>(g, p.tile_count, p.offsets, p.tile_chunks, p.parts);
+  note_launch();
+  exclusive_scan_u32(p.tile_chunks, p.tile_count, p.tile_chunk_start, stream);
+  exclusive_scan_u32(p.parts, p.tile_count, p.part_start, stream);
+  ti2_chunk_fill_kernel<<<blocks, 256, 0, stream>>>(g, p.tile_count, p.offsets, p.tile_chunk_start, p.chunks);
+  note_launch();
+}
+
+void tc_interp_execute(const GridParams& g, const Ti2Launch& l, cudaStream_t stream) {
+  const int64_t tiles = tc_interp_tiles(g);
+  const int64_t stride = static_cast<int64_t>((l.batch + kTi2Vectors - 1) / kTi2Vectors) * kTi2Vectors;
+  if (l.count > 0) {
+    switch (g.width) {
+      case 2: launch_interp<2>(g, l, tiles, stride, stream); break;
+      case 3: launch_interp<3>(g, l, tiles, stride, stream); break;
+      case 4: launch_interp<4>(g, l, tiles, stride, stream); break;
+      case 5: launch_interp<5>(g, l, tiles, stride, stream); break;
+      case 6: launch_interp<6>(g, l, tiles, stride, stream); break;
+      default: launch_interp<7>(g, l, tiles, stride, stream); break;
+    }
+  }
+  unpermute_values(l.staged, stride, l.inverse, l.count, l.batch, l.output, stream);
+}
+
+}  // namespace b200nufft

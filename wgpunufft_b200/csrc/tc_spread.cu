@@ -29,108 +29,26 @@
 
 #include <algorithm>
 
+#include "tc_common.cuh"
+
 namespace b200nufft {
 
 namespace {
+
+using namespace tc;
+
+// Instruction descriptor of the spread MMAs: M = 128, N = 16 w.
+template <int W>
+__host__ __device__ constexpr uint32_t tc_idesc() {
+  return idesc_tf32(128, 16 * W);
+}
 
 constexpr int kTcTeams = 4;          // converter teams, each converting every fourth chunk
 constexpr int kTcTeamThreads = 64;
 constexpr int kTcThreads = 64 + kTcTeams * kTcTeamThreads;  // producer warp, MMA warp, converters
 constexpr int kTcCopyStages = 8;     // chunks whose copies are in flight or unread
 constexpr int kTcOperandStages = 4;  // chunks whose MMAs may still read their operands
-constexpr uint32_t kSpinLimit = 1u << 22;
 constexpr size_t kTcSharedBytes = 108 * 1024;  // two CTAs per SM, 256 tensor-memory columns each
-
-__device__ __forceinline__ uint32_t smem_u32(const void* p) {
-  return static_cast<uint32_t>(__cvta_generic_to_shared(p));
-}
-
-// UMMA shared-memory descriptor of a K-major operand without swizzling: core
-// matrices of 8 rows x 16 bytes; the two 4-element K halves 128 bytes apart
-// (leading byte offset), consecutive 8-row groups 256 bytes apart (stride
-// byte offset); descriptor version 1.
-__device__ __forceinline__ uint64_t kmajor_desc(uint32_t addr) {
-  return static_cast<uint64_t>((addr >> 4) & 0x3FFFu) | (static_cast<uint64_t>(128 >> 4) << 16) |
-         (static_cast<uint64_t>(256 >> 4) << 32) | (1ull << 46);
-}
-// Byte offset of the 4-element K unit (row, h) in such an operand.
-__device__ __forceinline__ int kmajor_unit(int row, int h) {
-  return (row >> 3) * 256 + h * 128 + (row & 7) * 16;
-}
-
-// Instruction descriptor: tf32 x tf32 -> f32, both operands K-major,
-// M = 128, N = 16 w.
-template <int W>
-__host__ __device__ constexpr uint32_t tc_idesc() {
-  return (1u << 4) | (2u << 7) | (2u << 10) | ((16u * W >> 3) << 17) | ((128u >> 4) << 24);
-}
-
-__device__ __forceinline__ void mma_tf32(uint32_t d, uint64_t a, uint64_t b, uint32_t idesc) {
-  asm volatile(
-      "{\n.reg .pred p;\nsetp.ne.b32 p, %4, 0;\n"
-      "tcgen05.mma.cta_group::1.kind::tf32 [%0], %1, %2, %3, {%5, %5, %5, %5}, p;\n}\n" ::"r"(d),
-      "l"(a), "l"(b), "r"(idesc), "r"(1), "r"(0));
-}
-__device__ __forceinline__ void mma_commit(uint32_t bar) {
-  asm volatile("tcgen05.commit.cta_group::1.mbarrier::arrive::one.shared::cluster.b64 [%0];" ::"r"(bar)
-               : "memory");
-}
-__device__ __forceinline__ void tc_fence_before() { asm volatile("tcgen05.fence::before_thread_sync;" ::: "memory"); }
-__device__ __forceinline__ void tc_fence_after() { asm volatile("tcgen05.fence::after_thread_sync;" ::: "memory"); }
-
-__device__ __forceinline__ void mbar_init(uint64_t* bar, uint32_t count) {
-  asm volatile("mbarrier.init.shared::cta.b64 [%0], %1;" ::"r"(smem_u32(bar)), "r"(count));
-}
-__device__ __forceinline__ bool mbar_try(uint32_t bar, uint32_t parity) {
-  uint32_t done;
-  asm volatile(
-      "{\n.reg .pred p;\nmbarrier.try_wait.parity.shared::cta.b64 p, [%1], %2;\nselp.u32 %0, 1, 0, p;\n}\n"
-      : "=r"(done)
-      : "r"(bar), "r"(parity)
-      : "memory");
-  return done != 0;
-}
-// Waits for the phase of the given parity to complete; false when it gave up
-// or when another role raised the CTA's abort flag (which a failed wait
-// raises).
-__device__ __noinline__ bool mbar_wait(uint32_t bar, uint32_t parity, volatile int* abort_flag) {
-  for (uint32_t i = 0; i < kSpinLimit; ++i) {
-    if (mbar_try(bar, parity)) return true;
-    if (abort_flag != nullptr && *abort_flag) return false;
-    if (i >= 32) __nanosleep(32);
-  }
-  if (abort_flag != nullptr) *abort_flag = 1;
-  return false;
-}
-__device__ __forceinline__ void mbar_arrive(uint32_t bar) {
-  asm volatile("mbarrier.arrive.shared::cta.b64 _, [%0];" ::"r"(bar) : "memory");
-}
-__device__ __forceinline__ void mbar_expect(uint32_t bar, uint32_t bytes) {
-  asm volatile("mbarrier.arrive.expect_tx.shared::cta.b64 _, [%0], %1;" ::"r"(bar), "r"(bytes) : "memory");
-}
-// Bulk copy global -> shared, completing on `bar` (16-byte aligned, size a multiple of 16).
-__device__ __forceinline__ void bulk_load(uint32_t dst, const void* src, uint32_t bytes, uint32_t bar) {
-  asm volatile("cp.async.bulk.shared::cluster.global.mbarrier::complete_tx::bytes [%0], [%1], %2, [%3];" ::"r"(dst),
-               "l"(src), "r"(bytes), "r"(bar)
-               : "memory");
-}
-
-__device__ __forceinline__ void tmem_zero8(uint32_t addr) {
-  asm volatile("tcgen05.st.sync.aligned.32x32b.x8.b32 [%0], {%1, %1, %1, %1, %1, %1, %1, %1};" ::"r"(addr),
-               "r"(0));
-}
-__device__ __forceinline__ void tmem_ld8(uint32_t addr, uint32_t* v) {
-  asm volatile("tcgen05.ld.sync.aligned.32x32b.x8.b32 {%0, %1, %2, %3, %4, %5, %6, %7}, [%8];"
-               : "=r"(v[0]), "=r"(v[1]), "=r"(v[2]), "=r"(v[3]), "=r"(v[4]), "=r"(v[5]), "=r"(v[6]), "=r"(v[7])
-               : "r"(addr));
-}
-
-// tf32 split: hi keeps the sign, exponent and 10 mantissa bits the tensor
-// core reads; lo = x - hi is exact in f32.
-__device__ __forceinline__ void split_tf32(float x, float& hi, float& lo) {
-  hi = __uint_as_float(__float_as_uint(x) & 0xFFFFE000u);
-  lo = x - hi;
-}
 
 // Window records in slot order and the slot of every original index.
 template <int W>
