@@ -110,3 +110,48 @@ def test_uneven_problems_in_one_graph_match_direct_sums():
         bound = 20e-6 if len(modes) == 2 else 32e-6
         assert rel_l2(outs[k].cpu().numpy()[:, select], ref) < bound, (k, modes, p.shape[0])
     del graph
+
+
+@pytest.mark.parametrize("kind,modes,batch,precision", [(1, (64, 48), 1, w.Precision.F32), (1, (64, 48), 32, w.Precision.F32),
+                                                        (2, (64, 48), 1, w.Precision.F32), (2, (64, 48), 16, w.Precision.F32),
+                                                        (1, (24, 20, 16), 2, w.Precision.F32),
+                                                        (1, (40, 36), 1, w.Precision.F64), (2, (40, 36), 3, w.Precision.F64)])
+def test_captured_sort_and_execution_follow_new_points(kind, modes, batch, precision):
+    """The whole one-shot transform (stable bin sort, window preparation,
+    spread or interpolation, FFT, deconvolution) captured in one CUDA graph
+    after a warm-up of the same point count: replays on new coordinates
+    written into the same buffer give the bits of eager one-shot executions
+    on those coordinates."""
+    rng = np.random.default_rng(kind * 1000 + batch)
+    m = 20000
+    real = torch.float32 if precision == w.Precision.F32 else torch.float64
+    cplx = torch.complex64 if precision == w.Precision.F32 else torch.complex128
+    n = int(np.prod(modes))
+    in_len, out_len = (m, n) if kind == 1 else (n, m)
+    plan = (w.NufftPlan.type1_gpu if kind == 1 else w.NufftPlan.type2_gpu)(
+        w.NufftConfig(modes, 1e-6 if precision == w.Precision.F32 else 1e-9, batch=batch, precision=precision))
+    points = torch.from_numpy(uniform_points(rng, m, len(modes))).to(DEV, real)
+    inputs = torch.complex(torch.randn((batch, in_len), device=DEV, dtype=real),
+                           torch.randn((batch, in_len), device=DEV, dtype=real))
+    out = torch.empty((batch, out_len), dtype=cplx, device=DEV)
+    stream = torch.cuda.Stream()
+    with torch.cuda.stream(stream):
+        plan.encode_gpu_batch(batch, points, inputs, out, stream=stream)
+        stream.synchronize()
+        graph = torch.cuda.CUDAGraph()
+        with torch.cuda.graph(graph, stream=stream):
+            plan.encode_gpu_batch(batch, points, inputs, out, stream=stream)
+    for trial in range(2):
+        fresh = np.random.default_rng(trial + 5)
+        points.copy_(torch.from_numpy(uniform_points(fresh, m, len(modes))).to(DEV, real))
+        inputs.copy_(torch.complex(torch.randn((batch, in_len), device=DEV, dtype=real),
+                                   torch.randn((batch, in_len), device=DEV, dtype=real)))
+        out.zero_()
+        graph.replay()
+        torch.cuda.synchronize()
+        replayed = out.clone()
+        with torch.cuda.stream(stream):
+            plan.encode_gpu_batch(batch, points, inputs, out, stream=stream)
+        plan.synchronize(stream)
+        assert torch.equal(replayed.view(torch.int32), out.view(torch.int32))
+    del graph

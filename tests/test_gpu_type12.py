@@ -238,37 +238,77 @@ def test_execute_before_points_and_wrong_kind_fail():
         plan.execute_type2_gpu(out, out)
 
 
-@pytest.mark.parametrize("n_modes", [(64,), (24, 20), (16, 16, 12)])
-def test_invalid_points_leave_other_points_intact(n_modes):
-    """tests/gpu_invalid_points.rs: non-finite and far coordinates get zero
-    weight; type-2 values at the other points are unchanged bit for bit and
-    zero at the invalid ones; type-1 modes match those of the valid points."""
-    d = len(n_modes)
-    rng = np.random.default_rng(21)
-    valid = uniform_points(rng, 300, d)
-    invalid_values = [np.nan, np.inf, -np.inf, 1e30, -1e30, -40.0, 5 * np.pi]
+def with_invalid_points(valid, every, rng=None):
+    """`valid` with a point outside the fold's reach inserted after every
+    `every` points (non-finite, far, and just-outside coordinates on one axis,
+    cycling; tests/gpu_invalid_points.rs:20-34); returns the mixed set and each
+    mixed point's index among the valid ones (-1 for the inserted ones)."""
+    d = valid.shape[1]
+    invalid_values = [np.nan, np.inf, -np.inf, 1e30, -1e30, -40.0, 5 * np.pi, 1e20]
     mixed, index = [], []
     k = 0
     for i, p in enumerate(valid):
         mixed.append(p)
         index.append(i)
-        if (i + 1) % 25 == 0:
+        if (i + 1) % every == 0:
             q = p.copy()
             q[k % d] = invalid_values[k % len(invalid_values)]
             mixed.append(q)
             index.append(-1)
             k += 1
-    mixed = np.array(mixed, dtype=np.float32)
-    index = np.array(index)
+    return np.array(mixed, dtype=valid.dtype), np.array(index)
+
+
+@pytest.mark.parametrize("n_modes", [(64,), (24, 20), (16, 16, 12)])
+def test_invalid_points_leave_other_points_intact(n_modes):
+    """tests/gpu_invalid_points.rs: non-finite and far coordinates get zero
+    weight; type-2 values at the other points are unchanged bit for bit and
+    zero at the invalid ones; type-1 modes equal, bit for bit, those of the
+    valid points alone, whatever the invalid points' strengths."""
+    d = len(n_modes)
+    rng = np.random.default_rng(21)
+    valid = uniform_points(rng, 300, d)
+    mixed, index = with_invalid_points(valid, 25)
     coefficients = complex_normal(rng, int(np.prod(n_modes)))
     only, _ = run_type2(n_modes, 1e-6, valid, coefficients)
     both, _ = run_type2(n_modes, 1e-6, mixed, coefficients)
     assert np.array_equal(both[0, index >= 0].view(np.uint32), only[0].view(np.uint32))
     assert np.all(both[0, index < 0] == 0)
     strengths = complex_normal(rng, len(mixed))
+    strengths[index < 0] *= 1e3  # larger than every valid strength: must not set the scale
     with_invalid, _ = run_type1(n_modes, 1e-6, mixed, strengths)
     without, _ = run_type1(n_modes, 1e-6, valid, strengths[index >= 0])
-    assert rel_l2(with_invalid, without) < 1e-6
+    assert np.array_equal(with_invalid.view(np.uint32), without.view(np.uint32))
+
+
+@pytest.mark.parametrize("n_modes,count,precision,method", [
+    ((48, 40), 400_000, "f32", 1), ((16, 16, 12), 300_000, "f32", 1), ((40, 36), 200_000, "f64", 1),
+    ((64, 48), 200_000, "f32", 2)])
+def test_invalid_points_leave_type1_bitwise_intact_at_scale(n_modes, count, precision, method):
+    """Crowded small grids above 150,000 points, where the parts are sized by
+    the point count: points outside the reach change no part, no run and no
+    scale, so the modes equal those of the valid points bit for bit (CUDA-core
+    spreader in 2D, 3D and f64; tensor-core spreader for 16 vectors)."""
+    d = len(n_modes)
+    rng = np.random.default_rng(count + d)
+    dtype = np.float32 if precision == "f32" else np.float64
+    valid = clustered_points(rng, count, d, centres=3, spread=0.3, dtype=dtype)
+    mixed, index = with_invalid_points(valid, 97)
+    batch = 16 if method == 2 else 1
+    cdtype = np.complex64 if precision == "f32" else np.complex128
+    strengths = complex_normal(rng, (batch, len(mixed)), dtype=cdtype)
+    outs = []
+    for pts, st in ((mixed, strengths), (valid, np.ascontiguousarray(strengths[:, index >= 0]))):
+        config = w.NufftConfig(n_modes, 1e-6 if precision == "f32" else 1e-9, batch=batch, spread_method=method,
+                               precision=w.Precision.F32 if precision == "f32" else w.Precision.F64)
+        plan = w.NufftPlan.type1_gpu(config)
+        out = torch.empty((batch, config.mode_count()), dtype=torch.complex64 if precision == "f32" else torch.complex128,
+                          device=DEV)
+        plan.encode_gpu_batch(batch, to_gpu(pts), to_gpu(st), out)
+        plan.synchronize()
+        outs.append(out.cpu().numpy())
+    view = np.uint32 if precision == "f32" else np.uint64
+    assert np.array_equal(outs[0].view(view), outs[1].view(view))
 
 
 def test_clustered_and_heavy_tiles_match_direct():

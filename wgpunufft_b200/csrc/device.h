@@ -94,7 +94,11 @@ struct SortBuffers {
 // Key kinds: the reference's type-1 stable bins of support starts
 // (src/gpu_nd_bins.rs:474-554), or its type-2 grouped bins of plain-f32
 // position cells (src/gpu_point_bins.rs:422-465).
-enum class KeyKind { SupportStart, ApproximateCell };
+// SupportStartValidFirst: the support-start keys of the points within the
+// fold's reach, and key `bins` (after every bin) for the others, which no
+// spreading tile then reaches; the reference's order, with those points in
+// bin 0, is rebuilt on request (reference_bin_order).
+enum class KeyKind { SupportStart, ApproximateCell, SupportStartValidFirst };
 
 // Sorts `count` points; on return `*perm` and `*sorted_keys` point into the
 // buffers at the permutation and the sorted keys. Writes bin offsets
@@ -103,10 +107,27 @@ void sort_points(const float* points, int64_t count, const GridParams& grid, Key
                  uint64_t bins, SortBuffers buffers, uint32_t* offsets, uint32_t** perm,
                  uint32_t** sorted_keys, cudaStream_t stream, StageTimer* timer = nullptr);
 
-// The same for f64 coordinates folded in native f64 (support-start keys).
+// With KeyKind::SupportStartValidFirst the sort runs over bins + 1 keys and
+// writes bins + 2 offsets (offsets[bins] = points within reach), and
+// `valid_mask` (ceil(count / 32) words, bit i % 32 of word i / 32) marks the
+// points within reach in the caller's order.
+void sort_points_valid_first(const float* points, int64_t count, const GridParams& grid, uint64_t bins,
+                             SortBuffers buffers, uint32_t* offsets, uint32_t* valid_mask, uint32_t** perm,
+                             uint32_t** sorted_keys, cudaStream_t stream, StageTimer* timer = nullptr);
+
+// The same for f64 coordinates folded in native f64 (support-start keys);
+// with `valid_mask` non-null the points outside the fold's reach sort after
+// every bin as above.
 void sort_points64(const double* points, int64_t count, const GridParams& grid, uint64_t bins,
                    SortBuffers buffers, uint32_t* offsets, uint32_t** perm, uint32_t** sorted_keys,
-                   cudaStream_t stream, StageTimer* timer = nullptr);
+                   cudaStream_t stream, StageTimer* timer = nullptr, uint32_t* valid_mask = nullptr);
+
+// The reference's order from a valid-first sort: the points outside the
+// fold's reach merged into bin 0 by original index, and bin offsets that
+// count them in bin 0 (bins + 1 words). `ref_keys` receives the sorted keys.
+void reference_bin_order(const uint32_t* perm, const uint32_t* keys, const uint32_t* offsets, int64_t count,
+                         uint64_t bins, uint32_t* ref_perm, uint32_t* ref_keys, uint32_t* ref_offsets,
+                         cudaStream_t stream);
 
 // The coordinates of `count` points in the bin order `perm`.
 void gather_sorted_points(const float* points, const uint32_t* perm, int64_t count, int dimensions,

@@ -386,7 +386,10 @@ void NufftPlan::configure_tiles() {
   const int w = kernel_.width;
   int64_t tile[3] = {1, 1, 1};
   if (dim_ == 1) tile[0] = 1024;
-  if (dim_ == 2) tile[0] = tile[1] = 32;
+  // 2D f32 register runs (w <= 7) slide along the rows of 64 x 64 tiles:
+  // a thread's range of consecutive records then spans more starts of a row.
+  const bool runs2d = dim_ == 2 && precision_ == B200NUFFT_PRECISION_F32 && 2 * w * w * 4 < 400;
+  if (dim_ == 2) tile[0] = tile[1] = runs2d ? 64 : 32;
   if (dim_ == 3) tile[0] = tile[1] = tile[2] = 16;
   for (int a = 0; a < dim_; ++a) tile[a] = std::min(tile[a], pow2_ceil(fine_[a]));
   // The tensor-core spreader needs one-cell bin rows, column bins of at most
@@ -471,6 +474,23 @@ void NufftPlan::configure_tiles() {
   const int64_t part_cap = dim_ == 3 ? 2048 : (precision_ == B200NUFFT_PRECISION_F32 ? 16384 : kPartCap);
   cap = std::min<int64_t>(part_cap, std::max<int64_t>(256, (cap + 255) / 256 * 256));
   sp.part_cap = static_cast<int32_t>(cap);
+  // The device sizes the parts from the points within reach (the others sort
+  // after every bin), so that such points change no part; the host bounds the
+  // parts for any count up to point_count_: valid / cap(valid) is at most
+  // 4 x 148, or point_count_ / part_cap once the cap saturates.
+  int64_t records_per_cap = 4 * 148;
+  if (type_ == 1) {
+    sp.part_cap_device = static_cast<int32_t*>(part_cap_.reserve(sizeof(int32_t), "part cap"));
+    sp.cap_ctas = 4 * 148;
+    sp.cap_ctas_crowded = 148;
+    sp.cap_max = static_cast<int32_t>(part_cap);
+    sp.crowded_points = runs && one_cell_bins ? 8 * grid_.fine_count : std::numeric_limits<int64_t>::max();
+    sp.cap_bins = bins_;
+    records_per_cap = std::max<int64_t>(4 * 148, (std::max<int64_t>(point_count_, 0) + part_cap - 1) / part_cap);
+  }
+  const int64_t part_bound = type_ == 1 ? sp.tile_count + tiles_per_bin * records_per_cap + 1
+                                        : sp.tile_count + (std::max<int64_t>(point_count_, 0) * tiles_per_bin +
+                                                           sp.part_cap - 1) / sp.part_cap + 1;
   // Candidate (tile, local) pairs of every coordinate of every axis: tile t
   // covers cells (t * tile + l) mod n for l < pad. They depend on the grid
   // and tile shape only, so later point sets reuse them.
@@ -480,8 +500,7 @@ void NufftPlan::configure_tiles() {
       sp.candidate_base[a] = kept_candidate_base[a];
       sp.candidate_count[a] = kept_candidate_count[a];
     }
-    part_upper_bound_ = sp.tile_count + (std::max<int64_t>(point_count_, 0) * tiles_per_bin +
-                                         sp.part_cap - 1) / sp.part_cap + 1;
+    part_upper_bound_ = part_bound;
     return;
   }
   host_candidates_.clear();
@@ -509,10 +528,8 @@ void NufftPlan::configure_tiles() {
   check_cuda(cudaMemcpy(cand, host_candidates_.data(), host_candidates_.size() * sizeof(int2),
                         cudaMemcpyHostToDevice),
              "upload fold candidates");
-  (void)tiles_per_bin;
   spread_.grid = grid_;
-  part_upper_bound_ = sp.tile_count + (std::max<int64_t>(point_count_, 0) * tiles_per_bin +
-                                       sp.part_cap - 1) / sp.part_cap + 1;
+  part_upper_bound_ = part_bound;
 }
 
 int NufftPlan::choose_geometry(int64_t point_count) const {
@@ -576,8 +593,15 @@ void NufftPlan::set_points(int64_t count, const void* points, cudaStream_t strea
   buf.hist = static_cast<uint32_t*>(hist_.get());
   buf.status = static_cast<uint32_t*>(status_.reserve(sort_status_bytes(count), "look-back words"));
   buf.counters = static_cast<uint32_t*>(counters_.get());
-  uint32_t* offsets =
-      static_cast<uint32_t*>(offsets_.reserve((bins_ + 1) * sizeof(uint32_t), "bin offsets"));
+  // Type-1 plans sort the points outside the fold's reach after every bin
+  // (one more offset word) and mark the others in valid_mask_.
+  const bool valid_first = type_ == 1;
+  uint32_t* offsets = static_cast<uint32_t*>(
+      offsets_.reserve((bins_ + (valid_first ? 2 : 1)) * sizeof(uint32_t), "bin offsets"));
+  uint32_t* valid_mask = valid_first ? static_cast<uint32_t*>(valid_mask_.reserve(
+                                           static_cast<size_t>((std::max<int64_t>(count, 1) + 31) / 32) * sizeof(uint32_t),
+                                           "reach mask"))
+                                     : nullptr;
   const size_t sorted_bytes = static_cast<size_t>(std::max<int64_t>(count, 1)) * dim_ * scalar_bytes();
   if (precision_ == B200NUFFT_PRECISION_F32) {
     tc2_active_ = tc2_enabled_ && tc_interp_supported(grid_);
@@ -615,9 +639,13 @@ void NufftPlan::set_points(int64_t count, const void* points, cudaStream_t strea
       tc_interp_prepare(tc2_grid_, p, stream);
       tc2_part_upper_bound_ = tiles + chunk_bound / kTi2ChunksPerPart + 1;
     }
-    sort_points(static_cast<const float*>(points), count, grid_,
-                type_ == 1 ? KeyKind::SupportStart : KeyKind::ApproximateCell, bins_, buf, offsets,
-                &perm_, &sorted_keys_, stream, &timer_);
+    if (valid_first) {
+      sort_points_valid_first(static_cast<const float*>(points), count, grid_, bins_, buf, offsets, valid_mask,
+                              &perm_, &sorted_keys_, stream, &timer_);
+    } else {
+      sort_points(static_cast<const float*>(points), count, grid_, KeyKind::ApproximateCell, bins_, buf, offsets,
+                  &perm_, &sorted_keys_, stream, &timer_);
+    }
     float* sorted = static_cast<float*>(sorted_points_.reserve(sorted_bytes, "sorted coordinates"));
     gather_sorted_points(static_cast<const float*>(points), perm_, count, dim_, sorted, stream,
                          &timer_);
@@ -639,7 +667,7 @@ void NufftPlan::set_points(int64_t count, const void* points, cudaStream_t strea
       points64 = converted;
     }
     sort_points64(points64, count, grid_, bins_, buf, offsets, &perm_, &sorted_keys_, stream,
-                  &timer_);
+                  &timer_, valid_mask);
     double* sorted = static_cast<double*>(sorted_points_.reserve(sorted_bytes, "sorted coordinates"));
     gather_sorted_points64(points64, perm_, count, dim_, sorted, stream, &timer_);
   }
@@ -796,6 +824,7 @@ void NufftPlan::execute_f32(int batch, const void* input, void* output, uint64_t
     l.scratch = static_cast<float2*>(scratch_.reserve(scratch_bytes, "spreading tiles"));
     l.candidates = static_cast<const int2*>(candidates_.get());
     l.fine = fine;
+    l.valid_mask = static_cast<const uint32_t*>(valid_mask_.get());
     spread_execute(spread_, l, stream, &timer_);
     run_fft(fine, batch, direction, stream);
     StageScope scope(&timer_, kStageDeconvolution, stream);
@@ -910,6 +939,7 @@ void NufftPlan::execute_f64(int batch, const void* input, void* output, uint64_t
     l.scratch = static_cast<double2*>(scratch_.reserve(scratch_bytes, "spreading tiles"));
     l.candidates = static_cast<const int2*>(candidates_.get());
     l.fine = fine;
+    l.valid_mask = static_cast<const uint32_t*>(valid_mask_.get());
     spread_execute64(spread_, l, stream, &timer_);
     run_fft(fine, batch, direction, stream);
     StageScope scope(&timer_, kStageDeconvolution, stream);
@@ -1081,6 +1111,7 @@ void NufftPlan::spread_to(int64_t active_batch, const void* strengths, void* gri
         "spreading tiles"));
     l.candidates = static_cast<const int2*>(candidates_.get());
     l.fine = static_cast<float2*>(grid);
+    l.valid_mask = static_cast<const uint32_t*>(valid_mask_.get());
     spread_execute(spread_, l, stream, &timer_);
   } else {
     SpreadLaunch64 l;
@@ -1098,6 +1129,7 @@ void NufftPlan::spread_to(int64_t active_batch, const void* strengths, void* gri
         "spreading tiles"));
     l.candidates = static_cast<const int2*>(candidates_.get());
     l.fine = static_cast<double2*>(grid);
+    l.valid_mask = static_cast<const uint32_t*>(valid_mask_.get());
     spread_execute64(spread_, l, stream, &timer_);
   }
   check_cuda(cudaGetLastError(), "spread launch");
@@ -1109,16 +1141,35 @@ void NufftPlan::copy_bin_order(uint32_t* permutation, uint32_t* bin_offsets, cud
   if (point_count_ < 0) {
     throw NufftFailure{B200NUFFT_GPU_EXECUTION_UNAVAILABLE, "no point set"};
   }
+  const uint32_t* order = perm_;
+  const uint32_t* offsets = static_cast<const uint32_t*>(offsets_.get());
+  if (type_ == 1) {
+    // Type-1 points outside the fold's reach were sorted after every bin:
+    // the reference's order holds them in bin 0.
+    reference_order(stream);
+    order = static_cast<const uint32_t*>(ref_perm_.get());
+    offsets = static_cast<const uint32_t*>(ref_offsets_.get());
+  }
   if (permutation && point_count_ > 0) {
-    check_cuda(cudaMemcpyAsync(permutation, perm_, point_count_ * sizeof(uint32_t),
+    check_cuda(cudaMemcpyAsync(permutation, order, point_count_ * sizeof(uint32_t),
                                cudaMemcpyDeviceToDevice, stream),
                "copy permutation");
   }
   if (bin_offsets) {
-    check_cuda(cudaMemcpyAsync(bin_offsets, offsets_.get(), (bins_ + 1) * sizeof(uint32_t),
+    check_cuda(cudaMemcpyAsync(bin_offsets, offsets, (bins_ + 1) * sizeof(uint32_t),
                                cudaMemcpyDeviceToDevice, stream),
                "copy bin offsets");
   }
+}
+
+void NufftPlan::reference_order(cudaStream_t stream) {
+  const size_t words = static_cast<size_t>(std::max<int64_t>(point_count_, 1));
+  uint32_t* ref_perm = static_cast<uint32_t*>(ref_perm_.reserve(words * sizeof(uint32_t), "reference order"));
+  uint32_t* ref_keys = static_cast<uint32_t*>(ref_keys_.reserve(words * sizeof(uint32_t), "reference keys"));
+  uint32_t* ref_offsets =
+      static_cast<uint32_t*>(ref_offsets_.reserve((bins_ + 1) * sizeof(uint32_t), "reference bin offsets"));
+  reference_bin_order(perm_, sorted_keys_, static_cast<const uint32_t*>(offsets_.get()), point_count_, bins_,
+                      ref_perm, ref_keys, ref_offsets, stream);
 }
 
 void NufftPlan::copy_prepared_slots(int32_t* starts, float* offsets, cudaStream_t stream) {
@@ -1128,8 +1179,10 @@ void NufftPlan::copy_prepared_slots(int32_t* starts, float* offsets, cudaStream_
     throw NufftFailure{B200NUFFT_GPU_EXECUTION_UNAVAILABLE, "no type-1 point set"};
   }
   if (!starts || !offsets) throw NufftFailure{B200NUFFT_INVALID_ARGUMENT, "null buffer"};
-  prepare_reference_slots(static_cast<const float*>(points_), point_count_, grid_, perm_,
-                          sorted_keys_, starts, offsets, stream);
+  reference_order(stream);
+  prepare_reference_slots(static_cast<const float*>(points_), point_count_, grid_,
+                          static_cast<const uint32_t*>(ref_perm_.get()), static_cast<const uint32_t*>(ref_keys_.get()),
+                          starts, offsets, stream);
 }
 
 void NufftPlan::synchronize(cudaStream_t stream) {

@@ -60,6 +60,9 @@ class NufftPlan {
   void configure_bins(int geometry);
   void configure_type2_bins();
   void configure_tiles();
+  // The reference's bin order of a type-1 point set (ref_perm_, ref_keys_,
+  // ref_offsets_): its points outside the fold's reach back in bin 0.
+  void reference_order(cudaStream_t stream);
   cufftHandle fft_for(int batch);
   void run_fft(void* fine, int batch, int direction, cudaStream_t stream);
   void execute_f32(int batch, const void* input, void* output, uint64_t out_bytes,
@@ -116,6 +119,9 @@ class NufftPlan {
   uint32_t* sorted_keys_ = nullptr;
   DeviceBuffer keys_a_, keys_b_, vals_a_, vals_b_, hist_, status_, counters_, offsets_;
   DeviceBuffer sorted_points_;
+  DeviceBuffer valid_mask_;  // type-1 plans: points within the fold's reach, caller order
+  DeviceBuffer ref_perm_, ref_keys_, ref_offsets_;  // type-1 plans: the reference's order, on request
+  DeviceBuffer part_cap_;    // type-1 plans: records per part, sized on the device
   DeviceBuffer windows_;  // f32 plans: PreparedWindow per slot
   DeviceBuffer inverse_;  // batched 2D f32 type-2 plans: slot of every point
   DeviceBuffer staged_;   // batched 2D f32 type-2 plans: values in slot order

@@ -83,26 +83,49 @@ __device__ __forceinline__ uint32_t approximate_cell_key(const float* p, const G
   return key;
 }
 
-// Computes every point's key and the digit histograms of all passes.
+// Computes every point's key and the digit histograms of all passes. A warp
+// takes 32 consecutive points per iteration; with valid-first keys its
+// ballot of the points within reach is one word of `valid_mask`.
 template <int D, KeyKind K>
 __global__ void __launch_bounds__(256) bin_keys_kernel(const float* __restrict__ points,
                                                        int64_t count, GridParams g,
                                                        uint32_t* __restrict__ keys,
-                                                       uint32_t* __restrict__ hist, int passes) {
+                                                       uint32_t* __restrict__ hist, int passes,
+                                                       uint32_t invalid_key, uint32_t* __restrict__ valid_mask) {
   __shared__ uint32_t local[4][kRadix];
   for (int i = threadIdx.x; i < 4 * kRadix; i += blockDim.x) (&local[0][0])[i] = 0;
   __syncthreads();
+  const int lane = threadIdx.x & 31;
   const int64_t stride = static_cast<int64_t>(gridDim.x) * blockDim.x;
-  for (int64_t i = static_cast<int64_t>(blockIdx.x) * blockDim.x + threadIdx.x; i < count;
-       i += stride) {
-    float p[D];
+  for (int64_t base = static_cast<int64_t>(blockIdx.x) * blockDim.x + (threadIdx.x & ~31); base < count;
+       base += stride) {
+    const int64_t i = base + lane;
+    const bool inside = i < count;
+    bool reach = false;
+    uint32_t key = 0;
+    if (inside) {
+      float p[D];
 #pragma unroll
-    for (int a = 0; a < D; ++a) p[a] = points[i * D + a];
-    const uint32_t key =
-        K == KeyKind::SupportStart ? support_start_key<D>(p, g) : approximate_cell_key<D>(p, g);
-    keys[i] = key;
-    for (int pass = 0; pass < passes; ++pass) {
-      atomicAdd(&local[pass][(key >> (8 * pass)) & 0xFF], 1u);
+      for (int a = 0; a < D; ++a) p[a] = points[i * D + a];
+      if constexpr (K == KeyKind::ApproximateCell) {
+        key = approximate_cell_key<D>(p, g);
+      } else {
+        key = support_start_key<D>(p, g);
+        reach = true;
+#pragma unroll
+        for (int a = 0; a < D; ++a) reach = reach && in_fold_reach(p[a]);
+        if (K == KeyKind::SupportStartValidFirst && !reach) key = invalid_key;
+      }
+    }
+    if constexpr (K == KeyKind::SupportStartValidFirst) {
+      const uint32_t ballot = __ballot_sync(0xFFFFFFFFu, reach);
+      if (lane == 0) valid_mask[base >> 5] = ballot;
+    }
+    if (inside) {
+      keys[i] = key;
+      for (int pass = 0; pass < passes; ++pass) {
+        atomicAdd(&local[pass][(key >> (8 * pass)) & 0xFF], 1u);
+      }
     }
   }
   __syncthreads();
@@ -118,34 +141,47 @@ template <int D>
 __global__ void __launch_bounds__(256) bin_keys64_kernel(const double* __restrict__ points,
                                                          int64_t count, GridParams g,
                                                          uint32_t* __restrict__ keys,
-                                                         uint32_t* __restrict__ hist, int passes) {
+                                                         uint32_t* __restrict__ hist, int passes,
+                                                         uint32_t invalid_key, uint32_t* __restrict__ valid_mask) {
   __shared__ uint32_t local[4][kRadix];
   for (int i = threadIdx.x; i < 4 * kRadix; i += blockDim.x) (&local[0][0])[i] = 0;
   __syncthreads();
+  const int lane = threadIdx.x & 31;
   const int64_t stride = static_cast<int64_t>(gridDim.x) * blockDim.x;
-  for (int64_t i = static_cast<int64_t>(blockIdx.x) * blockDim.x + threadIdx.x; i < count;
-       i += stride) {
-    double p[D];
-    bool reach = true;
-#pragma unroll
-    for (int a = 0; a < D; ++a) {
-      p[a] = points[i * D + a];
-      reach = reach && in_fold_reach64(p[a]);
-    }
+  for (int64_t base = static_cast<int64_t>(blockIdx.x) * blockDim.x + (threadIdx.x & ~31); base < count;
+       base += stride) {
+    const int64_t i = base + lane;
+    const bool inside = i < count;
+    bool reach = inside;
     uint32_t key = 0;
+    if (inside) {
+      double p[D];
 #pragma unroll
-    for (int a = 0; a < D; ++a) {
-      int32_t start = 0;
-      if (reach) {
-        double offset;
-        support_of64(p[a], g.axis64[a], g.half_width64, start, offset);
+      for (int a = 0; a < D; ++a) {
+        p[a] = points[i * D + a];
+        reach = reach && in_fold_reach64(p[a]);
       }
-      const int32_t wrapped = wrap_start(start, g.axis[a].length);
-      key += (static_cast<uint32_t>(wrapped) >> g.axis[a].shift) * g.axis[a].stride;
+#pragma unroll
+      for (int a = 0; a < D; ++a) {
+        int32_t start = 0;
+        if (reach) {
+          double offset;
+          support_of64(p[a], g.axis64[a], g.half_width64, start, offset);
+        }
+        const int32_t wrapped = wrap_start(start, g.axis[a].length);
+        key += (static_cast<uint32_t>(wrapped) >> g.axis[a].shift) * g.axis[a].stride;
+      }
+      if (valid_mask != nullptr && !reach) key = invalid_key;
     }
-    keys[i] = key;
-    for (int pass = 0; pass < passes; ++pass) {
-      atomicAdd(&local[pass][(key >> (8 * pass)) & 0xFF], 1u);
+    if (valid_mask != nullptr) {
+      const uint32_t ballot = __ballot_sync(0xFFFFFFFFu, reach);
+      if (lane == 0) valid_mask[base >> 5] = ballot;
+    }
+    if (inside) {
+      keys[i] = key;
+      for (int pass = 0; pass < passes; ++pass) {
+        atomicAdd(&local[pass][(key >> (8 * pass)) & 0xFF], 1u);
+      }
     }
   }
   __syncthreads();
@@ -435,16 +471,60 @@ __global__ void prepare_slots_kernel(const float* __restrict__ points, int64_t c
 
 template <int D>
 void launch_keys(const float* points, int64_t count, const GridParams& g, KeyKind kind,
-                 uint32_t* keys, uint32_t* hist, int passes, cudaStream_t stream) {
+                 uint32_t* keys, uint32_t* hist, int passes, uint32_t invalid_key, uint32_t* valid_mask,
+                 cudaStream_t stream) {
   const int blocks = static_cast<int>(std::min<int64_t>((count + 255) / 256, 148 * 16));
   if (kind == KeyKind::SupportStart) {
     bin_keys_kernel<D, KeyKind::SupportStart>
-        <<<blocks, 256, 0, stream>>>(points, count, g, keys, hist, passes);
+        <<<blocks, 256, 0, stream>>>(points, count, g, keys, hist, passes, 0u, nullptr);
+  } else if (kind == KeyKind::SupportStartValidFirst) {
+    bin_keys_kernel<D, KeyKind::SupportStartValidFirst>
+        <<<blocks, 256, 0, stream>>>(points, count, g, keys, hist, passes, invalid_key, valid_mask);
   } else {
     bin_keys_kernel<D, KeyKind::ApproximateCell>
-        <<<blocks, 256, 0, stream>>>(points, count, g, keys, hist, passes);
+        <<<blocks, 256, 0, stream>>>(points, count, g, keys, hist, passes, 0u, nullptr);
   }
   note_launch();
+}
+
+// The reference order from a valid-first order: with a = points in bin 0,
+// v = points within reach (offsets[bins]) and M points, slot s < a (bin 0)
+// and slot s >= v (outside the reach, after every bin) hold two index-sorted
+// runs merged into the reference's bin 0; slots a <= s < v move up by M - v.
+__global__ void reference_order_kernel(const uint32_t* __restrict__ perm, const uint32_t* __restrict__ keys,
+                                       const uint32_t* __restrict__ offsets, int64_t count, uint64_t bins,
+                                       uint32_t* __restrict__ ref_perm, uint32_t* __restrict__ ref_keys) {
+  const int64_t s = static_cast<int64_t>(blockIdx.x) * blockDim.x + threadIdx.x;
+  if (s >= count) return;
+  const int64_t a = offsets[1 < bins ? 1 : bins];
+  const int64_t v = offsets[bins];
+  const int64_t invalid = count - v;
+  const uint32_t x = perm[s];
+  int64_t dst;
+  if (s < a || s >= v) {
+    // Rank among the other run: the number of its indices below x.
+    const bool first_run = s < a;
+    int64_t low = first_run ? v : 0, high = first_run ? count : a;
+    const int64_t begin = low;
+    while (low < high) {
+      const int64_t mid = (low + high) >> 1;
+      if (perm[mid] < x) low = mid + 1; else high = mid;
+    }
+    dst = (first_run ? s : s - v) + (low - begin);
+    ref_keys[dst] = 0u;
+  } else {
+    dst = s + invalid;
+    ref_keys[dst] = keys[s];
+  }
+  ref_perm[dst] = x;
+}
+
+__global__ void reference_offsets_kernel(const uint32_t* __restrict__ offsets, int64_t count, uint64_t bins,
+                                         uint32_t* __restrict__ ref_offsets) {
+  const int64_t b = static_cast<int64_t>(blockIdx.x) * blockDim.x + threadIdx.x;
+  if (b > static_cast<int64_t>(bins)) return;
+  const uint32_t invalid = static_cast<uint32_t>(count) - offsets[bins];
+  ref_offsets[b] = b == 0 ? 0u : offsets[b] + invalid;
 }
 
 }  // namespace
@@ -560,10 +640,12 @@ void sort_from_keys(int64_t count, uint64_t bins, int passes, SortBuffers buf, u
 
 void sort_points64(const double* points, int64_t count, const GridParams& g, uint64_t bins,
                    SortBuffers buf, uint32_t* offsets, uint32_t** perm, uint32_t** sorted_keys,
-                   cudaStream_t stream, StageTimer* timer) {
-  const int passes = radix_passes(bins);
+                   cudaStream_t stream, StageTimer* timer, uint32_t* valid_mask) {
+  // Valid-first keys add one key after the bins.
+  const uint64_t keys_range = valid_mask != nullptr ? bins + 1 : bins;
+  const int passes = radix_passes(keys_range);
   if (count == 0) {
-    check_cuda(cudaMemsetAsync(offsets, 0, (bins + 1) * sizeof(uint32_t), stream), "clear offsets");
+    check_cuda(cudaMemsetAsync(offsets, 0, (keys_range + 1) * sizeof(uint32_t), stream), "clear offsets");
     *perm = buf.vals_a;
     *sorted_keys = buf.keys_a;
     return;
@@ -573,22 +655,36 @@ void sort_points64(const double* points, int64_t count, const GridParams& g, uin
     check_cuda(cudaMemsetAsync(buf.hist, 0, 4 * kRadix * sizeof(uint32_t), stream), "clear histogram");
     check_cuda(cudaMemsetAsync(buf.counters, 0, 7 * sizeof(uint32_t), stream), "clear tickets");
     const int blocks = static_cast<int>(std::min<int64_t>((count + 255) / 256, 148 * 16));
+    const uint32_t invalid_key = static_cast<uint32_t>(bins);
     switch (g.dimensions) {
-      case 1: bin_keys64_kernel<1><<<blocks, 256, 0, stream>>>(points, count, g, buf.keys_a, buf.hist, passes); break;
-      case 2: bin_keys64_kernel<2><<<blocks, 256, 0, stream>>>(points, count, g, buf.keys_a, buf.hist, passes); break;
-      default: bin_keys64_kernel<3><<<blocks, 256, 0, stream>>>(points, count, g, buf.keys_a, buf.hist, passes); break;
+      case 1:
+        bin_keys64_kernel<1><<<blocks, 256, 0, stream>>>(points, count, g, buf.keys_a, buf.hist, passes,
+                                                         invalid_key, valid_mask);
+        break;
+      case 2:
+        bin_keys64_kernel<2><<<blocks, 256, 0, stream>>>(points, count, g, buf.keys_a, buf.hist, passes,
+                                                         invalid_key, valid_mask);
+        break;
+      default:
+        bin_keys64_kernel<3><<<blocks, 256, 0, stream>>>(points, count, g, buf.keys_a, buf.hist, passes,
+                                                         invalid_key, valid_mask);
+        break;
     }
     note_launch();
   }
-  sort_from_keys(count, bins, passes, buf, offsets, perm, sorted_keys, stream, timer);
+  sort_from_keys(count, keys_range, passes, buf, offsets, perm, sorted_keys, stream, timer);
 }
 
-void sort_points(const float* points, int64_t count, const GridParams& g, KeyKind kind,
-                 uint64_t bins, SortBuffers buf, uint32_t* offsets, uint32_t** perm,
-                 uint32_t** sorted_keys, cudaStream_t stream, StageTimer* timer) {
-  const int passes = radix_passes(bins);
+namespace {
+
+void sort_points_kind(const float* points, int64_t count, const GridParams& g, KeyKind kind, uint64_t bins,
+                      SortBuffers buf, uint32_t* offsets, uint32_t* valid_mask, uint32_t** perm,
+                      uint32_t** sorted_keys, cudaStream_t stream, StageTimer* timer) {
+  // Valid-first keys add one key after the bins.
+  const uint64_t keys_range = kind == KeyKind::SupportStartValidFirst ? bins + 1 : bins;
+  const int passes = radix_passes(keys_range);
   if (count == 0) {
-    check_cuda(cudaMemsetAsync(offsets, 0, (bins + 1) * sizeof(uint32_t), stream), "clear offsets");
+    check_cuda(cudaMemsetAsync(offsets, 0, (keys_range + 1) * sizeof(uint32_t), stream), "clear offsets");
     *perm = buf.vals_a;
     *sorted_keys = buf.keys_a;
     return;
@@ -597,13 +693,42 @@ void sort_points(const float* points, int64_t count, const GridParams& g, KeyKin
     StageScope scope(timer, kStageBinKeys, stream);
     check_cuda(cudaMemsetAsync(buf.hist, 0, 4 * kRadix * sizeof(uint32_t), stream), "clear histogram");
     check_cuda(cudaMemsetAsync(buf.counters, 0, 7 * sizeof(uint32_t), stream), "clear tickets");
+    const uint32_t invalid_key = static_cast<uint32_t>(bins);
     switch (g.dimensions) {
-      case 1: launch_keys<1>(points, count, g, kind, buf.keys_a, buf.hist, passes, stream); break;
-      case 2: launch_keys<2>(points, count, g, kind, buf.keys_a, buf.hist, passes, stream); break;
-      default: launch_keys<3>(points, count, g, kind, buf.keys_a, buf.hist, passes, stream); break;
+      case 1: launch_keys<1>(points, count, g, kind, buf.keys_a, buf.hist, passes, invalid_key, valid_mask, stream); break;
+      case 2: launch_keys<2>(points, count, g, kind, buf.keys_a, buf.hist, passes, invalid_key, valid_mask, stream); break;
+      default: launch_keys<3>(points, count, g, kind, buf.keys_a, buf.hist, passes, invalid_key, valid_mask, stream); break;
     }
   }
-  sort_from_keys(count, bins, passes, buf, offsets, perm, sorted_keys, stream, timer);
+  sort_from_keys(count, keys_range, passes, buf, offsets, perm, sorted_keys, stream, timer);
+}
+
+}  // namespace
+
+void sort_points(const float* points, int64_t count, const GridParams& g, KeyKind kind,
+                 uint64_t bins, SortBuffers buf, uint32_t* offsets, uint32_t** perm,
+                 uint32_t** sorted_keys, cudaStream_t stream, StageTimer* timer) {
+  sort_points_kind(points, count, g, kind, bins, buf, offsets, nullptr, perm, sorted_keys, stream, timer);
+}
+
+void sort_points_valid_first(const float* points, int64_t count, const GridParams& g, uint64_t bins,
+                             SortBuffers buf, uint32_t* offsets, uint32_t* valid_mask, uint32_t** perm,
+                             uint32_t** sorted_keys, cudaStream_t stream, StageTimer* timer) {
+  sort_points_kind(points, count, g, KeyKind::SupportStartValidFirst, bins, buf, offsets, valid_mask, perm,
+                   sorted_keys, stream, timer);
+}
+
+void reference_bin_order(const uint32_t* perm, const uint32_t* keys, const uint32_t* offsets, int64_t count,
+                         uint64_t bins, uint32_t* ref_perm, uint32_t* ref_keys, uint32_t* ref_offsets,
+                         cudaStream_t stream) {
+  if (count > 0) {
+    reference_order_kernel<<<static_cast<unsigned>((count + 255) / 256), 256, 0, stream>>>(
+        perm, keys, offsets, count, bins, ref_perm, ref_keys);
+    note_launch();
+  }
+  reference_offsets_kernel<<<static_cast<unsigned>((bins + 1 + 255) / 256), 256, 0, stream>>>(offsets, count, bins,
+                                                                                              ref_offsets);
+  note_launch();
 }
 
 namespace {

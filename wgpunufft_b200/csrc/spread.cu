@@ -138,19 +138,40 @@ struct SpreadLaunchT {
   typename T::Complex* scratch;
   const int2* candidates;
   typename T::Complex* fine;
+  const uint32_t* valid_mask;
 };
 
-// Largest |re| or |im| of every strength vector, as magnitude bits.
+// Records per part of this point set.
+__device__ __forceinline__ int32_t part_cap_of(const SpreadParams& sp) {
+  return sp.part_cap_device != nullptr ? *sp.part_cap_device : sp.part_cap;
+}
+
+// The part cap from the number of points within reach (SpreadParams).
+__global__ void part_cap_kernel(SpreadParams sp, const uint32_t* __restrict__ offsets) {
+  const long long valid = offsets[sp.cap_bins];
+  const long long ctas = valid >= sp.crowded_points ? sp.cap_ctas_crowded : sp.cap_ctas;
+  long long cap = ((valid > 1 ? valid : 1ll) + ctas - 1) / ctas;
+  cap = (cap + 255) / 256 * 256;
+  cap = cap < 256 ? 256 : cap;
+  cap = cap > sp.cap_max ? static_cast<long long>(sp.cap_max) : cap;
+  *sp.part_cap_device = static_cast<int32_t>(cap);
+}
+
+// Largest |re| or |im| of every strength vector, as magnitude bits, over
+// the points within reach when a mask is given (others get zero weight, so
+// their strengths must not change the fixed-point scale).
 template <typename T>
 __global__ void strength_magnitude_kernel(const typename T::Complex* __restrict__ values,
                                           int64_t count, int batch,
-                                          typename T::Bits* __restrict__ max_bits) {
+                                          typename T::Bits* __restrict__ max_bits,
+                                          const uint32_t* __restrict__ valid_mask) {
   const int b = blockIdx.y;
   const typename T::Complex* v = values + static_cast<int64_t>(b) * count;
   typename T::Bits m = 0;
   const int64_t stride = static_cast<int64_t>(gridDim.x) * blockDim.x;
   for (int64_t i = static_cast<int64_t>(blockIdx.x) * blockDim.x + threadIdx.x; i < count;
        i += stride) {
+    if (valid_mask != nullptr && !((__ldg(&valid_mask[i >> 5]) >> (i & 31)) & 1u)) continue;
     const typename T::Complex s = v[i];
     m = max(m, T::magnitude_bits(s.x));
     m = max(m, T::magnitude_bits(s.y));
@@ -188,7 +209,8 @@ __global__ void tile_records_kernel(SpreadParams sp, const uint32_t* __restrict_
       count += offsets[row + hi[0] + 1] - offsets[row + lo[0]];
     }
   }
-  parts[t] = static_cast<uint32_t>((count + sp.part_cap - 1) / sp.part_cap);
+  const uint32_t cap = static_cast<uint32_t>(part_cap_of(sp));
+  parts[t] = static_cast<uint32_t>((count + cap - 1) / cap);
 }
 
 // Exclusive scan of the parts per tile in one block; part_start[tile_count]
@@ -345,6 +367,30 @@ __device__ __forceinline__ void flush_run(typename T::Word* acc, int padded, int
       T::add(acc, padded, 1, base + i, ai[j][i]);
       ar[j][i] = ai[j][i] = typename T::Real(0);
     }
+  }
+}
+
+// 2D register windows slide along x: when a thread's next record starts
+// d columns to the right in the same row, the d leftmost window columns are
+// complete (no later record of the thread's range reaches them), so they
+// are added to the tile and the window shifts left, instead of adding all
+// w^2 cells at every change of start. Records of one-cell bins come in
+// (row, column) order, so a thread's range of consecutive records flushes
+// about one column per distinct start.
+template <int W, typename T>
+__device__ __forceinline__ void flush_first_column(typename T::Word* acc, int padded, int pad0, int x, int y,
+                                                   typename T::Real (*ar)[W], typename T::Real (*ai)[W]) {
+#pragma unroll
+  for (int j = 0; j < W; ++j) {
+    const int c = (y + j) * pad0 + x;
+    T::add(acc, padded, 0, c, ar[j][0]);
+    T::add(acc, padded, 1, c, ai[j][0]);
+#pragma unroll
+    for (int i = 0; i + 1 < W; ++i) {
+      ar[j][i] = ar[j][i + 1];
+      ai[j][i] = ai[j][i + 1];
+    }
+    ar[j][W - 1] = ai[j][W - 1] = typename T::Real(0);
   }
 }
 
@@ -907,8 +953,9 @@ __global__ void __launch_bounds__(kSpreadThreads, spread_min_blocks<D, W, T>()) 
   }
   __syncthreads();
   const uint32_t tile_total = row_prefix[rows];
-  const uint32_t record_begin = part_in_tile * static_cast<uint32_t>(sp.part_cap);
-  const uint32_t record_end = min(tile_total, record_begin + static_cast<uint32_t>(sp.part_cap));
+  const uint32_t part_cap = static_cast<uint32_t>(part_cap_of(sp));
+  const uint32_t record_begin = part_in_tile * part_cap;
+  const uint32_t record_end = min(tile_total, record_begin + part_cap);
   // Runs of records with one support start add up in registers first (a
   // fixed order within the run) and reach the fixed-point tile once per run,
   // which leaves that much headroom in the scale.
@@ -1068,7 +1115,17 @@ __global__ void __launch_bounds__(kSpreadThreads, spread_min_blocks<D, W, T>()) 
         s.x = (s.x * scale_lo) * scale_hi;
         s.y = (s.y * scale_lo) * scale_hi;
         const int l1 = D == 2 ? local_start[D - 1] : 0;
-        if (local_start[0] != run0 || l1 != run1) {
+        if constexpr (D == 2) {
+          const int l0 = local_start[0];
+          if (run0 >= 0 && l1 == run1 && l0 > run0 && l0 < run0 + W) {
+            // Same row, a few columns on: flush and drop the passed columns.
+            for (; run0 < l0; ++run0) flush_first_column<W, T>(acc, padded, sp.pad[0], run0, run1, ar, ai);
+          } else if (l0 != run0 || l1 != run1) {
+            if (run0 >= 0) flush_run<D, W, T>(acc, padded, sp.pad[0], run0, run1, ar, ai);
+            run0 = l0;
+            run1 = l1;
+          }
+        } else if (local_start[0] != run0 || l1 != run1) {
           if (run0 >= 0) flush_run<D, W, T>(acc, padded, sp.pad[0], run0, run1, ar, ai);
           run0 = local_start[0];
           run1 = l1;
@@ -1372,7 +1429,7 @@ void spread_execute_impl(const SpreadParams& sp, const SpreadLaunchT<T>& l, cuda
       const unsigned blocks =
           static_cast<unsigned>(std::min<int64_t>((l.point_count + 255) / 256, 148 * 8));
       strength_magnitude_kernel<T><<<dim3(blocks, l.batch), 256, 0, stream>>>(
-          l.strengths, l.point_count, l.batch, l.max_bits);
+          l.strengths, l.point_count, l.batch, l.max_bits, l.valid_mask);
       note_launch();
     }
     StageScope scope(timer, kStageSpread, stream);
@@ -1391,6 +1448,10 @@ void spread_execute_impl(const SpreadParams& sp, const SpreadLaunchT<T>& l, cuda
 void spread_count_parts(const SpreadParams& sp, const uint32_t* offsets, uint32_t* parts,
                         uint32_t* part_start, cudaStream_t stream, StageTimer* timer) {
   StageScope scope(timer, kStageTileParts, stream);
+  if (sp.part_cap_device != nullptr) {
+    part_cap_kernel<<<1, 1, 0, stream>>>(sp, offsets);
+    note_launch();
+  }
   const unsigned blocks = static_cast<unsigned>((sp.tile_count + 255) / 256);
   switch (sp.grid.dimensions) {
     case 1: tile_records_kernel<1><<<blocks, 256, 0, stream>>>(sp, offsets, parts); break;
@@ -1410,7 +1471,7 @@ void spread_execute(const SpreadParams& sp, const SpreadLaunch& l, cudaStream_t 
                     StageTimer* timer) {
   SpreadLaunchT<F32Traits> t{l.points,   l.windows,  l.strengths,        l.point_count, l.batch,
                              l.perm,     l.offsets,          l.part_start,  l.part_upper_bound,
-                             l.max_bits, l.scratch,          l.candidates,  l.fine};
+                             l.max_bits, l.scratch,          l.candidates,  l.fine, l.valid_mask};
   spread_execute_impl<F32Traits>(sp, t, stream, timer);
 }
 
@@ -1467,7 +1528,7 @@ void spread_execute64(const SpreadParams& sp, const SpreadLaunch64& l, cudaStrea
                       StageTimer* timer) {
   SpreadLaunchT<F64Traits> t{l.points,   nullptr,    l.strengths,        l.point_count, l.batch,
                              l.perm,     l.offsets,          l.part_start,  l.part_upper_bound,
-                             l.max_bits, l.scratch,          l.candidates,  l.fine};
+                             l.max_bits, l.scratch,          l.candidates,  l.fine, l.valid_mask};
   spread_execute_impl<F64Traits>(sp, t, stream, timer);
 }
 

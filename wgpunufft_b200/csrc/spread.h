@@ -24,6 +24,17 @@ struct SpreadParams {
   int64_t tile_count;
   int32_t padded_cells;
   int32_t part_cap;     // records per part, at most
+  // Plans whose out-of-reach points sort after every bin size their parts
+  // on the device from the number of points within reach (offsets[cap_bins]):
+  // part_cap_device receives min(cap_max, max(256, ceil(valid / ctas)
+  // rounded up to 256)), ctas = cap_ctas_crowded when valid >=
+  // crowded_points, else cap_ctas; null keeps the host's part_cap.
+  int32_t* part_cap_device;
+  int32_t cap_ctas;
+  int32_t cap_ctas_crowded;
+  int32_t cap_max;
+  int64_t crowded_points;
+  uint64_t cap_bins;
   // For each axis, candidate (tile, local) pairs of every coordinate:
   // candidate_count[a] entries per coordinate from candidate_base[a], ended
   // by a negative tile when fewer.
@@ -81,6 +92,9 @@ struct SpreadLaunch {
   float2* scratch;       // part_upper_bound * batch * padded_cells
   const int2* candidates;
   float2* fine;          // batch * fine_count
+  // Points within the fold's reach in the caller's order (bit i % 32 of word
+  // i / 32); null: every strength sets the fixed-point scale.
+  const uint32_t* valid_mask;
 };
 
 // The f64 plan's launch: double coordinates and complex128 values.
@@ -97,6 +111,7 @@ struct SpreadLaunch64 {
   double2* scratch;
   const int2* candidates;
   double2* fine;
+  const uint32_t* valid_mask;
 };
 
 // Parts of every tile and their exclusive scan (tile_count + 1 words).
