@@ -342,6 +342,29 @@ const char *b200nufft_last_error(void);
 /* The library version. */
 const char *b200nufft_version(void);
 
+/* Launch choices of the type-1 spreader and the tensor-core paths. This has
+ * no counterpart in the reference, which fixes them per rank and precision
+ * (src/gpu_nd_spread.rs:55-135,562-593); here a table measured on a B200
+ * (wgpunufft_b200/tune.py) holds them per workload key: plan type,
+ * dimension, precision, window width, log2 of the fine-grid cells and log2
+ * of the points per cell. Plans look the key up at set_points, so a key
+ * always gets the same choices and outputs stay bitwise repeatable. */
+typedef struct b200nufft_tuning {
+  int32_t tile;                /* spreading tile side in cells (power of two) */
+  int32_t ctas_per_sm;         /* CTAs per SM the tile parts are sized for */
+  int32_t crowded_ctas_per_sm; /* the same on one-cell bins of >= 8 points per cell */
+  int32_t tensor_min_batch;    /* smallest active batch on the tensor cores (AUTO) */
+} b200nufft_tuning;
+
+/* The choices the table gives a workload (type 1 or 2, B200NUFFT_PRECISION_*). */
+int b200nufft_tuning_lookup(int32_t type, int32_t dimensions, int32_t precision, int32_t width,
+                            int64_t fine_cells, int64_t point_count, b200nufft_tuning *out);
+
+/* Process-wide override of the table for plans whose points are set later,
+ * for the tuner's measurements; zero fields keep the table's choice, null
+ * restores the table. Not for concurrent use with set_points. */
+int b200nufft_tuning_override(const b200nufft_tuning *tuning);
+
 /* Number of this library's kernel launches since the process started, for
  * accounting in benchmarks. */
 uint64_t b200nufft_launch_count(void);

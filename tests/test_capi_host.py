@@ -138,3 +138,31 @@ def test_cpp_layout_matches_oracle_layout(shape, eps):
             assert g.value == lay.choose_geometry(m)
     finally:
         lib.b200nufft_plan_destroy(handle)
+
+
+def test_tuning_lookup_is_frozen_per_key_and_override_validates():
+    """The tuning table gives one answer per workload key (so outputs repeat
+    bit for bit); the tuner's override replaces only its non-zero fields and
+    rejects tile sides that are not powers of two."""
+    from wgpunufft_b200 import _native
+
+    lib = _native.library()
+
+    def lookup(*key):
+        out = _native.Tuning()
+        assert lib.b200nufft_tuning_lookup(*key, ctypes.byref(out)) == 0
+        return (out.tile, out.ctas_per_sm, out.crowded_ctas_per_sm, out.tensor_min_batch)
+
+    key = (1, 2, 3, 6, 2048 * 2048, 10_000_000)
+    first = lookup(*key)
+    assert lookup(*key) == first
+    assert first[1] >= 1 and first[2] >= 1 and first[3] >= 1
+    assert lib.b200nufft_tuning_override(_native.Tuning(32, 0, 0, 0)) == 0
+    try:
+        overridden = lookup(*key)
+        assert overridden[0] == 32 and overridden[1:] == first[1:]
+    finally:
+        assert lib.b200nufft_tuning_override(None) == 0
+    assert lookup(*key) == first
+    assert lib.b200nufft_tuning_override(_native.Tuning(48, 0, 0, 0)) == 25
+    assert lookup(*key) == first

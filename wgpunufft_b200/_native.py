@@ -93,6 +93,15 @@ class Type3Info(ctypes.Structure):
     ]
 
 
+class Tuning(ctypes.Structure):
+    _fields_ = [
+        ("tile", c_int32),
+        ("ctas_per_sm", c_int32),
+        ("crowded_ctas_per_sm", c_int32),
+        ("tensor_min_batch", c_int32),
+    ]
+
+
 class WgpuOpts(ctypes.Structure):
     _fields_ = [
         ("backend", c_int32),
@@ -140,6 +149,8 @@ SIGNATURES: dict[str, tuple] = {
     "b200nufft_last_error": (c_char_p, []),
     "b200nufft_version": (c_char_p, []),
     "b200nufft_launch_count": (c_uint64, []),
+    "b200nufft_tuning_lookup": (c_int, [c_int32, c_int32, c_int32, c_int32, c_int64, c_int64, P(Tuning)]),
+    "b200nufft_tuning_override": (c_int, [P(Tuning)]),
     # wgpu_nufft.h
     "wgpu_nufft_default_opts": (None, [P(WgpuOpts)]),
     "wgpu_nufft_list_adapters": (c_int, [c_void_p, c_int32, P(c_int32)]),

@@ -7,6 +7,7 @@
 #include <cstring>
 #include <limits>
 
+#include "tuning.h"
 #include "util.h"
 
 namespace b200nufft {
@@ -384,6 +385,7 @@ void NufftPlan::configure_tiles() {
   std::memset(&sp, 0, sizeof(sp));
   sp.grid = grid_;
   const int w = kernel_.width;
+  const b200nufft_tuning tuning = tuned_;
   int64_t tile[3] = {1, 1, 1};
   if (dim_ == 1) tile[0] = 1024;
   // 2D f32 register runs (w <= 7) slide along the rows of 64 x 64 tiles:
@@ -391,6 +393,9 @@ void NufftPlan::configure_tiles() {
   const bool runs2d = dim_ == 2 && precision_ == B200NUFFT_PRECISION_F32 && 2 * w * w * 4 < 400;
   if (dim_ == 2) tile[0] = tile[1] = runs2d ? 64 : 32;
   if (dim_ == 3) tile[0] = tile[1] = tile[2] = 16;
+  if (tuning.tile > 0) {
+    for (int a = 0; a < dim_; ++a) tile[a] = tuning.tile;
+  }
   for (int a = 0; a < dim_; ++a) tile[a] = std::min(tile[a], pow2_ceil(fine_[a]));
   // The tensor-core spreader needs one-cell bin rows, column bins of at most
   // 8 cells, and its own tile shape (16 cells x 22 - w rows).
@@ -466,7 +471,7 @@ void NufftPlan::configure_tiles() {
   bool one_cell_bins = true;
   for (int a = 0; a < dim_; ++a) one_cell_bins = one_cell_bins && grid_.axis[a].shift == 0;
   const bool crowded = runs && one_cell_bins && point_count_ >= 8 * grid_.fine_count;
-  const int64_t spread_ctas = (crowded ? 1 : 4) * 148;
+  const int64_t spread_ctas = (crowded ? tuning.crowded_ctas_per_sm : tuning.ctas_per_sm) * int64_t{148};
   int64_t cap = (std::max<int64_t>(point_count_, 1) + spread_ctas - 1) / spread_ctas;
   // 3D parts stay within the 2048 records that crowded tiles bucket in shared
   // memory; 1D and 2D f32 parts take up to 16384 records, so that a thread's
@@ -478,15 +483,16 @@ void NufftPlan::configure_tiles() {
   // after every bin), so that such points change no part; the host bounds the
   // parts for any count up to point_count_: valid / cap(valid) is at most
   // 4 x 148, or point_count_ / part_cap once the cap saturates.
-  int64_t records_per_cap = 4 * 148;
+  const int64_t most_ctas = std::max(tuning.ctas_per_sm, tuning.crowded_ctas_per_sm) * int64_t{148};
+  int64_t records_per_cap = most_ctas;
   if (type_ == 1) {
     sp.part_cap_device = static_cast<int32_t*>(part_cap_.reserve(sizeof(int32_t), "part cap"));
-    sp.cap_ctas = 4 * 148;
-    sp.cap_ctas_crowded = 148;
+    sp.cap_ctas = tuning.ctas_per_sm * 148;
+    sp.cap_ctas_crowded = tuning.crowded_ctas_per_sm * 148;
     sp.cap_max = static_cast<int32_t>(part_cap);
     sp.crowded_points = runs && one_cell_bins ? 8 * grid_.fine_count : std::numeric_limits<int64_t>::max();
     sp.cap_bins = bins_;
-    records_per_cap = std::max<int64_t>(4 * 148, (std::max<int64_t>(point_count_, 0) + part_cap - 1) / part_cap);
+    records_per_cap = std::max<int64_t>(most_ctas, (std::max<int64_t>(point_count_, 0) + part_cap - 1) / part_cap);
   }
   const int64_t part_bound = type_ == 1 ? sp.tile_count + tiles_per_bin * records_per_cap + 1
                                         : sp.tile_count + (std::max<int64_t>(point_count_, 0) * tiles_per_bin +
@@ -554,6 +560,7 @@ void NufftPlan::set_points(int64_t count, const void* points, cudaStream_t strea
   }
   point_count_ = count;
   points_ = points;
+  tuned_ = tuning_for(tuning_key(type_, dim_, precision_, kernel_.width, fine_count_, count));
   if (dim_ > 3) {
     // No bins: the coordinates are kept (in f64 for Df64 plans) as given.
     const size_t coords = static_cast<size_t>(std::max<int64_t>(count, 1)) * dim_;
@@ -781,7 +788,7 @@ void NufftPlan::execute_f32(int batch, const void* input, void* output, uint64_t
       check_cuda(cudaMemsetAsync(output, 0, out_bytes, stream), "zero type-1 output");
       return;
     }
-    if (tc_active_ && batch >= tc_min_batch_) {
+    if (tc_active_ && batch >= tensor_min_batch()) {
       const int64_t groups = (batch + kTcVectors - 1) / kTcVectors;
       TcLaunch t;
       t.strengths = static_cast<const float2*>(input);
@@ -837,7 +844,7 @@ void NufftPlan::execute_f32(int batch, const void* input, void* output, uint64_t
                         static_cast<const float*>(amplitudes_.get()), fine, stream);
     }
     run_fft(fine, batch, direction, stream);
-    if (tc2_active_ && batch >= tc_min_batch_) {
+    if (tc2_active_ && batch >= tensor_min_batch()) {
       const int64_t groups = (batch + kTi2Vectors - 1) / kTi2Vectors;
       Ti2Launch t;
       t.fine = fine;

@@ -3,6 +3,7 @@
 
 #include <cufft.h>
 
+#include <algorithm>
 #include <map>
 #include <memory>
 #include <vector>
@@ -60,6 +61,11 @@ class NufftPlan {
   void configure_bins(int geometry);
   void configure_type2_bins();
   void configure_tiles();
+  // Smallest active batch on the tensor cores: 1 when the configuration
+  // forces them, else the tuned threshold (at least kTcMinBatch).
+  int64_t tensor_min_batch() const {
+    return tc_min_batch_ == 1 ? 1 : std::max<int64_t>(tc_min_batch_, tuned_.tensor_min_batch);
+  }
   // The reference's bin order of a type-1 point set (ref_perm_, ref_keys_,
   // ref_offsets_): its points outside the fold's reach back in bin 0.
   void reference_order(cudaStream_t stream);
@@ -139,6 +145,7 @@ class NufftPlan {
   bool tc_enabled_ = false;
   bool tc_active_ = false;
   int64_t tc_min_batch_ = kTcMinBatch;  // smallest active batch run on the tensor cores
+  b200nufft_tuning tuned_{0, 4, 1, kTcMinBatch};  // the tuning of the last point set
   DeviceBuffer tc_weights_, tc_inverse_, tc_tile_chunks_, tc_tile_chunk_start_, tc_chunks_;
   DeviceBuffer tc_parts_, tc_part_start_, tc_packed_;
   int64_t tc_part_upper_bound_ = 0;

@@ -1,0 +1,179 @@
+"""Autotuner of the spreader's launch choices, run on a B200:
+
+    python -m wgpunufft_b200.tune [--out PATH] [--repeats N]
+
+For every workload below (the benchmark configurations and the sizes of the
+uneven-problems batch), it measures type-1 executions on prepared points
+under every candidate choice (tile side, CTAs per SM the tile parts are
+sized for, the same on crowded one-cell bins) and, for batched workloads,
+the smallest batch at which the tensor cores beat the CUDA cores; then it
+writes the fastest choice per workload key (plan type, dimension,
+precision, window width, log2 fine-grid cells, log2 points per cell) as
+tuning_table.h. The library compiles that table in, so a key always gets
+the same choices and outputs stay bitwise repeatable. Inputs are seeded
+synthetic points (uniform, clustered, radial) and N(0, 1) strengths.
+"""
+
+from __future__ import annotations
+
+import argparse
+import itertools
+import json
+import math
+import statistics
+from pathlib import Path
+
+HERE = Path(__file__).resolve().parent
+
+# (name, modes, points, eps, distribution, precision)
+WORKLOADS = [
+    ("2d_1024_1e7_uniform", (1024, 1024), 10_000_000, 1e-5, "uniform", "f32"),
+    ("2d_1024_1e7_clustered", (1024, 1024), 10_000_000, 1e-5, "clustered", "f32"),
+    ("2d_512_2e6_uniform", (512, 512), 2_000_000, 1e-6, "uniform", "f32"),
+    ("2d_64_1e5_uniform", (64, 64), 100_000, 1e-6, "uniform", "f32"),
+    ("2d_128_1e4_uniform", (128, 128), 10_000, 1e-6, "uniform", "f32"),
+    ("2d_128_1e6_clustered", (128, 128), 1_000_000, 1e-6, "clustered", "f32"),
+    ("2d_256_1e5_uniform", (256, 256), 100_000, 1e-6, "uniform", "f32"),
+    ("3d_256_5e7_radial", (256, 256, 256), 4096 * 12207, 1e-5, "radial", "f32"),
+    ("3d_64_1e6_uniform", (64, 64, 64), 1_000_000, 1e-6, "uniform", "f32"),
+    ("3d_32_1e5_clustered", (32, 32, 32), 100_000, 1e-6, "clustered", "f32"),
+    ("2d_512_2e6_f64_1e-9", (512, 512), 2_000_000, 1e-9, "uniform", "f64"),
+]
+
+CANDIDATES = {
+    2: {"tile": (32, 64), "ctas_per_sm": (2, 4, 8), "crowded_ctas_per_sm": (1, 2)},
+    3: {"tile": (8, 16), "ctas_per_sm": (2, 4), "crowded_ctas_per_sm": (1,)},
+}
+F64_CANDIDATES = {"tile": (16, 32), "ctas_per_sm": (2, 4, 8), "crowded_ctas_per_sm": (1,)}
+
+
+def _points(torch, workloads, dist, count, d, dtype):
+    p = workloads.points(dist, count, d, seed=11)
+    return p.to(dtype).contiguous()
+
+
+def _time(torch, fn, repeats):
+    for _ in range(2):
+        fn()
+    torch.cuda.synchronize()
+    times = []
+    for _ in range(repeats):
+        start, end = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        start.record()
+        fn()
+        end.record()
+        end.synchronize()
+        times.append(start.elapsed_time(end))
+    return statistics.median(times)
+
+
+def tune_workload(torch, w, workloads, native, spec, repeats):
+    name, modes, count, eps, dist, precision = spec
+    d = len(modes)
+    f64 = precision == "f64"
+    real = torch.float64 if f64 else torch.float32
+    pts = _points(torch, workloads, dist, count, d, real)
+    c = workloads.values(1, count, seed=12).to(torch.complex128 if f64 else torch.complex64)
+    config = w.NufftConfig(modes, eps, precision=w.Precision.F64 if f64 else w.Precision.F32)
+    out = torch.empty((1, config.mode_count()), dtype=c.dtype, device="cuda")
+    grid = F64_CANDIDATES if f64 else CANDIDATES[d]
+    results = []
+    for tile, ctas, crowded in itertools.product(grid["tile"], grid["ctas_per_sm"], grid["crowded_ctas_per_sm"]):
+        t = native.Tuning(tile, ctas, crowded, 0)
+        native.library().b200nufft_tuning_override(t)
+        plan = w.NufftPlan.type1_gpu(config)
+        plan.set_points_gpu(pts)
+        ms = _time(torch, lambda: plan.execute_gpu_batch(1, c, out), repeats)
+        results.append({"tile": tile, "ctas_per_sm": ctas, "crowded_ctas_per_sm": crowded, "ms": ms})
+        del plan
+    native.library().b200nufft_tuning_override(None)
+    plan = w.NufftPlan.type1_gpu(config)
+    info = plan.info()
+    fine_cells = math.prod(info.fine_shape[a] for a in range(d))
+    best = min(results, key=lambda r: r["ms"])
+    key = {"type": 1, "dimensions": d, "precision": 1 if f64 else 3, "width": info.kernel_width,
+           "log2_cells": int(math.floor(math.log2(fine_cells))),
+           "log2_density": max(-16, min(16, int(math.floor(math.log2(count / fine_cells)))))}
+    del plan, pts, c, out
+    torch.cuda.empty_cache()
+    return {"workload": name, "key": key, "best": best, "candidates": results}
+
+
+def tune_tensor_threshold(torch, w, workloads, native, kind, repeats):
+    """Smallest batch in {16, 32, 64} at which the tensor cores are faster
+    (2D 512^2 modes, 2e6 uniform points, eps 1e-6); 0 for none."""
+    modes, count = (512, 512), 2_000_000
+    pts = workloads.points("uniform", count, 2, seed=13)
+    n = modes[0] * modes[1]
+    for batch in (16, 32, 64):
+        inputs = workloads.values(batch, count if kind == 1 else n, seed=14)
+        out = torch.empty((batch, n if kind == 1 else count), dtype=torch.complex64, device="cuda")
+        ms = {}
+        for method in (w.SpreadMethod.TENSOR_CORES, w.SpreadMethod.CUDA_CORES):
+            plan = (w.NufftPlan.type1_gpu if kind == 1 else w.NufftPlan.type2_gpu)(
+                w.NufftConfig(modes, 1e-6, batch=batch, spread_method=method))
+            plan.set_points_gpu(pts)
+            ms[method] = _time(torch, lambda: plan.execute_gpu_batch(batch, inputs, out), repeats)
+            del plan
+        del inputs, out
+        if ms[w.SpreadMethod.TENSOR_CORES] < ms[w.SpreadMethod.CUDA_CORES]:
+            return batch, ms
+    return 0, ms
+
+
+def table_header(entries):
+    lines = ["// Tuned launch choices per workload key, written by wgpunufft_b200/tune.py",
+             "// from measurements on a B200. Fields: type, dimensions, precision, width,",
+             "// log2 fine-grid cells, log2 density; tile side, CTAs per SM, CTAs per SM",
+             "// on crowded one-cell bins, smallest tensor-core batch.",
+             "#pragma once", "", "namespace b200nufft {", "",
+             "struct TuningEntry {",
+             "  int type, dimensions, precision, width, log2_cells, log2_density;",
+             "  int tile, ctas_per_sm, crowded_ctas_per_sm, tensor_min_batch;",
+             "};", "", "constexpr TuningEntry kTuningTable[] = {"]
+    for e in entries:
+        k, b = e["key"], e["best"]
+        lines.append(f"    {{{k['type']}, {k['dimensions']}, {k['precision']}, {k['width']}, {k['log2_cells']}, "
+                     f"{k['log2_density']}, {b['tile']}, {b['ctas_per_sm']}, {b['crowded_ctas_per_sm']}, "
+                     f"{e.get('tensor_min_batch', 16)}}},  // {e['workload']}: {b['ms']:.4f} ms")
+    lines += ["};", f"constexpr int kTuningEntries = {len(entries)};", "", "}  // namespace b200nufft", ""]
+    return "\n".join(lines)
+
+
+def main():
+    parser = argparse.ArgumentParser(description=__doc__, formatter_class=argparse.RawDescriptionHelpFormatter)
+    parser.add_argument("--out", default=str(HERE / "csrc" / "tuning_table.h"))
+    parser.add_argument("--report", default=None, help="JSON file for every measurement")
+    parser.add_argument("--repeats", type=int, default=5)
+    args = parser.parse_args()
+    import torch
+
+    import wgpunufft_b200 as w
+    from wgpunufft_b200 import _native as native
+    from wgpunufft_b200 import workloads
+
+    entries = []
+    for spec in WORKLOADS:
+        entry = tune_workload(torch, w, workloads, native, spec, args.repeats)
+        entries.append(entry)
+        print(json.dumps({"workload": entry["workload"], "best": entry["best"]}), flush=True)
+    threshold1, ms1 = tune_tensor_threshold(torch, w, workloads, native, 1, args.repeats)
+    threshold2, ms2 = tune_tensor_threshold(torch, w, workloads, native, 2, args.repeats)
+    # The tensor-core threshold of the batched configuration's key (type 1 and 2).
+    for entry in entries:
+        if entry["workload"] == "2d_512_2e6_uniform":
+            entry["tensor_min_batch"] = threshold1 or 1 << 30
+            type2 = dict(entry, key=dict(entry["key"], type=2), workload="2d_512_2e6_uniform_type2",
+                         tensor_min_batch=threshold2 or 1 << 30)
+            entries.append(type2)
+            break
+    Path(args.out).write_text(table_header(entries))
+    report = {"entries": entries, "tensor_threshold": {"type1": [threshold1, {str(k): v for k, v in ms1.items()}],
+                                                        "type2": [threshold2, {str(k): v for k, v in ms2.items()}]}}
+    if args.report:
+        Path(args.report).write_text(json.dumps(report, indent=1))
+    print(json.dumps({"written": args.out, "tensor_threshold": report["tensor_threshold"]}), flush=True)
+
+
+if __name__ == "__main__":
+    main()
