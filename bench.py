@@ -648,14 +648,41 @@ def uneven_problems_line(r):
         r.barrier()
         eager_ms = r.timed(run_all, steps, stream)
         graph_ms = r.timed(graph.replay, steps, stream)
-    del graph
-    eager_ms, graph_ms = max_over_ranks([eager_ms, graph_ms], r.dev)
+        # The same problems as one batch: one persistent spreading launch over
+        # every problem's tile parts, then per-problem folds, FFTs and
+        # deconvolutions on forked streams.
+        batch = w.NufftBatch(plans)
+        strengths = [c for _, _, c in problems]
+        batch_outs = [torch.empty_like(o) for o in outs]
+
+        def run_batch():
+            batch.execute(strengths, batch_outs, stream=stream)
+
+        run_batch()
+        stream.synchronize()
+        identical = all(torch.equal(a.view(torch.int32), b.view(torch.int32)) for a, b in zip(batch_outs, outs))
+        batch_graph = torch.cuda.CUDAGraph()
+        with torch.cuda.graph(batch_graph, stream=stream):
+            run_batch()
+        for _ in range(max(2, r.args.warmup)):
+            run_batch()
+            batch_graph.replay()
+        r.barrier()
+        batch_ms = r.timed(run_batch, steps, stream)
+        batch_graph_ms = r.timed(batch_graph.replay, steps, stream)
+    del graph, batch_graph, batch
+    eager_ms, graph_ms, batch_ms, batch_graph_ms = max_over_ranks([eager_ms, graph_ms, batch_ms, batch_graph_ms],
+                                                                  r.dev)
     total_points = sum(int(p.shape[0]) for _, p, _ in problems)
     return {"problems": len(problems), "points": total_points, "eps": 1e-6, "unit": UNIT,
             "graph": {"value": replica_throughput(r.world, total_points, graph_ms, steps),
                       "ms_per_step": graph_ms / steps},
             "eager": {"value": replica_throughput(r.world, total_points, eager_ms, steps),
                       "ms_per_step": eager_ms / steps},
+            "persistent_batch": {"value": replica_throughput(r.world, total_points, batch_ms, steps),
+                                 "ms_per_step": batch_ms / steps, "same_bits_as_plans": identical},
+            "persistent_batch_graph": {"value": replica_throughput(r.world, total_points, batch_graph_ms, steps),
+                                       "ms_per_step": batch_graph_ms / steps},
             "note": "one plan per problem (prepared points); a step executes all 256"}
 
 
@@ -710,7 +737,8 @@ def summary_of(line):
         s["radial_3d"] = {k: {q: rad[k].get(q) for q in ("value", "rel_l2", "meets_eps")} for k in ("type1", "type2")}
     u = line.get("uneven_problems")
     if u:
-        s["uneven_graph_ms"] = u["graph"]["ms_per_step"]
+        s["uneven_ms"] = {k: u[k]["ms_per_step"] for k in ("graph", "persistent_batch", "persistent_batch_graph")
+                          if k in u}
     t3 = line.get("type3")
     if t3:
         s["type3_f64"] = {q: t3.get(q) for q in ("value", "rel_l2")}

@@ -342,6 +342,24 @@ const char *b200nufft_last_error(void);
 /* The library version. */
 const char *b200nufft_version(void);
 
+/* Many independent type-1 problems executed together. This has no
+ * counterpart in the reference, which executes every plan on its own
+ * (src/plan.rs). A batch holds 2D and 3D f32 type-1 plans of one window
+ * width (one eps) on one device, each with its own grid and point set
+ * (b200nufft_set_points before the first execution, which must not be
+ * captured in a CUDA graph; later executions can be). An execution spreads
+ * every problem's strengths from one persistent launch whose CTAs take
+ * (problem, tile part) items from a device work counter, then runs each
+ * problem's fold, FFT and deconvolution on streams forked from `stream` and
+ * joined back to it. Every problem's modes are the bits of its own
+ * execution. `strengths[p]` and `outputs[p]`: device buffers of problem p
+ * (one vector). Executions of one batch stay in stream order. */
+typedef struct b200nufft_batch_s *b200nufft_batch;
+int b200nufft_batch_create(const b200nufft_plan *plans, int32_t count, b200nufft_batch *batch);
+void b200nufft_batch_destroy(b200nufft_batch batch);
+int b200nufft_batch_execute(b200nufft_batch batch, const void *const *strengths, void *const *outputs,
+                            void *stream);
+
 /* Launch choices of the type-1 spreader and the tensor-core paths. This has
  * no counterpart in the reference, which fixes them per rank and precision
  * (src/gpu_nd_spread.rs:55-135,562-593); here a table measured on a B200

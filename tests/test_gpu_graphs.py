@@ -155,3 +155,53 @@ def test_captured_sort_and_execution_follow_new_points(kind, modes, batch, preci
         plan.synchronize(stream)
         assert torch.equal(replayed.view(torch.int32), out.view(torch.int32))
     del graph
+
+
+def test_persistent_batch_of_uneven_problems_matches_their_own_executions():
+    """Independent 2D and 3D problems (uneven sizes, uniform and clustered)
+    spread by one persistent launch over a device work counter, folded and
+    transformed on forked streams: every problem's modes equal its own plan's
+    execution bit for bit, eagerly and replayed from a CUDA graph, and after
+    some problems get new points."""
+    from wgpunufft_b200 import workloads
+
+    problems = workloads.uneven_problems(40, seed=91)
+    plans, outs, refs = [], [], []
+    for modes, p, c in problems:
+        plan = w.NufftPlan.type1_gpu(w.NufftConfig(modes, 1e-6))
+        plan.set_points_gpu(p)
+        ref = torch.empty((1, int(np.prod(modes))), dtype=torch.complex64, device=DEV)
+        plan.execute_gpu_batch(1, c, ref)
+        plans.append(plan)
+        refs.append(ref)
+        outs.append(torch.zeros_like(ref))
+    torch.cuda.synchronize()
+    batch = w.NufftBatch(plans)
+    strengths = [c for _, _, c in problems]
+    batch.execute(strengths, outs)
+    torch.cuda.synchronize()
+    for k, (out, ref) in enumerate(zip(outs, refs)):
+        assert torch.equal(out.view(torch.int32), ref.view(torch.int32)), k
+    stream = torch.cuda.Stream()
+    with torch.cuda.stream(stream):
+        graph = torch.cuda.CUDAGraph()
+        with torch.cuda.graph(graph, stream=stream):
+            batch.execute(strengths, outs, stream=stream)
+    for out in outs:
+        out.zero_()
+    graph.replay()
+    torch.cuda.synchronize()
+    for k, (out, ref) in enumerate(zip(outs, refs)):
+        assert torch.equal(out.view(torch.int32), ref.view(torch.int32)), k
+    del graph
+    # New points for some problems: the batch takes the new point sets.
+    for k in (0, 7, 19):
+        modes, p, c = problems[k]
+        fresh = workloads.points("uniform", p.shape[0], len(modes), seed=500 + k)
+        plans[k].set_points_gpu(fresh)
+        problems[k] = (modes, fresh, c)
+        plans[k].execute_gpu_batch(1, c, refs[k])
+    batch.execute(strengths, outs)
+    torch.cuda.synchronize()
+    for k, (out, ref) in enumerate(zip(outs, refs)):
+        assert torch.equal(out.view(torch.int32), ref.view(torch.int32)), k

@@ -27,6 +27,7 @@ __all__ = [
     "SpreadMethod",
     "NufftSign",
     "launch_count",
+    "NufftBatch",
     "version",
 ]
 
@@ -317,14 +318,19 @@ class NufftPlan:
         self._count = count
         self._sizes = {}
 
+    def _io_sizes(self, active_batch: int):
+        """(input bytes, output bytes) of an execution on the current points."""
+        sizes = self._sizes.get(active_batch)
+        if sizes is None:
+            sizes = (self.required_input_buffer_size_bytes(self._count, active_batch),
+                     self.required_output_buffer_size_bytes(self._count, active_batch))
+            self._sizes[active_batch] = sizes
+        return sizes
+
     def execute_gpu_batch(self, active_batch: int, inputs, output, stream=None) -> None:
         count = getattr(self, "_count", None)
         if count is not None and 0 < active_batch <= self.config.batch:
-            sizes = self._sizes.get(active_batch)
-            if sizes is None:
-                sizes = (self.required_input_buffer_size_bytes(count, active_batch),
-                         self.required_output_buffer_size_bytes(count, active_batch))
-                self._sizes[active_batch] = sizes
+            sizes = self._io_sizes(active_batch)
             _require_bytes(inputs, sizes[0], "the input buffer")
             _require_bytes(output, sizes[1], "the output buffer")
         _check(_native.library().b200nufft_execute(self._handle, active_batch, _ptr(inputs), _ptr(output),
@@ -499,6 +505,40 @@ class NufftType3Plan:
     def encode_gpu_batch(self, active_batch, sources, strengths, targets, output, stream=None) -> None:
         self.set_points_gpu(sources, targets, stream)
         self.execute_gpu_batch(active_batch, strengths, output, stream)
+
+
+class NufftBatch:
+    """Many independent 2D/3D f32 type-1 plans (one window width, points set)
+    executed together: one persistent spreading launch over every problem's
+    tile parts, then each problem's fold, FFT and deconvolution on streams
+    forked from the caller's (b200nufft_batch_*). Each problem's modes are
+    the bits of its own execution."""
+
+    def __init__(self, plans):
+        self.plans = list(plans)
+        handles = (ctypes.c_void_p * len(self.plans))(*[p._handle.value for p in self.plans])
+        self._handle = ctypes.c_void_p()
+        _check(_native.library().b200nufft_batch_create(handles, len(self.plans), ctypes.byref(self._handle)))
+
+    def __del__(self):
+        handle = getattr(self, "_handle", None)
+        if handle and _native is not None:
+            _native.library().b200nufft_batch_destroy(handle)
+            self._handle = None
+
+    def execute(self, strengths, outputs, stream=None) -> None:
+        """strengths[p], outputs[p]: CUDA tensors of problem p (one vector)."""
+        if len(strengths) != len(self.plans) or len(outputs) != len(self.plans):
+            raise NufftError(25, "one strength and one output tensor per plan")
+        for plan, s, o in zip(self.plans, strengths, outputs):
+            if getattr(plan, "_count", None) is None:
+                raise NufftError(19, "every plan of a batch needs its points set")
+            sizes = plan._io_sizes(1)
+            _require_bytes(s, sizes[0], "a strength buffer")
+            _require_bytes(o, sizes[1], "an output buffer")
+        ins = (ctypes.c_void_p * len(self.plans))(*[_ptr(s) for s in strengths])
+        outs = (ctypes.c_void_p * len(self.plans))(*[_ptr(o) for o in outputs])
+        _check(_native.library().b200nufft_batch_execute(self._handle, ins, outs, _stream_handle(stream)))
 
 
 def launch_count() -> int:

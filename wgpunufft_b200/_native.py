@@ -149,6 +149,9 @@ SIGNATURES: dict[str, tuple] = {
     "b200nufft_last_error": (c_char_p, []),
     "b200nufft_version": (c_char_p, []),
     "b200nufft_launch_count": (c_uint64, []),
+    "b200nufft_batch_create": (c_int, [P(PLAN), c_int32, P(PLAN)]),
+    "b200nufft_batch_destroy": (None, [PLAN]),
+    "b200nufft_batch_execute": (c_int, [PLAN, P(c_void_p), P(c_void_p), c_void_p]),
     "b200nufft_tuning_lookup": (c_int, [c_int32, c_int32, c_int32, c_int32, c_int64, c_int64, P(Tuning)]),
     "b200nufft_tuning_override": (c_int, [P(Tuning)]),
     # wgpu_nufft.h

@@ -19,6 +19,8 @@ struct b200nufft_type3_plan_s {
   explicit b200nufft_type3_plan_s(const b200nufft_type3_config& c) : impl(c) {}
 };
 
+b200nufft::NufftPlan* b200nufft_plan_impl(b200nufft_plan plan) { return &plan->impl; }
+
 namespace {
 
 template <typename F>

@@ -560,6 +560,7 @@ void NufftPlan::set_points(int64_t count, const void* points, cudaStream_t strea
   }
   point_count_ = count;
   points_ = points;
+  ++points_generation_;
   tuned_ = tuning_for(tuning_key(type_, dim_, precision_, kernel_.width, fine_count_, count));
   if (dim_ > 3) {
     // No bins: the coordinates are kept (in f64 for Df64 plans) as given.
@@ -1190,6 +1191,53 @@ void NufftPlan::copy_prepared_slots(int32_t* starts, float* offsets, cudaStream_
   prepare_reference_slots(static_cast<const float*>(points_), point_count_, grid_,
                           static_cast<const uint32_t*>(ref_perm_.get()), static_cast<const uint32_t*>(ref_keys_.get()),
                           starts, offsets, stream);
+}
+
+bool NufftPlan::batch_problem(BatchProblem* out) {
+  if (!has_device_ || type_ != 1 || precision_ != B200NUFFT_PRECISION_F32 || (dim_ != 2 && dim_ != 3) ||
+      point_count_ < 0) {
+    return false;
+  }
+  make_current();
+  std::memset(out, 0, sizeof(*out));
+  out->sp = spread_;
+  out->windows = windows_.get();
+  out->perm = perm_;
+  out->offsets = static_cast<const uint32_t*>(offsets_.get());
+  out->part_start = static_cast<const uint32_t*>(part_start_.get());
+  out->valid_mask = static_cast<const uint32_t*>(valid_mask_.get());
+  out->point_count = point_count_;
+  out->max_bits = static_cast<uint32_t*>(max_bits_.get());
+  out->scratch = static_cast<float2*>(scratch_.reserve(
+      static_cast<size_t>(std::max<int64_t>(part_upper_bound_, 1)) * spread_.padded_cells * sizeof(float2),
+      "spreading tiles"));
+  return true;
+}
+
+void NufftPlan::finish_batch(void* output, cudaStream_t stream) {
+  make_current();
+  float2* fine = static_cast<float2*>(fine_grid_.get());
+  if (point_count_ == 0) {
+    check_cuda(cudaMemsetAsync(output, 0, static_cast<size_t>(mode_count_) * sizeof(float2), stream),
+               "zero type-1 output");
+    return;
+  }
+  SpreadLaunch l{};
+  l.batch = 1;
+  l.part_start = static_cast<const uint32_t*>(part_start_.get());
+  l.part_upper_bound = part_upper_bound_;
+  l.scratch = static_cast<float2*>(scratch_.get());
+  l.candidates = static_cast<const int2*>(candidates_.get());
+  l.fine = fine;
+  {
+    StageScope scope(&timer_, kStageFold, stream);
+    spread_fold(spread_, l, stream);
+  }
+  run_fft(fine, 1, isign_ >= 0 ? CUFFT_INVERSE : CUFFT_FORWARD, stream);
+  StageScope scope(&timer_, kStageDeconvolution, stream);
+  deconvolve_f32(modes_params_, 1, fine, static_cast<const float*>(amplitudes_.get()), static_cast<float2*>(output),
+                 stream);
+  check_cuda(cudaGetLastError(), "batch finish launch");
 }
 
 void NufftPlan::synchronize(cudaStream_t stream) {

@@ -44,6 +44,16 @@ class NufftPlan {
   void copy_prepared_slots(int32_t* starts, float* offsets, cudaStream_t stream);
   // Waits for the plan's work on `stream` and reports a device wait that gave up.
   void synchronize(cudaStream_t stream);
+  // Persistent execution of many problems (batch.cpp): this plan's spreading
+  // descriptor for one vector (false when the plan cannot join: not a 2D or
+  // 3D f32 type-1 plan with points set), and the rest of its execution once
+  // the batch has spread its tiles: fold, FFT, deconvolution.
+  bool batch_problem(BatchProblem* out);
+  void finish_batch(void* output, cudaStream_t stream);
+  // Incremented by every set_points.
+  uint64_t points_generation() const { return points_generation_; }
+  // Points of the last set_points (-1 before the first).
+  int64_t points_set_count() const { return point_count_; }
   StageTimer& timer() { return timer_; }
 
   int type() const { return type_; }
@@ -117,6 +127,7 @@ class NufftPlan {
   std::map<int64_t, cufftHandle> nd_ffts_;    // by first axis of the group and batch
 
   // Remembered points and their bin order.
+  uint64_t points_generation_ = 0;
   int64_t point_count_ = -1;
   const void* points_ = nullptr;
   int geometry_ = -1;

@@ -847,15 +847,17 @@ __host__ __device__ constexpr int spread_min_blocks() {
   return (spread_run<D, W, T>() > 1 || sizeof(typename T::Real) == 8 || warp_capable<D, W, T>()) ? 2 : 3;
 }
 
-// One CTA per (part, vector): spreads the part's records into a padded tile
-// of fixed-point sums and writes the tile out in floating point.
+// Spreads part `part` of vector `b` (one CTA): the part's records into a
+// padded tile of fixed-point sums, written out in floating point. Called
+// once per CTA by spread_tiles_kernel, and per work item by the persistent
+// kernel of many problems (batch.cu), whose CTAs run it again and again.
 template <int D, int W, typename T>
-__global__ void __launch_bounds__(kSpreadThreads, spread_min_blocks<D, W, T>()) spread_tiles_kernel(
-    SpreadParams sp, const typename T::Real* __restrict__ points, const void* __restrict__ windows,
+__device__ __forceinline__ void spread_part(
+    const SpreadParams& sp, const typename T::Real* __restrict__ points, const void* __restrict__ windows,
     const typename T::Complex* __restrict__ strengths, int64_t point_count, int batch,
     const uint32_t* __restrict__ perm, const uint32_t* __restrict__ offsets,
     const uint32_t* __restrict__ part_start, const typename T::Bits* __restrict__ max_bits,
-    typename T::Complex* __restrict__ scratch) {
+    typename T::Complex* __restrict__ scratch, uint32_t part, int b) {
   using Real = typename T::Real;
   using Word = typename T::Word;
   extern __shared__ __align__(16) unsigned char shared_bytes[];
@@ -865,8 +867,6 @@ __global__ void __launch_bounds__(kSpreadThreads, spread_min_blocks<D, W, T>()) 
   __shared__ int64_t s_tile;
   __shared__ uint32_t warp_totals[kSpreadThreads / 32];
 
-  const uint32_t part = blockIdx.x;
-  const int b = blockIdx.y;
   const uint32_t total_parts = part_start[sp.tile_count];
   if (part >= total_parts) return;
   const int tid = threadIdx.x;
@@ -1167,6 +1167,18 @@ __global__ void __launch_bounds__(kSpreadThreads, spread_min_blocks<D, W, T>()) 
   }
 }
 
+// One CTA per (part, vector).
+template <int D, int W, typename T>
+__global__ void __launch_bounds__(kSpreadThreads, spread_min_blocks<D, W, T>()) spread_tiles_kernel(
+    SpreadParams sp, const typename T::Real* __restrict__ points, const void* __restrict__ windows,
+    const typename T::Complex* __restrict__ strengths, int64_t point_count, int batch,
+    const uint32_t* __restrict__ perm, const uint32_t* __restrict__ offsets,
+    const uint32_t* __restrict__ part_start, const typename T::Bits* __restrict__ max_bits,
+    typename T::Complex* __restrict__ scratch) {
+  spread_part<D, W, T>(sp, points, windows, strengths, point_count, batch, perm, offsets, part_start, max_bits,
+                       scratch, blockIdx.x, blockIdx.y);
+}
+
 constexpr int kFoldThreads = 256;
 
 // Every fine-grid cell as the sum, in a fixed order, of the padded tiles and
@@ -1443,7 +1455,178 @@ void spread_execute_impl(const SpreadParams& sp, const SpreadLaunchT<T>& l, cuda
   fold_any(sp, l.batch, l.scratch, l.part_start, l.part_upper_bound, l.candidates, l.fine, stream);
 }
 
+// ---------------------------------------------------------------------------
+// Many independent problems from one persistent launch.
+
+// Work list: work[p] = first item of problem p (its parts, in order), work[count]
+// = all items; work[count + 1] = the queue counter. Clears the scale words.
+__global__ void __launch_bounds__(1024) batch_work_kernel(const BatchProblem* __restrict__ problems, int count,
+                                                          uint32_t* __restrict__ work) {
+  __shared__ uint32_t warp_sums[32];
+  __shared__ uint32_t carry_shared;
+  if (threadIdx.x == 0) carry_shared = 0;
+  __syncthreads();
+  const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
+  for (int base = 0; base < count; base += 1024) {
+    const int p = base + threadIdx.x;
+    uint32_t v = 0;
+    if (p < count) {
+      const BatchProblem& bp = problems[p];
+      v = bp.point_count > 0 ? bp.part_start[bp.sp.tile_count] : 0u;
+      *bp.max_bits = 0u;
+    }
+    uint32_t x = v;
+#pragma unroll
+    for (int offset = 1; offset < 32; offset <<= 1) {
+      const uint32_t y = __shfl_up_sync(0xFFFFFFFFu, x, offset);
+      if (lane >= offset) x += y;
+    }
+    if (lane == 31) warp_sums[warp] = x;
+    __syncthreads();
+    if (warp == 0) {
+      uint32_t t = warp_sums[lane];
+#pragma unroll
+      for (int offset = 1; offset < 32; offset <<= 1) {
+        const uint32_t y = __shfl_up_sync(0xFFFFFFFFu, t, offset);
+        if (lane >= offset) t += y;
+      }
+      warp_sums[lane] = t;
+    }
+    __syncthreads();
+    const uint32_t carry = carry_shared;
+    const uint32_t inclusive = x + (warp > 0 ? warp_sums[warp - 1] : 0u);
+    if (p < count) work[p] = carry + inclusive - v;
+    __syncthreads();
+    if (threadIdx.x == 1023) carry_shared = carry + inclusive;
+    __syncthreads();
+  }
+  if (threadIdx.x == 0) {
+    work[count] = carry_shared;
+    work[count + 1] = 0u;
+  }
+}
+
+// Largest |re| or |im| of every problem's strengths over its points within
+// reach (blockIdx.y = problem).
+__global__ void batch_magnitude_kernel(const BatchProblem* __restrict__ problems, const __grid_constant__ BatchStrengths strengths) {
+  const BatchProblem& bp = problems[blockIdx.y];
+  const float2* v = strengths.ptr[blockIdx.y];
+  const int64_t count = bp.point_count;
+  const uint32_t* valid_mask = bp.valid_mask;
+  uint32_t m = 0;
+  const int64_t stride = static_cast<int64_t>(gridDim.x) * blockDim.x;
+  for (int64_t i = static_cast<int64_t>(blockIdx.x) * blockDim.x + threadIdx.x; i < count; i += stride) {
+    if (valid_mask != nullptr && !((__ldg(&valid_mask[i >> 5]) >> (i & 31)) & 1u)) continue;
+    const float2 s = v[i];
+    m = max(m, F32Traits::magnitude_bits(s.x));
+    m = max(m, F32Traits::magnitude_bits(s.y));
+  }
+#pragma unroll
+  for (int offset = 16; offset > 0; offset >>= 1) m = max(m, __shfl_xor_sync(0xFFFFFFFFu, m, offset));
+  if ((threadIdx.x & 31) == 0 && m) atomicMax(bp.max_bits, m);
+}
+
+// Persistent spreading: every CTA takes the next (problem, part) item from
+// the queue counter until none is left, copies that problem's parameters
+// into shared memory and spreads the part as spread_tiles_kernel does, so
+// each problem's padded tiles are the same bits as from its own launch.
+template <int W, bool Has2D, bool Has3D>
+__global__ void __launch_bounds__(kSpreadThreads, 1) batch_spread_kernel(const BatchProblem* __restrict__ problems,
+                                                                         const __grid_constant__ BatchStrengths strengths,
+                                                                         int count, uint32_t* __restrict__ work) {
+  __shared__ __align__(16) SpreadParams s_sp;
+  __shared__ uint32_t s_item;
+  const uint32_t total = work[count];
+  for (;;) {
+    __syncthreads();  // the previous item's tile and parameters are no longer read
+    if (threadIdx.x == 0) s_item = atomicAdd(&work[count + 1], 1u);
+    __syncthreads();
+    const uint32_t item = s_item;
+    if (item >= total) break;
+    // The problem whose items include `item` (last start at or below it).
+    int low = 0, high = count - 1;
+    while (low < high) {
+      const int mid = (low + high + 1) >> 1;
+      if (work[mid] <= item) low = mid; else high = mid - 1;
+    }
+    const BatchProblem* bp = problems + low;
+    {
+      const uint32_t* src = reinterpret_cast<const uint32_t*>(&bp->sp);
+      uint32_t* dst = reinterpret_cast<uint32_t*>(&s_sp);
+      for (int i = threadIdx.x; i < static_cast<int>(sizeof(SpreadParams) / 4); i += kSpreadThreads) dst[i] = src[i];
+    }
+    __syncthreads();
+    const uint32_t part = item - work[low];
+    if constexpr (Has2D) {
+      if (s_sp.grid.dimensions == 2) {
+        spread_part<2, W, F32Traits>(s_sp, nullptr, bp->windows, strengths.ptr[low], bp->point_count, 1, bp->perm,
+                                     bp->offsets, bp->part_start, bp->max_bits, bp->scratch, part, 0);
+      }
+    }
+    if constexpr (Has3D) {
+      if (s_sp.grid.dimensions == 3) {
+        spread_part<3, W, F32Traits>(s_sp, nullptr, bp->windows, strengths.ptr[low], bp->point_count, 1, bp->perm,
+                                     bp->offsets, bp->part_start, bp->max_bits, bp->scratch, part, 0);
+      }
+    }
+  }
+}
+
+template <int W>
+void launch_batch_spread(const BatchProblem* problems, const BatchStrengths& strengths, int count, bool has_2d,
+                         bool has_3d, size_t shared_bytes, uint32_t* work, cudaStream_t stream) {
+  auto launch = [&](auto kernel) {
+    check_cuda(cudaFuncSetAttribute(kernel, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                    static_cast<int>(shared_bytes)),
+               "batch spread shared memory");
+    int per_sm = 0;
+    check_cuda(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, kernel, kSpreadThreads, shared_bytes),
+               "batch spread occupancy");
+    int sms = 0, device = 0;
+    check_cuda(cudaGetDevice(&device), "current device");
+    check_cuda(cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, device), "SM count");
+    const unsigned grid = static_cast<unsigned>(std::max(1, per_sm) * sms);
+    kernel<<<grid, kSpreadThreads, shared_bytes, stream>>>(problems, strengths, count, work);
+    note_launch();
+  };
+  if (has_2d && has_3d) {
+    launch(batch_spread_kernel<W, true, true>);
+  } else if (has_3d) {
+    launch(batch_spread_kernel<W, false, true>);
+  } else {
+    launch(batch_spread_kernel<W, true, false>);
+  }
+}
+
 }  // namespace
+
+void batch_spread(const BatchProblem* problems, const BatchStrengths& strengths, int count, int width, bool has_2d,
+                  bool has_3d, size_t shared_bytes, uint32_t* work, cudaStream_t stream) {
+  if (count <= 0) return;
+  if (count > kMaxBatchProblems) throw NufftFailure{B200NUFFT_INVALID_ARGUMENT, "too many problems in one batch"};
+  batch_work_kernel<<<1, 1024, 0, stream>>>(problems, count, work);
+  batch_magnitude_kernel<<<dim3(16, static_cast<unsigned>(count)), 256, 0, stream>>>(problems, strengths);
+  note_launch(2);
+  switch (width) {
+    case 2: launch_batch_spread<2>(problems, strengths, count, has_2d, has_3d, shared_bytes, work, stream); break;
+    case 3: launch_batch_spread<3>(problems, strengths, count, has_2d, has_3d, shared_bytes, work, stream); break;
+    case 4: launch_batch_spread<4>(problems, strengths, count, has_2d, has_3d, shared_bytes, work, stream); break;
+    case 5: launch_batch_spread<5>(problems, strengths, count, has_2d, has_3d, shared_bytes, work, stream); break;
+    case 6: launch_batch_spread<6>(problems, strengths, count, has_2d, has_3d, shared_bytes, work, stream); break;
+    case 7: launch_batch_spread<7>(problems, strengths, count, has_2d, has_3d, shared_bytes, work, stream); break;
+    default: launch_batch_spread<8>(problems, strengths, count, has_2d, has_3d, shared_bytes, work, stream); break;
+  }
+}
+
+void spread_fold(const SpreadParams& sp, const SpreadLaunch& l, cudaStream_t stream) {
+  fold_any(sp, l.batch, l.scratch, l.part_start, l.part_upper_bound, l.candidates, l.fine, stream);
+}
+
+size_t spread_shared_bytes(const SpreadParams& sp) {
+  const int w = sp.grid.width;
+  const bool warp = sp.grid.dimensions == 3 && w >= kWarpMinWidth && w <= kWarpMaxWidth && sp.span > 0;
+  return static_cast<size_t>(F32Traits::kWordsPerCell) * (warp ? sp.span : sp.padded_cells) * sizeof(uint32_t);
+}
 
 void spread_count_parts(const SpreadParams& sp, const uint32_t* offsets, uint32_t* parts,
                         uint32_t* part_start, cudaStream_t stream, StageTimer* timer) {

@@ -114,6 +114,40 @@ struct SpreadLaunch64 {
   const uint32_t* valid_mask;
 };
 
+// One problem of a set of independent type-1 f32 problems spread by one
+// persistent launch (batch.cpp): its spreading parameters and the buffers
+// of its prepared point set.
+struct BatchProblem {
+  SpreadParams sp;
+  const void* windows;
+  const uint32_t* perm;
+  const uint32_t* offsets;
+  const uint32_t* part_start;
+  const uint32_t* valid_mask;
+  int64_t point_count;
+  uint32_t* max_bits;   // one word
+  float2* scratch;      // the problem's padded tiles
+};
+
+// The strengths of every problem of one execution, passed by value (kernel
+// parameters), so that an execution needs no host-to-device copy.
+constexpr int kMaxBatchProblems = 1024;
+struct BatchStrengths {
+  const float2* ptr[kMaxBatchProblems];
+};
+
+// Strength scales, then every (problem, tile part) of `count` problems from
+// one persistent launch whose CTAs take the items from a device counter in
+// order (`work`: count + 2 words). All problems share the window width.
+void batch_spread(const BatchProblem* problems, const BatchStrengths& strengths, int count, int width,
+                  bool has_2d, bool has_3d, size_t shared_bytes, uint32_t* work, cudaStream_t stream);
+
+// The fold of one problem's padded tiles onto its fine grid (after batch_spread).
+void spread_fold(const SpreadParams& sp, const SpreadLaunch& launch, cudaStream_t stream);
+
+// Dynamic shared memory of one spreading CTA of this plan.
+size_t spread_shared_bytes(const SpreadParams& sp);
+
 // Parts of every tile and their exclusive scan (tile_count + 1 words).
 void spread_count_parts(const SpreadParams& sp, const uint32_t* offsets, uint32_t* parts,
                         uint32_t* part_start, cudaStream_t stream, StageTimer* timer = nullptr);

@@ -121,6 +121,31 @@ def tune_tensor_threshold(torch, w, workloads, native, kind, repeats):
     return 0, ms
 
 
+def merge_keys(entries):
+    """One entry per key: workloads of the same key (uniform and clustered
+    points of one size and density) take the candidate with the least total
+    time over all of them."""
+    merged = {}
+    for e in entries:
+        k = tuple(sorted(e["key"].items()))
+        merged.setdefault(k, []).append(e)
+    out = []
+    for group in merged.values():
+        if len(group) == 1 or not all(g.get("candidates") for g in group):
+            out.append(group[0])
+            continue
+        totals = {}
+        for g in group:
+            for c in g["candidates"]:
+                choice = (c["tile"], c["ctas_per_sm"], c["crowded_ctas_per_sm"])
+                totals[choice] = totals.get(choice, 0.0) + c["ms"]
+        choice = min(totals, key=totals.get)
+        best = {"tile": choice[0], "ctas_per_sm": choice[1], "crowded_ctas_per_sm": choice[2], "ms": totals[choice]}
+        names = "+".join(g["workload"] for g in group)
+        out.append(dict(group[0], workload=names, best=best))
+    return out
+
+
 def table_header(entries):
     lines = ["// Tuned launch choices per workload key, written by wgpunufft_b200/tune.py",
              "// from measurements on a B200. Fields: type, dimensions, precision, width,",
@@ -144,8 +169,13 @@ def main():
     parser = argparse.ArgumentParser(description=__doc__, formatter_class=argparse.RawDescriptionHelpFormatter)
     parser.add_argument("--out", default=str(HERE / "csrc" / "tuning_table.h"))
     parser.add_argument("--report", default=None, help="JSON file for every measurement")
+    parser.add_argument("--from-report", default=None, help="write the table from an earlier report, no GPU")
     parser.add_argument("--repeats", type=int, default=5)
     args = parser.parse_args()
+    if args.from_report:
+        entries = json.loads(Path(args.from_report).read_text())["entries"]
+        Path(args.out).write_text(table_header(merge_keys(entries)))
+        return
     import torch
 
     import wgpunufft_b200 as w
@@ -167,7 +197,7 @@ def main():
                          tensor_min_batch=threshold2 or 1 << 30)
             entries.append(type2)
             break
-    Path(args.out).write_text(table_header(entries))
+    Path(args.out).write_text(table_header(merge_keys(entries)))
     report = {"entries": entries, "tensor_threshold": {"type1": [threshold1, {str(k): v for k, v in ms1.items()}],
                                                         "type2": [threshold2, {str(k): v for k, v in ms2.items()}]}}
     if args.report:
