@@ -54,7 +54,6 @@ class BatchExecutor {
       joins_.push_back(e);
     }
     check_cuda(cudaEventCreateWithFlags(&fork_, cudaEventDisableTiming), "batch event");
-    generations_.assign(plans_.size(), ~uint64_t{0});
   }
 
   ~BatchExecutor() {
@@ -89,34 +88,37 @@ class BatchExecutor {
   }
 
  private:
-  // Rebuilds the device descriptors after any plan's points changed (a
-  // synchronous upload: the first execution after set_points must not be
-  // captured in a graph).
+  // The device descriptors: rebuilt on the host every execution (a plan's
+  // own executions can grow its scratch buffer, set_points replaces its point
+  // set) and uploaded when they differ from the last upload. The upload is
+  // synchronous, so the first execution after set_points must not be
+  // captured in a graph.
   void refresh() {
-    bool stale = problems_.get() == nullptr;
-    for (size_t p = 0; p < plans_.size(); ++p) stale = stale || generations_[p] != plans_[p]->points_generation();
-    if (!stale) return;
     std::vector<BatchProblem> host(plans_.size());
-    shared_bytes_ = 0;
-    has_2d_ = has_3d_ = false;
+    size_t shared = 0;
+    bool has_2d = false, has_3d = false;
     for (size_t p = 0; p < plans_.size(); ++p) {
       if (!plans_[p]->batch_problem(&host[p])) {
         throw NufftFailure{B200NUFFT_GPU_EXECUTION_UNAVAILABLE,
                            "problem " + std::to_string(p) + " has no point set (b200nufft_set_points)"};
       }
-      generations_[p] = plans_[p]->points_generation();
-      shared_bytes_ = std::max(shared_bytes_, spread_shared_bytes(host[p].sp));
-      has_2d_ = has_2d_ || plans_[p]->dimensions() == 2;
-      has_3d_ = has_3d_ || plans_[p]->dimensions() == 3;
+      shared = std::max(shared, spread_shared_bytes(host[p].sp));
+      has_2d = has_2d || plans_[p]->dimensions() == 2;
+      has_3d = has_3d || plans_[p]->dimensions() == 3;
     }
-    void* d = problems_.reserve(host.size() * sizeof(BatchProblem), "batch descriptors");
-    check_cuda(cudaMemcpy(d, host.data(), host.size() * sizeof(BatchProblem), cudaMemcpyHostToDevice),
-               "upload batch descriptors");
+    const size_t bytes = host.size() * sizeof(BatchProblem);
+    if (uploaded_.size() == host.size() && std::memcmp(uploaded_.data(), host.data(), bytes) == 0) return;
+    void* d = problems_.reserve(bytes, "batch descriptors");
+    check_cuda(cudaMemcpy(d, host.data(), bytes, cudaMemcpyHostToDevice), "upload batch descriptors");
     work_.reserve((plans_.size() + 2) * sizeof(uint32_t), "batch work list");
+    uploaded_ = std::move(host);
+    shared_bytes_ = shared;
+    has_2d_ = has_2d;
+    has_3d_ = has_3d;
   }
 
   std::vector<NufftPlan*> plans_;
-  std::vector<uint64_t> generations_;
+  std::vector<BatchProblem> uploaded_;
   int device_ = 0;
   int width_ = 0;
   bool has_2d_ = false, has_3d_ = false;

@@ -560,7 +560,6 @@ void NufftPlan::set_points(int64_t count, const void* points, cudaStream_t strea
   }
   point_count_ = count;
   points_ = points;
-  ++points_generation_;
   tuned_ = tuning_for(tuning_key(type_, dim_, precision_, kernel_.width, fine_count_, count));
   if (dim_ > 3) {
     // No bins: the coordinates are kept (in f64 for Df64 plans) as given.

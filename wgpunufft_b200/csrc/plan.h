@@ -50,8 +50,6 @@ class NufftPlan {
   // the batch has spread its tiles: fold, FFT, deconvolution.
   bool batch_problem(BatchProblem* out);
   void finish_batch(void* output, cudaStream_t stream);
-  // Incremented by every set_points.
-  uint64_t points_generation() const { return points_generation_; }
   // Points of the last set_points (-1 before the first).
   int64_t points_set_count() const { return point_count_; }
   StageTimer& timer() { return timer_; }
@@ -127,7 +125,6 @@ class NufftPlan {
   std::map<int64_t, cufftHandle> nd_ffts_;    // by first axis of the group and batch
 
   // Remembered points and their bin order.
-  uint64_t points_generation_ = 0;
   int64_t point_count_ = -1;
   const void* points_ = nullptr;
   int geometry_ = -1;

@@ -2,6 +2,7 @@
 configurations, generated on the GPU, and a runner for profiling them.
 
     python -m wgpunufft_b200.workloads CASE [--batch B] [--executes N] [--kind 1|2|both]
+                                      [--method auto|cuda|tensor]
 
 Cases:
   small     2D 64^2 modes, 1e5 uniform points, eps 1e-6
@@ -152,7 +153,7 @@ def run_type3_small(d: int, executes: int) -> None:
     torch.cuda.synchronize()
 
 
-def run(case: str, batch: int, executes: int, kinds) -> None:
+def run(case: str, batch: int, executes: int, kinds, method: int = 0) -> None:
     import torch
 
     import wgpunufft_b200 as w
@@ -184,7 +185,7 @@ def run(case: str, batch: int, executes: int, kinds) -> None:
     for m in modes:
         n *= m
     for kind in kinds:
-        config = w.NufftConfig(modes, eps, batch=batch)
+        config = w.NufftConfig(modes, eps, batch=batch, spread_method=method)
         plan = (w.NufftPlan.type1_gpu if kind == 1 else w.NufftPlan.type2_gpu)(config)
         plan.set_points_gpu(p)
         inputs = values(batch, count if kind == 1 else n)
@@ -202,10 +203,13 @@ def main() -> None:
     parser.add_argument("--batch", type=int, default=None)
     parser.add_argument("--executes", type=int, default=2)
     parser.add_argument("--kind", choices=["1", "2", "both"], default="both")
+    parser.add_argument("--method", choices=["auto", "cuda", "tensor"], default="auto",
+                        help="spreading / interpolation engine (the plan's spread_method)")
     args = parser.parse_args()
     batch = args.batch if args.batch is not None else (64 if args.case == "batched" else 1)
     kinds = (1, 2) if args.kind == "both" else (int(args.kind),)
-    run(args.case, batch, args.executes, kinds)
+    method = {"auto": 0, "cuda": 1, "tensor": 2}[args.method]
+    run(args.case, batch, args.executes, kinds, method)
     print("ok")
 
 
