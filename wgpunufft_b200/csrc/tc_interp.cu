@@ -14,17 +14,20 @@
 // the runs of at most 32 points of one (row, group) bin, in row order.
 //
 // Per execution, one CTA per (tile part, 64 vectors) walks its chunks in row
-// order. The fine-grid rows the chunks reach (16 columns x 64 vectors) are
-// brought into shared memory by bulk copies two rows ahead, converted into
-// tf32 high and low parts in the UMMA K-major layout (128 rows: real and
-// imaginary part of every vector) and kept in a ring of w + 1 rows. A chunk
-// at row y is 2 w MMA steps (window row j, column half h) of M = 128,
-// N = 16 or 32 points, K = 8 cells: A = ring row y + j, B = the points'
-// weights wy[j] wx over the same cells (zero outside their windows), each
-// split into three tf32 MMAs (A_hi B_hi + A_hi B_lo + A_lo B_hi) into one of
-// four tensor-memory accumulators. Two chunks later the accumulator is read
-// out to the values in tensor-core slot order, and a final pass writes them
-// in the caller's point order. Every output comes from the MMAs of one chunk
+// order with warp-specialised roles joined by mbarriers. A producer warp
+// brings the fine-grid rows the chunks reach (16 columns x 64 vectors) into
+// shared memory by bulk copies, three rows ahead; two converter warps split
+// every row into tf32 high and low parts in the UMMA K-major layout (128
+// rows: real and imaginary part of every vector) into a ring of w + 1 rows;
+// two builder teams take alternate chunks, bulk-copy their points' window
+// records and write B = wy[j] wx over the chunk's cells (zero outside each
+// window); one thread issues, per chunk at row y, 2 w MMA steps (window row
+// j, column half h) of M = 128, N = 16 or 32 points, K = 8 cells, A = ring
+// row y + j, each split into three tf32 MMAs (A_hi B_hi + A_hi B_lo + A_lo
+// B_hi), into one of four tensor-memory accumulators, and retires ring rows
+// the next chunk no longer reads; four read-out warps move each accumulator
+// to the values in tensor-core slot order, and a final pass writes them in
+// the caller's point order. Every output comes from the MMAs of one chunk
 // issued in a fixed order, so results are bitwise repeatable.
 //
 // Every wait is bounded: a wait that gives up stops the CTA's work, lets the
@@ -44,23 +47,35 @@ namespace {
 
 using namespace tc;
 
-constexpr int kThreads = 256;
+// Warp roles.
+constexpr int kProducerWarp = 0;
+constexpr int kMmaWarp = 1;
+constexpr int kConvertWarp0 = 2;   // two warps: 64 threads convert every row
+constexpr int kBuildWarp0 = 4;     // four warps: two teams of 64 threads, alternate chunks
+constexpr int kReadWarp0 = 8;      // four warps: one per tensor-memory lane quadrant
+constexpr int kThreads = 12 * 32;
+constexpr int kConvertThreads = 64;
+constexpr int kTeamThreads = 64;
+constexpr int kReadThreads = 128;
+
 constexpr int kBuffers = 4;            // tensor-memory accumulators of 32 columns
 constexpr int kTmemColumns = 128;
-constexpr int kRawSlots = 2;           // rows fetched ahead
+constexpr int kRawSlots = 3;           // rows fetched ahead
+constexpr int kBStages = 2;            // one per builder team
 constexpr int kRawPitch = 144;         // bytes per vector of a fetched row (128 + 16 against bank conflicts)
 constexpr int kRawBytes = kTi2Vectors * kRawPitch;
 constexpr int kRowHalf = 8192;         // one tf32 part of a converted row: 128 rows x 16 columns
 constexpr int kRowBytes = 2 * kRowHalf;
+constexpr int kWeightStage = kTi2ChunkPoints * static_cast<int>(sizeof(TcWeights));
 
 template <int W>
 struct Ti2Layout {
   static constexpr int kRing = W + 1;
   static constexpr int kBHalf = kTi2ChunkPoints * kTi2Pitch * W * 4;  // one tf32 part of B: 32 x 16 W
   static constexpr int kBBase = kRing * kRowBytes;
-  static constexpr int kRawBase = kBBase + 2 * 2 * kBHalf;
+  static constexpr int kRawBase = kBBase + kBStages * 2 * kBHalf;
   static constexpr int kWeightsBase = kRawBase + kRawSlots * kRawBytes;
-  static constexpr int kBytes = kWeightsBase + kTi2ChunkPoints * static_cast<int>(sizeof(TcWeights));
+  static constexpr int kBytes = kWeightsBase + kBStages * kWeightStage;
   static constexpr uint32_t kBStride = 512u * W;  // bytes between 8-point groups of B
 };
 
@@ -158,11 +173,12 @@ __global__ void ti2_chunk_fill_kernel(GridParams g, int64_t tiles, const uint32_
 
 // Converts fetched row `raw` (64 vectors x 16 complex cells at kRawPitch)
 // into tf32 high and low parts at `ring` (K-major: 4 K blocks of 128 bytes,
-// 16 groups of 8 rows 512 bytes apart; row m = 2 v + part).
-__device__ __forceinline__ void ti2_convert_row(const unsigned char* raw, unsigned char* ring, int nv, int tid) {
+// 16 groups of 8 rows 512 bytes apart; row m = 2 v + part), with the 64
+// converter threads (t = thread index among them).
+__device__ __forceinline__ void ti2_convert_row(const unsigned char* raw, unsigned char* ring, int nv, int t) {
 #pragma unroll
-  for (int i = 0; i < 2; ++i) {
-    const int u = tid + i * kThreads;
+  for (int i = 0; i < 512 / kConvertThreads; ++i) {
+    const int u = t + i * kConvertThreads;
     const int kb = u >> 7, m = u & 127, v = m >> 1, part = m & 1;
     float4 value = make_float4(0.0f, 0.0f, 0.0f, 0.0f);
     if (v < nv) {
@@ -189,11 +205,13 @@ __global__ void __launch_bounds__(kThreads, 1) tc_interp_kernel(
     uint32_t* __restrict__ error_flag) {
   using L = Ti2Layout<W>;
   extern __shared__ __align__(1024) unsigned char smem[];
-  __shared__ __align__(8) uint64_t done_bar[kBuffers];
-  __shared__ __align__(8) uint64_t raw_bar[kRawSlots];
+  __shared__ __align__(8) uint64_t raw_full[kRawSlots], raw_empty[kRawSlots];
+  __shared__ __align__(8) uint64_t a_full[L::kRing], a_empty[L::kRing];
+  __shared__ __align__(8) uint64_t b_full[kBStages], b_empty[kBStages], w_full[kBStages], w_empty[kBStages];
+  __shared__ __align__(8) uint64_t d_full[kBuffers], d_empty[kBuffers];
   __shared__ uint32_t tmem_base;
   __shared__ int64_t s_tile;
-  __shared__ int s_ok;
+  __shared__ int s_abort;
   __shared__ Ti2Chunk s_chunks[kTi2ChunksPerPart];
 
   const uint32_t part = blockIdx.x;
@@ -207,11 +225,25 @@ __global__ void __launch_bounds__(kThreads, 1) tc_interp_kernel(
       if (part_start[mid] <= part) low = mid; else high = mid - 1;
     }
     s_tile = low;
-    s_ok = 1;
-#pragma unroll
-    for (int b = 0; b < kBuffers; ++b) mbar_init(&done_bar[b], 1);
-#pragma unroll
-    for (int s = 0; s < kRawSlots; ++s) mbar_init(&raw_bar[s], 1);
+    s_abort = 0;
+    for (int s = 0; s < kRawSlots; ++s) {
+      mbar_init(&raw_full[s], 1);
+      mbar_init(&raw_empty[s], kConvertThreads);
+    }
+    for (int s = 0; s < L::kRing; ++s) {
+      mbar_init(&a_full[s], kConvertThreads);
+      mbar_init(&a_empty[s], 1);
+    }
+    for (int s = 0; s < kBStages; ++s) {
+      mbar_init(&b_full[s], kTeamThreads);
+      mbar_init(&b_empty[s], 1);
+      mbar_init(&w_full[s], 1);
+      mbar_init(&w_empty[s], kTeamThreads);
+    }
+    for (int b = 0; b < kBuffers; ++b) {
+      mbar_init(&d_full[b], 1);
+      mbar_init(&d_empty[b], kReadThreads);
+    }
     asm volatile("fence.mbarrier_init.release.cluster;" ::: "memory");
   }
   if (warp == 0) {
@@ -236,192 +268,214 @@ __global__ void __launch_bounds__(kThreads, 1) tc_interp_kernel(
   const int x0 = tx * kTi2GroupX, y0 = ty * kTi2TileRows;
   const int vb = group * kTi2Vectors;
   const int nv = min(kTi2Vectors, batch - vb);
-  // Rows [r_begin, r_end) relative to y0 are fetched and converted in order.
+  // Rows [r_begin, r_begin + rows) relative to y0 are fetched and converted in order.
   const int r_begin = n > 0 ? s_chunks[0].row : 0;
-  const int r_end = n > 0 ? s_chunks[n - 1].row + W : 0;
+  const int rows = n > 0 ? s_chunks[n - 1].row + W - r_begin : 0;
   unsigned char* ring = smem;
   unsigned char* raw = smem + L::kRawBase;
-  const TcWeights* s_w = reinterpret_cast<const TcWeights*>(smem + L::kWeightsBase);
+  volatile int* abort_flag = &s_abort;
 
-  // Fetches relative row r (its k-th fetch, k = r - r_begin) into raw slot k % 2.
-  auto fetch = [&](int r) {
-    const int k = r - r_begin;
-    const uint32_t bar = smem_u32(&raw_bar[k % kRawSlots]);
-    unsigned char* dst = raw + (k % kRawSlots) * kRawBytes;
-    int y = (y0 + r) % n1;
-    const int64_t row = static_cast<int64_t>(y) * n0;
-    mbar_expect(bar, static_cast<uint32_t>(nv) * 128u);
-    for (int v = 0; v < nv; ++v) {
-      const float2* grid = fine + static_cast<int64_t>(vb + v) * g.fine_count + row;
-      const uint32_t d = smem_u32(dst + v * kRawPitch);
-      if (x0 + 2 * kTi2GroupX <= n0) {
-        bulk_load(d, grid + x0, 128, bar);
-      } else {
-        bulk_load(d, grid + x0, 64, bar);
-        bulk_load(d + 64, grid, 64, bar);
-      }
-    }
-  };
-  int fetched = r_begin;  // rows [r_begin, fetched) have been fetched
-  if (tid == 0) {
-    for (; fetched < min(r_end, r_begin + kRawSlots); ++fetched) fetch(fetched);
-  }
-
-  int ring_hi = r_begin;  // rows [.., ring_hi) are converted
-  int issued = 0;
-  bool aborted = false;
-  for (int c = 0; c < n + 2 && !aborted; ++c) {
-    const int r = c < n ? s_chunks[c].row : 0;
-    const int rows_now = c < n ? min(r + W, ring_hi + kRawSlots) - ring_hi : 0;
-    if (tid == 0) {
+  if (warp == kProducerWarp) {
+    // Row k into raw slot k % 3 once the converters are done with row k - 3.
+    int issued = 0;
+    for (int k = 0; k < rows; ++k) {
+      const int slot = k % kRawSlots;
       bool ok = true;
-      if (c >= 2) ok = mbar_wait(smem_u32(&done_bar[(c - 2) % kBuffers]), static_cast<uint32_t>((c - 2) / kBuffers) & 1u,
-                                 nullptr);
-      // New rows overwrite ring slots of rows that chunk c - 1 may still read
-      // when chunk c starts two or more rows below it.
-      if (ok && c >= 1 && c < n && r >= s_chunks[c - 1].row + 2) {
-        ok = mbar_wait(smem_u32(&done_bar[(c - 1) % kBuffers]), static_cast<uint32_t>((c - 1) / kBuffers) & 1u,
-                       nullptr);
+      if (lane == 0 && k >= kRawSlots) {
+        ok = mbar_wait(smem_u32(&raw_empty[slot]), static_cast<uint32_t>(k / kRawSlots - 1) & 1u, abort_flag);
       }
-      for (int q = 0; ok && q < rows_now; ++q) {
-        const int k = ring_hi + q - r_begin;
-        ok = mbar_wait(smem_u32(&raw_bar[k % kRawSlots]), static_cast<uint32_t>(k / kRawSlots) & 1u, nullptr);
+      ok = __shfl_sync(0xFFFFFFFFu, ok ? 1 : 0, 0) != 0;
+      if (!ok) break;
+      const uint32_t bar = smem_u32(&raw_full[slot]);
+      if (lane == 0) mbar_expect(bar, static_cast<uint32_t>(nv) * 128u);
+      __syncwarp();
+      const int y = (y0 + r_begin + k) % n1;
+      const int64_t row = static_cast<int64_t>(y) * n0;
+      unsigned char* dst = raw + slot * kRawBytes;
+      for (int v = lane; v < nv; v += 32) {
+        const float2* grid = fine + static_cast<int64_t>(vb + v) * g.fine_count + row;
+        const uint32_t d = smem_u32(dst + v * kRawPitch);
+        if (x0 + 2 * kTi2GroupX <= n0) {
+          bulk_load(d, grid + x0, 128, bar);
+        } else {
+          bulk_load(d, grid + x0, 64, bar);
+          bulk_load(d + 64, grid, 64, bar);
+        }
       }
-      s_ok = ok ? 1 : 0;
+      issued = k + 1;
     }
-    __syncthreads();
-    if (!s_ok) {
-      aborted = true;
-      break;
+    // Copies in flight land before the CTA leaves (bounded, without abort).
+    if (lane == 0) {
+      for (int k = max(0, issued - kRawSlots); k < issued; ++k) {
+        if (!mbar_wait(smem_u32(&raw_full[k % kRawSlots]), static_cast<uint32_t>(k / kRawSlots) & 1u, nullptr)) {
+          *abort_flag = 1;
+        }
+      }
     }
-    tc_fence_after();
-    if (c >= 2) {
-      // Read out chunk c - 2: warp w holds rows 32 (w % 4) + lane (vector
-      // m / 2, real part when m is even) of columns 16 (w / 4) .. + 15.
-      const int cc = c - 2;
-      const Ti2Chunk ch = s_chunks[cc];
-      const int col0 = warp >= 4 ? 16 : 0;
-      if (col0 < ch.count) {
-        uint32_t v[16];
-        tmem_ld16(tm + (static_cast<uint32_t>((warp & 3) * 32) << 16) + static_cast<uint32_t>((cc % kBuffers) * 32 + col0),
-                  v);
-        tmem_wait_ld();
-        const int m = (warp & 3) * 32 + lane;
-        const int vec = m >> 1;
+  } else if (warp == kMmaWarp) {
+    if (lane == 0) {
+      int ready = 0;    // rows [0, ready) relative to r_begin are converted
+      int retired = 0;  // rows [0, retired) are released to the converters
+      int issued = 0;
+      bool ok = true;
+      for (int c = 0; c < n && ok; ++c) {
+        const Ti2Chunk ch = s_chunks[c];
+        const int r = ch.row - r_begin;
+        while (ok && ready < r + W) {
+          ok = mbar_wait(smem_u32(&a_full[ready % L::kRing]), static_cast<uint32_t>(ready / L::kRing) & 1u, abort_flag);
+          ready += ok ? 1 : 0;
+          // Rows below this chunk's first row are read by no later chunk:
+          // release them at once, so rows skipped between chunks free their
+          // ring slots while this chunk waits for its own rows.
+          for (; retired < min(r, ready); ++retired) mma_commit(smem_u32(&a_empty[retired % L::kRing]));
+        }
+        ok = ok && mbar_wait(smem_u32(&b_full[c % kBStages]), static_cast<uint32_t>(c / kBStages) & 1u, abort_flag);
+        if (ok && c >= kBuffers) {
+          ok = mbar_wait(smem_u32(&d_empty[c % kBuffers]), static_cast<uint32_t>(c / kBuffers - 1) & 1u, abort_flag);
+        }
+        if (!ok) break;
+        tc_fence_after();
+        const int cols = ch.count <= 16 ? 16 : 32;
+        const uint32_t idesc = idesc_tf32(128, static_cast<uint32_t>(cols));
+        const uint32_t d = tm + static_cast<uint32_t>((c % kBuffers) * 32);
+        const uint32_t bh = smem_u32(smem + L::kBBase + (c % kBStages) * 2 * L::kBHalf);
+        const uint32_t bl = bh + L::kBHalf;
+#pragma unroll 1
+        for (int j = 0; j < W; ++j) {
+          const uint32_t rb = smem_u32(ring + ((r + j) % L::kRing) * kRowBytes);
+#pragma unroll
+          for (int h = 0; h < 2; ++h) {
+            const uint64_t ahi = kmajor_desc(rb + h * 256, 128, 512);
+            const uint64_t alo = kmajor_desc(rb + kRowHalf + h * 256, 128, 512);
+            const uint64_t bhi = kmajor_desc(bh + (4 * j + 2 * h) * 128, 128, L::kBStride);
+            const uint64_t blo = kmajor_desc(bl + (4 * j + 2 * h) * 128, 128, L::kBStride);
+            mma_tf32(d, ahi, bhi, idesc, j > 0 || h > 0);
+            mma_tf32(d, ahi, blo, idesc, true);
+            mma_tf32(d, alo, bhi, idesc, true);
+          }
+        }
+        mma_commit(smem_u32(&b_empty[c % kBStages]));
+        mma_commit(smem_u32(&d_full[c % kBuffers]));
+        issued = c + 1;
+        // Rows below the next chunk's first row are read by no later chunk.
+        const int next = c + 1 < n ? s_chunks[c + 1].row - r_begin : rows;
+        for (; retired < min(next, ready); ++retired) mma_commit(smem_u32(&a_empty[retired % L::kRing]));
+      }
+      if (issued > 0 &&
+          !mbar_wait(smem_u32(&d_full[(issued - 1) % kBuffers]), static_cast<uint32_t>((issued - 1) / kBuffers) & 1u,
+                     nullptr)) {
+        *abort_flag = 1;
+      }
+      if (!ok) *abort_flag = 1;
+    }
+  } else if (warp < kBuildWarp0) {
+    // Converters.
+    const int t = tid - kConvertWarp0 * 32;
+    for (int k = 0; k < rows; ++k) {
+      if (!mbar_wait(smem_u32(&raw_full[k % kRawSlots]), static_cast<uint32_t>(k / kRawSlots) & 1u, abort_flag)) break;
+      if (k >= L::kRing &&
+          !mbar_wait(smem_u32(&a_empty[k % L::kRing]), static_cast<uint32_t>(k / L::kRing - 1) & 1u, abort_flag)) {
+        break;
+      }
+      ti2_convert_row(raw + (k % kRawSlots) * kRawBytes, ring + (k % L::kRing) * kRowBytes, nv, t);
+      asm volatile("fence.proxy.async.shared::cta;" ::: "memory");
+      mbar_arrive(smem_u32(&a_full[k % L::kRing]));
+      mbar_arrive(smem_u32(&raw_empty[k % kRawSlots]));
+    }
+  } else if (warp < kReadWarp0) {
+    // Builder teams: team e takes chunks c = e (mod 2) into B stage e.
+    const int team = (warp - kBuildWarp0) >> 1;
+    const int t = tid - kBuildWarp0 * 32 - team * kTeamThreads;
+    unsigned char* wst = smem + L::kWeightsBase + team * kWeightStage;
+    const TcWeights* s_w = reinterpret_cast<const TcWeights*>(wst);
+    unsigned char* b_hi = smem + L::kBBase + team * 2 * L::kBHalf;
+    unsigned char* b_lo = b_hi + L::kBHalf;
+    int loads = 0;
+    for (int c = team; c < n; c += kBStages) {
+      const Ti2Chunk ch = s_chunks[c];
+      const int use = c / kBStages;
+      const uint32_t wbar = smem_u32(&w_full[team]);
+      if (t == 0) {
+        // The team's previous records are read (every team thread arrived).
+        if (use >= 1 && !mbar_wait(smem_u32(&w_empty[team]), static_cast<uint32_t>(use - 1) & 1u, abort_flag)) break;
+        const uint32_t bytes = static_cast<uint32_t>(ch.count) * static_cast<uint32_t>(sizeof(TcWeights));
+        mbar_expect(wbar, bytes);
+        bulk_load(smem_u32(wst), weights + ch.slot, bytes, wbar);
+        loads = use + 1;
+      }
+      if (!mbar_wait(wbar, static_cast<uint32_t>(use) & 1u, abort_flag)) break;
+      if (use >= 1 && !mbar_wait(smem_u32(&b_empty[team]), static_cast<uint32_t>(use - 1) & 1u, abort_flag)) break;
+      const int cols = ch.count <= 16 ? 16 : 32;
+      for (int u = t; u < cols * 4 * W; u += kTeamThreads) {
+        const int kb = u / cols, pn = u - kb * cols;
+        float4 value = make_float4(0.0f, 0.0f, 0.0f, 0.0f);
+        if (pn < ch.count) {
+          const float wy = s_w[pn].wy[kb >> 2];
+          const float4 wx = *reinterpret_cast<const float4*>(&s_w[pn].wxs[4 * (kb & 3)]);
+          value = make_float4(wy * wx.x, wy * wx.y, wy * wx.z, wy * wx.w);
+        }
+        float4 hi, lo;
+        split_tf32(value.x, hi.x, lo.x);
+        split_tf32(value.y, hi.y, lo.y);
+        split_tf32(value.z, hi.z, lo.z);
+        split_tf32(value.w, hi.w, lo.w);
+        const int off = kb * 128 + (pn >> 3) * static_cast<int>(L::kBStride) + (pn & 7) * 16;
+        *reinterpret_cast<float4*>(b_hi + off) = hi;
+        *reinterpret_cast<float4*>(b_lo + off) = lo;
+      }
+      asm volatile("fence.proxy.async.shared::cta;" ::: "memory");
+      mbar_arrive(smem_u32(&b_full[team]));
+      mbar_arrive(smem_u32(&w_empty[team]));
+    }
+    // A weight copy in flight lands before the CTA leaves.
+    if (t == 0 && loads > 0 &&
+        !mbar_wait(smem_u32(&w_full[team]), static_cast<uint32_t>(loads - 1) & 1u, nullptr)) {
+      *abort_flag = 1;
+    }
+  } else {
+    // Read-out: warp q holds rows 32 q + lane (vector m / 2, real part when
+    // m is even) of each accumulator; values go out in tensor-core slot order.
+    const int q = warp - kReadWarp0;
+    const int m = q * 32 + lane;
+    const int vec = m >> 1;
+    for (int c = 0; c < n; ++c) {
+      if (!mbar_wait(smem_u32(&d_full[c % kBuffers]), static_cast<uint32_t>(c / kBuffers) & 1u, abort_flag)) break;
+      tc_fence_after();
+      const Ti2Chunk ch = s_chunks[c];
+      const uint32_t addr = tm + (static_cast<uint32_t>(q * 32) << 16) + static_cast<uint32_t>((c % kBuffers) * 32);
+      uint32_t v0[16], v1[16];
+      tmem_ld16(addr, v0);
+      if (ch.count > 16) tmem_ld16(addr + 16, v1);
+      tmem_wait_ld();
+      tc_fence_before();
+      mbar_arrive(smem_u32(&d_empty[c % kBuffers]));
+#pragma unroll
+      for (int i = 0; i < 16; ++i) {
+        const float x = __uint_as_float(v0[i]);
+        const float y = __shfl_xor_sync(0xFFFFFFFFu, x, 1);
+        if ((m & 1) == 0 && i < ch.count && vec < nv) {
+          staged[(static_cast<int64_t>(ch.slot) + i) * staged_stride + vb + vec] = make_float2(x, y);
+        }
+      }
+      if (ch.count > 16) {
 #pragma unroll
         for (int i = 0; i < 16; ++i) {
-          const float x = __uint_as_float(v[i]);
+          const float x = __uint_as_float(v1[i]);
           const float y = __shfl_xor_sync(0xFFFFFFFFu, x, 1);
-          const int p = col0 + i;
-          if ((m & 1) == 0 && p < ch.count && vec < nv) {
-            staged[(static_cast<int64_t>(ch.slot) + p) * staged_stride + vb + vec] = make_float2(x, y);
+          if ((m & 1) == 0 && 16 + i < ch.count && vec < nv) {
+            staged[(static_cast<int64_t>(ch.slot) + 16 + i) * staged_stride + vb + vec] = make_float2(x, y);
           }
         }
       }
     }
-    if (c >= n) continue;
-    const Ti2Chunk ch = s_chunks[c];
-    // Rows fetched ahead, converted into the ring; the chunk's window records.
-    for (int q = 0; q < rows_now; ++q) {
-      const int rr = ring_hi + q;
-      ti2_convert_row(raw + ((rr - r_begin) % kRawSlots) * kRawBytes, ring + (rr % L::kRing) * kRowBytes, nv, tid);
-    }
-    if (tid < 7 * ch.count) {
-      const float4* src = reinterpret_cast<const float4*>(weights + ch.slot);
-      reinterpret_cast<float4*>(smem + L::kWeightsBase)[tid] = src[tid];
-    }
-    __syncthreads();
-    ring_hi += rows_now;
-    if (tid == 0) {
-      for (; fetched < min(r_end, ring_hi + kRawSlots); ++fetched) fetch(fetched);
-    }
-    // A chunk far below the last one needs more rows than were fetched ahead.
-    while (ring_hi < r + W) {
-      if (tid == 0) {
-        const int k = ring_hi - r_begin;
-        s_ok = mbar_wait(smem_u32(&raw_bar[k % kRawSlots]), static_cast<uint32_t>(k / kRawSlots) & 1u, nullptr) ? 1 : 0;
-      }
-      __syncthreads();
-      if (!s_ok) {
-        aborted = true;
-        break;
-      }
-      ti2_convert_row(raw + ((ring_hi - r_begin) % kRawSlots) * kRawBytes, ring + (ring_hi % L::kRing) * kRowBytes, nv,
-                      tid);
-      __syncthreads();
-      ++ring_hi;
-      if (tid == 0) {
-        for (; fetched < min(r_end, ring_hi + kRawSlots); ++fetched) fetch(fetched);
-      }
-    }
-    if (aborted) break;
-    // B: point n, K unit kb (window row kb / 4, columns 4 (kb % 4) .. + 3).
-    const int cols = ch.count <= 16 ? 16 : 32;
-    unsigned char* b_hi = smem + L::kBBase + (c & 1) * 2 * L::kBHalf;
-    unsigned char* b_lo = b_hi + L::kBHalf;
-    for (int u = tid; u < cols * 4 * W; u += kThreads) {
-      const int kb = u / cols, pn = u - kb * cols;
-      float4 value = make_float4(0.0f, 0.0f, 0.0f, 0.0f);
-      if (pn < ch.count) {
-        const float wy = s_w[pn].wy[kb >> 2];
-        const float4 wx = *reinterpret_cast<const float4*>(&s_w[pn].wxs[4 * (kb & 3)]);
-        value = make_float4(wy * wx.x, wy * wx.y, wy * wx.z, wy * wx.w);
-      }
-      float4 hi, lo;
-      split_tf32(value.x, hi.x, lo.x);
-      split_tf32(value.y, hi.y, lo.y);
-      split_tf32(value.z, hi.z, lo.z);
-      split_tf32(value.w, hi.w, lo.w);
-      const int off = kb * 128 + (pn >> 3) * static_cast<int>(L::kBStride) + (pn & 7) * 16;
-      *reinterpret_cast<float4*>(b_hi + off) = hi;
-      *reinterpret_cast<float4*>(b_lo + off) = lo;
-    }
-    asm volatile("fence.proxy.async.shared::cta;" ::: "memory");
-    tc_fence_before();
-    __syncthreads();
-    if (tid == 0) {
-      tc_fence_after();
-      const uint32_t idesc = idesc_tf32(128, static_cast<uint32_t>(cols));
-      const uint32_t d = tm + static_cast<uint32_t>((c % kBuffers) * 32);
-      const uint32_t bh = smem_u32(b_hi), bl = smem_u32(b_lo);
-#pragma unroll 1
-      for (int j = 0; j < W; ++j) {
-        const uint32_t rb = smem_u32(ring + ((ch.row + j) % L::kRing) * kRowBytes);
-#pragma unroll
-        for (int h = 0; h < 2; ++h) {
-          const uint64_t ahi = kmajor_desc(rb + h * 256, 128, 512);
-          const uint64_t alo = kmajor_desc(rb + kRowHalf + h * 256, 128, 512);
-          const uint64_t bhi = kmajor_desc(bh + (4 * j + 2 * h) * 128, 128, L::kBStride);
-          const uint64_t blo = kmajor_desc(bl + (4 * j + 2 * h) * 128, 128, L::kBStride);
-          mma_tf32(d, ahi, bhi, idesc, j > 0 || h > 0);
-          mma_tf32(d, ahi, blo, idesc, true);
-          mma_tf32(d, alo, bhi, idesc, true);
-        }
-      }
-      mma_commit(smem_u32(&done_bar[c % kBuffers]));
-    }
-    issued = c + 1;
   }
 
-  // Drain: the MMAs and the fetches in flight finish before the CTA leaves.
-  if (tid == 0) {
-    bool drained = true;
-    if (issued > 0) {
-      drained = mbar_wait(smem_u32(&done_bar[(issued - 1) % kBuffers]),
-                          static_cast<uint32_t>((issued - 1) / kBuffers) & 1u, nullptr);
-    }
-    for (int r = ring_hi; r < fetched; ++r) {
-      const int k = r - r_begin;
-      drained = mbar_wait(smem_u32(&raw_bar[k % kRawSlots]), static_cast<uint32_t>(k / kRawSlots) & 1u, nullptr) &&
-                drained;
-    }
-    if (aborted || !drained) atomicAdd(error_flag, 1u);
-  }
   tc_fence_before();
   __syncthreads();
   if (warp == 0) {
     asm volatile("tcgen05.dealloc.cta_group::1.sync.aligned.b32 %0, %1;" ::"r"(tm), "r"(kTmemColumns));
   }
+  if (tid == 0 && *abort_flag) atomicAdd(error_flag, 1u);
 }
 
 template <int W>
@@ -434,7 +488,7 @@ void launch_weights(const GridParams& g, const Ti2Prepare& p, cudaStream_t strea
 template <int W>
 void launch_interp(const GridParams& g, const Ti2Launch& l, int64_t tiles, int64_t stride, cudaStream_t stream) {
   using L = Ti2Layout<W>;
-  static_assert(L::kBytes <= 227 * 1024, "tensor-core interpolation stages exceed shared memory");
+  static_assert(L::kBytes + 4096 <= 227 * 1024, "tensor-core interpolation stages exceed shared memory");
   auto kernel = tc_interp_kernel<W>;
   check_cuda(cudaFuncSetAttribute(kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, L::kBytes),
              "tensor-core interpolation shared memory");
