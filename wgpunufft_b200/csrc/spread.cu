@@ -159,7 +159,9 @@ __global__ void part_cap_kernel(SpreadParams sp, const uint32_t* __restrict__ of
 
 // Largest |re| or |im| of every strength vector, as magnitude bits, over
 // the points within reach when a mask is given (others get zero weight, so
-// their strengths must not change the fixed-point scale).
+// their strengths must not change the fixed-point scale). A thread takes
+// four consecutive values (two 16-byte loads when the vector is 16-byte
+// aligned) and the mask bits of those four points.
 template <typename T>
 __global__ void strength_magnitude_kernel(const typename T::Complex* __restrict__ values,
                                           int64_t count, int batch,
@@ -168,13 +170,17 @@ __global__ void strength_magnitude_kernel(const typename T::Complex* __restrict_
   const int b = blockIdx.y;
   const typename T::Complex* v = values + static_cast<int64_t>(b) * count;
   typename T::Bits m = 0;
-  const int64_t stride = static_cast<int64_t>(gridDim.x) * blockDim.x;
-  for (int64_t i = static_cast<int64_t>(blockIdx.x) * blockDim.x + threadIdx.x; i < count;
-       i += stride) {
-    if (valid_mask != nullptr && !((__ldg(&valid_mask[i >> 5]) >> (i & 31)) & 1u)) continue;
-    const typename T::Complex s = v[i];
-    m = max(m, T::magnitude_bits(s.x));
-    m = max(m, T::magnitude_bits(s.y));
+  const int64_t stride = static_cast<int64_t>(gridDim.x) * blockDim.x * 4;
+  for (int64_t i = (static_cast<int64_t>(blockIdx.x) * blockDim.x + threadIdx.x) * 4; i < count; i += stride) {
+    const uint32_t bits = valid_mask != nullptr ? (__ldg(&valid_mask[i >> 5]) >> (i & 31)) : 0xFu;
+#pragma unroll
+    for (int k = 0; k < 4; ++k) {
+      if (i + k < count && ((bits >> k) & 1u)) {
+        const typename T::Complex s = v[i + k];
+        m = max(m, T::magnitude_bits(s.x));
+        m = max(m, T::magnitude_bits(s.y));
+      }
+    }
   }
 #pragma unroll
   for (int offset = 16; offset > 0; offset >>= 1) m = max(m, __shfl_xor_sync(0xFFFFFFFFu, m, offset));
@@ -1439,7 +1445,7 @@ void spread_execute_impl(const SpreadParams& sp, const SpreadLaunchT<T>& l, cuda
       check_cuda(cudaMemsetAsync(l.max_bits, 0, sizeof(typename T::Bits) * l.batch, stream),
                  "clear maxima");
       const unsigned blocks =
-          static_cast<unsigned>(std::min<int64_t>((l.point_count + 255) / 256, 148 * 8));
+          static_cast<unsigned>(std::min<int64_t>((l.point_count + 1023) / 1024, 148 * 8));
       strength_magnitude_kernel<T><<<dim3(blocks, l.batch), 256, 0, stream>>>(
           l.strengths, l.point_count, l.batch, l.max_bits, l.valid_mask);
       note_launch();
