@@ -88,19 +88,21 @@ def test_f64_matches_direct_sums(n_modes, eps, factor):
 
 
 @pytest.mark.parametrize("n_modes", [(32, 28), (10, 12, 8)])
-def test_df64_storage_matches_direct_sums(n_modes):
+@pytest.mark.parametrize("eps,bound", [(1e-9, 24e-9), (1e-11, 5e-11)])
+def test_df64_storage_matches_direct_sums(n_modes, eps, bound):
+    """Df64 plans within the reference's bounds (tests/gpu_nufft_df64.rs:16-20:
+    24 eps; 5e-11 at eps 1e-11)."""
     d = len(n_modes)
-    eps = 1e-11
-    rng = np.random.default_rng(d)
+    rng = np.random.default_rng([d, int(-np.log10(eps))])
     points = uniform64(rng, 1500, d)
     strengths = cnormal(rng, 1500)
     coefficients = cnormal(rng, int(np.prod(n_modes)))
     got1, _ = run(1, n_modes, eps, points, strengths, precision=w.Precision.DF64)
     ref1 = native.direct_type1(points, strengths, n_modes)
-    assert rel_l2(got1, ref1) < 5e-11
+    assert rel_l2(got1, ref1) < bound
     got2, _ = run(2, n_modes, eps, points, coefficients, precision=w.Precision.DF64)
     ref2 = native.direct_type2(points, coefficients, n_modes)
-    assert rel_l2(got2, ref2) < 5e-11
+    assert rel_l2(got2, ref2) < bound
 
 
 @pytest.mark.parametrize("n_modes", [(300,), (64, 64), (16, 12, 10)])
