@@ -385,3 +385,47 @@ def test_f64_type2_staged_regions_match_the_gather_bitwise():
     assert np.array_equal(outs[0][0].view(np.int64), outs[1][0].view(np.int64))
     ref = native.direct_type2(points, coefficients[:1], n_modes)
     assert rel_l2(outs[0], ref) < 20 * 1e-12 + 1e-13
+
+
+def test_type2_crowded_bins_are_split_over_many_parts():
+    """Type 2 on tight clusters (bins of 8 x 8 cells holding thousands of
+    points, served in parts of 512 slots): one vector on the staged-region
+    kernel, a batch of 40 on the batched bin kernel, and f64 on its staged
+    regions give the bits of the per-point sums (the batch's first vector, the
+    f64 gather) and stay within the direct-sum bound."""
+    rng = np.random.default_rng(83)
+    n_modes = (96, 80)
+    m = 300_000
+    points = np.concatenate([clustered_points(rng, m - 20_000, 2, centres=3, spread=0.004),
+                             uniform_points(rng, 20_000, 2)])
+    coefficients = complex_normal(rng, (40, 96 * 80))
+    outs32 = []
+    for batch in (1, 40):
+        config = w.NufftConfig(n_modes, 1e-6, batch=batch, spread_method=w.SpreadMethod.CUDA_CORES)
+        plan = w.NufftPlan.type2_gpu(config)
+        assert plan.kernel_width() == 7
+        plan.set_points_gpu(to_gpu(points))
+        out = torch.empty((batch, m), dtype=torch.complex64, device=DEV)
+        plan.execute_gpu_batch(batch, to_gpu(coefficients[:batch]), out)
+        plan.synchronize()
+        outs32.append(out.cpu().numpy())
+    one, many = outs32
+    assert np.array_equal(one[0].view(np.uint32), many[0].view(np.uint32))
+    pick = np.sort(rng.choice(m, 3000, replace=False))
+    for b in (0, 39):
+        ref = native.direct_type2(points[pick].astype(np.float64), coefficients[b:b + 1], n_modes)
+        assert rel_l2(many[b, pick], ref[0]) < tolerance(2, 1e-6)
+    points64 = points.astype(np.float64)
+    coefficients64 = coefficients[:2].astype(np.complex128)
+    outs = []
+    for batch in (1, 2):
+        config = w.NufftConfig(n_modes, 1e-12, batch=batch, precision=w.Precision.F64)
+        plan64 = w.NufftPlan.type2_gpu(config)
+        plan64.set_points_gpu(to_gpu(points64))
+        out = torch.empty((batch, m), dtype=torch.complex128, device=DEV)
+        plan64.execute_gpu_batch(batch, to_gpu(coefficients64[:batch]), out)
+        plan64.synchronize()
+        outs.append(out.cpu().numpy())
+    assert np.array_equal(outs[0][0].view(np.int64), outs[1][0].view(np.int64))
+    ref64 = native.direct_type2(points64[pick], coefficients64[:1], n_modes)
+    assert rel_l2(outs[0][0, pick], ref64[0]) < 20 * 1e-12 + 1e-13

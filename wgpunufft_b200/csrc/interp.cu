@@ -17,6 +17,7 @@
 
 #include "device.h"
 #include "interp.h"
+#include "spread.h"
 
 namespace b200nufft {
 
@@ -193,17 +194,47 @@ constexpr int kBinPitch = kBinVectors + 1;  // float2 per staged cell, padded ag
 template <int W>
 __host__ __device__ constexpr int bin_region_side() { return 8 + W + 3; }
 
+// The bin and the slots [first, last) of part blockIdx.x; false for a CTA
+// beyond the last part. Each point's sum is the same whichever part (and
+// CTA) serves it.
+__device__ __forceinline__ bool bin_part(const InterpParts& parts, const uint32_t* __restrict__ offsets,
+                                         uint64_t bins, int64_t& bin, uint32_t& first, uint32_t& last) {
+  const uint32_t part = blockIdx.x;
+  if (part >= parts.part_start[bins]) return false;
+  const uint32_t b = parts.part_bin[part];
+  const uint32_t begin = offsets[b], end = offsets[b + 1];
+  first = begin + (part - parts.part_start[b]) * kInterpPartSlots;
+  last = min(first + kInterpPartSlots, end);
+  bin = b;
+  return first < last;
+}
+
+__global__ void interp_part_count_kernel(const uint32_t* __restrict__ offsets, uint64_t bins,
+                                         uint32_t* __restrict__ parts) {
+  const uint64_t b = static_cast<uint64_t>(blockIdx.x) * blockDim.x + threadIdx.x;
+  if (b >= bins) return;
+  parts[b] = (offsets[b + 1] - offsets[b] + kInterpPartSlots - 1) / kInterpPartSlots;
+}
+
+__global__ void interp_part_fill_kernel(const uint32_t* __restrict__ part_start, uint64_t bins,
+                                        uint32_t* __restrict__ part_bin) {
+  const uint64_t b = static_cast<uint64_t>(blockIdx.x) * blockDim.x + threadIdx.x;
+  if (b >= bins) return;
+  for (uint32_t p = part_start[b]; p < part_start[b + 1]; ++p) part_bin[p] = static_cast<uint32_t>(b);
+}
+
 template <int W>
 __global__ void __launch_bounds__(256) interpolate_bins_kernel(GridParams g, const void* __restrict__ windows,
                                                                int64_t count, const uint32_t* __restrict__ perm,
                                                                const uint32_t* __restrict__ offsets,
                                                                const float2* __restrict__ fine, int batch,
-                                                               float2* __restrict__ staged, int64_t staged_stride) {
+                                                               float2* __restrict__ staged, int64_t staged_stride,
+                                                               InterpParts parts) {
   constexpr int S = bin_region_side<W>();
   extern __shared__ float2 region[];  // S * S cells x kBinPitch
-  const int64_t bin = blockIdx.x;
-  const uint32_t first = offsets[bin], last = offsets[bin + 1];
-  if (first == last) return;
+  int64_t bin;
+  uint32_t first, last;
+  if (!bin_part(parts, offsets, g.axis[0].bins * static_cast<uint64_t>(g.axis[1].bins), bin, first, last)) return;
   const int vb = blockIdx.y * kBinVectors;
   const int nv = min(kBinVectors, batch - vb);
   const int bins0 = static_cast<int>(g.axis[0].bins);
@@ -311,36 +342,17 @@ __global__ void __launch_bounds__(256) interpolate_bins_kernel(GridParams g, con
 // values); windows beyond the region read the grid directly.
 constexpr int kRegionThreads = 128;
 
-// CTAs per bin of the region kernels: a bin holding many points (a small
-// grid under a large point set) splits its slots over gridDim.y CTAs that
-// each stage the same region, so that the launch still fills every SM. Each
-// point's sum is the same whichever CTA serves it.
-inline unsigned region_splits(int64_t points, uint64_t bins) {
-  const int64_t per_bin = points / static_cast<int64_t>(bins > 0 ? bins : 1);
-  return static_cast<unsigned>(std::min<int64_t>(64, std::max<int64_t>(1, per_bin / (4 * kRegionThreads))));
-}
-
-// The slots [first, last) of this CTA's share of its bin.
-__device__ __forceinline__ void region_share(const uint32_t* __restrict__ offsets, int64_t bin, uint32_t& first,
-                                             uint32_t& last) {
-  const uint64_t begin = offsets[bin], end = offsets[bin + 1];
-  const uint64_t share = (end - begin + gridDim.y - 1) / gridDim.y;
-  const uint64_t lo = begin + share * blockIdx.y, hi = lo + share;
-  first = static_cast<uint32_t>(lo < end ? lo : end);
-  last = static_cast<uint32_t>(hi < end ? hi : end);
-}
 
 template <int W>
 __global__ void __launch_bounds__(kRegionThreads) interpolate_region_kernel(
     GridParams g, const void* __restrict__ windows, int64_t count, const uint32_t* __restrict__ perm,
     const uint32_t* __restrict__ offsets, const float2* __restrict__ fine, int batch,
-    float2* __restrict__ output) {
+    float2* __restrict__ output, InterpParts parts) {
   constexpr int S = bin_region_side<W>();
   __shared__ float2 region[S * S];
-  const int64_t bin = blockIdx.x;
+  int64_t bin;
   uint32_t first, last;
-  region_share(offsets, bin, first, last);
-  if (first >= last) return;
+  if (!bin_part(parts, offsets, g.axis[0].bins * static_cast<uint64_t>(g.axis[1].bins), bin, first, last)) return;
   const int bins0 = static_cast<int>(g.axis[0].bins);
   const int n0 = g.axis[0].length, n1 = g.axis[1].length;
   const int ox = static_cast<int>(bin % bins0) * 8 - W / 2 - 2;
@@ -426,13 +438,12 @@ template <int W>
 __global__ void __launch_bounds__(kRegionThreads) interpolate_region64_kernel(
     GridParams g, const double* __restrict__ points, int64_t count, const uint32_t* __restrict__ perm,
     const uint32_t* __restrict__ offsets, const double2* __restrict__ fine, int batch,
-    double2* __restrict__ output) {
+    double2* __restrict__ output, InterpParts parts) {
   constexpr int S = 4 + W - 1;
   __shared__ double2 region[S * S];
-  const int64_t bin = blockIdx.x;
+  int64_t bin;
   uint32_t first, last;
-  region_share(offsets, bin, first, last);
-  if (first >= last) return;
+  if (!bin_part(parts, offsets, g.axis[0].bins * static_cast<uint64_t>(g.axis[1].bins), bin, first, last)) return;
   const int bins0 = static_cast<int>(g.axis[0].bins);
   const int n0 = g.axis[0].length, n1 = g.axis[1].length;
   const int ox = static_cast<int>(bin % bins0) * 4;
@@ -530,10 +541,11 @@ void launch_bins_width(const GridParams& g, const InterpBinsLaunch& l, cudaStrea
   auto kernel = interpolate_bins_kernel<W>;
   check_cuda(cudaFuncSetAttribute(kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, static_cast<int>(smem)),
              "interpolation region shared memory");
-  const dim3 grid(static_cast<unsigned>(l.bins), static_cast<unsigned>((l.batch + kBinVectors - 1) / kBinVectors));
+  const dim3 grid(static_cast<unsigned>(l.parts.upper_bound),
+                  static_cast<unsigned>((l.batch + kBinVectors - 1) / kBinVectors));
   const int64_t stride = (l.batch + kBinVectors - 1) / kBinVectors * kBinVectors;
   kernel<<<grid, 256, smem, stream>>>(g, l.windows, l.point_count, l.perm, l.offsets, l.fine, l.batch, l.staged,
-                                      stride);
+                                      stride, l.parts);
   const dim3 grid2(static_cast<unsigned>((l.point_count + 31) / 32), static_cast<unsigned>((l.batch + 63) / 64));
   unpermute_kernel<<<grid2, 256, 0, stream>>>(l.staged, stride, l.inverse, l.point_count, l.batch, l.output);
   note_launch(2);
@@ -598,12 +610,12 @@ void interpolate_execute(const GridParams& g, const InterpLaunch& l, cudaStream_
 
 void interpolate_region_execute(const GridParams& g, const InterpBinsLaunch& l, cudaStream_t stream) {
   if (l.point_count == 0) return;
-  const dim3 grid(static_cast<unsigned>(l.bins), region_splits(l.point_count, l.bins));
+  const dim3 grid(static_cast<unsigned>(l.parts.upper_bound));
   switch (g.width) {
 #define B200NUFFT_REGION_CASE(WIDTH)                                                                   \
   case WIDTH:                                                                                          \
     interpolate_region_kernel<WIDTH><<<grid, kRegionThreads, 0, stream>>>(                              \
-        g, l.windows, l.point_count, l.perm, l.offsets, l.fine, l.batch, l.output);                     \
+        g, l.windows, l.point_count, l.perm, l.offsets, l.fine, l.batch, l.output, l.parts);            \
     break;
     B200NUFFT_REGION_CASE(2)
     B200NUFFT_REGION_CASE(3)
@@ -648,14 +660,15 @@ bool interpolate_region64_supported(const GridParams& g) {
 }
 
 void interpolate_region64_execute(const GridParams& g, const InterpLaunch64& l, const uint32_t* offsets,
-                                  uint64_t bins, cudaStream_t stream) {
+                                  uint64_t bins, const InterpParts& parts, cudaStream_t stream) {
   if (l.point_count == 0) return;
-  const dim3 grid(static_cast<unsigned>(bins), region_splits(l.point_count, bins));
+  (void)bins;
+  const dim3 grid(static_cast<unsigned>(parts.upper_bound));
   switch (g.width) {
 #define B200NUFFT_REGION64_CASE(WIDTH)                                                                  \
   case WIDTH:                                                                                          \
     interpolate_region64_kernel<WIDTH><<<grid, kRegionThreads, 0, stream>>>(                            \
-        g, l.points, l.point_count, l.perm, offsets, l.fine, l.batch, l.output);                        \
+        g, l.points, l.point_count, l.perm, offsets, l.fine, l.batch, l.output, parts);                 \
     break;
     B200NUFFT_REGION64_CASE(2)
     B200NUFFT_REGION64_CASE(3)
@@ -676,6 +689,15 @@ void interpolate_region64_execute(const GridParams& g, const InterpLaunch64& l, 
 #undef B200NUFFT_REGION64_CASE
   }
   note_launch();
+}
+
+void interp_bin_parts(const uint32_t* offsets, uint64_t bins, uint32_t* parts, uint32_t* part_start,
+                      uint32_t* part_bin, cudaStream_t stream) {
+  const unsigned blocks = static_cast<unsigned>((bins + 255) / 256);
+  interp_part_count_kernel<<<blocks, 256, 0, stream>>>(offsets, bins, parts);
+  exclusive_scan_u32(parts, static_cast<int64_t>(bins), part_start, stream);
+  interp_part_fill_kernel<<<blocks, 256, 0, stream>>>(part_start, bins, part_bin);
+  note_launch(2);
 }
 
 void interpolate_execute64(const GridParams& g, const InterpLaunch64& l, cudaStream_t stream) {

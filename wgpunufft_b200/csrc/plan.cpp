@@ -545,6 +545,24 @@ int NufftPlan::choose_geometry(int64_t point_count) const {
   return layout_.choose_geometry(point_count);
 }
 
+void NufftPlan::prepare_interp_parts(const uint32_t* offsets, cudaStream_t stream) {
+  interp_parts_bound_ = interp_parts_bound(point_count_, bins_);
+  uint32_t* parts = static_cast<uint32_t*>(interp_parts_.reserve(bins_ * sizeof(uint32_t), "bin parts"));
+  uint32_t* part_start =
+      static_cast<uint32_t*>(interp_part_start_.reserve((bins_ + 1) * sizeof(uint32_t), "bin part offsets"));
+  uint32_t* part_bin = static_cast<uint32_t*>(
+      interp_part_bin_.reserve(static_cast<size_t>(interp_parts_bound_) * sizeof(uint32_t), "part bins"));
+  interp_bin_parts(offsets, bins_, parts, part_start, part_bin, stream);
+}
+
+InterpParts NufftPlan::interp_parts() const {
+  InterpParts p;
+  p.part_bin = static_cast<const uint32_t*>(interp_part_bin_.get());
+  p.part_start = static_cast<const uint32_t*>(interp_part_start_.get());
+  p.upper_bound = interp_parts_bound_;
+  return p;
+}
+
 void NufftPlan::set_points(int64_t count, const void* points, cudaStream_t stream) {
   if (!has_device_) {
     throw NufftFailure{B200NUFFT_GPU_EXECUTION_UNAVAILABLE,
@@ -666,6 +684,7 @@ void NufftPlan::set_points(int64_t count, const void* points, cudaStream_t strea
                                        "point slots");
       invert_permutation(perm_, count, static_cast<uint32_t*>(inverse), stream);
     }
+    if (type_ == 2 && dim_ == 2) prepare_interp_parts(offsets, stream);
   } else {
     const double* points64 = static_cast<const double*>(points);
     if (precision_ == B200NUFFT_PRECISION_DF64 && count > 0) {
@@ -677,6 +696,10 @@ void NufftPlan::set_points(int64_t count, const void* points, cudaStream_t strea
                   &timer_, valid_mask);
     double* sorted = static_cast<double*>(sorted_points_.reserve(sorted_bytes, "sorted coordinates"));
     gather_sorted_points64(points64, perm_, count, dim_, sorted, stream, &timer_);
+    if (type_ == 2 && dim_ == 2) {
+      StageScope scope(&timer_, kStageBinOffsets, stream);
+      prepare_interp_parts(offsets, stream);
+    }
   }
   if (type_ == 1) {
     configure_tiles();
@@ -878,6 +901,7 @@ void NufftPlan::execute_f32(int batch, const void* input, void* output, uint64_t
       b.staged = static_cast<float2*>(staged_.reserve(
           static_cast<size_t>(std::max<int64_t>(point_count_, 1)) * ((batch + 31) / 32 * 32) * sizeof(float2),
           "staged type-2 values"));
+      b.parts = interp_parts();
       StageScope scope(&timer_, kStageInterpolation, stream);
       interpolate_bins_execute(grid_, b, stream);
       return;
@@ -892,6 +916,7 @@ void NufftPlan::execute_f32(int batch, const void* input, void* output, uint64_t
       b.fine = fine;
       b.batch = batch;
       b.output = static_cast<float2*>(output);
+      b.parts = interp_parts();
       StageScope scope(&timer_, kStageInterpolation, stream);
       interpolate_region_execute(grid_, b, stream);
       return;
@@ -971,7 +996,8 @@ void NufftPlan::execute_f64(int batch, const void* input, void* output, uint64_t
     // 1.5x faster; w 10 even; batches of 16 slower, whose window weights the
     // thread-per-point kernel reuses across vectors).
     if (batch == 1 && kernel_.width >= 11 && interpolate_region64_supported(grid_)) {
-      interpolate_region64_execute(grid_, l, static_cast<const uint32_t*>(offsets_.get()), bins_, stream);
+      interpolate_region64_execute(grid_, l, static_cast<const uint32_t*>(offsets_.get()), bins_, interp_parts(),
+                                   stream);
     } else {
       interpolate_execute64(grid_, l, stream);
     }

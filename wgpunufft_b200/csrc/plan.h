@@ -138,6 +138,12 @@ class NufftPlan {
   DeviceBuffer part_cap_;    // type-1 plans: records per part, sized on the device
   DeviceBuffer windows_;  // f32 plans: PreparedWindow per slot
   DeviceBuffer inverse_;  // batched 2D f32 type-2 plans: slot of every point
+  // 2D type-2 plans: the bins' slots in parts of at most kInterpPartSlots
+  // (work items of the bin interpolation kernels).
+  DeviceBuffer interp_parts_, interp_part_start_, interp_part_bin_;
+  int64_t interp_parts_bound_ = 0;
+  void prepare_interp_parts(const uint32_t* offsets, cudaStream_t stream);
+  InterpParts interp_parts() const;
   DeviceBuffer staged_;   // batched 2D f32 type-2 plans: values in slot order
 
   // Spreading state.
