@@ -55,6 +55,14 @@ __device__ __forceinline__ void mma_tf32(uint32_t d, uint64_t a, uint64_t b, uin
       "tcgen05.mma.cta_group::1.kind::tf32 [%0], %1, %2, %3, {%5, %5, %5, %5}, p;\n}\n" ::"r"(d),
       "l"(a), "l"(b), "r"(idesc), "r"(accumulate ? 1 : 0), "r"(0));
 }
+// D = A B or D += A B with A (M = 128 rows in the 128 lanes, one tf32 K
+// element per column) in tensor memory at `a`, B in shared memory.
+__device__ __forceinline__ void mma_tf32_tmem_a(uint32_t d, uint32_t a, uint64_t b, uint32_t idesc, bool accumulate) {
+  asm volatile(
+      "{\n.reg .pred p;\nsetp.ne.b32 p, %4, 0;\n"
+      "tcgen05.mma.cta_group::1.kind::tf32 [%0], [%1], %2, %3, {%5, %5, %5, %5}, p;\n}\n" ::"r"(d),
+      "r"(a), "l"(b), "r"(idesc), "r"(accumulate ? 1 : 0), "r"(0));
+}
 __device__ __forceinline__ void mma_commit(uint32_t bar) {
   asm volatile("tcgen05.commit.cta_group::1.mbarrier::arrive::one.shared::cluster.b64 [%0];" ::"r"(bar)
                : "memory");
@@ -74,10 +82,9 @@ __device__ __forceinline__ bool mbar_try(uint32_t bar, uint32_t parity) {
       : "memory");
   return done != 0;
 }
-// Waits for the phase of the given parity to complete; false when it gave up
-// or when another role raised the CTA's abort flag (which a failed wait
-// raises).
-static __device__ __noinline__ bool mbar_wait(uint32_t bar, uint32_t parity, volatile int* abort_flag) {
+// The polling loop of mbar_wait (out of line: waits that find the phase
+// complete do not pay for it).
+static __device__ __noinline__ bool mbar_wait_slow(uint32_t bar, uint32_t parity, volatile int* abort_flag) {
   for (uint32_t i = 0; i < kSpinLimit; ++i) {
     if (mbar_try(bar, parity)) return true;
     if (abort_flag != nullptr && *abort_flag) return false;
@@ -85,6 +92,21 @@ static __device__ __noinline__ bool mbar_wait(uint32_t bar, uint32_t parity, vol
   }
   if (abort_flag != nullptr) *abort_flag = 1;
   return false;
+}
+// Waits for the phase of the given parity to complete; false when it gave up
+// or when another role raised the CTA's abort flag (which a failed wait
+// raises).
+__device__ __forceinline__ bool mbar_wait(uint32_t bar, uint32_t parity, volatile int* abort_flag) {
+  return mbar_try(bar, parity) || mbar_wait_slow(bar, parity, abort_flag);
+}
+// One lane of the (converged) warp: the lane that issues a tensor-core
+// instruction while the warp computes its operands together.
+__device__ __forceinline__ bool elect_one() {
+  uint32_t elected = 0;
+  asm volatile(
+      "{\n.reg .pred p;\nelect.sync _|p, 0xFFFFFFFF;\nselp.u32 %0, 1, 0, p;\n}\n"
+      : "=r"(elected));
+  return elected != 0;
 }
 __device__ __forceinline__ void mbar_arrive(uint32_t bar) {
   asm volatile("mbarrier.arrive.shared::cta.b64 _, [%0];" ::"r"(bar) : "memory");
@@ -118,6 +140,18 @@ __device__ __forceinline__ void tmem_ld16(uint32_t addr, uint32_t* v) {
       : "r"(addr));
 }
 __device__ __forceinline__ void tmem_wait_ld() { asm volatile("tcgen05.wait::ld.sync.aligned;" ::: "memory"); }
+// Each lane of the warp writes 32 consecutive columns of its own lane.
+__device__ __forceinline__ void tmem_st32(uint32_t addr, const uint32_t* v) {
+  asm volatile(
+      "tcgen05.st.sync.aligned.32x32b.x32.b32 [%0], {%1, %2, %3, %4, %5, %6, %7, %8, %9, %10, %11, %12, %13, %14, "
+      "%15, %16, %17, %18, %19, %20, %21, %22, %23, %24, %25, %26, %27, %28, %29, %30, %31, %32};" ::"r"(addr),
+      "r"(v[0]), "r"(v[1]), "r"(v[2]), "r"(v[3]), "r"(v[4]), "r"(v[5]), "r"(v[6]), "r"(v[7]), "r"(v[8]), "r"(v[9]),
+      "r"(v[10]), "r"(v[11]), "r"(v[12]), "r"(v[13]), "r"(v[14]), "r"(v[15]), "r"(v[16]), "r"(v[17]), "r"(v[18]),
+      "r"(v[19]), "r"(v[20]), "r"(v[21]), "r"(v[22]), "r"(v[23]), "r"(v[24]), "r"(v[25]), "r"(v[26]), "r"(v[27]),
+      "r"(v[28]), "r"(v[29]), "r"(v[30]), "r"(v[31])
+      : "memory");
+}
+__device__ __forceinline__ void tmem_wait_st() { asm volatile("tcgen05.wait::st.sync.aligned;" ::: "memory"); }
 
 // tf32 split: hi keeps the sign, exponent and 10 mantissa bits the tensor
 // core reads; lo = x - hi is exact in f32.

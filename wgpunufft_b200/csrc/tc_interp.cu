@@ -47,32 +47,34 @@ namespace {
 
 using namespace tc;
 
-// Warp roles.
+// Warp roles. Converter and read-out warps access the tensor-memory lane
+// quadrant warp % 4.
 constexpr int kProducerWarp = 0;
 constexpr int kMmaWarp = 1;
-constexpr int kConvertWarp0 = 2;   // two warps: 64 threads convert every row
-constexpr int kBuildWarp0 = 4;     // four warps: two teams of 64 threads, alternate chunks
-constexpr int kReadWarp0 = 8;      // four warps: one per tensor-memory lane quadrant
-constexpr int kThreads = 12 * 32;
-constexpr int kConvertThreads = 64;
-constexpr int kTeamThreads = 64;
+constexpr int kConvertWarp0 = 2;   // four warps: every lane converts one A row (vector part) of a fetched row
+constexpr int kBuildWarp0 = 6;     // four warps: one builder team each, chunks c = team (mod 4)
+constexpr int kReadWarp0 = 10;     // four warps: one per tensor-memory lane quadrant
+constexpr int kThreads = 14 * 32;
+constexpr int kConvertThreads = 128;
+constexpr int kTeamThreads = 32;
 constexpr int kReadThreads = 128;
 
-constexpr int kBuffers = 4;            // tensor-memory accumulators of 32 columns
-constexpr int kTmemColumns = 128;
-constexpr int kRawSlots = 3;           // rows fetched ahead
-constexpr int kBStages = 2;            // one per builder team
+constexpr int kBuffers = 4;            // accumulators of 32 columns (tensor-memory columns 0 .. 127)
+constexpr int kRing = 12;              // converted rows in tensor memory (32 columns each, from column 128)
+constexpr int kRingColumn0 = kBuffers * 32;
+constexpr int kTmemColumns = 512;
+static_assert(kRingColumn0 + kRing * 32 <= kTmemColumns, "tensor-memory ring exceeds the allocation");
+static_assert(kRing > kTi2MaxWidth, "the ring holds a chunk's window rows and one more");
+constexpr int kRawSlots = 10;          // fetched rows in flight
+constexpr int kBStages = 4;            // one per builder team
 constexpr int kRawPitch = 144;         // bytes per vector of a fetched row (128 + 16 against bank conflicts)
 constexpr int kRawBytes = kTi2Vectors * kRawPitch;
-constexpr int kRowHalf = 8192;         // one tf32 part of a converted row: 128 rows x 16 columns
-constexpr int kRowBytes = 2 * kRowHalf;
 constexpr int kWeightStage = kTi2ChunkPoints * static_cast<int>(sizeof(TcWeights));
 
 template <int W>
 struct Ti2Layout {
-  static constexpr int kRing = W + 1;
   static constexpr int kBHalf = kTi2ChunkPoints * kTi2Pitch * W * 4;  // one tf32 part of B: 32 x 16 W
-  static constexpr int kBBase = kRing * kRowBytes;
+  static constexpr int kBBase = 0;
   static constexpr int kRawBase = kBBase + kBStages * 2 * kBHalf;
   static constexpr int kWeightsBase = kRawBase + kRawSlots * kRawBytes;
   static constexpr int kBytes = kWeightsBase + kBStages * kWeightStage;
@@ -171,29 +173,27 @@ __global__ void ti2_chunk_fill_kernel(GridParams g, int64_t tiles, const uint32_
   }
 }
 
-// Converts fetched row `raw` (64 vectors x 16 complex cells at kRawPitch)
-// into tf32 high and low parts at `ring` (K-major: 4 K blocks of 128 bytes,
-// 16 groups of 8 rows 512 bytes apart; row m = 2 v + part), with the 64
-// converter threads (t = thread index among them).
-__device__ __forceinline__ void ti2_convert_row(const unsigned char* raw, unsigned char* ring, int nv, int t) {
+// Converts A row m = 2 v + part of fetched row `raw` (vector v's 16 complex
+// cells at kRawPitch) into 16 tf32 high parts followed by 16 low parts, the
+// 32 columns of a ring slot (zero for vectors at or beyond nv).
+__device__ __forceinline__ void ti2_convert_lane(const unsigned char* raw, int m, int nv, uint32_t* out) {
+  const int v = m >> 1, part = m & 1;
+  const float4* row = reinterpret_cast<const float4*>(raw + v * kRawPitch);
+  float4 cells[8];
 #pragma unroll
-  for (int i = 0; i < 512 / kConvertThreads; ++i) {
-    const int u = t + i * kConvertThreads;
-    const int kb = u >> 7, m = u & 127, v = m >> 1, part = m & 1;
-    float4 value = make_float4(0.0f, 0.0f, 0.0f, 0.0f);
-    if (v < nv) {
-      const float4 a = *reinterpret_cast<const float4*>(raw + v * kRawPitch + kb * 32);
-      const float4 b = *reinterpret_cast<const float4*>(raw + v * kRawPitch + kb * 32 + 16);
-      value = part ? make_float4(a.y, a.w, b.y, b.w) : make_float4(a.x, a.z, b.x, b.z);
-    }
-    float4 hi, lo;
-    split_tf32(value.x, hi.x, lo.x);
-    split_tf32(value.y, hi.y, lo.y);
-    split_tf32(value.z, hi.z, lo.z);
-    split_tf32(value.w, hi.w, lo.w);
-    const int off = kb * 128 + (m >> 3) * 512 + (m & 7) * 16;
-    *reinterpret_cast<float4*>(ring + off) = hi;
-    *reinterpret_cast<float4*>(ring + kRowHalf + off) = lo;
+  for (int i = 0; i < 8; ++i) cells[i] = row[i];
+  const bool live = v < nv;
+#pragma unroll
+  for (int i = 0; i < 8; ++i) {
+    const float x0 = live ? (part ? cells[i].y : cells[i].x) : 0.0f;
+    const float x1 = live ? (part ? cells[i].w : cells[i].z) : 0.0f;
+    float hi, lo;
+    split_tf32(x0, hi, lo);
+    out[2 * i] = __float_as_uint(hi);
+    out[16 + 2 * i] = __float_as_uint(lo);
+    split_tf32(x1, hi, lo);
+    out[2 * i + 1] = __float_as_uint(hi);
+    out[16 + 2 * i + 1] = __float_as_uint(lo);
   }
 }
 
@@ -206,7 +206,7 @@ __global__ void __launch_bounds__(kThreads, 1) tc_interp_kernel(
   using L = Ti2Layout<W>;
   extern __shared__ __align__(1024) unsigned char smem[];
   __shared__ __align__(8) uint64_t raw_full[kRawSlots], raw_empty[kRawSlots];
-  __shared__ __align__(8) uint64_t a_full[L::kRing], a_empty[L::kRing];
+  __shared__ __align__(8) uint64_t a_full[kRing], a_empty[kRing];
   __shared__ __align__(8) uint64_t b_full[kBStages], b_empty[kBStages], w_full[kBStages], w_empty[kBStages];
   __shared__ __align__(8) uint64_t d_full[kBuffers], d_empty[kBuffers];
   __shared__ uint32_t tmem_base;
@@ -230,7 +230,7 @@ __global__ void __launch_bounds__(kThreads, 1) tc_interp_kernel(
       mbar_init(&raw_full[s], 1);
       mbar_init(&raw_empty[s], kConvertThreads);
     }
-    for (int s = 0; s < L::kRing; ++s) {
+    for (int s = 0; s < kRing; ++s) {
       mbar_init(&a_full[s], kConvertThreads);
       mbar_init(&a_empty[s], 1);
     }
@@ -271,12 +271,11 @@ __global__ void __launch_bounds__(kThreads, 1) tc_interp_kernel(
   // Rows [r_begin, r_begin + rows) relative to y0 are fetched and converted in order.
   const int r_begin = n > 0 ? s_chunks[0].row : 0;
   const int rows = n > 0 ? s_chunks[n - 1].row + W - r_begin : 0;
-  unsigned char* ring = smem;
   unsigned char* raw = smem + L::kRawBase;
   volatile int* abort_flag = &s_abort;
 
   if (warp == kProducerWarp) {
-    // Row k into raw slot k % 3 once the converters are done with row k - 3.
+    // Row k into raw slot k % kRawSlots once the converters are done with row k - kRawSlots.
     int issued = 0;
     for (int k = 0; k < rows; ++k) {
       const int slot = k % kRawSlots;
@@ -313,54 +312,69 @@ __global__ void __launch_bounds__(kThreads, 1) tc_interp_kernel(
       }
     }
   } else if (warp == kMmaWarp) {
-    if (lane == 0) {
-      int ready = 0;    // rows [0, ready) relative to r_begin are converted
-      int retired = 0;  // rows [0, retired) are released to the converters
-      int issued = 0;
-      bool ok = true;
-      for (int c = 0; c < n && ok; ++c) {
-        const Ti2Chunk ch = s_chunks[c];
-        const int r = ch.row - r_begin;
-        while (ok && ready < r + W) {
-          ok = mbar_wait(smem_u32(&a_full[ready % L::kRing]), static_cast<uint32_t>(ready / L::kRing) & 1u, abort_flag);
-          ready += ok ? 1 : 0;
-          // Rows below this chunk's first row are read by no later chunk:
-          // release them at once, so rows skipped between chunks free their
-          // ring slots while this chunk waits for its own rows.
-          for (; retired < min(r, ready); ++retired) mma_commit(smem_u32(&a_empty[retired % L::kRing]));
+    // The whole warp walks the chunks (operands warp-uniform); one elected
+    // lane issues each MMA and commit.
+    int ready = 0;    // rows [0, ready) relative to r_begin are converted
+    int retired = 0;  // rows [0, retired) are released to the converters
+    int issued = 0;
+    bool ok = true;
+    for (int c = 0; c < n && ok; ++c) {
+      const Ti2Chunk ch = s_chunks[c];
+      const int r = ch.row - r_begin;
+      while (ok && ready < r + W) {
+        ok = mbar_wait(smem_u32(&a_full[ready % kRing]), static_cast<uint32_t>(ready / kRing) & 1u, abort_flag);
+        ok = __all_sync(0xFFFFFFFFu, ok);
+        ready += ok ? 1 : 0;
+        // Rows below this chunk's first row are read by no later chunk:
+        // release them at once, so rows skipped between chunks free their
+        // ring slots while this chunk waits for its own rows.
+        for (; retired < min(r, ready); ++retired) {
+          if (elect_one()) mma_commit(smem_u32(&a_empty[retired % kRing]));
+          __syncwarp();
         }
-        ok = ok && mbar_wait(smem_u32(&b_full[c % kBStages]), static_cast<uint32_t>(c / kBStages) & 1u, abort_flag);
-        if (ok && c >= kBuffers) {
-          ok = mbar_wait(smem_u32(&d_empty[c % kBuffers]), static_cast<uint32_t>(c / kBuffers - 1) & 1u, abort_flag);
-        }
-        if (!ok) break;
-        tc_fence_after();
-        const int cols = ch.count <= 16 ? 16 : 32;
-        const uint32_t idesc = idesc_tf32(128, static_cast<uint32_t>(cols));
-        const uint32_t d = tm + static_cast<uint32_t>((c % kBuffers) * 32);
-        const uint32_t bh = smem_u32(smem + L::kBBase + (c % kBStages) * 2 * L::kBHalf);
-        const uint32_t bl = bh + L::kBHalf;
-#pragma unroll 1
-        for (int j = 0; j < W; ++j) {
-          const uint32_t rb = smem_u32(ring + ((r + j) % L::kRing) * kRowBytes);
+      }
+      ok = ok && mbar_wait(smem_u32(&b_full[c % kBStages]), static_cast<uint32_t>(c / kBStages) & 1u, abort_flag);
+      if (ok && c >= kBuffers) {
+        ok = mbar_wait(smem_u32(&d_empty[c % kBuffers]), static_cast<uint32_t>(c / kBuffers - 1) & 1u, abort_flag);
+      }
+      ok = __all_sync(0xFFFFFFFFu, ok);
+      if (!ok) break;
+      tc_fence_after();
+      const int cols = ch.count <= 16 ? 16 : 32;
+      const uint32_t idesc = idesc_tf32(128, static_cast<uint32_t>(cols));
+      const uint32_t d = tm + static_cast<uint32_t>((c % kBuffers) * 32);
+      const uint32_t bh = smem_u32(smem + L::kBBase + (c % kBStages) * 2 * L::kBHalf);
+      const uint32_t bl = bh + L::kBHalf;
 #pragma unroll
-          for (int h = 0; h < 2; ++h) {
-            const uint64_t ahi = kmajor_desc(rb + h * 256, 128, 512);
-            const uint64_t alo = kmajor_desc(rb + kRowHalf + h * 256, 128, 512);
-            const uint64_t bhi = kmajor_desc(bh + (4 * j + 2 * h) * 128, 128, L::kBStride);
-            const uint64_t blo = kmajor_desc(bl + (4 * j + 2 * h) * 128, 128, L::kBStride);
-            mma_tf32(d, ahi, bhi, idesc, j > 0 || h > 0);
-            mma_tf32(d, ahi, blo, idesc, true);
-            mma_tf32(d, alo, bhi, idesc, true);
+      for (int j = 0; j < W; ++j) {
+        // Ring slot of window row j: high parts in columns 0 .. 15, low parts in 16 .. 31.
+        const uint32_t a = tm + static_cast<uint32_t>(kRingColumn0 + ((r + j) % kRing) * 32);
+#pragma unroll
+        for (int h = 0; h < 2; ++h) {
+          const uint64_t bhi = kmajor_desc(bh + (4 * j + 2 * h) * 128, 128, L::kBStride);
+          const uint64_t blo = kmajor_desc(bl + (4 * j + 2 * h) * 128, 128, L::kBStride);
+          if (elect_one()) {
+            mma_tf32_tmem_a(d, a + 8 * h, bhi, idesc, j > 0 || h > 0);
+            mma_tf32_tmem_a(d, a + 8 * h, blo, idesc, true);
+            mma_tf32_tmem_a(d, a + 16 + 8 * h, bhi, idesc, true);
           }
+          __syncwarp();
         }
+      }
+      if (elect_one()) {
         mma_commit(smem_u32(&b_empty[c % kBStages]));
         mma_commit(smem_u32(&d_full[c % kBuffers]));
-        issued = c + 1;
-        // Rows below the next chunk's first row are read by no later chunk.
-        const int next = c + 1 < n ? s_chunks[c + 1].row - r_begin : rows;
-        for (; retired < min(next, ready); ++retired) mma_commit(smem_u32(&a_empty[retired % L::kRing]));
       }
+      __syncwarp();
+      issued = c + 1;
+      // Rows below the next chunk's first row are read by no later chunk.
+      const int next = c + 1 < n ? s_chunks[c + 1].row - r_begin : rows;
+      for (; retired < min(next, ready); ++retired) {
+        if (elect_one()) mma_commit(smem_u32(&a_empty[retired % kRing]));
+        __syncwarp();
+      }
+    }
+    if (lane == 0) {
       if (issued > 0 &&
           !mbar_wait(smem_u32(&d_full[(issued - 1) % kBuffers]), static_cast<uint32_t>((issued - 1) / kBuffers) & 1u,
                      nullptr)) {
@@ -369,73 +383,106 @@ __global__ void __launch_bounds__(kThreads, 1) tc_interp_kernel(
       if (!ok) *abort_flag = 1;
     }
   } else if (warp < kBuildWarp0) {
-    // Converters.
-    const int t = tid - kConvertWarp0 * 32;
+    // Converters: lane (warp % 4, lane) owns A row m = 32 (warp % 4) + lane
+    // and writes its 32 columns of every ring slot.
+    const int quadrant = warp & 3;
+    const int m = quadrant * 32 + lane;
+    const uint32_t lane_base = tm + (static_cast<uint32_t>(quadrant * 32) << 16);
     for (int k = 0; k < rows; ++k) {
       if (!mbar_wait(smem_u32(&raw_full[k % kRawSlots]), static_cast<uint32_t>(k / kRawSlots) & 1u, abort_flag)) break;
-      if (k >= L::kRing &&
-          !mbar_wait(smem_u32(&a_empty[k % L::kRing]), static_cast<uint32_t>(k / L::kRing - 1) & 1u, abort_flag)) {
+      uint32_t cols[32];
+      ti2_convert_lane(raw + (k % kRawSlots) * kRawBytes, m, nv, cols);
+      mbar_arrive(smem_u32(&raw_empty[k % kRawSlots]));
+      if (k >= kRing &&
+          !mbar_wait(smem_u32(&a_empty[k % kRing]), static_cast<uint32_t>(k / kRing - 1) & 1u, abort_flag)) {
         break;
       }
-      ti2_convert_row(raw + (k % kRawSlots) * kRawBytes, ring + (k % L::kRing) * kRowBytes, nv, t);
-      asm volatile("fence.proxy.async.shared::cta;" ::: "memory");
-      mbar_arrive(smem_u32(&a_full[k % L::kRing]));
-      mbar_arrive(smem_u32(&raw_empty[k % kRawSlots]));
+      tc_fence_after();
+      tmem_st32(lane_base + static_cast<uint32_t>(kRingColumn0 + (k % kRing) * 32), cols);
+      tmem_wait_st();
+      tc_fence_before();
+      mbar_arrive(smem_u32(&a_full[k % kRing]));
     }
   } else if (warp < kReadWarp0) {
-    // Builder teams: team e takes chunks c = e (mod 2) into B stage e.
-    const int team = (warp - kBuildWarp0) >> 1;
-    const int t = tid - kBuildWarp0 * 32 - team * kTeamThreads;
+    // Builder teams: team e takes chunks c = e (mod 4) into B stage e. A
+    // lane holds one point's window record in registers and writes its share
+    // of the window rows of that point's B column; the team's next record
+    // copy is issued as soon as every lane holds its record, so it lands
+    // while the team builds.
+    const int team = warp - kBuildWarp0;
     unsigned char* wst = smem + L::kWeightsBase + team * kWeightStage;
     const TcWeights* s_w = reinterpret_cast<const TcWeights*>(wst);
     unsigned char* b_hi = smem + L::kBBase + team * 2 * L::kBHalf;
     unsigned char* b_lo = b_hi + L::kBHalf;
+    const uint32_t wbar = smem_u32(&w_full[team]);
     int loads = 0;
+    if (lane == 0 && team < n) {
+      const Ti2Chunk ch = s_chunks[team];
+      const uint32_t bytes = static_cast<uint32_t>(ch.count) * static_cast<uint32_t>(sizeof(TcWeights));
+      mbar_expect(wbar, bytes);
+      bulk_load(smem_u32(wst), weights + ch.slot, bytes, wbar);
+      loads = 1;
+    }
     for (int c = team; c < n; c += kBStages) {
       const Ti2Chunk ch = s_chunks[c];
       const int use = c / kBStages;
-      const uint32_t wbar = smem_u32(&w_full[team]);
-      if (t == 0) {
-        // The team's previous records are read (every team thread arrived).
-        if (use >= 1 && !mbar_wait(smem_u32(&w_empty[team]), static_cast<uint32_t>(use - 1) & 1u, abort_flag)) break;
-        const uint32_t bytes = static_cast<uint32_t>(ch.count) * static_cast<uint32_t>(sizeof(TcWeights));
-        mbar_expect(wbar, bytes);
-        bulk_load(smem_u32(wst), weights + ch.slot, bytes, wbar);
-        loads = use + 1;
-      }
       if (!mbar_wait(wbar, static_cast<uint32_t>(use) & 1u, abort_flag)) break;
+      const int shift = ch.count <= 16 ? 4 : 5;  // log2 of the B columns
+      const int pn = lane & ((1 << shift) - 1);  // the lane's point (B column)
+      const int share = lane >> shift, shares = 32 >> shift;
+      float wy[W];
+      float4 wx[4];
+      if (pn < ch.count) {
+#pragma unroll
+        for (int j = 0; j < W; ++j) wy[j] = s_w[pn].wy[j];
+#pragma unroll
+        for (int q = 0; q < 4; ++q) wx[q] = *reinterpret_cast<const float4*>(&s_w[pn].wxs[4 * q]);
+      } else {
+#pragma unroll
+        for (int j = 0; j < W; ++j) wy[j] = 0.0f;
+#pragma unroll
+        for (int q = 0; q < 4; ++q) wx[q] = make_float4(0.0f, 0.0f, 0.0f, 0.0f);
+      }
+      mbar_arrive(smem_u32(&w_empty[team]));
+      if (lane == 0 && c + kBStages < n) {
+        // Every lane holds its record: the stage takes the next chunk's.
+        if (!mbar_wait(smem_u32(&w_empty[team]), static_cast<uint32_t>(use) & 1u, abort_flag)) break;
+        const Ti2Chunk nx = s_chunks[c + kBStages];
+        const uint32_t bytes = static_cast<uint32_t>(nx.count) * static_cast<uint32_t>(sizeof(TcWeights));
+        mbar_expect(wbar, bytes);
+        bulk_load(smem_u32(wst), weights + nx.slot, bytes, wbar);
+        loads = use + 2;
+      }
       if (use >= 1 && !mbar_wait(smem_u32(&b_empty[team]), static_cast<uint32_t>(use - 1) & 1u, abort_flag)) break;
-      const int cols = ch.count <= 16 ? 16 : 32;
-      for (int u = t; u < cols * 4 * W; u += kTeamThreads) {
-        const int kb = u / cols, pn = u - kb * cols;
-        float4 value = make_float4(0.0f, 0.0f, 0.0f, 0.0f);
-        if (pn < ch.count) {
-          const float wy = s_w[pn].wy[kb >> 2];
-          const float4 wx = *reinterpret_cast<const float4*>(&s_w[pn].wxs[4 * (kb & 3)]);
-          value = make_float4(wy * wx.x, wy * wx.y, wy * wx.z, wy * wx.w);
+      const int column = (pn >> 3) * static_cast<int>(L::kBStride) + (pn & 7) * 16;
+#pragma unroll
+      for (int j = 0; j < W; ++j) {
+        if (j % shares != share) continue;
+#pragma unroll
+        for (int q = 0; q < 4; ++q) {
+          float4 hi, lo;
+          split_tf32(wy[j] * wx[q].x, hi.x, lo.x);
+          split_tf32(wy[j] * wx[q].y, hi.y, lo.y);
+          split_tf32(wy[j] * wx[q].z, hi.z, lo.z);
+          split_tf32(wy[j] * wx[q].w, hi.w, lo.w);
+          const int off = (4 * j + q) * 128 + column;
+          *reinterpret_cast<float4*>(b_hi + off) = hi;
+          *reinterpret_cast<float4*>(b_lo + off) = lo;
         }
-        float4 hi, lo;
-        split_tf32(value.x, hi.x, lo.x);
-        split_tf32(value.y, hi.y, lo.y);
-        split_tf32(value.z, hi.z, lo.z);
-        split_tf32(value.w, hi.w, lo.w);
-        const int off = kb * 128 + (pn >> 3) * static_cast<int>(L::kBStride) + (pn & 7) * 16;
-        *reinterpret_cast<float4*>(b_hi + off) = hi;
-        *reinterpret_cast<float4*>(b_lo + off) = lo;
       }
       asm volatile("fence.proxy.async.shared::cta;" ::: "memory");
       mbar_arrive(smem_u32(&b_full[team]));
-      mbar_arrive(smem_u32(&w_empty[team]));
     }
     // A weight copy in flight lands before the CTA leaves.
-    if (t == 0 && loads > 0 &&
+    if (lane == 0 && loads > 0 &&
         !mbar_wait(smem_u32(&w_full[team]), static_cast<uint32_t>(loads - 1) & 1u, nullptr)) {
       *abort_flag = 1;
     }
   } else {
-    // Read-out: warp q holds rows 32 q + lane (vector m / 2, real part when
-    // m is even) of each accumulator; values go out in tensor-core slot order.
-    const int q = warp - kReadWarp0;
+    // Read-out: warp (warp % 4 = q) holds rows 32 q + lane (vector m / 2,
+    // real part when m is even) of each accumulator; values go out in
+    // tensor-core slot order.
+    const int q = warp & 3;
     const int m = q * 32 + lane;
     const int vec = m >> 1;
     for (int c = 0; c < n; ++c) {
