@@ -70,7 +70,7 @@ def parse():
     p.add_argument("--steps", type=int, default=10)
     p.add_argument("--warmup", type=int, default=3)
     p.add_argument("--impl", default="b200", choices=["b200", "reference"])
-    for name in ("e2e", "cpu", "clustered", "small", "batched", "uneven", "radial", "f64", "type3"):
+    for name in ("e2e", "cpu", "clustered", "small", "batched", "uneven", "radial", "f64", "type3", "peak"):
         p.add_argument(f"--no-{name}", action="store_true")
     return p.parse_args()
 
@@ -501,6 +501,37 @@ def batched_sweep(r):
     return result
 
 
+def tensor_peak_line(r):
+    """tcgen05.mma throughput on this GPU (b200nufft_tf32_peak: every SM
+    issuing back-to-back M=128 MMAs from one elected lane, 16 straight-line
+    MMAs per block): kind::tf32 (K=8) at N=256 is the dense tf32 peak, N=16
+    and 32 the narrow MMAs of the tensor-core interpolation; kind::f16 (K=16)
+    beside it. Cycles per MMA come from the SM clock counter of CTA 0 (issue
+    plus drain), independent of the clock frequency."""
+    import ctypes
+
+    from wgpunufft_b200 import _native
+
+    lib = _native.library()
+    sms = r.torch.cuda.get_device_properties(r.local).multi_processor_count
+    out = {"unit": "TFLOP/s", "sms": sms}
+    for kind, f16, k in (("tf32", 0, 8), ("f16", 1, 16)):
+        for n in (256, 32, 16):
+            for where, a_tmem in (("a_smem", 0), ("a_tmem", 1)):
+                iters = 40000
+                ms = ctypes.c_float(0.0)
+                cycles = (ctypes.c_uint64 * 2)()
+                status = lib.b200nufft_tf32_peak(n, a_tmem, iters, 1, f16, 16, 0, ctypes.byref(ms), cycles)
+                key = f"{kind}_n{n}_{where}"
+                if status != 0 or ms.value <= 0:
+                    out[key] = {"status": status}
+                    continue
+                flops = 2.0 * 128 * n * k * iters * sms
+                out[key] = {"tflops": flops / (ms.value / 1e3) / 1e12, "ms": ms.value,
+                            "cycles_per_mma": cycles[1] / iters}
+    return out
+
+
 def to_df64(torch, x):
     """Double-float storage of an f64 (or c128) tensor: (hi, lo) f32 pairs per scalar."""
     real = torch.view_as_real(x) if x.is_complex() else x
@@ -836,6 +867,7 @@ def main():
     uneven = None if args.no_uneven else uneven_problems_line(r)
     radial = None if args.no_radial else radial_3d_line(r)
     type3 = None if args.no_type3 else type3_line(r)
+    tensor_peak = None if args.no_peak else tensor_peak_line(r)
 
     if rank == 0:
         peaks = json.loads((ROOT / "MEASURED_PEAKS.json").read_text()) if (ROOT / "MEASURED_PEAKS.json").exists() else {}
@@ -876,6 +908,7 @@ def main():
             "radial_3d": compact(radial) if radial else None,
             "uneven_problems": compact(uneven) if uneven else None,
             "type3": compact(type3) if type3 else None,
+            "tf32_tensor_peak": compact(tensor_peak) if tensor_peak else None,
             "stages_ms_per_step": stage_ms(stages, args.steps),
             "type2": compact(type2),
             "one_shot": {"value": one_shot, "unit": UNIT, "ms_per_step": one_shot_ms / args.steps,

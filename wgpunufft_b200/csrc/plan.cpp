@@ -663,6 +663,7 @@ void NufftPlan::set_points(int64_t count, const void* points, cudaStream_t strea
           tc2_part_start_.reserve((tiles + 1) * sizeof(uint32_t), "tensor-core part offsets"));
       tc_interp_prepare(tc2_grid_, p, stream);
       tc2_part_upper_bound_ = tiles + chunk_bound / kTi2ChunksPerPart + 1;
+      tc2_vector_max_.reserve(static_cast<size_t>(std::max<int64_t>(batch_, 1)) * sizeof(uint32_t), "vector maxima");
     }
     if (valid_first) {
       sort_points_valid_first(static_cast<const float*>(points), count, grid_, bins_, buf, offsets, valid_mask,
@@ -882,6 +883,7 @@ void NufftPlan::execute_f32(int batch, const void* input, void* output, uint64_t
       t.staged = static_cast<float2*>(staged_.reserve(
           static_cast<size_t>(point_count_) * groups * kTi2Vectors * sizeof(float2), "staged type-2 values"));
       t.output = static_cast<float2*>(output);
+      t.vector_max = static_cast<uint32_t*>(tc2_vector_max_.get());
       t.error_flag = static_cast<uint32_t*>(counters_.get()) + 7;
       StageScope scope(&timer_, kStageInterpolation, stream);
       tc_interp_execute(tc2_grid_, t, stream);

@@ -172,6 +172,7 @@ class NufftPlan {
   GridParams tc2_grid_{};
   DeviceBuffer tc2_offsets_, tc2_weights_, tc2_inverse_, tc2_tile_chunks_, tc2_tile_chunk_start_, tc2_chunks_;
   DeviceBuffer tc2_parts_, tc2_part_start_;
+  DeviceBuffer tc2_vector_max_;  // batch words: largest grid magnitude of every vector
   int64_t tc2_part_upper_bound_ = 0;
 };
 

@@ -1,13 +1,14 @@
 // Batched 2D type-2 interpolation on the tcgen05 tensor cores (tc_interp.cu).
 //
 // When many coefficient vectors share one point set, interpolating the
-// points whose support starts in one row y of an 8-cell column group is a
-// dense contraction: the fine-grid values of 64 vectors over the w window
-// rows y .. y + w - 1 and 16 columns of the group (128 rows: real and
-// imaginary parts; K = 16 w cells) times each point's separable window
-// weights over the same cells (N = the points). Such a group of points is a
-// chunk of at most 32 points; it is 2 w MMAs of M = 128, N = 16 or 32,
-// K = 8, each split into 3 tf32 MMAs (hi*hi + hi*lo + lo*hi) to keep FP32
+// points whose support starts in one band of 4 rows of an 8-cell column group
+// is a dense contraction: the fine-grid values of 64 vectors over the w + 3
+// window rows of the band and 16 columns of the group (128 rows: real and
+// imaginary parts; K = 16 cells per row) times each point's separable window
+// weights over the same cells (N = the points, zero outside each window).
+// Such a group of points is a chunk of at most 128 points; it is w + 3 MMA
+// steps of M = 128, N = 16 .. 128, K = 16, each split into 3 f16 MMAs
+// (hi*hi + hi*lo + lo*hi of power-of-two-scaled values) that keep FP32
 // accuracy, in a fixed order, so results are bitwise repeatable.
 #pragma once
 
@@ -21,24 +22,25 @@
 namespace b200nufft {
 
 constexpr int kTi2Vectors = 64;        // vectors per CTA (M = 128 rows)
-constexpr int kTi2ChunkPoints = 32;    // points per chunk at most (N = 16 or 32)
+constexpr int kTi2ChunkPoints = 128;   // points per chunk at most (N = 16 .. 128)
 constexpr int kTi2GroupX = 8;          // cells per column group (chunk starts)
 constexpr int kTi2Pitch = 16;          // region columns per window row (K per row)
 constexpr int kTi2MaxWidth = 7;        // widest window
-constexpr int kTi2TileRows = 64;       // rows of one tile
+constexpr int kTi2BandRows = 4;        // rows of one chunk band (support starts)
+constexpr int kTi2TileRows = 128;      // rows of one tile (a multiple of the band rows)
 constexpr int kTi2ChunksPerPart = 256; // chunks per CTA at most
 
-// One chunk: up to 32 consecutive slots of one (row, column group) bin.
+// One chunk: up to 128 consecutive slots of one (band, column group) bin.
 struct Ti2Chunk {
   uint32_t slot;
   uint16_t count;
-  uint16_t row;  // support row relative to the tile's first row
+  uint16_t row;  // first row of the band relative to the tile's first row
 };
 
 // Whether a plan of this fine grid and window can interpolate on the tensor cores.
 bool tc_interp_supported(const GridParams& g);
 
-// The bin geometry of the tensor-core order: bins of 8 x 1 cells keyed by
+// The bin geometry of the tensor-core order: bins of 8 x 4 cells keyed by
 // the exact support start (a copy of `g` with those shifts and strides).
 GridParams tc_interp_bins(const GridParams& g, uint64_t* bins);
 
@@ -72,6 +74,7 @@ struct Ti2Launch {
   const uint32_t* inverse;
   float2* staged;            // count x groups x 64 values, tensor-core slot order
   float2* output;            // batch x count, caller's point order
+  uint32_t* vector_max;      // batch words of scratch: largest |re|, |im| of every vector's fine grid
   uint32_t* error_flag;      // incremented when a wait gives up
 };
 void tc_interp_execute(const GridParams& g, const Ti2Launch& l, cudaStream_t stream);
