@@ -30,10 +30,11 @@ constexpr int kBOffset = 4096;         // B: up to 256 rows x 8 tf32 (8 KB)
 constexpr int kTmemA = 256;            // A in tensor memory: columns 256 .. 263
 
 // Issues MMAs in blocks of U straight-line instructions per elected lane.
-template <int U>
+template <int U, bool Commits>
 __device__ __forceinline__ void issue_block(int mode, uint32_t& d, uint32_t d_begin, uint32_t d_end, uint32_t n,
                                             uint32_t a_tmem, uint64_t a, uint64_t b, uint32_t idesc, int i,
-                                            int accumulators, int commit_every, uint32_t spare_bar) {
+                                            int accumulators, int commit_every, int& until_commit,
+                                            uint32_t spare_bar) {
   if (elect_one()) {
 #pragma unroll
     for (int u = 0; u < U; ++u) {
@@ -45,7 +46,10 @@ __device__ __forceinline__ void issue_block(int mode, uint32_t& d, uint32_t d_be
         default: mma_f16_tmem_a(d, a_tmem, b, idesc, acc); break;
       }
       // A commit every commit_every MMAs onto a barrier nothing waits for.
-      if (commit_every > 0 && (i + u + 1) % commit_every == 0) mma_commit(spare_bar);
+      if (Commits && --until_commit == 0) {
+        mma_commit(spare_bar);
+        until_commit = commit_every;
+      }
       d += n;
       if (d == d_end) d = d_begin;
     }
@@ -94,16 +98,19 @@ __global__ void __launch_bounds__(kPeakThreads, 1) tf32_peak_kernel(int n, int a
     const uint32_t d_end = tm + static_cast<uint32_t>(accumulators * n);
     uint32_t d = tm;
     const int mode = (f16 ? 2 : 0) + (a_in_tmem ? 1 : 0);
+    int until_commit = -1;  // MMAs before the next interleaved commit (-1: none)
     const long long t0 = clock64();
     for (int i = 0; i < iters; i += unroll) {
       const uint32_t spare_bar = smem_u32(&spare);
-      if (unroll == 16) {
-        issue_block<16>(mode, d, tm, d_end, n, tm + kTmemA, a, b, idesc, i, accumulators, commit_every, spare_bar);
-      } else if (unroll == 4) {
-        issue_block<4>(mode, d, tm, d_end, n, tm + kTmemA, a, b, idesc, i, accumulators, commit_every, spare_bar);
+      if (i == 0) until_commit = commit_every > 0 ? commit_every : -1;
+#define B200NUFFT_ISSUE(U, C) \
+  issue_block<U, C>(mode, d, tm, d_end, n, tm + kTmemA, a, b, idesc, i, accumulators, commit_every, until_commit, spare_bar)
+      if (commit_every > 0) {
+        if (unroll == 16) B200NUFFT_ISSUE(16, true); else if (unroll == 4) B200NUFFT_ISSUE(4, true); else B200NUFFT_ISSUE(1, true);
       } else {
-        issue_block<1>(mode, d, tm, d_end, n, tm + kTmemA, a, b, idesc, i, accumulators, commit_every, spare_bar);
+        if (unroll == 16) B200NUFFT_ISSUE(16, false); else if (unroll == 4) B200NUFFT_ISSUE(4, false); else B200NUFFT_ISSUE(1, false);
       }
+#undef B200NUFFT_ISSUE
     }
     const long long t1 = clock64();
     if (elect_one()) mma_commit(smem_u32(&done));

@@ -12,17 +12,17 @@ struct TuningEntry {
 };
 
 constexpr TuningEntry kTuningTable[] = {
-    {1, 2, 3, 6, 22, 1, 64, 4, 2, 16},  // 2d_1024_1e7_uniform+2d_1024_1e7_clustered: 0.9285 ms
-    {1, 2, 3, 7, 20, 0, 32, 4, 1, 16},  // 2d_512_2e6_uniform: 0.1856 ms
-    {1, 2, 3, 7, 14, 2, 32, 2, 2, 16},  // 2d_64_1e5_uniform: 0.0564 ms
-    {1, 2, 3, 7, 16, -3, 32, 2, 2, 16},  // 2d_128_1e4_uniform: 0.0596 ms
-    {1, 2, 3, 7, 16, 3, 32, 4, 2, 16},  // 2d_128_1e6_clustered: 0.1293 ms
-    {1, 2, 3, 7, 18, -2, 32, 2, 1, 16},  // 2d_256_1e5_uniform: 0.0572 ms
-    {1, 3, 3, 6, 27, -2, 16, 2, 1, 16},  // 3d_256_5e7_radial: 13.7233 ms
-    {1, 3, 3, 7, 21, -2, 16, 4, 1, 16},  // 3d_64_1e6_uniform: 0.5531 ms
-    {1, 3, 3, 7, 18, -2, 8, 2, 1, 16},  // 3d_32_1e5_clustered: 0.0967 ms
-    {1, 2, 1, 10, 20, 0, 16, 2, 1, 16},  // 2d_512_2e6_f64_1e-9: 1.0748 ms
-    {2, 2, 3, 7, 20, 0, 32, 4, 1, 64},  // 2d_512_2e6_uniform_type2: 0.1856 ms
+    {1, 2, 3, 6, 22, 1, 64, 2, 2, 16},  // 2d_1024_1e7_uniform+2d_1024_1e7_clustered: 0.9342 ms
+    {1, 2, 3, 7, 20, 0, 32, 4, 1, 16},  // 2d_512_2e6_uniform: 0.1855 ms
+    {1, 2, 3, 7, 14, 2, 32, 2, 2, 16},  // 2d_64_1e5_uniform: 0.0559 ms
+    {1, 2, 3, 7, 16, -3, 32, 8, 2, 16},  // 2d_128_1e4_uniform: 0.0589 ms
+    {1, 2, 3, 7, 16, 3, 32, 4, 2, 16},  // 2d_128_1e6_clustered: 0.1298 ms
+    {1, 2, 3, 7, 18, -2, 32, 2, 2, 16},  // 2d_256_1e5_uniform: 0.0572 ms
+    {1, 3, 3, 6, 27, -2, 16, 2, 1, 16},  // 3d_256_5e7_radial: 13.7454 ms
+    {1, 3, 3, 7, 21, -2, 16, 4, 1, 16},  // 3d_64_1e6_uniform: 0.5508 ms
+    {1, 3, 3, 7, 18, -2, 8, 2, 1, 16},  // 3d_32_1e5_clustered: 0.0966 ms
+    {1, 2, 1, 10, 20, 0, 16, 8, 1, 16},  // 2d_512_2e6_f64_1e-9: 1.0739 ms
+    {2, 2, 3, 7, 20, 0, 32, 4, 1, 64},  // 2d_512_2e6_uniform_type2: 0.1855 ms
 };
 constexpr int kTuningEntries = 11;
 
