@@ -1,7 +1,8 @@
 """The NumPy plans (wgpunufft_b200.numpy_api) against the reference's Python
 binding tests (python/tests/test_bindings.py): direct sums, NumPy axis
-order, batches, concurrent calls on one plan, type 3, empty transforms and
-validation messages."""
+order, batches, concurrent calls on one plan, type 3, empty transforms,
+validation messages, the error type's pickle round trip, a clean shutdown of
+a fresh process and plans destroyed on another thread."""
 
 from __future__ import annotations
 
@@ -187,3 +188,83 @@ def test_context_describes_the_device(context):
     assert context.device_type == "DiscreteGpu"
     with pytest.raises(wn.WgpuNufftError):
         wn.Context(force_fallback=True)
+
+
+ROOT = __import__("pathlib").Path(__file__).resolve().parents[1]
+
+
+def _run_script(script: str):
+    import subprocess
+    import sys
+
+    return subprocess.run([sys.executable, "-c", script], cwd=str(ROOT), check=False, capture_output=True,
+                          text=True, timeout=300)
+
+
+def test_error_pickles_and_the_interface_is_documented():
+    """The reference's metadata test (test_bindings.py:18-25): the error type
+    survives a pickle round trip with its message, and the plans document
+    themselves."""
+    import pickle
+
+    error = pickle.loads(pickle.dumps(wn.WgpuNufftError("test error")))
+    assert isinstance(error, wn.WgpuNufftError)
+    assert str(error) == "test error"
+    assert wn.Context.__doc__
+    assert wn.Type1Plan.execute.__doc__
+    assert wn.Type2Plan.execute.__doc__
+
+
+def test_gpu_resources_shut_down_cleanly_in_a_fresh_process():
+    """A process that makes a context and a plan, executes and exits without
+    releasing them ends with status 0 (test_bindings.py:28-46)."""
+    completed = _run_script("""
+import numpy as np
+from wgpunufft_b200 import numpy_api as wn
+
+context = wn.Context()
+plan = wn.Type1Plan(context, (8,), eps=1e-4)
+points = np.array([-0.5, 0.25], dtype=np.float32)
+strengths = np.array([1.0 + 0.2j, -0.3 + 0.4j], dtype=np.complex64)
+plan.execute(points, strengths)
+""")
+    assert completed.returncode == 0, completed.stderr
+
+
+def test_gpu_plans_can_be_destroyed_on_another_thread():
+    """Plans made on the main thread and released on a worker thread (after
+    their context is gone) leave the process healthy (test_bindings.py:49-90)."""
+    completed = _run_script("""
+import gc
+import queue
+import threading
+
+from wgpunufft_b200 import numpy_api as wn
+
+objects = queue.Queue()
+stop = object()
+
+def worker():
+    while True:
+        obj = objects.get()
+        if obj is stop:
+            objects.task_done()
+            return
+        del obj
+        gc.collect()
+        objects.task_done()
+
+thread = threading.Thread(target=worker)
+thread.start()
+for _ in range(8):
+    context = wn.Context()
+    plan = wn.Type1Plan(context, (8,), eps=1e-4)
+    del context
+    objects.put(plan)
+    del plan
+    objects.join()
+objects.put(stop)
+objects.join()
+thread.join()
+""")
+    assert completed.returncode == 0, completed.stderr

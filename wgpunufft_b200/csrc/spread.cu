@@ -550,9 +550,20 @@ __device__ void spread_warp3(const SpreadParams& sp, const PreparedWindow<3>* wi
 
   constexpr int L = warp_segment_cells(W);
   constexpr int R = warp_rounds(W);
+  // Staged x weights: one block of up to 8, or (w = 6) the two 3-cell
+  // segments at offsets 0 and 4, so a lane reads its segment with one
+  // aligned load from an offset fixed for the part.
+  constexpr bool kSplitX = W / L == 2;
+  static_assert(W / L == 1 || (kSplitX && L <= 4), "x segments are one block or two aligned halves");
   uint32_t desc[R];
+  int xo[R], yo[R], zo[R];  // the lane's stage offsets of each round: x segment, wy[j], wz[k]
 #pragma unroll
-  for (int r = 0; r < R; ++r) desc[r] = sp.warp_segments[r * 32 + lane];
+  for (int r = 0; r < R; ++r) {
+    desc[r] = sp.warp_segments[r * 32 + lane];
+    xo[r] = 4 * static_cast<int>((desc[r] >> 16) & 15);
+    yo[r] = 8 + static_cast<int>((desc[r] >> 20) & 15);
+    zo[r] = 16 + static_cast<int>((desc[r] >> 24) & 15);
+  }
   float ar[R][L], ai[R][L];
 #pragma unroll
   for (int r = 0; r < R; ++r) {
@@ -632,8 +643,13 @@ __device__ void spread_warp3(const SpreadParams& sp, const PreparedWindow<3>* wi
           }
         }
       }
+      if (kSplitX && a == 0) {
 #pragma unroll
-      for (int j = 0; j < 8; ++j) my_stage[g][a * 8 + j] = j < W ? w[j] : 0.0f;
+        for (int j = 0; j < 8; ++j) my_stage[g][j] = (j & 3) < L ? w[(j >> 2) * L + (j & 3)] : 0.0f;
+      } else {
+#pragma unroll
+        for (int j = 0; j < 8; ++j) my_stage[g][a * 8 + j] = j < W ? w[j] : 0.0f;
+      }
       if (a == 0) my_stage[g][26] = __int_as_float(base);
     }
     __syncwarp();
@@ -648,25 +664,27 @@ __device__ void spread_warp3(const SpreadParams& sp, const PreparedWindow<3>* wi
         run_length = 0;
       }
       ++run_length;
-      const float4 x_lo = *reinterpret_cast<const float4*>(st);
-      const float4 x_hi = *reinterpret_cast<const float4*>(st + 4);
-      const float wx[8] = {x_lo.x, x_lo.y, x_lo.z, x_lo.w, x_hi.x, x_hi.y, x_hi.z, x_hi.w};
       const float2 c = *reinterpret_cast<const float2*>(st + 24);
+      float wx[8];
+      if (!kSplitX) {
+        const float4 x_lo = *reinterpret_cast<const float4*>(st);
+        const float4 x_hi = *reinterpret_cast<const float4*>(st + 4);
+        wx[0] = x_lo.x; wx[1] = x_lo.y; wx[2] = x_lo.z; wx[3] = x_lo.w;
+        wx[4] = x_hi.x; wx[5] = x_hi.y; wx[6] = x_hi.z; wx[7] = x_hi.w;
+      }
 #pragma unroll
       for (int r = 0; r < R; ++r) {
-        const uint32_t d = desc[r];
-        const int s = (d >> 16) & 15, j = (d >> 20) & 15, k = (d >> 24) & 15;
-        const float wyz = st[8 + j] * st[16 + k];
+        const float wyz = st[yo[r]] * st[zo[r]];
         const float wr = c.x * wyz, wi = c.y * wyz;
         float wxs[L];
+        if (kSplitX) {
+          const float4 seg = *reinterpret_cast<const float4*>(st + xo[r]);
+          const float v[4] = {seg.x, seg.y, seg.z, seg.w};
 #pragma unroll
-        for (int t = 0; t < L; ++t) wxs[t] = wx[t];
+          for (int t = 0; t < L; ++t) wxs[t] = v[t];
+        } else {
 #pragma unroll
-        for (int q = 1; q < W / L; ++q) {
-          if (s == q) {
-#pragma unroll
-            for (int t = 0; t < L; ++t) wxs[t] = wx[q * L + t];
-          }
+          for (int t = 0; t < L; ++t) wxs[t] = wx[t];
         }
 #pragma unroll
         for (int t = 0; t < L; ++t) {

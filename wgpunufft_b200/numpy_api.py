@@ -238,6 +238,9 @@ class Type1Plan(_Type12):
     _kind = 1
 
     def execute(self, points: np.ndarray, strengths: np.ndarray) -> np.ndarray:
+        """Type-1 transform: points (M, d) float32 (or (M,) in 1D), strengths
+        (M,) or (B, M) complex64; returns the modes in NumPy axis order,
+        shape n_modes or (B, *n_modes)."""
         points = _c_array("points", points, np.float32)
         count = _check_type12_points("points", points, self.dimensions)
         strengths = _c_array("strengths", strengths, np.complex64)
@@ -256,6 +259,9 @@ class Type2Plan(_Type12):
     _kind = 2
 
     def execute(self, points: np.ndarray, coefficients: np.ndarray) -> np.ndarray:
+        """Type-2 transform: points (M, d) float32 (or (M,) in 1D),
+        coefficients of shape n_modes or (B, *n_modes) complex64 in NumPy axis
+        order; returns the values at the points, shape (M,) or (B, M)."""
         points = _c_array("points", points, np.float32)
         count = _check_type12_points("points", points, self.dimensions)
         coefficients = _c_array("coefficients", coefficients, np.complex64)
@@ -351,6 +357,9 @@ class Type3Plan:
         return count
 
     def execute(self, source_points: np.ndarray, strengths: np.ndarray, target_points: np.ndarray) -> np.ndarray:
+        """Type-3 transform from source_points (M, d) float32 with strengths
+        (M,) or (B, M) complex64 to target_points (N, d) float32, inside the
+        plan's bounds; returns (N,) or (B, N) complex64."""
         m = self._points("source_points", source_points, self._sources)
         n = self._points("target_points", target_points, self._targets)
         strengths = _c_array("strengths", strengths, np.complex64)
