@@ -222,4 +222,15 @@ __device__ __forceinline__ void horner32_window(float offset, const float (&tabl
   }
 }
 
+// Complex-by-real products and accumulations in paired instructions: the
+// real and imaginary parts take the same two correctly rounded operations as
+// two scalar fmaf / multiplies (the same bits), in one f32x2 instruction.
+__device__ __forceinline__ float2 cscale(float2 s, float x) { return __fmul2_rn(s, make_float2(x, x)); }
+__device__ __forceinline__ double2 cscale(double2 s, double x) { return make_double2(s.x * x, s.y * x); }
+// a + w x (each part one fused multiply-add).
+__device__ __forceinline__ float2 cfma(float2 w, float x, float2 a) { return __ffma2_rn(w, make_float2(x, x), a); }
+__device__ __forceinline__ double2 cfma(double2 w, double x, double2 a) {
+  return make_double2(fma(w.x, x, a.x), fma(w.y, x, a.y));
+}
+
 }  // namespace b200nufft

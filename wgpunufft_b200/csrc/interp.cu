@@ -123,14 +123,13 @@ __global__ void __launch_bounds__(256, InterpBlocks<D, W, T>::value)
   }
   for (int b = 0; b < batch; ++b) {
     const Complex* grid = fine + static_cast<int64_t>(b) * g.fine_count;
-    Real re = 0, im = 0;
+    // (re, im) sums: each part the fixed-order fused multiply-adds of the
+    // scalar form, two at a time (cfma).
+    Complex e;
+    e.x = e.y = Real(0);
     if (D == 1) {
 #pragma unroll
-      for (int i = 0; i < W; ++i) {
-        const Complex v = __ldg(&grid[x[i]]);
-        re = T::fma_(v.x, w[0][i], re);
-        im = T::fma_(v.y, w[0][i], im);
-      }
+      for (int i = 0; i < W; ++i) e = cfma(__ldg(&grid[x[i]]), w[0][i], e);
     } else if (D == 2) {
       const int32_t n1 = g.axis[1].length;
 #pragma unroll
@@ -138,15 +137,11 @@ __global__ void __launch_bounds__(256, InterpBlocks<D, W, T>::value)
         int y = first[1] + j;
         y = y >= n1 ? y - n1 : y;
         const Complex* row = grid + static_cast<int64_t>(y) * n0;
-        Real rr = 0, ri = 0;
+        Complex r;
+        r.x = r.y = Real(0);
 #pragma unroll
-        for (int i = 0; i < W; ++i) {
-          const Complex v = __ldg(&row[x[i]]);
-          rr = T::fma_(v.x, w[0][i], rr);
-          ri = T::fma_(v.y, w[0][i], ri);
-        }
-        re = T::fma_(rr, w[1][j], re);
-        im = T::fma_(ri, w[1][j], im);
+        for (int i = 0; i < W; ++i) r = cfma(__ldg(&row[x[i]]), w[0][i], r);
+        e = cfma(r, w[1][j], e);
       }
     } else {
       const int32_t n1 = g.axis[1].length;
@@ -155,30 +150,23 @@ __global__ void __launch_bounds__(256, InterpBlocks<D, W, T>::value)
       for (int k = 0; k < W; ++k) {
         int z = first[2] + k;
         z = z >= n2 ? z - n2 : z;
-        Real pr = 0, pi = 0;
+        Complex pl;
+        pl.x = pl.y = Real(0);
 #pragma unroll
         for (int j = 0; j < W; ++j) {
           int y = first[1] + j;
           y = y >= n1 ? y - n1 : y;
           const Complex* row = grid + (static_cast<int64_t>(z) * n1 + y) * n0;
-          Real rr = 0, ri = 0;
+          Complex r;
+          r.x = r.y = Real(0);
 #pragma unroll
-          for (int i = 0; i < W; ++i) {
-            const Complex v = __ldg(&row[x[i]]);
-            rr = T::fma_(v.x, w[0][i], rr);
-            ri = T::fma_(v.y, w[0][i], ri);
-          }
-          pr = T::fma_(rr, w[1][j], pr);
-          pi = T::fma_(ri, w[1][j], pi);
+          for (int i = 0; i < W; ++i) r = cfma(__ldg(&row[x[i]]), w[0][i], r);
+          pl = cfma(r, w[1][j], pl);
         }
-        re = T::fma_(pr, w[2][k], re);
-        im = T::fma_(pi, w[2][k], im);
+        e = cfma(pl, w[2][k], e);
       }
     }
-    Complex o;
-    o.x = re;
-    o.y = im;
-    output[static_cast<int64_t>(b) * count + point] = o;
+    output[static_cast<int64_t>(b) * count + point] = e;
   }
 }
 
@@ -286,7 +274,7 @@ __global__ void __launch_bounds__(256) interpolate_bins_kernel(GridParams g, con
   for (uint32_t slot = batch_first + warp; slot < batch_last; slot += blockDim.x >> 5) {
     const PreparedWindow<2> win = s_win[slot - batch_first];
     const uint32_t point = s_point[slot - batch_first];
-    float re = 0.0f, im = 0.0f;
+    float2 e = make_float2(0.0f, 0.0f);  // (re, im), paired fused multiply-adds
     if (win.start[0] >= 0) {
       float wx[W], wy[W];
       horner32_window<W>(win.offset[0], g.horner32, wx);
@@ -299,15 +287,13 @@ __global__ void __launch_bounds__(256) interpolate_bins_kernel(GridParams g, con
 #pragma unroll
         for (int j = 0; j < W; ++j) {
           const float2* row = region + ((dy + j) * S + dx) * kBinPitch + lane;
-          float rr = 0.0f, ri = 0.0f;
+          float2 r = make_float2(0.0f, 0.0f);
 #pragma unroll
           for (int i = 0; i < W; ++i) {
             const float2 v = row[i * kBinPitch];
-            rr = fmaf(v.x, wx[i], rr);
-            ri = fmaf(v.y, wx[i], ri);
+            r = cfma(v, wx[i], r);
           }
-          re = fmaf(rr, wy[j], re);
-          im = fmaf(ri, wy[j], im);
+          e = cfma(r, wy[j], e);
         }
       } else {
         // A window beyond the staged region: read the grid directly.
@@ -315,20 +301,18 @@ __global__ void __launch_bounds__(256) interpolate_bins_kernel(GridParams g, con
         for (int j = 0; j < W; ++j) {
           int y = win.start[1] + j;
           y = y >= n1 ? y - n1 : y;
-          float rr = 0.0f, ri = 0.0f;
+          float2 r = make_float2(0.0f, 0.0f);
           for (int i = 0; i < W; ++i) {
             int x = win.start[0] + i;
             x = x >= n0 ? x - n0 : x;
             const float2 v = __ldg(&grid[static_cast<int64_t>(y) * n0 + x]);
-            rr = fmaf(v.x, wx[i], rr);
-            ri = fmaf(v.y, wx[i], ri);
+            r = cfma(v, wx[i], r);
           }
-          re = fmaf(rr, wy[j], re);
-          im = fmaf(ri, wy[j], im);
+          e = cfma(r, wy[j], e);
         }
       }
     }
-    if (lane < nv) staged[static_cast<int64_t>(slot) * staged_stride + vb + lane] = make_float2(re, im);
+    if (lane < nv) staged[static_cast<int64_t>(slot) * staged_stride + vb + lane] = e;
     (void)point;
   }
   }
@@ -382,7 +366,7 @@ __global__ void __launch_bounds__(kRegionThreads) interpolate_region_kernel(
                                         ? next_win
                                         : static_cast<const PreparedWindow<2>*>(windows)[slot];
       const uint32_t point = slot == first + threadIdx.x ? next_point : perm[slot];
-      float re = 0.0f, im = 0.0f;
+      float2 e = make_float2(0.0f, 0.0f);  // (re, im), paired fused multiply-adds
       if (win.start[0] >= 0) {
         float wx[W], wy[W];
         horner32_window<W>(win.offset[0], g.horner32, wx);
@@ -395,35 +379,31 @@ __global__ void __launch_bounds__(kRegionThreads) interpolate_region_kernel(
 #pragma unroll
           for (int j = 0; j < W; ++j) {
             const float2* row = region + (dy + j) * S + dx;
-            float rr = 0.0f, ri = 0.0f;
+            float2 r = make_float2(0.0f, 0.0f);
 #pragma unroll
             for (int i = 0; i < W; ++i) {
               const float2 v = row[i];
-              rr = fmaf(v.x, wx[i], rr);
-              ri = fmaf(v.y, wx[i], ri);
+              r = cfma(v, wx[i], r);
             }
-            re = fmaf(rr, wy[j], re);
-            im = fmaf(ri, wy[j], im);
+            e = cfma(r, wy[j], e);
           }
         } else {
 #pragma unroll 1
           for (int j = 0; j < W; ++j) {
             int y = win.start[1] + j;
             y = y >= n1 ? y - n1 : y;
-            float rr = 0.0f, ri = 0.0f;
+            float2 r = make_float2(0.0f, 0.0f);
             for (int i = 0; i < W; ++i) {
               int x = win.start[0] + i;
               x = x >= n0 ? x - n0 : x;
               const float2 v = __ldg(&grid[static_cast<int64_t>(y) * n0 + x]);
-              rr = fmaf(v.x, wx[i], rr);
-              ri = fmaf(v.y, wx[i], ri);
+              r = cfma(v, wx[i], r);
             }
-            re = fmaf(rr, wy[j], re);
-            im = fmaf(ri, wy[j], im);
+            e = cfma(r, wy[j], e);
           }
         }
       }
-      output[static_cast<int64_t>(b) * count + point] = make_float2(re, im);
+      output[static_cast<int64_t>(b) * count + point] = e;
     }
   }
 }

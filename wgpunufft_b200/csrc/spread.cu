@@ -362,16 +362,16 @@ __device__ __forceinline__ bool prepared_record(const SpreadParams& sp, const Pr
 // and clears them.
 template <int D, int W, typename T>
 __device__ __forceinline__ void flush_run(typename T::Word* acc, int padded, int pad0, int x, int y,
-                                          typename T::Real (*ar)[W], typename T::Real (*ai)[W]) {
+                                          typename T::Complex (*a)[W]) {
   constexpr int R = D == 2 ? W : 1;
 #pragma unroll
   for (int j = 0; j < R; ++j) {
     const int base = (y + j) * pad0 + x;
 #pragma unroll
     for (int i = 0; i < W; ++i) {
-      T::add(acc, padded, 0, base + i, ar[j][i]);
-      T::add(acc, padded, 1, base + i, ai[j][i]);
-      ar[j][i] = ai[j][i] = typename T::Real(0);
+      T::add(acc, padded, 0, base + i, a[j][i].x);
+      T::add(acc, padded, 1, base + i, a[j][i].y);
+      a[j][i].x = a[j][i].y = typename T::Real(0);
     }
   }
 }
@@ -385,18 +385,15 @@ __device__ __forceinline__ void flush_run(typename T::Word* acc, int padded, int
 // about one column per distinct start.
 template <int W, typename T>
 __device__ __forceinline__ void flush_first_column(typename T::Word* acc, int padded, int pad0, int x, int y,
-                                                   typename T::Real (*ar)[W], typename T::Real (*ai)[W]) {
+                                                   typename T::Complex (*a)[W]) {
 #pragma unroll
   for (int j = 0; j < W; ++j) {
     const int c = (y + j) * pad0 + x;
-    T::add(acc, padded, 0, c, ar[j][0]);
-    T::add(acc, padded, 1, c, ai[j][0]);
+    T::add(acc, padded, 0, c, a[j][0].x);
+    T::add(acc, padded, 1, c, a[j][0].y);
 #pragma unroll
-    for (int i = 0; i + 1 < W; ++i) {
-      ar[j][i] = ar[j][i + 1];
-      ai[j][i] = ai[j][i + 1];
-    }
-    ar[j][W - 1] = ai[j][W - 1] = typename T::Real(0);
+    for (int i = 0; i + 1 < W; ++i) a[j][i] = a[j][i + 1];
+    a[j][W - 1].x = a[j][W - 1].y = typename T::Real(0);
   }
 }
 
@@ -564,11 +561,11 @@ __device__ void spread_warp3(const SpreadParams& sp, const PreparedWindow<3>* wi
     yo[r] = 8 + static_cast<int>((desc[r] >> 20) & 15);
     zo[r] = 16 + static_cast<int>((desc[r] >> 24) & 15);
   }
-  float ar[R][L], ai[R][L];
+  float2 a2[R][L];  // (re, im) register sums of the run
 #pragma unroll
   for (int r = 0; r < R; ++r) {
 #pragma unroll
-    for (int t = 0; t < L; ++t) ar[r][t] = ai[r][t] = 0.0f;
+    for (int t = 0; t < L; ++t) a2[r][t] = make_float2(0.0f, 0.0f);
   }
   int run = -1, run_length = 0;
   auto flush = [&]() {
@@ -578,12 +575,12 @@ __device__ void spread_warp3(const SpreadParams& sp, const PreparedWindow<3>* wi
         const int c = run + static_cast<int>(desc[r] & 0xFFFFu);
 #pragma unroll
         for (int t = 0; t < L; ++t) {
-          F32Traits::add(acc, span, 0, c + t, ar[r][t]);
-          F32Traits::add(acc, span, 1, c + t, ai[r][t]);
+          F32Traits::add(acc, span, 0, c + t, a2[r][t].x);
+          F32Traits::add(acc, span, 1, c + t, a2[r][t].y);
         }
       }
 #pragma unroll
-      for (int t = 0; t < L; ++t) ar[r][t] = ai[r][t] = 0.0f;
+      for (int t = 0; t < L; ++t) a2[r][t] = make_float2(0.0f, 0.0f);
     }
   };
   float (*my_stage)[kStageStride] = stage[warp];
@@ -675,7 +672,7 @@ __device__ void spread_warp3(const SpreadParams& sp, const PreparedWindow<3>* wi
 #pragma unroll
       for (int r = 0; r < R; ++r) {
         const float wyz = st[yo[r]] * st[zo[r]];
-        const float wr = c.x * wyz, wi = c.y * wyz;
+        const float2 wc = cscale(c, wyz);
         float wxs[L];
         if (kSplitX) {
           const float4 seg = *reinterpret_cast<const float4*>(st + xo[r]);
@@ -687,10 +684,7 @@ __device__ void spread_warp3(const SpreadParams& sp, const PreparedWindow<3>* wi
           for (int t = 0; t < L; ++t) wxs[t] = wx[t];
         }
 #pragma unroll
-        for (int t = 0; t < L; ++t) {
-          ar[r][t] = fmaf(wr, wxs[t], ar[r][t]);
-          ai[r][t] = fmaf(wi, wxs[t], ai[r][t]);
-        }
+        for (int t = 0; t < L; ++t) a2[r][t] = cfma(wc, wxs[t], a2[r][t]);
       }
     }
     __syncwarp();
@@ -1075,11 +1069,11 @@ __device__ __forceinline__ void spread_part(
     const uint32_t run = passes ? (count + kSpreadThreads * passes - 1) / (kSpreadThreads * passes) : 1u;
     for (uint32_t first = record_begin + tid * run; first < record_end; first += kSpreadThreads * run) {
       const uint32_t stop = min(first + run, record_end);
-      Real ar[R][W], ai[R][W];
+      typename T::Complex a2[R][W];  // (re, im) register sums of the run
 #pragma unroll
       for (int j = 0; j < R; ++j) {
 #pragma unroll
-        for (int i = 0; i < W; ++i) ar[j][i] = ai[j][i] = Real(0);
+        for (int i = 0; i < W; ++i) a2[j][i].x = a2[j][i].y = Real(0);
       }
       int run0 = -1, run1 = 0;
       // f32: records are loaded ahead of their use, so the load latency
@@ -1136,36 +1130,31 @@ __device__ __forceinline__ void spread_part(
         }
         // The strength in the fixed-point scale (a power of two: exact), so
         // the run sums reach the tile without another product.
-        s.x = (s.x * scale_lo) * scale_hi;
-        s.y = (s.y * scale_lo) * scale_hi;
+        s = cscale(cscale(s, scale_lo), scale_hi);
         const int l1 = D == 2 ? local_start[D - 1] : 0;
         if constexpr (D == 2) {
           const int l0 = local_start[0];
           if (run0 >= 0 && l1 == run1 && l0 > run0 && l0 < run0 + W) {
             // Same row, a few columns on: flush and drop the passed columns.
-            for (; run0 < l0; ++run0) flush_first_column<W, T>(acc, padded, sp.pad[0], run0, run1, ar, ai);
+            for (; run0 < l0; ++run0) flush_first_column<W, T>(acc, padded, sp.pad[0], run0, run1, a2);
           } else if (l0 != run0 || l1 != run1) {
-            if (run0 >= 0) flush_run<D, W, T>(acc, padded, sp.pad[0], run0, run1, ar, ai);
+            if (run0 >= 0) flush_run<D, W, T>(acc, padded, sp.pad[0], run0, run1, a2);
             run0 = l0;
             run1 = l1;
           }
         } else if (local_start[0] != run0 || l1 != run1) {
-          if (run0 >= 0) flush_run<D, W, T>(acc, padded, sp.pad[0], run0, run1, ar, ai);
+          if (run0 >= 0) flush_run<D, W, T>(acc, padded, sp.pad[0], run0, run1, a2);
           run0 = local_start[0];
           run1 = l1;
         }
 #pragma unroll
         for (int j = 0; j < R; ++j) {
-          const Real wr = D == 2 ? s.x * w[D - 1][j] : s.x;
-          const Real wi = D == 2 ? s.y * w[D - 1][j] : s.y;
+          const typename T::Complex wj = D == 2 ? cscale(s, w[D - 1][j]) : s;
 #pragma unroll
-          for (int i = 0; i < W; ++i) {
-            ar[j][i] += wr * w[0][i];
-            ai[j][i] += wi * w[0][i];
-          }
+          for (int i = 0; i < W; ++i) a2[j][i] = cfma(wj, w[0][i], a2[j][i]);
         }
       }
-      if (run0 >= 0) flush_run<D, W, T>(acc, padded, sp.pad[0], run0, run1, ar, ai);
+      if (run0 >= 0) flush_run<D, W, T>(acc, padded, sp.pad[0], run0, run1, a2);
     }
   }
   __syncthreads();
