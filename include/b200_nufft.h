@@ -387,6 +387,20 @@ int b200nufft_tuning_override(const b200nufft_tuning *tuning);
  * accounting in benchmarks. */
 uint64_t b200nufft_launch_count(void);
 
+/* Tensor-core throughput on the current device (no counterpart in the
+ * reference: the roofline of the tensor-core kernels). Every SM issues `iters`
+ * back-to-back tcgen05 MMAs of M = 128, N = n (16 .. 256, a multiple of 16),
+ * K = 8 (kind::tf32) or 16 (kind::f16 when f16 != 0) from one elected lane in
+ * blocks of `unroll` (1, 4 or 16; iters a multiple of it), rotating over
+ * `accumulators` accumulators (accumulators x n <= 256), A in tensor memory
+ * when a_in_tmem, a commit every `commit_every` MMAs (0: at the end only).
+ * Writes the launch's duration in milliseconds and, when cycles is not null,
+ * SM cycles of CTA 0's issue loop and of issue plus drain. Returns 0, the
+ * number of CTAs whose bounded wait gave up, or -1 on a CUDA error or bad
+ * argument. Allocates a few bytes of device memory per call. */
+int b200nufft_tf32_peak(int n, int a_in_tmem, int iters, int accumulators, int f16, int unroll, int commit_every,
+                        float *ms, unsigned long long *cycles);
+
 #ifdef __cplusplus
 }
 #endif

@@ -700,7 +700,7 @@ GridParams tc_interp_bins(const GridParams& g, uint64_t* bins) {
   b.axis[0].shift = 3;
   b.axis[0].bins = groups;
   b.axis[0].stride = 1;
-  b.axis[1].shift = 2;
+  b.axis[1].shift = kTi2BandRows == 4 ? 2 : (kTi2BandRows == 2 ? 1 : 0);
   b.axis[1].bins = bands;
   b.axis[1].stride = groups;
   *bins = static_cast<uint64_t>(groups) * static_cast<uint64_t>(bands);

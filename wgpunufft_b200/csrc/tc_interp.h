@@ -26,8 +26,9 @@ constexpr int kTi2ChunkPoints = 128;   // points per chunk at most (N = 16 .. 12
 constexpr int kTi2GroupX = 8;          // cells per column group (chunk starts)
 constexpr int kTi2Pitch = 16;          // region columns per window row (K per row)
 constexpr int kTi2MaxWidth = 7;        // widest window
-constexpr int kTi2BandRows = 4;        // rows of one chunk band (support starts)
+constexpr int kTi2BandRows = 4;        // rows of one chunk band (support starts): 1, 2 or 4
 constexpr int kTi2TileRows = 128;      // rows of one tile (a multiple of the band rows)
+static_assert(kTi2BandRows == 1 || kTi2BandRows == 2 || kTi2BandRows == 4, "bands of 1, 2 or 4 rows");
 constexpr int kTi2ChunksPerPart = 256; // chunks per CTA at most
 
 // One chunk: up to 128 consecutive slots of one (band, column group) bin.
