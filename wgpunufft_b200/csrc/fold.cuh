@@ -213,12 +213,22 @@ template <int W>
 __device__ __forceinline__ void horner32_window(float offset, const float (&table)[19][16], float* w) {
   const float local = fmaf(2.0f, offset, static_cast<float>(W - 1));
   const bool inside = fabsf(local) <= 1.0f;
+  // Taps in pairs: each lane of the paired fused multiply-add runs one tap's
+  // Horner steps (the bits of the scalar fmaf chain).
+  const float2 x = make_float2(local, local);
 #pragma unroll
-  for (int j = 0; j < W; ++j) {
+  for (int j = 0; j + 1 < W; j += 2) {
+    float2 v = make_float2(0.0f, 0.0f);
+#pragma unroll
+    for (int r = 19 - (W + 3); r < 19; ++r) v = __ffma2_rn(v, x, make_float2(table[r][j], table[r][j + 1]));
+    w[j] = inside ? v.x : 0.0f;
+    w[j + 1] = inside ? v.y : 0.0f;
+  }
+  if (W % 2 == 1) {
     float v = 0.0f;
 #pragma unroll
-    for (int r = 19 - (W + 3); r < 19; ++r) v = fmaf(v, local, table[r][j]);
-    w[j] = inside ? v : 0.0f;
+    for (int r = 19 - (W + 3); r < 19; ++r) v = fmaf(v, local, table[r][W - 1]);
+    w[W - 1] = inside ? v : 0.0f;
   }
 }
 

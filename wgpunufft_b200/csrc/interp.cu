@@ -70,6 +70,18 @@ struct InterpBlocks {
   static constexpr int value = (D <= 2 && W <= 4 && sizeof(typename T::Real) == 4) ? 3 : 2;
 };
 
+// v mod n in [0, n): one conditional add or subtract for the offsets the
+// region kernels meet (within one period), the remainder otherwise.
+__device__ __forceinline__ int wrap_index(int v, int n) {
+  if (v < 0) v += n;
+  if (v >= n) v -= n;
+  if (v < 0 || v >= n) {
+    v %= n;
+    if (v < 0) v += n;
+  }
+  return v;
+}
+
 template <int D, int W, typename T>
 __global__ void __launch_bounds__(256, InterpBlocks<D, W, T>::value)
     interpolate_kernel(GridParams g, const typename T::Real* __restrict__ points,
@@ -241,10 +253,8 @@ __global__ void __launch_bounds__(256) interpolate_bins_kernel(GridParams g, con
       const int v = e / (S * S), cell = e - v * (S * S);
       if (e < kTotal && v < nv) {
         const int r = cell / S, c = cell - r * S;
-        int y = (oy + r) % n1;
-        y = y < 0 ? y + n1 : y;
-        int x = (ox + c) % n0;
-        x = x < 0 ? x + n0 : x;
+        const int y = wrap_index(oy + r, n1);
+        const int x = wrap_index(ox + c, n0);
         value[q] = __ldg(&fine[static_cast<int64_t>(vb + v) * g.fine_count + static_cast<int64_t>(y) * n0 + x]);
       }
     }
@@ -279,10 +289,8 @@ __global__ void __launch_bounds__(256) interpolate_bins_kernel(GridParams g, con
       float wx[W], wy[W];
       horner32_window<W>(win.offset[0], g.horner32, wx);
       horner32_window<W>(win.offset[1], g.horner32, wy);
-      int dx = (win.start[0] - ox) % n0;
-      dx = dx < 0 ? dx + n0 : dx;
-      int dy = (win.start[1] - oy) % n1;
-      dy = dy < 0 ? dy + n1 : dy;
+      const int dx = wrap_index(win.start[0] - ox, n0);
+      const int dy = wrap_index(win.start[1] - oy, n1);
       if (dx + W <= S && dy + W <= S) {
 #pragma unroll
         for (int j = 0; j < W; ++j) {
@@ -354,10 +362,8 @@ __global__ void __launch_bounds__(kRegionThreads) interpolate_region_kernel(
     __syncthreads();  // the previous vector's reads are done
     for (int e = threadIdx.x; e < S * S; e += kRegionThreads) {
       const int r = e / S, c = e - r * S;
-      int y = (oy + r) % n1;
-      y = y < 0 ? y + n1 : y;
-      int x = (ox + c) % n0;
-      x = x < 0 ? x + n0 : x;
+      const int y = wrap_index(oy + r, n1);
+      const int x = wrap_index(ox + c, n0);
       region[e] = __ldg(&grid[static_cast<int64_t>(y) * n0 + x]);
     }
     __syncthreads();
@@ -371,10 +377,8 @@ __global__ void __launch_bounds__(kRegionThreads) interpolate_region_kernel(
         float wx[W], wy[W];
         horner32_window<W>(win.offset[0], g.horner32, wx);
         horner32_window<W>(win.offset[1], g.horner32, wy);
-        int dx = (win.start[0] - ox) % n0;
-        dx = dx < 0 ? dx + n0 : dx;
-        int dy = (win.start[1] - oy) % n1;
-        dy = dy < 0 ? dy + n1 : dy;
+        const int dx = wrap_index(win.start[0] - ox, n0);
+        const int dy = wrap_index(win.start[1] - oy, n1);
         if (dx + W <= S && dy + W <= S) {
 #pragma unroll
           for (int j = 0; j < W; ++j) {
@@ -433,7 +437,7 @@ __global__ void __launch_bounds__(kRegionThreads) interpolate_region64_kernel(
     __syncthreads();  // the previous vector's reads are done
     for (int e = threadIdx.x; e < S * S; e += kRegionThreads) {
       const int r = e / S, c = e - r * S;
-      const int y = (oy + r) % n1, x = (ox + c) % n0;
+      const int y = wrap_index(oy + r, n1), x = wrap_index(ox + c, n0);
       region[e] = __ldg(&grid[static_cast<int64_t>(y) * n0 + x]);
     }
     __syncthreads();
@@ -446,10 +450,8 @@ __global__ void __launch_bounds__(kRegionThreads) interpolate_region64_kernel(
         double wx[W], wy[W];
         F64Window::window<W>(px, g, 0, first_x, wx);
         F64Window::window<W>(py, g, 1, first_y, wy);
-        int dx = (first_x - ox) % n0;
-        dx = dx < 0 ? dx + n0 : dx;
-        int dy = (first_y - oy) % n1;
-        dy = dy < 0 ? dy + n1 : dy;
+        const int dx = wrap_index(first_x - ox, n0);
+        const int dy = wrap_index(first_y - oy, n1);
         if (dx + W <= S && dy + W <= S) {
 #pragma unroll
           for (int j = 0; j < W; ++j) {
