@@ -902,7 +902,13 @@ __device__ __forceinline__ void spread_part(
   constexpr bool kWarpCapable = warp_capable<D, W, T>();
   const bool warp_path = kWarpCapable && sp.span > 0;
   const int span = warp_path ? sp.span : padded;
-  for (int c = tid; c < T::kWordsPerCell * span; c += kSpreadThreads) acc[c] = Word(0);
+  {
+    // Cleared 16 bytes at a time (the tile's words are a multiple of 16 bytes).
+    static_assert(T::kWordsPerCell * sizeof(Word) % 16 == 0, "tile words clear in 16-byte units");
+    uint4* acc16 = reinterpret_cast<uint4*>(acc);
+    const int units = static_cast<int>(T::kWordsPerCell * sizeof(Word) / 16) * span;
+    for (int c = tid; c < units; c += kSpreadThreads) acc16[c] = make_uint4(0u, 0u, 0u, 0u);
+  }
   __syncthreads();
   const int64_t tile = s_tile;
   const uint32_t part_in_tile = part - part_start[tile];
@@ -1160,15 +1166,30 @@ __device__ __forceinline__ void spread_part(
   __syncthreads();
   typename T::Complex* out = scratch + (static_cast<int64_t>(part) * batch + b) * padded;
   if (warp_path) {
-    const int pad0 = sp.pad[0], pad01 = sp.pad[0] * sp.pad[1];
+    // The thread's cells c = tid + k kSpreadThreads: (x, y, z) stepped by
+    // the stride's own coordinates with one carry per axis, not divided.
+    const int pad0 = sp.pad[0], pad1 = sp.pad[1], pad01 = sp.pad[0] * sp.pad[1];
+    int z = tid / pad01, y = (tid - z * pad01) / pad0;
+    int x = tid - z * pad01 - y * pad0;
+    const int step_z = kSpreadThreads / pad01, step_y = (kSpreadThreads - step_z * pad01) / pad0;
+    const int step_x = kSpreadThreads - step_z * pad01 - step_y * pad0;
     for (int c = tid; c < padded; c += kSpreadThreads) {
-      const int z = c / pad01, rest = c - z * pad01;
-      const int y = rest / pad0, x = rest - y * pad0;
       const int at = x + y * sp.pitch0 + z * sp.pitch01;
       typename T::Complex v;
       v.x = T::value(acc, span, 0, at, S);
       v.y = T::value(acc, span, 1, at, S);
       out[c] = v;
+      x += step_x;
+      y += step_y;
+      z += step_z;
+      if (x >= pad0) {
+        x -= pad0;
+        ++y;
+      }
+      if (y >= pad1) {
+        y -= pad1;
+        ++z;
+      }
     }
     return;
   }
