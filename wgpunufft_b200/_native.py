@@ -155,6 +155,7 @@ SIGNATURES: dict[str, tuple] = {
     "b200nufft_batch_execute": (c_int, [PLAN, P(c_void_p), P(c_void_p), c_void_p]),
     "b200nufft_tuning_lookup": (c_int, [c_int32, c_int32, c_int32, c_int32, c_int64, c_int64, P(Tuning)]),
     "b200nufft_tuning_override": (c_int, [P(Tuning)]),
+    "b200nufft_set_fused_transforms": (c_int, [c_int]),
     "b200nufft_tf32_peak": (c_int, [c_int, c_int, c_int, c_int, c_int, c_int, c_int, P(c_float), P(c_uint64)]),
     # wgpu_nufft.h
     "wgpu_nufft_default_opts": (None, [P(WgpuOpts)]),

@@ -15,31 +15,6 @@ namespace b200nufft {
 
 namespace {
 
-// Fine-grid index of mode storage index k along an axis of N modes and n
-// cells (src/gpu_type1_nd.rs:642-652).
-__device__ __forceinline__ int64_t fine_index(int64_t k, int64_t N, int64_t n, bool centered) {
-  if (centered) {
-    const int64_t half = N / 2;
-    return k < half ? n - (half - k) : k - half;
-  }
-  const int64_t nonnegative = (N + 1) / 2;
-  return k < nonnegative ? k : n - (N - k);
-}
-
-// Mode storage index of fine-grid cell c, or -1 when no mode maps to it.
-__device__ __forceinline__ int64_t mode_index(int64_t c, int64_t N, int64_t n, bool centered) {
-  if (centered) {
-    const int64_t half = N / 2;
-    if (c < N - half) return c + half;
-    if (c >= n - half) return c - n + half;
-    return -1;
-  }
-  const int64_t nonnegative = (N + 1) / 2;
-  if (c < nonnegative) return c;
-  if (c >= n - (N - nonnegative)) return c - n + N;
-  return -1;
-}
-
 // Index: uint32_t when every mode and cell index fits (32-bit divisions are
 // far cheaper than 64-bit ones), else int64_t.
 template <typename Real, typename Complex, typename Index>

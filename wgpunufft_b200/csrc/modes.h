@@ -7,6 +7,31 @@
 
 namespace b200nufft {
 
+// Fine-grid index of mode storage index k along an axis of N modes and n
+// cells (src/gpu_type1_nd.rs:642-652).
+__host__ __device__ inline int64_t fine_index(int64_t k, int64_t N, int64_t n, bool centered) {
+  if (centered) {
+    const int64_t half = N / 2;
+    return k < half ? n - (half - k) : k - half;
+  }
+  const int64_t nonnegative = (N + 1) / 2;
+  return k < nonnegative ? k : n - (N - k);
+}
+
+// Mode storage index of fine-grid cell c, or -1 when no mode maps to it.
+__host__ __device__ inline int64_t mode_index(int64_t c, int64_t N, int64_t n, bool centered) {
+  if (centered) {
+    const int64_t half = N / 2;
+    if (c < N - half) return c + half;
+    if (c >= n - half) return c - n + half;
+    return -1;
+  }
+  const int64_t nonnegative = (N + 1) / 2;
+  if (c < nonnegative) return c;
+  if (c >= n - (N - nonnegative)) return c - n + N;
+  return -1;
+}
+
 struct ModeParams {
   int32_t dimensions;
   int32_t centered;  // centered mode order, else FFT order

@@ -7,6 +7,7 @@
 #include <cstring>
 #include <limits>
 
+#include "fft2d.h"
 #include "tuning.h"
 #include "util.h"
 
@@ -284,6 +285,30 @@ NufftPlan::NufftPlan(const b200nufft_config& c, bool with_device) : has_device_(
     modes_params_.fine[a] = fine_[a];
   }
   fine_grid_.reserve(static_cast<size_t>(batch_) * fine_count_ * 2 * scalar_bytes(), "fine grid");
+  // 2D f32 plans with power-of-two fine axes: the fused transforms and their
+  // twiddle tables, of the plan's exponent sign (isign >= 0: +1).
+  fft2d_active_ = precision_ == B200NUFFT_PRECISION_F32 && fft2d_enabled() &&
+                  fft2d_supported(dim_, fine_.data(), modes_);
+  if (fft2d_active_) {
+    std::memset(&fft2d_, 0, sizeof(fft2d_));
+    fft2d_.sign = isign_ >= 0 ? 1 : -1;
+    fft2d_.centered = modes_params_.centered;
+    size_t offsets[2];
+    std::vector<float2> tables;
+    for (int a = 0; a < 2; ++a) {
+      int k = 0;
+      while ((int64_t{1} << k) < fine_[a]) ++k;
+      fft2d_.log2n[a] = k;
+      fft2d_.modes[a] = static_cast<int32_t>(modes_[a]);
+      const std::vector<float2> t = fft2d_twiddles(fine_[a], fft2d_.sign);
+      offsets[a] = tables.size();
+      tables.insert(tables.end(), t.begin(), t.end());
+    }
+    float2* dev = static_cast<float2*>(fft2d_twiddles_.reserve(tables.size() * sizeof(float2), "twiddles"));
+    check_cuda(cudaMemcpy(dev, tables.data(), tables.size() * sizeof(float2), cudaMemcpyHostToDevice),
+               "upload twiddles");
+    for (int a = 0; a < 2; ++a) fft2d_.twiddle[a] = dev + offsets[a];
+  }
   counters_.reserve(8 * sizeof(uint32_t), "sort tickets");
   check_cuda(cudaMemset(counters_.get(), 0, 8 * sizeof(uint32_t)), "clear sort tickets");
   hist_.reserve(4 * 256 * sizeof(uint32_t), "digit histograms");
@@ -856,18 +881,33 @@ void NufftPlan::execute_f32(int batch, const void* input, void* output, uint64_t
     l.candidates = static_cast<const int2*>(candidates_.get());
     l.fine = fine;
     l.valid_mask = static_cast<const uint32_t*>(valid_mask_.get());
+    if (fused_fold(batch)) {
+      // The fold runs inside the row transforms.
+      l.fine = nullptr;
+      spread_execute(spread_, l, stream, &timer_);
+      float2* rows = static_cast<float2*>(fft2d_rows_.reserve(fft2d_rows_bytes(fft2d_, batch), "transformed rows"));
+      fft2d_type1(spread_, fft2d_, batch, l.scratch, l.part_start, l.part_upper_bound, l.candidates,
+                  static_cast<const float*>(amplitudes_.get()), rows, static_cast<float2*>(output), stream, &timer_);
+      return;
+    }
     spread_execute(spread_, l, stream, &timer_);
     run_fft(fine, batch, direction, stream);
     StageScope scope(&timer_, kStageDeconvolution, stream);
     deconvolve_f32(modes_params_, batch, fine, static_cast<const float*>(amplitudes_.get()),
                    static_cast<float2*>(output), stream);
   } else {
-    {
-      StageScope scope(&timer_, kStagePredeconvolution, stream);
-      predeconvolve_f32(modes_params_, batch, static_cast<const float2*>(input),
-                        static_cast<const float*>(amplitudes_.get()), fine, stream);
+    if (fft2d_active_) {
+      float2* rows = static_cast<float2*>(fft2d_rows_.reserve(fft2d_rows_bytes(fft2d_, batch), "transformed rows"));
+      fft2d_type2(fft2d_, batch, static_cast<const float2*>(input), static_cast<const float*>(amplitudes_.get()),
+                  rows, fine, stream, &timer_);
+    } else {
+      {
+        StageScope scope(&timer_, kStagePredeconvolution, stream);
+        predeconvolve_f32(modes_params_, batch, static_cast<const float2*>(input),
+                          static_cast<const float*>(amplitudes_.get()), fine, stream);
+      }
+      run_fft(fine, batch, direction, stream);
     }
-    run_fft(fine, batch, direction, stream);
     if (tc2_active_ && batch >= tensor_min_batch()) {
       const int64_t groups = (batch + kTi2Vectors - 1) / kTi2Vectors;
       Ti2Launch t;
@@ -1256,6 +1296,13 @@ void NufftPlan::finish_batch(void* output, cudaStream_t stream) {
   l.scratch = static_cast<float2*>(scratch_.get());
   l.candidates = static_cast<const int2*>(candidates_.get());
   l.fine = fine;
+  if (fused_fold(1)) {
+    float2* rows = static_cast<float2*>(fft2d_rows_.reserve(fft2d_rows_bytes(fft2d_, 1), "transformed rows"));
+    fft2d_type1(spread_, fft2d_, 1, l.scratch, l.part_start, l.part_upper_bound, l.candidates,
+                static_cast<const float*>(amplitudes_.get()), rows, static_cast<float2*>(output), stream, &timer_);
+    check_cuda(cudaGetLastError(), "batch finish launch");
+    return;
+  }
   {
     StageScope scope(&timer_, kStageFold, stream);
     spread_fold(spread_, l, stream);

@@ -10,6 +10,7 @@
 
 #include "device.h"
 #include "es_kernel.h"
+#include "fft2d.h"
 #include "interp.h"
 #include "layout.h"
 #include "modes.h"
@@ -119,6 +120,16 @@ class NufftPlan {
   DeviceBuffer points64_, input64_, output64_;
   DeviceBuffer fine_grid_;
   std::map<int, cufftHandle> ffts_;
+  // 2D f32 plans with power-of-two fine axes: the fused transforms (fft2d.cu),
+  // their twiddle tables and the row-transformed intermediate.
+  bool fft2d_active_ = false;
+  Fft2dParams fft2d_{};
+  DeviceBuffer fft2d_twiddles_, fft2d_rows_;
+  // Type 1: the fold runs inside the fused row transforms, for fewer than
+  // eight vectors (batches fold eight vectors per thread, sharing the tile
+  // lookups, and keep cuFFT) on grids above kWarpFoldCells cells (smaller
+  // ones keep the warp fold of crowded tiles).
+  bool fused_fold(int batch) const { return fft2d_active_ && fine_count_ > kWarpFoldCells && batch < 8; }
   // Plans of 4 to 8 dimensions.
   NdParams nd_{};
   DeviceBuffer nd_acc_;                       // 64-bit integer fine grids of type 1

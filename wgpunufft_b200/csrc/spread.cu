@@ -1301,7 +1301,6 @@ __global__ void fold_tiles_kernel(SpreadParams sp, int batch, const Complex* __r
 // 32nd part of each covering tile, in order, and a fixed butterfly adds the
 // 32 lane sums (every lane ends with the same bits). The order depends on the
 // grid alone, so single vectors and batches agree bit for bit.
-constexpr int64_t kWarpFoldCells = int64_t{1} << 16;
 constexpr int kWarpFoldThreads = 256;
 
 template <int D, typename Complex>
@@ -1485,6 +1484,8 @@ void spread_execute_impl(const SpreadParams& sp, const SpreadLaunchT<T>& l, cuda
       default: launch_spread_dim<3, T>(sp, l, stream); break;
     }
   }
+  // A null fine grid leaves the padded tiles for a fused fold (fft2d.cu).
+  if (l.fine == nullptr) return;
   StageScope scope(timer, kStageFold, stream);
   fold_any(sp, l.batch, l.scratch, l.part_start, l.part_upper_bound, l.candidates, l.fine, stream);
 }

@@ -91,7 +91,7 @@ struct SpreadLaunch {
   uint32_t* max_bits;    // batch words
   float2* scratch;       // part_upper_bound * batch * padded_cells
   const int2* candidates;
-  float2* fine;          // batch * fine_count
+  float2* fine;          // batch * fine_count; null: no fold (the padded tiles stay in scratch)
   // Points within the fold's reach in the caller's order (bit i % 32 of word
   // i / 32); null: every strength sets the fixed-point scale.
   const uint32_t* valid_mask;
@@ -141,6 +141,10 @@ struct BatchStrengths {
 // order (`work`: count + 2 words). All problems share the window width.
 void batch_spread(const BatchProblem* problems, const BatchStrengths& strengths, int count, int width,
                   bool has_2d, bool has_3d, size_t shared_bytes, uint32_t* work, cudaStream_t stream);
+
+// Fine grids of at most this many cells fold one cell per warp (crowded
+// small grids hold hundreds of parts per tile).
+constexpr int64_t kWarpFoldCells = int64_t{1} << 16;
 
 // The fold of one problem's padded tiles onto its fine grid (after batch_spread).
 void spread_fold(const SpreadParams& sp, const SpreadLaunch& launch, cudaStream_t stream);

@@ -1,6 +1,7 @@
 // Tuning table lookup and the process-wide override used by the tuner.
 #include "tuning.h"
 
+#include <atomic>
 #include <cmath>
 #include <cstdlib>
 #include <mutex>
@@ -15,6 +16,7 @@ namespace {
 std::mutex g_override_mutex;
 bool g_override_set = false;
 b200nufft_tuning g_override{};
+std::atomic<bool> g_fused_transforms{true};
 
 int floor_log2(double v) { return v > 0.0 ? static_cast<int>(std::floor(std::log2(v))) : -16; }
 
@@ -75,7 +77,14 @@ b200nufft_tuning tuning_for(const TuningKey& key) {
   return t;
 }
 
+bool fft2d_enabled() { return b200nufft::g_fused_transforms.load(); }
+
 }  // namespace b200nufft
+
+extern "C" int b200nufft_set_fused_transforms(int enable) {
+  b200nufft::g_fused_transforms.store(enable != 0);
+  return B200NUFFT_SUCCESS;
+}
 
 extern "C" int b200nufft_tuning_override(const b200nufft_tuning* tuning) {
   std::lock_guard<std::mutex> lock(b200nufft::g_override_mutex);
