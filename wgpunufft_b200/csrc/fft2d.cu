@@ -106,9 +106,10 @@ struct FftShape {
   // stay within one transform.
   static constexpr int THREADS = TPR > 256 ? TPR : 256;
   static constexpr int PER_CTA = THREADS / TPR;
-  // Resident CTAs per SM the register budget is set for (at most 80
-  // registers for 256 threads, 64 for 512).
-  static constexpr int BLOCKS = THREADS > 256 ? 2 : 3;
+  // Resident CTAs per SM the register budget is set for (at most 64
+  // registers: four CTAs of 256 threads or two of 512; more warps in flight
+  // beat more loads in flight per thread for the fold of the rows).
+  static constexpr int BLOCKS = THREADS > 256 ? 2 : 4;
   // Columns: at least four per CTA (up to 1024 threads), so that the strided
   // accesses to the row-major intermediate and the modes move whole 32-byte
   // sectors; they are staged through shared memory, four neighbouring
