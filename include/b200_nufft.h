@@ -383,12 +383,13 @@ int b200nufft_tuning_lookup(int32_t type, int32_t dimensions, int32_t precision,
  * restores the table. Not for concurrent use with set_points. */
 int b200nufft_tuning_override(const b200nufft_tuning *tuning);
 
-/* Process-wide choice of the fine-grid transform of 2D f32 plans created
- * later: nonzero (the default) takes the fused shared-memory transforms where
- * both fine axes are powers of two from 64 to 4096 (the fold, the row
- * transforms, the column transforms and the deconvolution in two kernels,
- * type 2 likewise), zero takes cuFFT for every plan. No counterpart in the
- * reference, whose FFT is a separate pass (wgpu-fft); for A/B comparisons. */
+/* Process-wide choice of the fine-grid transform of 2D and 3D f32 plans
+ * created later: nonzero (the default) takes the fused shared-memory
+ * transforms where every fine axis is a power of two from 64 to 4096 (one
+ * pass per axis, pruned to the kept modes; type 1 folds in the first pass and
+ * deconvolves in the last, type 2 predeconvolves in the first), zero takes
+ * cuFFT for every plan. No counterpart in the reference, whose FFT is a
+ * separate pass (wgpu-fft); for A/B comparisons. */
 int b200nufft_set_fused_transforms(int enable);
 
 /* Number of this library's kernel launches since the process started, for

@@ -7,7 +7,7 @@
 #include <cstring>
 #include <limits>
 
-#include "fft2d.h"
+#include "fused_fft.h"
 #include "tuning.h"
 #include "util.h"
 
@@ -285,29 +285,30 @@ NufftPlan::NufftPlan(const b200nufft_config& c, bool with_device) : has_device_(
     modes_params_.fine[a] = fine_[a];
   }
   fine_grid_.reserve(static_cast<size_t>(batch_) * fine_count_ * 2 * scalar_bytes(), "fine grid");
-  // 2D f32 plans with power-of-two fine axes: the fused transforms and their
-  // twiddle tables, of the plan's exponent sign (isign >= 0: +1).
-  fft2d_active_ = precision_ == B200NUFFT_PRECISION_F32 && fft2d_enabled() &&
-                  fft2d_supported(dim_, fine_.data(), modes_);
-  if (fft2d_active_) {
-    std::memset(&fft2d_, 0, sizeof(fft2d_));
-    fft2d_.sign = isign_ >= 0 ? 1 : -1;
-    fft2d_.centered = modes_params_.centered;
-    size_t offsets[2];
+  // 2D and 3D f32 plans with power-of-two fine axes: the fused transforms and
+  // their twiddle tables, of the plan's exponent sign (isign >= 0: +1).
+  fused_fft_active_ = precision_ == B200NUFFT_PRECISION_F32 && fused_fft_enabled() &&
+                      fused_fft_supported(dim_, fine_.data(), modes_);
+  if (fused_fft_active_) {
+    std::memset(&fused_fft_, 0, sizeof(fused_fft_));
+    fused_fft_.dims = dim_;
+    fused_fft_.sign = isign_ >= 0 ? 1 : -1;
+    fused_fft_.centered = modes_params_.centered;
+    size_t offsets[3] = {0, 0, 0};
     std::vector<float2> tables;
-    for (int a = 0; a < 2; ++a) {
+    for (int a = 0; a < dim_; ++a) {
       int k = 0;
       while ((int64_t{1} << k) < fine_[a]) ++k;
-      fft2d_.log2n[a] = k;
-      fft2d_.modes[a] = static_cast<int32_t>(modes_[a]);
-      const std::vector<float2> t = fft2d_twiddles(fine_[a], fft2d_.sign);
+      fused_fft_.log2n[a] = k;
+      fused_fft_.modes[a] = static_cast<int32_t>(modes_[a]);
+      const std::vector<float2> t = fused_fft_twiddles(fine_[a], fused_fft_.sign);
       offsets[a] = tables.size();
       tables.insert(tables.end(), t.begin(), t.end());
     }
-    float2* dev = static_cast<float2*>(fft2d_twiddles_.reserve(tables.size() * sizeof(float2), "twiddles"));
+    float2* dev = static_cast<float2*>(fused_fft_twiddles_.reserve(tables.size() * sizeof(float2), "twiddles"));
     check_cuda(cudaMemcpy(dev, tables.data(), tables.size() * sizeof(float2), cudaMemcpyHostToDevice),
                "upload twiddles");
-    for (int a = 0; a < 2; ++a) fft2d_.twiddle[a] = dev + offsets[a];
+    for (int a = 0; a < dim_; ++a) fused_fft_.twiddle[a] = dev + offsets[a];
   }
   counters_.reserve(8 * sizeof(uint32_t), "sort tickets");
   check_cuda(cudaMemset(counters_.get(), 0, 8 * sizeof(uint32_t)), "clear sort tickets");
@@ -885,9 +886,11 @@ void NufftPlan::execute_f32(int batch, const void* input, void* output, uint64_t
       // The fold runs inside the row transforms.
       l.fine = nullptr;
       spread_execute(spread_, l, stream, &timer_);
-      float2* rows = static_cast<float2*>(fft2d_rows_.reserve(fft2d_rows_bytes(fft2d_, batch), "transformed rows"));
-      fft2d_type1(spread_, fft2d_, batch, l.scratch, l.part_start, l.part_upper_bound, l.candidates,
-                  static_cast<const float*>(amplitudes_.get()), rows, static_cast<float2*>(output), stream, &timer_);
+      float2* rows = static_cast<float2*>(
+          fused_fft_rows_.reserve(fused_fft_buffer_bytes(fused_fft_, batch), "transformed rows"));
+      fused_fft_type1(spread_, fused_fft_, batch, l.scratch, l.part_start, l.part_upper_bound, l.candidates,
+                      static_cast<const float*>(amplitudes_.get()), rows, fine, static_cast<float2*>(output), stream,
+                      &timer_);
       return;
     }
     spread_execute(spread_, l, stream, &timer_);
@@ -896,10 +899,11 @@ void NufftPlan::execute_f32(int batch, const void* input, void* output, uint64_t
     deconvolve_f32(modes_params_, batch, fine, static_cast<const float*>(amplitudes_.get()),
                    static_cast<float2*>(output), stream);
   } else {
-    if (fft2d_active_) {
-      float2* rows = static_cast<float2*>(fft2d_rows_.reserve(fft2d_rows_bytes(fft2d_, batch), "transformed rows"));
-      fft2d_type2(fft2d_, batch, static_cast<const float2*>(input), static_cast<const float*>(amplitudes_.get()),
-                  rows, fine, stream, &timer_);
+    if (fused_fft_active_) {
+      float2* rows = static_cast<float2*>(
+          fused_fft_rows_.reserve(fused_fft_buffer_bytes(fused_fft_, batch), "transformed rows"));
+      fused_fft_type2(fused_fft_, batch, static_cast<const float2*>(input), static_cast<const float*>(amplitudes_.get()),
+                      rows, fine, fine, stream, &timer_);
     } else {
       {
         StageScope scope(&timer_, kStagePredeconvolution, stream);
@@ -1297,9 +1301,11 @@ void NufftPlan::finish_batch(void* output, cudaStream_t stream) {
   l.candidates = static_cast<const int2*>(candidates_.get());
   l.fine = fine;
   if (fused_fold(1)) {
-    float2* rows = static_cast<float2*>(fft2d_rows_.reserve(fft2d_rows_bytes(fft2d_, 1), "transformed rows"));
-    fft2d_type1(spread_, fft2d_, 1, l.scratch, l.part_start, l.part_upper_bound, l.candidates,
-                static_cast<const float*>(amplitudes_.get()), rows, static_cast<float2*>(output), stream, &timer_);
+    float2* rows = static_cast<float2*>(
+        fused_fft_rows_.reserve(fused_fft_buffer_bytes(fused_fft_, 1), "transformed rows"));
+    fused_fft_type1(spread_, fused_fft_, 1, l.scratch, l.part_start, l.part_upper_bound, l.candidates,
+                    static_cast<const float*>(amplitudes_.get()), rows, fine, static_cast<float2*>(output), stream,
+                    &timer_);
     check_cuda(cudaGetLastError(), "batch finish launch");
     return;
   }

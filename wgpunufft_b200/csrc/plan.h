@@ -10,7 +10,7 @@
 
 #include "device.h"
 #include "es_kernel.h"
-#include "fft2d.h"
+#include "fused_fft.h"
 #include "interp.h"
 #include "layout.h"
 #include "modes.h"
@@ -120,16 +120,17 @@ class NufftPlan {
   DeviceBuffer points64_, input64_, output64_;
   DeviceBuffer fine_grid_;
   std::map<int, cufftHandle> ffts_;
-  // 2D f32 plans with power-of-two fine axes: the fused transforms (fft2d.cu),
-  // their twiddle tables and the row-transformed intermediate.
-  bool fft2d_active_ = false;
-  Fft2dParams fft2d_{};
-  DeviceBuffer fft2d_twiddles_, fft2d_rows_;
-  // Type 1: the fold runs inside the fused row transforms, for fewer than
+  // 2D and 3D f32 plans with power-of-two fine axes: the fused transforms
+  // (fused_fft.cu), their twiddle tables and the buffer of the pass along
+  // axis 0 (the fine grid serves as the second buffer of 3D plans).
+  bool fused_fft_active_ = false;
+  FusedFftParams fused_fft_{};
+  DeviceBuffer fused_fft_twiddles_, fused_fft_rows_;
+  // Type 1: the fold runs inside the fused pass along axis 0, for fewer than
   // eight vectors (batches fold eight vectors per thread, sharing the tile
   // lookups, and keep cuFFT) on grids above kWarpFoldCells cells (smaller
   // ones keep the warp fold of crowded tiles).
-  bool fused_fold(int batch) const { return fft2d_active_ && fine_count_ > kWarpFoldCells && batch < 8; }
+  bool fused_fold(int batch) const { return fused_fft_active_ && fine_count_ > kWarpFoldCells && batch < 8; }
   // Plans of 4 to 8 dimensions.
   NdParams nd_{};
   DeviceBuffer nd_acc_;                       // 64-bit integer fine grids of type 1

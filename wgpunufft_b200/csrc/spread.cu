@@ -1484,7 +1484,7 @@ void spread_execute_impl(const SpreadParams& sp, const SpreadLaunchT<T>& l, cuda
       default: launch_spread_dim<3, T>(sp, l, stream); break;
     }
   }
-  // A null fine grid leaves the padded tiles for a fused fold (fft2d.cu).
+  // A null fine grid leaves the padded tiles for a fused fold (fused_fft.cu).
   if (l.fine == nullptr) return;
   StageScope scope(timer, kStageFold, stream);
   fold_any(sp, l.batch, l.scratch, l.part_start, l.part_upper_bound, l.candidates, l.fine, stream);

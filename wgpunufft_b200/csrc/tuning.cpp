@@ -77,7 +77,7 @@ b200nufft_tuning tuning_for(const TuningKey& key) {
   return t;
 }
 
-bool fft2d_enabled() { return b200nufft::g_fused_transforms.load(); }
+bool fused_fft_enabled() { return b200nufft::g_fused_transforms.load(); }
 
 }  // namespace b200nufft
 

@@ -35,8 +35,8 @@ b200nufft_tuning tuning_for(const TuningKey& key);
 // Defaults of every field (tile 0: the plan's own default tile).
 b200nufft_tuning default_tuning(int dimensions);
 
-// Whether plans created now take the fused 2D transforms where they apply
+// Whether plans created now take the fused transforms where they apply
 // (b200nufft_set_fused_transforms; default true).
-bool fft2d_enabled();
+bool fused_fft_enabled();
 
 }  // namespace b200nufft
