@@ -341,6 +341,37 @@ __global__ void __launch_bounds__(FftShape<L>::THREADS, FftShape<L>::BLOCKS) row
   }
 }
 
+// Type 1, pass along axis 0 from a folded fine grid: rows r of vector b
+// transformed, the kept modes written to out[b][r][0, m0).
+template <int L, int S>
+__global__ void __launch_bounds__(FftShape<L>::THREADS, FftShape<L>::BLOCKS) row_prune_fft_kernel(
+    FusedFftParams fp, int batch, int rows_total, const float2* __restrict__ fine, float2* __restrict__ out_all) {
+  using Sh = FftShape<L>;
+  extern __shared__ __align__(16) float2 fft_shared_mem[];
+  const int ri = threadIdx.x / Sh::TPR, t = threadIdx.x % Sh::TPR;
+  float2* buf0 = fft_shared_mem + ri * Sh::STRIDE;
+  float2* buf1 = buf0 + Sh::PADDED;
+  const int r = blockIdx.x * Sh::PER_CTA + ri;
+  const bool live = r < rows_total;
+  const int m0 = fp.modes[0];
+  for (int b = blockIdx.y; b < batch; b += gridDim.y) {
+    const float2* in = fine + (static_cast<int64_t>(b) * rows_total + r) * Sh::N;
+    float2 v[8];
+#pragma unroll
+    for (int q = 0; q < 8; ++q) v[q] = live ? in[t + q * Sh::TPR] : make_float2(0.0f, 0.0f);
+    fft_regs<L, S>(v, buf0, buf1, t, fp.twiddle[0]);
+    if (live) {
+      float2* out = out_all + (static_cast<int64_t>(b) * rows_total + r) * m0;
+#pragma unroll
+      for (int q = 0; q < 8; ++q) {
+        const int k = mode_index32(t + q * Sh::TPR, m0, Sh::N, fp.centered);
+        if (k >= 0) out[k] = v[q];
+      }
+    }
+    __syncthreads();
+  }
+}
+
 // Type 2, pass along axis 0: rows r (PER_CTA per CTA) of vector b: their
 // kept modes in[b][r][0, m0) at their fine cells (zero elsewhere),
 // transformed, written to every cell of the fine row.
@@ -482,6 +513,17 @@ void launch_row_fold(const SpreadParams& sp, const FusedFftParams& fp, int batch
 }
 
 template <int L, int S>
+void launch_row_prune(const FusedFftParams& fp, int batch, const float2* fine, float2* out, cudaStream_t stream) {
+  using Sh = FftShape<L>;
+  const int rows_total = 1 << (fp.log2n[1] + (fp.dims > 2 ? fp.log2n[2] : 0));
+  const dim3 grid(static_cast<unsigned>((rows_total + Sh::PER_CTA - 1) / Sh::PER_CTA), batches(batch));
+  auto kernel = row_prune_fft_kernel<L, S>;
+  allow_shared(kernel, row_smem<L>());
+  kernel<<<grid, Sh::THREADS, row_smem<L>(), stream>>>(fp, batch, rows_total, fine, out);
+  note_launch();
+}
+
+template <int L, int S>
 void launch_row_expand(const FusedFftParams& fp, int batch, const float2* in, float2* fine, cudaStream_t stream) {
   using Sh = FftShape<L>;
   const int rows_total = 1 << (fp.log2n[1] + (fp.dims > 2 ? fp.log2n[2] : 0));
@@ -612,7 +654,7 @@ void fused_fft_type1(const SpreadParams& sp, const FusedFftParams& fp, int batch
   const int64_t n1 = int64_t{1} << fp.log2n[1];
   const int64_t n2 = fp.dims > 2 ? int64_t{1} << fp.log2n[2] : 1;
   const int64_t m0 = fp.modes[0], m1 = fp.modes[1], m2 = fp.dims > 2 ? fp.modes[2] : 1;
-  {
+  if (scratch != nullptr) {
     StageScope scope(timer, kStageFold, stream);
 #define B200NUFFT_ROWS(LL, SS) \
   launch_row_fold<LL, SS>(sp, fp, batch, scratch, part_start, part_limit, candidates, rows, stream)
@@ -620,6 +662,11 @@ void fused_fft_type1(const SpreadParams& sp, const FusedFftParams& fp, int batch
 #undef B200NUFFT_ROWS
   }
   StageScope scope(timer, kStageFft, stream);
+  if (scratch == nullptr) {
+#define B200NUFFT_ROWS1(LL, SS) launch_row_prune<LL, SS>(fp, batch, spare, rows, stream)
+    B200NUFFT_FFT_SWITCH(fp.log2n[0], fp.sign, B200NUFFT_ROWS1)
+#undef B200NUFFT_ROWS1
+  }
   const int64_t mode_count = m0 * m1 * m2;
   if (fp.dims == 2) {
     // [y][kx] -> modes [ky][kx], scaled.

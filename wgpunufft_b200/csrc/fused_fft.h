@@ -44,7 +44,9 @@ size_t fused_fft_buffer_bytes(const FusedFftParams& fp, int batch);
 // Type 1: the fold of the padded tiles into every fine row and its
 // transform along axis 0, kept modes only, into `rows` (stage fold), then
 // the passes along the other axes (through `spare` in 3D), the last scaled
-// by the deconvolution amplitudes into `output` (stage fft).
+// by the deconvolution amplitudes into `output` (stage fft). With scratch
+// null the rows come from the fine grid already folded into `spare` (the
+// pass along axis 0 is then timed in stage fft).
 void fused_fft_type1(const SpreadParams& sp, const FusedFftParams& fp, int batch, const float2* scratch,
                      const uint32_t* part_start, int64_t part_limit, const int2* candidates, const float* amplitudes,
                      float2* rows, float2* spare, float2* output, cudaStream_t stream, StageTimer* timer);

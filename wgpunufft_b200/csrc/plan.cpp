@@ -883,14 +883,16 @@ void NufftPlan::execute_f32(int batch, const void* input, void* output, uint64_t
     l.fine = fine;
     l.valid_mask = static_cast<const uint32_t*>(valid_mask_.get());
     if (fused_fold(batch)) {
-      // The fold runs inside the row transforms.
-      l.fine = nullptr;
+      // 2D: the fold runs inside the pass along axis 0. 3D: the fold kernel
+      // (a thread per cell: the crowded tiles' long part lists overlap
+      // better) folds into the fine grid, which that pass reads.
+      if (dim_ == 2) l.fine = nullptr;
       spread_execute(spread_, l, stream, &timer_);
       float2* rows = static_cast<float2*>(
           fused_fft_rows_.reserve(fused_fft_buffer_bytes(fused_fft_, batch), "transformed rows"));
-      fused_fft_type1(spread_, fused_fft_, batch, l.scratch, l.part_start, l.part_upper_bound, l.candidates,
-                      static_cast<const float*>(amplitudes_.get()), rows, fine, static_cast<float2*>(output), stream,
-                      &timer_);
+      fused_fft_type1(spread_, fused_fft_, batch, dim_ == 2 ? l.scratch : nullptr, l.part_start,
+                      l.part_upper_bound, l.candidates, static_cast<const float*>(amplitudes_.get()), rows, fine,
+                      static_cast<float2*>(output), stream, &timer_);
       return;
     }
     spread_execute(spread_, l, stream, &timer_);
@@ -1303,9 +1305,13 @@ void NufftPlan::finish_batch(void* output, cudaStream_t stream) {
   if (fused_fold(1)) {
     float2* rows = static_cast<float2*>(
         fused_fft_rows_.reserve(fused_fft_buffer_bytes(fused_fft_, 1), "transformed rows"));
-    fused_fft_type1(spread_, fused_fft_, 1, l.scratch, l.part_start, l.part_upper_bound, l.candidates,
-                    static_cast<const float*>(amplitudes_.get()), rows, fine, static_cast<float2*>(output), stream,
-                    &timer_);
+    if (dim_ == 3) {
+      StageScope scope(&timer_, kStageFold, stream);
+      spread_fold(spread_, l, stream);
+    }
+    fused_fft_type1(spread_, fused_fft_, 1, dim_ == 2 ? l.scratch : nullptr, l.part_start, l.part_upper_bound,
+                    l.candidates, static_cast<const float*>(amplitudes_.get()), rows, fine,
+                    static_cast<float2*>(output), stream, &timer_);
     check_cuda(cudaGetLastError(), "batch finish launch");
     return;
   }
