@@ -122,11 +122,14 @@ struct FftShape {
   // Columns: up to sixteen neighbouring columns per CTA (up to 1024
   // threads), so that the strided accesses along the column axis move whole
   // 32-byte sectors or more; they are staged through shared memory with
-  // neighbouring columns in neighbouring lanes. Column c's pair starts COL_STRIDE c entries
-  // in (an odd multiple of 8: neighbouring columns fall 16 banks apart).
+  // neighbouring columns in neighbouring lanes, a warp covering COLS columns
+  // x 32 / COLS positions. Column c's pair starts c COL_STRIDE entries in,
+  // COL_STRIDE = 32 / COLS (mod 16): the warp's (column, position) pairs
+  // then fall on 32 consecutive entries modulo 16, two per bank pair (the
+  // two wavefronts of 32 eight-byte accesses).
   static constexpr int COLS = PER_CTA > (1024 / TPR < 16 ? 1024 / TPR : 16) ? PER_CTA : (1024 / TPR < 16 ? 1024 / TPR : 16);
   static constexpr int COL_THREADS = COLS * TPR;
-  static constexpr int COL_STRIDE = ((2 * PADDED + 7) / 16) * 16 + 8;
+  static constexpr int COL_STRIDE = ((2 * PADDED + 15) / 16) * 16 + ((COLS >= 32 ? 1 : 32 / COLS) % 16);
   static constexpr int COL_BLOCKS = COL_THREADS > 512 ? 1 : (COL_THREADS > 256 ? 2 : 3);
 };
 
