@@ -25,8 +25,8 @@
 // thread, with one exchange through a shared-memory ping-pong pair between
 // passes and its twiddles exp(sign 2 pi i m / n) from per-pass tables
 // computed in double on the host. Shared indexes are padded by one entry
-// every 32 (padded()), which keeps the strided writes of the first passes
-// within two-way bank conflicts.
+// every 16 (padded()): every exchange of every length then puts at most two
+// lanes on a bank pair, the two wavefronts that 32 eight-byte accesses take.
 #include "fused_fft.h"
 
 #include <algorithm>
@@ -36,7 +36,7 @@ namespace b200nufft {
 
 namespace {
 
-__device__ __forceinline__ int padded(int i) { return i + (i >> 5); }
+__device__ __forceinline__ int padded(int i) { return i + (i >> 4); }
 
 __device__ __forceinline__ float2 cadd(float2 a, float2 b) { return make_float2(a.x + b.x, a.y + b.y); }
 __device__ __forceinline__ float2 csub(float2 a, float2 b) { return make_float2(a.x - b.x, a.y - b.y); }
@@ -106,7 +106,7 @@ template <int L>
 struct FftShape {
   static constexpr int N = 1 << L;
   static constexpr int TPR = N / 8;
-  static constexpr int PADDED = N + N / 32;
+  static constexpr int PADDED = N + N / 16;
   // Shared floats2 per transform: the ping-pong pair, skewed by one entry so
   // that neighbouring transforms start in different banks.
   static constexpr int STRIDE = 2 * PADDED + 1;
