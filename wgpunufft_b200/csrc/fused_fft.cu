@@ -169,12 +169,17 @@ __device__ __forceinline__ void fft_regs(float2 (&v)[8], float2* buf0, float2* b
     dft8<S>(v);
     if (p == P8 - 1 && REM == 0) break;
     float2* buf = (p & 1) ? buf1 : buf0;
-    const int base = ((t >> nsl) << (nsl + 3)) + (t & ((1 << nsl) - 1));
+    // base mod 16 plus r Ns mod 16 stays below 16 (Ns = 1: base = 8 t;
+    // Ns = 8: base mod 16 < 8; Ns >= 16: r Ns mod 16 = 0), and t + q TPR
+    // likewise, so padded() of each entry is padded(base) (or padded(t)) plus
+    // a constant.
+    float2* wb = buf + padded(((t >> nsl) << (nsl + 3)) + (t & ((1 << nsl) - 1)));
 #pragma unroll
-    for (int r = 0; r < 8; ++r) buf[padded(base + (r << nsl))] = v[r];
+    for (int r = 0; r < 8; ++r) wb[(r << nsl) + ((r << nsl) >> 4)] = v[r];
     __syncthreads();
+    const float2* rb = buf + padded(t);
 #pragma unroll
-    for (int q = 0; q < 8; ++q) v[q] = buf[padded(t + q * TPR)];
+    for (int q = 0; q < 8; ++q) v[q] = rb[q * TPR + ((q * TPR) >> 4)];
   }
   constexpr int last = twiddle_offset(P8);
   if constexpr (REM == 2) {
@@ -428,49 +433,65 @@ __global__ void __launch_bounds__(FftShape<L>::COL_THREADS, FftShape<L>::COL_BLO
   const int c0 = blockIdx.x * Sh::COLS;
   const int in_positions = kExpand ? m : Sh::N;
   const int out_positions = kExpand ? Sh::N : m;
+  // Staging: thread (column sc, first position sp0) moves positions
+  // sp0 + k TPR, k < 8, of its column (padded(sp0 + k TPR) = padded(sp0) +
+  // k TPR + (k TPR) / 16, as in fft_regs).
+  const int sc = threadIdx.x % Sh::COLS, sp0 = threadIdx.x / Sh::COLS;
+  float2* stage = fft_shared_mem + sc * Sh::COL_STRIDE + padded(sp0);
+  const bool column = c0 + sc < inner;
   // Entries of one vector's array stay below 2^31 (fused_fft_supported).
   for (int b = blockIdx.z; b < batch; b += gridDim.z) {
-    const float2* in = in_all + b * in_vector_stride + static_cast<int64_t>(blockIdx.y) * in_positions * inner + c0;
-    float2* out = out_all + b * out_vector_stride + static_cast<int64_t>(blockIdx.y) * out_positions * inner + c0;
-    const float* amp = amplitudes + c0;
-    for (int i = threadIdx.x; i < Sh::COLS * Sh::N; i += Sh::COL_THREADS) {
-      const int c = i % Sh::COLS, pos = i / Sh::COLS;
+    const float2* in = in_all + b * in_vector_stride + static_cast<int64_t>(blockIdx.y) * in_positions * inner + c0 + sc;
+    float2* out = out_all + b * out_vector_stride + static_cast<int64_t>(blockIdx.y) * out_positions * inner + c0 + sc;
+    const float* amp = amplitudes + c0 + sc;
+#pragma unroll
+    for (int k = 0; k < 8; ++k) {
+      const int pos = sp0 + k * Sh::TPR;
       float2 x = make_float2(0.0f, 0.0f);
-      if (c0 + c < inner) {
+      if (column) {
         if constexpr (kExpand) {
           const int j = mode_index32(pos, m, Sh::N, centered);
           if (j >= 0) {
-            x = in[j * inner + c];
+            x = in[j * inner];
             if constexpr (kScale) {
-              const float amplitude = amp[j * inner + c];
+              const float amplitude = amp[j * inner];
               x = make_float2(x.x * amplitude, x.y * amplitude);
             }
           }
         } else {
-          x = in[pos * inner + c];
+          x = in[pos * inner];
         }
       }
-      fft_shared_mem[c * Sh::COL_STRIDE + padded(pos)] = x;
+      stage[k * Sh::TPR + ((k * Sh::TPR) >> 4)] = x;
     }
     __syncthreads();
     float2 v[8];
+    const float2* rb = buf0 + padded(t);
 #pragma unroll
-    for (int q = 0; q < 8; ++q) v[q] = buf0[padded(t + q * Sh::TPR)];
+    for (int q = 0; q < 8; ++q) v[q] = rb[q * Sh::TPR + ((q * Sh::TPR) >> 4)];
     fft_regs<L, S>(v, buf1, buf0, t, twiddle);
     __syncthreads();
+    float2* wb = buf0 + padded(t);
 #pragma unroll
-    for (int q = 0; q < 8; ++q) buf0[padded(t + q * Sh::TPR)] = v[q];
+    for (int q = 0; q < 8; ++q) wb[q * Sh::TPR + ((q * Sh::TPR) >> 4)] = v[q];
     __syncthreads();
-    for (int i = threadIdx.x; i < Sh::COLS * out_positions; i += Sh::COL_THREADS) {
-      const int c = i % Sh::COLS, j = i / Sh::COLS;
-      if (c0 + c < inner) {
-        const int pos = kExpand ? j : fine_index32(j, m, Sh::N, centered);
-        float2 x = fft_shared_mem[c * Sh::COL_STRIDE + padded(pos)];
-        if constexpr (kScale && !kExpand) {
-          const float amplitude = amp[j * inner + c];
-          x = make_float2(x.x * amplitude, x.y * amplitude);
+    if (column) {
+      if constexpr (kExpand) {
+#pragma unroll
+        for (int k = 0; k < 8; ++k) {
+          const int pos = sp0 + k * Sh::TPR;
+          out[pos * inner] = stage[k * Sh::TPR + ((k * Sh::TPR) >> 4)];
         }
-        out[j * inner + c] = x;
+      } else {
+        const float2* col = fft_shared_mem + sc * Sh::COL_STRIDE;
+        for (int j = sp0; j < out_positions; j += Sh::TPR) {
+          float2 x = col[padded(fine_index32(j, m, Sh::N, centered))];
+          if constexpr (kScale) {
+            const float amplitude = amp[j * inner];
+            x = make_float2(x.x * amplitude, x.y * amplitude);
+          }
+          out[j * inner] = x;
+        }
       }
     }
     __syncthreads();
