@@ -160,31 +160,55 @@ __global__ void part_cap_kernel(SpreadParams sp, const uint32_t* __restrict__ of
 // Largest |re| or |im| of every strength vector, as magnitude bits, over
 // the points within reach when a mask is given (others get zero weight, so
 // their strengths must not change the fixed-point scale). A thread takes
-// four consecutive values (two 16-byte loads when the vector is 16-byte
-// aligned) and the mask bits of those four points.
+// four consecutive values per step (two 16-byte loads for f32 vectors that
+// start 16-byte aligned) and the mask bits of those four points; the block
+// reduces its warps' maxima and adds one atomicMax (thousands of per-warp
+// atomics on one word serialize at its L2 slice).
 template <typename T>
-__global__ void strength_magnitude_kernel(const typename T::Complex* __restrict__ values,
-                                          int64_t count, int batch,
-                                          typename T::Bits* __restrict__ max_bits,
-                                          const uint32_t* __restrict__ valid_mask) {
+__global__ void __launch_bounds__(256) strength_magnitude_kernel(const typename T::Complex* __restrict__ values,
+                                                                 int64_t count, int batch,
+                                                                 typename T::Bits* __restrict__ max_bits,
+                                                                 const uint32_t* __restrict__ valid_mask) {
+  using Bits = typename T::Bits;
+  __shared__ Bits warp_max[8];
   const int b = blockIdx.y;
   const typename T::Complex* v = values + static_cast<int64_t>(b) * count;
-  typename T::Bits m = 0;
+  Bits m = 0;
   const int64_t stride = static_cast<int64_t>(gridDim.x) * blockDim.x * 4;
+  const bool vector16 =
+      sizeof(typename T::Complex) == 8 && (reinterpret_cast<uintptr_t>(v) & 15) == 0;
   for (int64_t i = (static_cast<int64_t>(blockIdx.x) * blockDim.x + threadIdx.x) * 4; i < count; i += stride) {
     const uint32_t bits = valid_mask != nullptr ? (__ldg(&valid_mask[i >> 5]) >> (i & 31)) : 0xFu;
+    if (vector16 && i + 4 <= count) {
+      const float4 p = __ldg(reinterpret_cast<const float4*>(v + i));
+      const float4 q = __ldg(reinterpret_cast<const float4*>(v + i) + 1);
+      const float r[8] = {p.x, p.y, p.z, p.w, q.x, q.y, q.z, q.w};
 #pragma unroll
-    for (int k = 0; k < 4; ++k) {
-      if (i + k < count && ((bits >> k) & 1u)) {
-        const typename T::Complex s = v[i + k];
-        m = max(m, T::magnitude_bits(s.x));
-        m = max(m, T::magnitude_bits(s.y));
+      for (int k = 0; k < 4; ++k) {
+        if ((bits >> k) & 1u) {
+          m = max(m, static_cast<Bits>(__float_as_uint(r[2 * k]) & 0x7fffffffu));
+          m = max(m, static_cast<Bits>(__float_as_uint(r[2 * k + 1]) & 0x7fffffffu));
+        }
+      }
+    } else {
+#pragma unroll
+      for (int k = 0; k < 4; ++k) {
+        if (i + k < count && ((bits >> k) & 1u)) {
+          const typename T::Complex s = v[i + k];
+          m = max(m, T::magnitude_bits(s.x));
+          m = max(m, T::magnitude_bits(s.y));
+        }
       }
     }
   }
 #pragma unroll
   for (int offset = 16; offset > 0; offset >>= 1) m = max(m, __shfl_xor_sync(0xFFFFFFFFu, m, offset));
-  if ((threadIdx.x & 31) == 0 && m) atomicMax(&max_bits[b], m);
+  if ((threadIdx.x & 31) == 0) warp_max[threadIdx.x >> 5] = m;
+  __syncthreads();
+  if (threadIdx.x == 0) {
+    for (int w = 1; w < static_cast<int>(blockDim.x >> 5); ++w) m = max(m, warp_max[w]);
+    if (m) atomicMax(&max_bits[b], m);
+  }
 }
 
 // Records in the reach of every tile's bins, and the parts of every tile.
