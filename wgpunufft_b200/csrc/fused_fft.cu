@@ -349,6 +349,145 @@ __global__ void __launch_bounds__(FftShape<L>::THREADS, FftShape<L>::BLOCKS) row
   }
 }
 
+// Segment fold: the same sums for fine grids whose axis 0 holds whole
+// tiles (n0 a multiple of tile[0], w - 1 < tile[0], at least two tiles, at
+// least 32 threads per row). Every cell's candidates along axis 0 are its
+// own tile s and, for its first w - 1 cells, tile s - 1 (tile 0: the last
+// tile, wrapped) in ascending tile order, so per candidate of the other axes
+// a row is folded in three rounds over its tiles: (A) each tile's overhang,
+// cells [tile0, pad0) of its padded rows, into the next tile's first cells;
+// (B) each tile's own cells; (C) the last tile's overhang into tile 0 (it
+// follows tile 0 in ascending order). Within a round the tiles' cells are
+// disjoint; a warp takes one tile, its lanes neighbouring cells, and adds the
+// tile's parts in order. Every cell thus receives the per-cell kernel's
+// additions in its order, from coalesced row segments of the padded tiles.
+template <int L, int S, int D>
+__global__ void __launch_bounds__(FftShape<L>::THREADS, FftShape<L>::BLOCKS) row_segment_fold_fft_kernel(
+    SpreadParams sp, FusedFftParams fp, int batch, int rows_total, const float2* __restrict__ scratch,
+    const uint32_t* __restrict__ part_start, int64_t part_limit, const int2* __restrict__ candidates,
+    float2* __restrict__ out_all) {
+  using Sh = FftShape<L>;
+  static_assert(Sh::TPR >= 32, "a row takes whole warps");
+  extern __shared__ __align__(16) float2 fft_shared_mem[];
+  const int ri = threadIdx.x / Sh::TPR, t = threadIdx.x % Sh::TPR;
+  float2* buf0 = fft_shared_mem + ri * Sh::STRIDE;
+  float2* acc = buf0 + Sh::PADDED;
+  const int r = blockIdx.x * Sh::PER_CTA + ri;
+  const bool live = r < rows_total;
+  const int y = D > 2 ? (r & ((1 << fp.log2n[1]) - 1)) : r;
+  const int z = D > 2 ? (r >> fp.log2n[1]) : 0;
+  const int m0 = fp.modes[0];
+  const uint32_t limit = static_cast<uint32_t>(min(part_limit, static_cast<int64_t>(UINT32_MAX)));
+  const int2* c1 = candidates + sp.candidate_base[1] + static_cast<int64_t>(y) * sp.candidate_count[1];
+  const int2* c2 = D > 2 ? candidates + sp.candidate_base[2] + static_cast<int64_t>(z) * sp.candidate_count[2] : c1;
+  const int k2n = D > 2 ? sp.candidate_count[2] : 1;
+  const int k1n = sp.candidate_count[1];
+  const int warp = t >> 5, lane = t & 31;
+  constexpr int kWarps = Sh::TPR / 32;
+  const int tile0 = sp.tile[0], nt0 = sp.ntiles[0], over = sp.pad[0] - sp.tile[0];
+  const int64_t part_stride = static_cast<int64_t>(batch) * sp.padded_cells;
+  for (int b = blockIdx.y; b < batch; b += gridDim.y) {
+    for (int i = t; i < Sh::PADDED; i += Sh::TPR) acc[i] = make_float2(0.0f, 0.0f);
+    __syncthreads();
+    // Every row of the CTA takes the same rounds (its missing candidates
+    // idle), so that the barriers match.
+    for (int k2 = 0; k2 < k2n; ++k2) {
+      for (int k1 = 0; k1 < k1n; ++k1) {
+        int2 e1 = c1[k1], e2 = make_int2(0, 0);
+        if (D > 2) e2 = c2[k2];
+        const bool active = live && e1.x >= 0 && e2.x >= 0;
+        const int64_t tile_yz = static_cast<int64_t>(nt0) * (e1.x + static_cast<int64_t>(sp.ntiles[1]) * e2.x);
+        const int local_yz = sp.pad[0] * (e1.y + sp.pad[1] * e2.y);
+        for (int round = 0; round < 3; ++round) {
+          if (active) {
+            const int s_begin = round == 2 ? nt0 - 1 : 0;
+            const int s_end = round == 0 ? nt0 - 1 : nt0;
+            const int len = round == 1 ? tile0 : over;
+            const int lx0 = round == 1 ? 0 : tile0;
+            // Four of the warp's tiles at a time, two 32-cell chunks each:
+            // the first part of all eight chunks loaded before any is added.
+            for (int s0 = s_begin + warp; s0 < s_end; s0 += 4 * kWarps) {
+              uint32_t lo[4], hi[4];
+              float2 first[4][2];
+#pragma unroll
+              for (int k = 0; k < 4; ++k) {
+                const int s = s0 + k * kWarps;
+                lo[k] = hi[k] = 0;
+                if (s < s_end) {
+                  const int64_t tile = s + tile_yz;
+                  lo[k] = part_start[tile];
+                  hi[k] = min(part_start[tile + 1], limit);
+                }
+#pragma unroll
+                for (int j = 0; j < 2; ++j) {
+                  const int c = lane + 32 * j;
+                  first[k][j] = make_float2(0.0f, 0.0f);
+                  if (c < len && lo[k] < hi[k]) {
+                    first[k][j] = scratch[static_cast<int64_t>(lo[k]) * part_stride +
+                                          static_cast<int64_t>(b) * sp.padded_cells + local_yz + lx0 + c];
+                  }
+                }
+              }
+#pragma unroll
+              for (int k = 0; k < 4; ++k) {
+                const int s = s0 + k * kWarps;
+                if (s >= s_end || lo[k] >= hi[k]) continue;
+                const int cell0 = round == 1 ? s * tile0 : (s + 1 == nt0 ? 0 : (s + 1) * tile0);
+#pragma unroll
+                for (int j = 0; j < 2; ++j) {
+                  const int c = lane + 32 * j;
+                  if (c >= len) continue;
+                  float2* a = acc + padded(cell0 + c);
+                  float2 sum = *a;
+                  sum.x += first[k][j].x;
+                  sum.y += first[k][j].y;
+                  const float2* src = scratch + static_cast<int64_t>(lo[k] + 1) * part_stride +
+                                      static_cast<int64_t>(b) * sp.padded_cells + local_yz + lx0 + c;
+                  for (uint32_t p = lo[k] + 1; p < hi[k]; ++p, src += part_stride) {
+                    const float2 x = *src;
+                    sum.x += x.x;
+                    sum.y += x.y;
+                  }
+                  *a = sum;
+                }
+                // Tiles wider than 64 cells: the rest of the row segment.
+                for (int c = lane + 64; c < len; c += 32) {
+                  float2* a = acc + padded(cell0 + c);
+                  const float2* src = scratch + static_cast<int64_t>(lo[k]) * part_stride +
+                                      static_cast<int64_t>(b) * sp.padded_cells + local_yz + lx0 + c;
+                  float2 sum = *a;
+                  for (uint32_t p = lo[k]; p < hi[k]; ++p, src += part_stride) {
+                    const float2 x = *src;
+                    sum.x += x.x;
+                    sum.y += x.y;
+                  }
+                  *a = sum;
+                }
+              }
+            }
+          }
+          __syncthreads();
+        }
+      }
+    }
+    float2 v[8];
+    const float2* rb = acc + padded(t);
+#pragma unroll
+    for (int q = 0; q < 8; ++q) v[q] = rb[q * Sh::TPR + ((q * Sh::TPR) >> 4)];
+    // Pass 0 writes buf0; acc is written again only after pass 0's barrier.
+    fft_regs<L, S>(v, buf0, acc, t, fp.twiddle[0]);
+    if (live) {
+      float2* out = out_all + (static_cast<int64_t>(b) * rows_total + r) * m0;
+#pragma unroll
+      for (int q = 0; q < 8; ++q) {
+        const int k = mode_index32(t + q * Sh::TPR, m0, Sh::N, fp.centered);
+        if (k >= 0) out[k] = v[q];
+      }
+    }
+    __syncthreads();
+  }
+}
+
 // Type 1, pass along axis 0 from a folded fine grid: rows r of vector b
 // transformed, the kept modes written to out[b][r][0, m0).
 template <int L, int S>
@@ -522,17 +661,27 @@ void launch_row_fold(const SpreadParams& sp, const FusedFftParams& fp, int batch
   using Sh = FftShape<L>;
   const int rows_total = 1 << (fp.log2n[1] + (fp.dims > 2 ? fp.log2n[2] : 0));
   const dim3 grid(static_cast<unsigned>((rows_total + Sh::PER_CTA - 1) / Sh::PER_CTA), batches(batch));
-  if (fp.dims > 2) {
-    auto kernel = row_fold_fft_kernel<L, S, 3>;
-    allow_shared(kernel, row_smem<L>());
-    kernel<<<grid, Sh::THREADS, row_smem<L>(), stream>>>(sp, fp, batch, rows_total, scratch, part_start, part_limit,
-                                                          candidates, out);
-  } else {
-    auto kernel = row_fold_fft_kernel<L, S, 2>;
-    allow_shared(kernel, row_smem<L>());
-    kernel<<<grid, Sh::THREADS, row_smem<L>(), stream>>>(sp, fp, batch, rows_total, scratch, part_start, part_limit,
-                                                          candidates, out);
+  const int64_t n0 = int64_t{1} << L;
+  const bool segments = Sh::TPR >= 32 && n0 % sp.tile[0] == 0 && sp.pad[0] - sp.tile[0] < sp.tile[0] &&
+                        sp.ntiles[0] >= 2;
+#define B200NUFFT_ROW_FOLD(KERNEL)                                                                          \
+  {                                                                                                         \
+    auto kernel = KERNEL;                                                                                   \
+    allow_shared(kernel, row_smem<L>());                                                                    \
+    kernel<<<grid, Sh::THREADS, row_smem<L>(), stream>>>(sp, fp, batch, rows_total, scratch, part_start,   \
+                                                          part_limit, candidates, out);                     \
   }
+  if constexpr (Sh::TPR >= 32) {
+    if (segments) {
+      if (fp.dims > 2) B200NUFFT_ROW_FOLD((row_segment_fold_fft_kernel<L, S, 3>))
+      else B200NUFFT_ROW_FOLD((row_segment_fold_fft_kernel<L, S, 2>))
+      note_launch();
+      return;
+    }
+  }
+  if (fp.dims > 2) B200NUFFT_ROW_FOLD((row_fold_fft_kernel<L, S, 3>))
+  else B200NUFFT_ROW_FOLD((row_fold_fft_kernel<L, S, 2>))
+#undef B200NUFFT_ROW_FOLD
   note_launch();
 }
 
