@@ -331,12 +331,15 @@ __global__ void __launch_bounds__(256) interpolate_bins_kernel(GridParams g, con
 // staged in shared memory one vector at a time (coalesced row loads, mostly
 // L2 hits shared with the neighbouring bins), and a thread serves one point
 // from it, summing in the order of interpolate_kernel (bitwise the same
-// values); windows beyond the region read the grid directly.
+// values); windows beyond the region read the grid directly. For several
+// vectors the part's points are served in the order of their support
+// starts, so that a warp's lanes share neighbouring region cells.
 constexpr int kRegionThreads = 128;
 
-
+// One vector: the points in bin order (sorting them pays only when the
+// staged region serves several vectors).
 template <int W>
-__global__ void __launch_bounds__(kRegionThreads) interpolate_region_kernel(
+__global__ void __launch_bounds__(kRegionThreads) interpolate_region_single_kernel(
     GridParams g, const void* __restrict__ windows, int64_t count, const uint32_t* __restrict__ perm,
     const uint32_t* __restrict__ offsets, const float2* __restrict__ fine, int batch,
     float2* __restrict__ output, InterpParts parts) {
@@ -402,6 +405,146 @@ __global__ void __launch_bounds__(kRegionThreads) interpolate_region_kernel(
               x = x >= n0 ? x - n0 : x;
               const float2 v = __ldg(&grid[static_cast<int64_t>(y) * n0 + x]);
               r = cfma(v, wx[i], r);
+            }
+            e = cfma(r, wy[j], e);
+          }
+        }
+      }
+      output[static_cast<int64_t>(b) * count + point] = e;
+    }
+  }
+}
+
+// Several vectors: the part's points ordered by support start first.
+template <int W>
+__global__ void __launch_bounds__(kRegionThreads) interpolate_region_kernel(
+    GridParams g, const void* __restrict__ windows, int64_t count, const uint32_t* __restrict__ perm,
+    const uint32_t* __restrict__ offsets, const float2* __restrict__ fine, int batch,
+    float2* __restrict__ output, InterpParts parts) {
+  constexpr int S = bin_region_side<W>();
+  constexpr int kKeys = S * S + 1;  // start cells of the region, then the windows that leave it
+  __shared__ float2 region[S * S];
+  __shared__ PreparedWindow<2> part_win[kInterpPartSlots];
+  __shared__ uint32_t part_point[kInterpPartSlots];
+  __shared__ uint16_t order[kInterpPartSlots];
+  __shared__ uint32_t key_start[kKeys];
+  __shared__ uint32_t warp_total[kRegionThreads / 32];
+  int64_t bin;
+  uint32_t first, last;
+  if (!bin_part(parts, offsets, g.axis[0].bins * static_cast<uint64_t>(g.axis[1].bins), bin, first, last)) return;
+  const int bins0 = static_cast<int>(g.axis[0].bins);
+  const int n0 = g.axis[0].length, n1 = g.axis[1].length;
+  const int ox = static_cast<int>(bin % bins0) * 8 - W / 2 - 2;
+  const int oy = static_cast<int>(bin / bins0) * 8 - W / 2 - 2;
+  const int n = static_cast<int>(last - first);
+  // The part's points ordered by support start (a counting sort in shared
+  // memory; the order within a start is arbitrary, and each point's sum does
+  // not depend on it), so that a warp's lanes read neighbouring region cells
+  // and share them instead of colliding in the banks.
+  for (int k = threadIdx.x; k < kKeys; k += kRegionThreads) key_start[k] = 0;
+  __syncthreads();
+  constexpr int kPerThread = kInterpPartSlots / kRegionThreads;
+  int key[kPerThread];
+  uint32_t rank[kPerThread];
+#pragma unroll
+  for (int q = 0; q < kPerThread; ++q) {
+    const int i = threadIdx.x + q * kRegionThreads;
+    key[q] = -1;
+    rank[q] = 0;
+    if (i < n) {
+      const PreparedWindow<2> win = static_cast<const PreparedWindow<2>*>(windows)[first + i];
+      part_win[i] = win;
+      part_point[i] = perm[first + i];
+      int k = S * S;
+      if (win.start[0] >= 0) {
+        const int dx = wrap_index(win.start[0] - ox, n0);
+        const int dy = wrap_index(win.start[1] - oy, n1);
+        if (dx + W <= S && dy + W <= S) k = dy * S + dx;
+      }
+      key[q] = k;
+      rank[q] = atomicAdd(&key_start[k], 1u);
+    }
+  }
+  __syncthreads();
+  {
+    // Exclusive scan of the key counts: a thread sums a few consecutive
+    // keys, the warps and then the block add up.
+    constexpr int kKeysPerThread = (kKeys + kRegionThreads - 1) / kRegionThreads;
+    uint32_t local[kKeysPerThread];
+    uint32_t sum = 0;
+#pragma unroll
+    for (int k = 0; k < kKeysPerThread; ++k) {
+      const int e = threadIdx.x * kKeysPerThread + k;
+      local[k] = e < kKeys ? key_start[e] : 0u;
+      sum += local[k];
+    }
+    const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
+    uint32_t x = sum;
+#pragma unroll
+    for (int offset = 1; offset < 32; offset <<= 1) {
+      const uint32_t y = __shfl_up_sync(0xFFFFFFFFu, x, offset);
+      if (lane >= offset) x += y;
+    }
+    if (lane == 31) warp_total[warp] = x;
+    __syncthreads();
+    uint32_t running = x - sum;
+    for (int w = 0; w < warp; ++w) running += warp_total[w];
+#pragma unroll
+    for (int k = 0; k < kKeysPerThread; ++k) {
+      const int e = threadIdx.x * kKeysPerThread + k;
+      if (e < kKeys) key_start[e] = running;
+      running += local[k];
+    }
+  }
+  __syncthreads();
+#pragma unroll
+  for (int q = 0; q < kPerThread; ++q) {
+    if (key[q] >= 0) order[key_start[key[q]] + rank[q]] = static_cast<uint16_t>(threadIdx.x + q * kRegionThreads);
+  }
+  for (int b = 0; b < batch; ++b) {
+    const float2* grid = fine + static_cast<int64_t>(b) * g.fine_count;
+    __syncthreads();  // the order is written; the previous vector's reads are done
+    for (int e = threadIdx.x; e < S * S; e += kRegionThreads) {
+      const int r = e / S, c = e - r * S;
+      const int y = wrap_index(oy + r, n1);
+      const int x = wrap_index(ox + c, n0);
+      region[e] = __ldg(&grid[static_cast<int64_t>(y) * n0 + x]);
+    }
+    __syncthreads();
+    for (int pos = threadIdx.x; pos < n; pos += kRegionThreads) {
+      const int i = order[pos];
+      const PreparedWindow<2> win = part_win[i];
+      const uint32_t point = part_point[i];
+      float2 e = make_float2(0.0f, 0.0f);  // (re, im), paired fused multiply-adds
+      if (win.start[0] >= 0) {
+        float wx[W], wy[W];
+        horner32_window<W>(win.offset[0], g.horner32, wx);
+        horner32_window<W>(win.offset[1], g.horner32, wy);
+        const int dx = wrap_index(win.start[0] - ox, n0);
+        const int dy = wrap_index(win.start[1] - oy, n1);
+        if (dx + W <= S && dy + W <= S) {
+#pragma unroll
+          for (int j = 0; j < W; ++j) {
+            const float2* row = region + (dy + j) * S + dx;
+            float2 r = make_float2(0.0f, 0.0f);
+#pragma unroll
+            for (int k = 0; k < W; ++k) {
+              const float2 v = row[k];
+              r = cfma(v, wx[k], r);
+            }
+            e = cfma(r, wy[j], e);
+          }
+        } else {
+#pragma unroll 1
+          for (int j = 0; j < W; ++j) {
+            int y = win.start[1] + j;
+            y = y >= n1 ? y - n1 : y;
+            float2 r = make_float2(0.0f, 0.0f);
+            for (int k = 0; k < W; ++k) {
+              int x = win.start[0] + k;
+              x = x >= n0 ? x - n0 : x;
+              const float2 v = __ldg(&grid[static_cast<int64_t>(y) * n0 + x]);
+              r = cfma(v, wx[k], r);
             }
             e = cfma(r, wy[j], e);
           }
@@ -596,8 +739,13 @@ void interpolate_region_execute(const GridParams& g, const InterpBinsLaunch& l, 
   switch (g.width) {
 #define B200NUFFT_REGION_CASE(WIDTH)                                                                   \
   case WIDTH:                                                                                          \
-    interpolate_region_kernel<WIDTH><<<grid, kRegionThreads, 0, stream>>>(                              \
-        g, l.windows, l.point_count, l.perm, l.offsets, l.fine, l.batch, l.output, l.parts);            \
+    if (l.batch > 1) {                                                                                 \
+      interpolate_region_kernel<WIDTH><<<grid, kRegionThreads, 0, stream>>>(                            \
+          g, l.windows, l.point_count, l.perm, l.offsets, l.fine, l.batch, l.output, l.parts);          \
+    } else {                                                                                           \
+      interpolate_region_single_kernel<WIDTH><<<grid, kRegionThreads, 0, stream>>>(                     \
+          g, l.windows, l.point_count, l.perm, l.offsets, l.fine, l.batch, l.output, l.parts);          \
+    }                                                                                                  \
     break;
     B200NUFFT_REGION_CASE(2)
     B200NUFFT_REGION_CASE(3)
