@@ -5,7 +5,9 @@ against the cuFFT path of the same plans and against FP64 direct sums.
 
 Both paths spread and interpolate the same way; they differ only in the
 rounding of the FFT, so their outputs agree to a few f32 ulps of the largest
-mode (relative l2 below 2e-6), and each stays within the reference's
+mode (relative l2 below 2e-6 at the default upsampling factor 2; below 2e-5
+at 1.25 and 1.5, where the edge modes' deconvolution amplitudes amplify the
+rounding of both paths), and each stays within the reference's
 accuracy bars of the direct sums (20 eps in 2D, tests/gpu_nufft_2d.rs:15-16;
 32 eps in 3D, tests/gpu_nufft_3d.rs:14-15).
 """
@@ -40,9 +42,9 @@ def _restore_fused():
     set_fused(True)
 
 
-def run(kind, modes, eps, points, values, isign, order, batch, fused):
+def run(kind, modes, eps, points, values, isign, order, batch, fused, sigma=2.0):
     set_fused(fused)
-    config = w.NufftConfig(modes, eps, isign=isign, mode_order=order, batch=batch)
+    config = w.NufftConfig(modes, eps, isign=isign, mode_order=order, batch=batch, sigma=sigma)
     plan = (w.NufftPlan.type1_gpu if kind == 1 else w.NufftPlan.type2_gpu)(config)
     set_fused(True)
     n = config.mode_count()
@@ -64,7 +66,10 @@ def power_of_two(n: int) -> bool:
 
 
 CASES = [
-    # modes, points, eps, isign, mode order, batch, distribution
+    # modes, points, eps, isign, mode order, batch, distribution[, upsampling factor]
+    ((203, 407), 80_000, 1e-5, 1, 1, 1, "uniform", 1.25),
+    ((339, 170), 60_000, 1e-5, -1, 0, 2, "clustered", 1.5),
+    ((101, 102, 203), 150_000, 1e-3, 1, 1, 1, "uniform", 1.25),
     ((64, 32, 31), 120_000, 1e-5, 1, 0, 1, "uniform"),
     ((31, 64, 64), 100_000, 1e-6, -1, 1, 2, "clustered"),
     ((128, 127, 32), 150_000, 1e-4, -1, 0, 1, "uniform"),
@@ -78,16 +83,18 @@ CASES = [
 
 
 @pytest.mark.parametrize("kind", [1, 2])
-@pytest.mark.parametrize("case", CASES, ids=lambda c: f"{c[0][0]}x{c[0][1]}_b{c[5]}_s{c[3]}_o{c[4]}")
+@pytest.mark.parametrize("case", CASES,
+                         ids=lambda c: "x".join(map(str, c[0])) + f"_b{c[5]}_s{c[3]}_o{c[4]}" + (f"_u{c[7]}" if len(c) > 7 else ""))
 def test_fused_transforms_match_cufft_and_direct_sums(kind, case):
-    modes, count, eps, isign, order, batch, dist = case
+    modes, count, eps, isign, order, batch, dist = case[:7]
+    sigma = case[7] if len(case) > 7 else 2.0
     rng = np.random.default_rng(sum(modes) + count + kind)
     d = len(modes)
     points = (uniform_points(rng, count, d) if dist == "uniform" else clustered_points(rng, count, d)).astype(np.float32)
     n = int(np.prod(modes))
     values = complex_normal(rng, batch * (count if kind == 1 else n)).astype(np.complex64)
-    fused, stages, fine = run(kind, modes, eps, points, values, isign, order, batch, True)
-    plain, plain_stages, _ = run(kind, modes, eps, points, values, isign, order, batch, False)
+    fused, stages, fine = run(kind, modes, eps, points, values, isign, order, batch, True, sigma)
+    plain, plain_stages, _ = run(kind, modes, eps, points, values, isign, order, batch, False, sigma)
     assert all(power_of_two(f) for f in fine), fine
     if kind == 1 and np.prod(fine) > 1 << 16:
         assert "deconvolution" not in stages and "fold" in stages  # fold, row and column transforms
@@ -95,8 +102,12 @@ def test_fused_transforms_match_cufft_and_direct_sums(kind, case):
         assert stages["predeconvolution"][1] == 1  # one launch: predeconvolution + column transforms
     if kind == 1:
         assert "deconvolution" in plain_stages
+    # Smaller upsampling factors keep modes nearer the fine grid's edge, whose
+    # deconvolution amplitudes (1 / phi_hat) grow large and amplify both
+    # FFTs' rounding alike.
+    agree = 2e-6 if sigma == 2.0 else 2e-5
     for b in range(batch):
-        assert rel_l2(fused[b], plain[b]) < 2e-6, (b, rel_l2(fused[b], plain[b]))
+        assert rel_l2(fused[b], plain[b]) < agree, (b, rel_l2(fused[b], plain[b]))
     # Against FP64 direct sums, on a subset.
     total = n if kind == 1 else count
     sel = np.arange(0, total, max(1, total // 600))
