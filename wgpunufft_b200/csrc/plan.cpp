@@ -691,6 +691,33 @@ void NufftPlan::set_points(int64_t count, const void* points, cudaStream_t strea
       tc2_part_upper_bound_ = tiles + chunk_bound / kTi2ChunksPerPart + 1;
       tc2_vector_max_.reserve(static_cast<size_t>(std::max<int64_t>(batch_, 1)) * sizeof(uint32_t), "vector maxima");
     }
+    // 3D type 2: the interpolation takes the points in the order of their
+    // support starts' (z, y) rows and 16-cell segments of x, so that a warp's
+    // 32 points gather from few grid rows; that order is sorted first (its
+    // permutation kept), then the reference's bins in the same buffers.
+    rows_order_ = type_ == 2 && dim_ == 3 && count > 0;
+    if (rows_order_) {
+      GridParams rows = grid_;
+      uint64_t stride = 1;
+      for (int a = 0; a < 3; ++a) {
+        const int shift = a == 0 ? std::min(4, ilog2(fine_[0])) : 0;
+        rows.axis[a].shift = shift;
+        rows.axis[a].bins = static_cast<uint32_t>((fine_[a] + (int64_t{1} << shift) - 1) >> shift);
+        rows.axis[a].stride = static_cast<uint32_t>(stride);
+        stride *= rows.axis[a].bins;
+      }
+      uint32_t* rows_offsets = static_cast<uint32_t*>(rows_offsets_.reserve((stride + 1) * sizeof(uint32_t),
+                                                                           "row-order offsets"));
+      uint32_t* order = nullptr;
+      uint32_t* keys = nullptr;
+      sort_points(static_cast<const float*>(points), count, rows, KeyKind::SupportStart, stride, buf, rows_offsets,
+                  &order, &keys, stream, &timer_);
+      uint32_t* kept = static_cast<uint32_t*>(rows_perm_.reserve(static_cast<size_t>(count) * sizeof(uint32_t),
+                                                                 "row-order permutation"));
+      check_cuda(cudaMemcpyAsync(kept, order, static_cast<size_t>(count) * sizeof(uint32_t), cudaMemcpyDeviceToDevice,
+                                 stream),
+                 "keep row order");
+    }
     if (valid_first) {
       sort_points_valid_first(static_cast<const float*>(points), count, grid_, bins_, buf, offsets, valid_mask,
                               &perm_, &sorted_keys_, stream, &timer_);
@@ -699,7 +726,7 @@ void NufftPlan::set_points(int64_t count, const void* points, cudaStream_t strea
                   &perm_, &sorted_keys_, stream, &timer_);
     }
     float* sorted = static_cast<float*>(sorted_points_.reserve(sorted_bytes, "sorted coordinates"));
-    gather_sorted_points(static_cast<const float*>(points), perm_, count, dim_, sorted, stream,
+    gather_sorted_points(static_cast<const float*>(points), interp_perm(), count, dim_, sorted, stream,
                          &timer_);
     // The spreader and interpolator read each point's window start and offset.
     void* windows = windows_.reserve(static_cast<size_t>(std::max<int64_t>(count, 1)) * prepared_window_bytes(dim_),
@@ -973,7 +1000,7 @@ void NufftPlan::execute_f32(int batch, const void* input, void* output, uint64_t
     l.points = static_cast<const float*>(sorted_points_.get());
     l.windows = windows_.get();
     l.point_count = point_count_;
-    l.perm = perm_;
+    l.perm = interp_perm();
     l.fine = fine;
     l.batch = batch;
     l.output = static_cast<float2*>(output);

@@ -157,6 +157,14 @@ class NufftPlan {
   void prepare_interp_parts(const uint32_t* offsets, cudaStream_t stream);
   InterpParts interp_parts() const;
   DeviceBuffer staged_;   // batched 2D f32 type-2 plans: values in slot order
+  // 3D f32 type-2 plans: the interpolation's point order (support starts'
+  // (z, y) rows, 16-cell x segments), in which the sorted coordinates and the
+  // prepared windows are kept; the reference's bin order stays in perm_.
+  bool rows_order_ = false;
+  DeviceBuffer rows_perm_, rows_offsets_;
+  const uint32_t* interp_perm() const {
+    return rows_order_ ? static_cast<const uint32_t*>(rows_perm_.get()) : perm_;
+  }
 
   // Spreading state.
   DeviceBuffer parts_, part_start_, max_bits_, scratch_, candidates_;
