@@ -692,7 +692,7 @@ void NufftPlan::set_points(int64_t count, const void* points, cudaStream_t strea
       tc2_vector_max_.reserve(static_cast<size_t>(std::max<int64_t>(batch_, 1)) * sizeof(uint32_t), "vector maxima");
     }
     // 3D type 2: the interpolation takes the points in the order of their
-    // support starts' (z, y) rows and 16-cell segments of x, so that a warp's
+    // support starts' (z, y) rows and 8-cell segments of x, so that a warp's
     // 32 points gather from few grid rows; that order is sorted first (its
     // permutation kept), then the reference's bins in the same buffers.
     rows_order_ = type_ == 2 && dim_ == 3 && count > 0;
@@ -700,7 +700,7 @@ void NufftPlan::set_points(int64_t count, const void* points, cudaStream_t strea
       GridParams rows = grid_;
       uint64_t stride = 1;
       for (int a = 0; a < 3; ++a) {
-        const int shift = a == 0 ? std::min(4, ilog2(fine_[0])) : 0;
+        const int shift = a == 0 ? std::min(3, ilog2(fine_[0])) : 0;
         rows.axis[a].shift = shift;
         rows.axis[a].bins = static_cast<uint32_t>((fine_[a] + (int64_t{1} << shift) - 1) >> shift);
         rows.axis[a].stride = static_cast<uint32_t>(stride);

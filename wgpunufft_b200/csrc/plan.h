@@ -158,7 +158,7 @@ class NufftPlan {
   InterpParts interp_parts() const;
   DeviceBuffer staged_;   // batched 2D f32 type-2 plans: values in slot order
   // 3D f32 type-2 plans: the interpolation's point order (support starts'
-  // (z, y) rows, 16-cell x segments), in which the sorted coordinates and the
+  // (z, y) rows, 8-cell x segments), in which the sorted coordinates and the
   // prepared windows are kept; the reference's bin order stays in perm_.
   bool rows_order_ = false;
   DeviceBuffer rows_perm_, rows_offsets_;
