@@ -697,26 +697,15 @@ void NufftPlan::set_points(int64_t count, const void* points, cudaStream_t strea
     // permutation kept), then the reference's bins in the same buffers.
     rows_order_ = type_ == 2 && dim_ == 3 && count > 0;
     if (rows_order_) {
-      GridParams rows = grid_;
-      uint64_t stride = 1;
-      for (int a = 0; a < 3; ++a) {
-        const int shift = a == 0 ? std::min(3, ilog2(fine_[0])) : 0;
-        rows.axis[a].shift = shift;
-        rows.axis[a].bins = static_cast<uint32_t>((fine_[a] + (int64_t{1} << shift) - 1) >> shift);
-        rows.axis[a].stride = static_cast<uint32_t>(stride);
-        stride *= rows.axis[a].bins;
-      }
+      uint64_t stride = 0;
+      const GridParams rows = rows_grid(&stride);
       uint32_t* rows_offsets = static_cast<uint32_t*>(rows_offsets_.reserve((stride + 1) * sizeof(uint32_t),
                                                                            "row-order offsets"));
       uint32_t* order = nullptr;
       uint32_t* keys = nullptr;
       sort_points(static_cast<const float*>(points), count, rows, KeyKind::SupportStart, stride, buf, rows_offsets,
                   &order, &keys, stream, &timer_);
-      uint32_t* kept = static_cast<uint32_t*>(rows_perm_.reserve(static_cast<size_t>(count) * sizeof(uint32_t),
-                                                                 "row-order permutation"));
-      check_cuda(cudaMemcpyAsync(kept, order, static_cast<size_t>(count) * sizeof(uint32_t), cudaMemcpyDeviceToDevice,
-                                 stream),
-                 "keep row order");
+      keep_rows_order(order, count, stream);
     }
     if (valid_first) {
       sort_points_valid_first(static_cast<const float*>(points), count, grid_, bins_, buf, offsets, valid_mask,
@@ -746,10 +735,22 @@ void NufftPlan::set_points(int64_t count, const void* points, cudaStream_t strea
       df64_to_f64(static_cast<const float*>(points), count * dim_, converted, stream);
       points64 = converted;
     }
+    // 3D type 2: the interpolation's row order first, as for f32 plans.
+    rows_order_ = type_ == 2 && dim_ == 3 && count > 0;
+    if (rows_order_) {
+      uint64_t stride = 0;
+      const GridParams rows = rows_grid(&stride);
+      uint32_t* rows_offsets = static_cast<uint32_t*>(rows_offsets_.reserve((stride + 1) * sizeof(uint32_t),
+                                                                           "row-order offsets"));
+      uint32_t* order = nullptr;
+      uint32_t* keys = nullptr;
+      sort_points64(points64, count, rows, stride, buf, rows_offsets, &order, &keys, stream, &timer_, nullptr);
+      keep_rows_order(order, count, stream);
+    }
     sort_points64(points64, count, grid_, bins_, buf, offsets, &perm_, &sorted_keys_, stream,
                   &timer_, valid_mask);
     double* sorted = static_cast<double*>(sorted_points_.reserve(sorted_bytes, "sorted coordinates"));
-    gather_sorted_points64(points64, perm_, count, dim_, sorted, stream, &timer_);
+    gather_sorted_points64(points64, interp_perm(), count, dim_, sorted, stream, &timer_);
     if (type_ == 2 && dim_ == 2) {
       StageScope scope(&timer_, kStageBinOffsets, stream);
       prepare_interp_parts(offsets, stream);
@@ -1062,7 +1063,7 @@ void NufftPlan::execute_f64(int batch, const void* input, void* output, uint64_t
     InterpLaunch64 l;
     l.points = static_cast<const double*>(sorted_points_.get());
     l.point_count = point_count_;
-    l.perm = perm_;
+    l.perm = interp_perm();
     l.fine = fine;
     l.batch = batch;
     l.output = out;
@@ -1241,6 +1242,31 @@ void NufftPlan::spread_to(int64_t active_batch, const void* strengths, void* gri
     spread_execute64(spread_, l, stream, &timer_);
   }
   check_cuda(cudaGetLastError(), "spread launch");
+}
+
+GridParams NufftPlan::rows_grid(uint64_t* bins) const {
+  // Bins of one cell along y and z and 8 cells along x: sorted by these
+  // keys, the points come in the order of their support starts' (z, y)
+  // rows and 8-cell x segments.
+  GridParams rows = grid_;
+  uint64_t stride = 1;
+  for (int a = 0; a < 3; ++a) {
+    const int shift = a == 0 ? std::min(3, ilog2(fine_[0])) : 0;
+    rows.axis[a].shift = shift;
+    rows.axis[a].bins = static_cast<uint32_t>((fine_[a] + (int64_t{1} << shift) - 1) >> shift);
+    rows.axis[a].stride = static_cast<uint32_t>(stride);
+    stride *= rows.axis[a].bins;
+  }
+  *bins = stride;
+  return rows;
+}
+
+void NufftPlan::keep_rows_order(const uint32_t* order, int64_t count, cudaStream_t stream) {
+  uint32_t* kept = static_cast<uint32_t*>(rows_perm_.reserve(static_cast<size_t>(count) * sizeof(uint32_t),
+                                                             "row-order permutation"));
+  check_cuda(cudaMemcpyAsync(kept, order, static_cast<size_t>(count) * sizeof(uint32_t), cudaMemcpyDeviceToDevice,
+                             stream),
+             "keep row order");
 }
 
 void NufftPlan::copy_bin_order(uint32_t* permutation, uint32_t* bin_offsets, cudaStream_t stream) {

@@ -157,14 +157,19 @@ class NufftPlan {
   void prepare_interp_parts(const uint32_t* offsets, cudaStream_t stream);
   InterpParts interp_parts() const;
   DeviceBuffer staged_;   // batched 2D f32 type-2 plans: values in slot order
-  // 3D f32 type-2 plans: the interpolation's point order (support starts'
-  // (z, y) rows, 8-cell x segments), in which the sorted coordinates and the
-  // prepared windows are kept; the reference's bin order stays in perm_.
+  // 3D type-2 plans: the interpolation's point order (support starts'
+  // (z, y) rows, 8-cell x segments), in which the sorted coordinates (and the
+  // prepared windows of f32 plans) are kept; the reference's bin order stays
+  // in perm_.
   bool rows_order_ = false;
   DeviceBuffer rows_perm_, rows_offsets_;
   const uint32_t* interp_perm() const {
     return rows_order_ ? static_cast<const uint32_t*>(rows_perm_.get()) : perm_;
   }
+  // The bins of that order (one cell along y and z, 8 along x) and their count.
+  GridParams rows_grid(uint64_t* bins) const;
+  // Copies a sort's permutation into rows_perm_ (the sort buffers are reused).
+  void keep_rows_order(const uint32_t* order, int64_t count, cudaStream_t stream);
 
   // Spreading state.
   DeviceBuffer parts_, part_start_, max_bits_, scratch_, candidates_;
