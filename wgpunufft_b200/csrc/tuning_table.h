@@ -23,7 +23,9 @@ constexpr TuningEntry kTuningTable[] = {
     {1, 3, 3, 7, 18, -2, 8, 2, 1, 16},  // 3d_32_1e5_clustered: 0.0966 ms
     {1, 2, 1, 10, 20, 0, 16, 8, 1, 16},  // 2d_512_2e6_f64_1e-9: 1.0739 ms
     {2, 2, 3, 7, 20, 0, 32, 4, 1, 64},  // 2d_512_2e6_uniform_type2: 0.1855 ms
+    {1, 2, 3, 4, 20, 0, 0, 4, 1, 16},  // 2d_512_2e6_uniform_eps0.001_type1_cuda_cores_B16: 1.2732 ms
+    {2, 2, 3, 4, 20, 0, 0, 4, 1, 128},  // 2d_512_2e6_uniform_eps0.001_type2_cuda_cores_B16: 1.0525 ms
 };
-constexpr int kTuningEntries = 11;
+constexpr int kTuningEntries = 13;
 
 }  // namespace b200nufft

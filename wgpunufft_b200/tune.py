@@ -1,15 +1,17 @@
 """Autotuner of the spreader's launch choices, run on a B200:
 
-    python -m wgpunufft_b200.tune [--out PATH] [--repeats N]
+    python -m wgpunufft_b200.tune [--out PATH] [--repeats N] [--tensor-only]
 
 For every workload below (the benchmark configurations and the sizes of the
 uneven-problems batch), it measures type-1 executions on prepared points
 under every candidate choice (tile side, CTAs per SM the tile parts are
 sized for, the same on crowded one-cell bins) and, for batched workloads,
-the smallest batch at which the tensor cores beat the CUDA cores; then it
-writes the fastest choice per workload key (plan type, dimension,
-precision, window width, log2 fine-grid cells, log2 points per cell) as
-tuning_table.h. The library compiles that table in, so a key always gets
+the smallest batch at which the tensor cores beat the CUDA cores, per
+plan type and window width (eps 1e-3 and 1e-6); then it writes the fastest
+choice per workload key (plan type, dimension, precision, window width,
+log2 fine-grid cells, log2 points per cell) as tuning_table.h.
+`--tensor-only` measures the tensor-core thresholds alone and merges them
+into the table already written. The library compiles that table in, so a key always gets
 the same choices and outputs stay bitwise repeatable. Inputs are seeded
 synthetic points (uniform, clustered, radial) and N(0, 1) strengths.
 """
@@ -20,6 +22,7 @@ import argparse
 import itertools
 import json
 import math
+import re
 import statistics
 from pathlib import Path
 
@@ -99,26 +102,92 @@ def tune_workload(torch, w, workloads, native, spec, repeats):
     return {"workload": name, "key": key, "best": best, "candidates": results}
 
 
-def tune_tensor_threshold(torch, w, workloads, native, kind, repeats):
-    """Smallest batch in {16, 32, 64} at which the tensor cores are faster
-    (2D 512^2 modes, 2e6 uniform points, eps 1e-6); 0 for none."""
-    modes, count = (512, 512), 2_000_000
+# The batched configuration the tensor-core thresholds are measured on (2D
+# 512^2 modes, 2e6 uniform points), its window widths (eps) and batches.
+TENSOR_MODES, TENSOR_POINTS = (512, 512), 2_000_000
+TENSOR_EPS = (1e-3, 1e-6)
+TENSOR_BATCHES = (16, 32, 64, 128, 256)
+
+
+def tune_tensor_threshold(torch, w, workloads, native, kind, eps, repeats):
+    """Smallest batch of TENSOR_BATCHES at which the tensor cores are faster
+    on the batched configuration at `eps` (0 for none), the window width and
+    the times per batch."""
+    modes, count = TENSOR_MODES, TENSOR_POINTS
     pts = workloads.points("uniform", count, 2, seed=13)
     n = modes[0] * modes[1]
-    for batch in (16, 32, 64):
+    times = {}
+    width = 0
+    for batch in TENSOR_BATCHES:
         inputs = workloads.values(batch, count if kind == 1 else n, seed=14)
         out = torch.empty((batch, n if kind == 1 else count), dtype=torch.complex64, device="cuda")
         ms = {}
         for method in (w.SpreadMethod.TENSOR_CORES, w.SpreadMethod.CUDA_CORES):
             plan = (w.NufftPlan.type1_gpu if kind == 1 else w.NufftPlan.type2_gpu)(
-                w.NufftConfig(modes, 1e-6, batch=batch, spread_method=method))
+                w.NufftConfig(modes, eps, batch=batch, spread_method=method))
+            width = plan.kernel_width()
             plan.set_points_gpu(pts)
             ms[method] = _time(torch, lambda: plan.execute_gpu_batch(batch, inputs, out), repeats)
             del plan
         del inputs, out
+        torch.cuda.empty_cache()
+        times[batch] = {"tensor_cores": ms[w.SpreadMethod.TENSOR_CORES], "cuda_cores": ms[w.SpreadMethod.CUDA_CORES]}
         if ms[w.SpreadMethod.TENSOR_CORES] < ms[w.SpreadMethod.CUDA_CORES]:
-            return batch, ms
-    return 0, ms
+            return batch, width, times
+    return 0, width, times
+
+
+def tensor_entries(torch, w, workloads, native, entries, repeats):
+    """Sets the tensor-core threshold of every (type, width) of the batched
+    configuration's key: the tuned entry's where the key exists, else a new
+    entry with the plan's default launch choices. Returns the measurements."""
+    modes, count = TENSOR_MODES, TENSOR_POINTS
+    fine_cells = 4 * modes[0] * modes[1]
+    cells = int(math.floor(math.log2(fine_cells)))
+    density = max(-16, min(16, int(math.floor(math.log2(count / fine_cells)))))
+    measured = []
+    for kind in (1, 2):
+        for eps in TENSOR_EPS:
+            threshold, width, times = tune_tensor_threshold(torch, w, workloads, native, kind, eps, repeats)
+            measured.append({"type": kind, "eps": eps, "width": width, "threshold": threshold, "ms": times})
+            print(json.dumps(measured[-1]), flush=True)
+            key = {"type": kind, "dimensions": 2, "precision": 3, "width": width, "log2_cells": cells,
+                   "log2_density": density}
+            value = threshold or 1 << 30
+            found = False
+            for e in entries:
+                if e["key"] == key:
+                    e["tensor_min_batch"] = value
+                    found = True
+            if not found:
+                # Type 2 takes the type-1 entry's launch choices where that
+                # key was tuned (they do not apply to interpolation), else
+                # the plan's defaults; the time noted is the CUDA cores' on
+                # the smallest batch.
+                source = next((e for e in entries if e["key"] == dict(key, type=1)), None)
+                best = dict(source["best"]) if source else {"tile": 0, "ctas_per_sm": 4, "crowded_ctas_per_sm": 1}
+                first = TENSOR_BATCHES[0]
+                best["ms"] = times[first]["cuda_cores"]
+                name = f"2d_512_2e6_uniform_eps{eps:g}_type{kind}_cuda_cores_B{first}"
+                entries.append({"workload": name, "key": key, "best": best, "tensor_min_batch": value})
+    return measured
+
+
+ENTRY = re.compile(r"^\s*\{([-\d, ]+)\},\s*// (\S+): ([\d.]+) ms")
+
+
+def read_table(path):
+    """The entries of a tuning_table.h written by table_header."""
+    entries = []
+    for line in Path(path).read_text().splitlines():
+        m = ENTRY.match(line)
+        if not m:
+            continue
+        v = [int(x) for x in m.group(1).split(",")]
+        key = dict(zip(("type", "dimensions", "precision", "width", "log2_cells", "log2_density"), v[:6]))
+        best = {"tile": v[6], "ctas_per_sm": v[7], "crowded_ctas_per_sm": v[8], "ms": float(m.group(3))}
+        entries.append({"workload": m.group(2), "key": key, "best": best, "tensor_min_batch": v[9]})
+    return entries
 
 
 def merge_keys(entries):
@@ -171,6 +240,8 @@ def main():
     parser.add_argument("--report", default=None, help="JSON file for every measurement")
     parser.add_argument("--from-report", default=None, help="write the table from an earlier report, no GPU")
     parser.add_argument("--repeats", type=int, default=5)
+    parser.add_argument("--tensor-only", action="store_true",
+                        help="measure the tensor-core thresholds alone and merge them into --out")
     args = parser.parse_args()
     if args.from_report:
         entries = json.loads(Path(args.from_report).read_text())["entries"]
@@ -182,27 +253,22 @@ def main():
     from wgpunufft_b200 import _native as native
     from wgpunufft_b200 import workloads
 
-    entries = []
-    for spec in WORKLOADS:
-        entry = tune_workload(torch, w, workloads, native, spec, args.repeats)
-        entries.append(entry)
-        print(json.dumps({"workload": entry["workload"], "best": entry["best"]}), flush=True)
-    threshold1, ms1 = tune_tensor_threshold(torch, w, workloads, native, 1, args.repeats)
-    threshold2, ms2 = tune_tensor_threshold(torch, w, workloads, native, 2, args.repeats)
-    # The tensor-core threshold of the batched configuration's key (type 1 and 2).
-    for entry in entries:
-        if entry["workload"] == "2d_512_2e6_uniform":
-            entry["tensor_min_batch"] = threshold1 or 1 << 30
-            type2 = dict(entry, key=dict(entry["key"], type=2), workload="2d_512_2e6_uniform_type2",
-                         tensor_min_batch=threshold2 or 1 << 30)
-            entries.append(type2)
-            break
-    Path(args.out).write_text(table_header(merge_keys(entries)))
-    report = {"entries": entries, "tensor_threshold": {"type1": [threshold1, {str(k): v for k, v in ms1.items()}],
-                                                        "type2": [threshold2, {str(k): v for k, v in ms2.items()}]}}
+    if args.tensor_only:
+        entries = read_table(args.out)
+    else:
+        entries = []
+        for spec in WORKLOADS:
+            entry = tune_workload(torch, w, workloads, native, spec, args.repeats)
+            entries.append(entry)
+            print(json.dumps({"workload": entry["workload"], "best": entry["best"]}), flush=True)
+        entries = merge_keys(entries)
+    measured = tensor_entries(torch, w, workloads, native, entries, args.repeats)
+    Path(args.out).write_text(table_header(entries))
+    report = {"entries": entries, "tensor_thresholds": measured}
     if args.report:
         Path(args.report).write_text(json.dumps(report, indent=1))
-    print(json.dumps({"written": args.out, "tensor_threshold": report["tensor_threshold"]}), flush=True)
+    print(json.dumps({"written": args.out, "tensor_thresholds": [(m["type"], m["width"], m["threshold"])
+                                                                  for m in measured]}), flush=True)
 
 
 if __name__ == "__main__":
