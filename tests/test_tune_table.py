@@ -23,8 +23,10 @@ def test_committed_table_reads_back_to_the_same_file():
 def test_tensor_thresholds_merge_per_type_and_width(monkeypatch, tmp_path):
     entries = tune.read_table(TABLE)
     before = {tuple(sorted(e["key"].items())): dict(e) for e in entries}
-    widths = {1e-3: 4, 1e-6: 7}
-    thresholds = {(1, 4): 16, (2, 4): 256, (1, 7): 16, (2, 7): 0}
+    widths = {1e-2: 3, 1e-3: 4, 1e-4: 5, 1e-5: 6, 1e-6: 7}
+    thresholds = {(1, 3): 16, (2, 3): 256, (1, 4): 16, (2, 4): 256, (1, 5): 32, (2, 5): 128, (1, 6): 16,
+                  (2, 6): 64, (1, 7): 16, (2, 7): 0}
+    assert tuple(widths) == tune.TENSOR_EPS
 
     def fake(torch, w, workloads, native, kind, eps, repeats):
         width = widths[eps]
@@ -34,13 +36,18 @@ def test_tensor_thresholds_merge_per_type_and_width(monkeypatch, tmp_path):
     monkeypatch.setattr(tune, "tune_tensor_threshold", fake)
     measured = tune.tensor_entries(None, None, None, None, entries, 1)
     assert [(m["type"], m["width"], m["threshold"]) for m in measured] == [
-        (1, 4, 16), (1, 7, 16), (2, 4, 256), (2, 7, 0)]
+        (kind, width, thresholds[(kind, width)]) for kind in (1, 2) for width in widths.values()]
     by_key = {tuple(sorted(e["key"].items())): e for e in entries}
     assert len(by_key) == len(entries), "one entry per key"
     for (kind, width), threshold in thresholds.items():
         key = {"type": kind, "dimensions": 2, "precision": 3, "width": width, "log2_cells": 20, "log2_density": 0}
         entry = by_key[tuple(sorted(key.items()))]
         assert entry["tensor_min_batch"] == (threshold or 1 << 30)
+    # A new key keeps the launch choices the library gave it before: those
+    # of the nearest type-1 entry of its width (the 1024^2 entry for w 6).
+    w6 = by_key[tuple(sorted({"type": 1, "dimensions": 2, "precision": 3, "width": 6, "log2_cells": 20,
+                              "log2_density": 0}.items()))]
+    assert (w6["best"]["tile"], w6["best"]["ctas_per_sm"]) == (64, 2)
     # Launch choices of existing keys are kept; other keys are untouched.
     for k, old in before.items():
         new = by_key[k]

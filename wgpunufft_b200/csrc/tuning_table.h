@@ -25,7 +25,13 @@ constexpr TuningEntry kTuningTable[] = {
     {2, 2, 3, 7, 20, 0, 32, 4, 1, 64},  // 2d_512_2e6_uniform_type2: 0.1855 ms
     {1, 2, 3, 4, 20, 0, 0, 4, 1, 16},  // 2d_512_2e6_uniform_eps0.001_type1_cuda_cores_B16: 1.2732 ms
     {2, 2, 3, 4, 20, 0, 0, 4, 1, 128},  // 2d_512_2e6_uniform_eps0.001_type2_cuda_cores_B16: 1.0525 ms
+    {1, 2, 3, 3, 20, 0, 0, 4, 1, 16},  // 2d_512_2e6_uniform_eps0.01_type1_cuda_cores_B16: 1.5491 ms
+    {1, 2, 3, 5, 20, 0, 0, 4, 1, 16},  // 2d_512_2e6_uniform_eps0.0001_type1_cuda_cores_B16: 1.3940 ms
+    {1, 2, 3, 6, 20, 0, 64, 2, 2, 16},  // 2d_512_2e6_uniform_eps1e-05_type1_cuda_cores_B16: 1.4690 ms
+    {2, 2, 3, 3, 20, 0, 0, 4, 1, 1073741824},  // 2d_512_2e6_uniform_eps0.01_type2_cuda_cores_B16: 0.9279 ms
+    {2, 2, 3, 5, 20, 0, 0, 4, 1, 128},  // 2d_512_2e6_uniform_eps0.0001_type2_cuda_cores_B16: 1.1592 ms
+    {2, 2, 3, 6, 20, 0, 64, 2, 2, 64},  // 2d_512_2e6_uniform_eps1e-05_type2_cuda_cores_B16: 1.5501 ms
 };
-constexpr int kTuningEntries = 13;
+constexpr int kTuningEntries = 19;
 
 }  // namespace b200nufft

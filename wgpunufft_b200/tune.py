@@ -105,7 +105,7 @@ def tune_workload(torch, w, workloads, native, spec, repeats):
 # The batched configuration the tensor-core thresholds are measured on (2D
 # 512^2 modes, 2e6 uniform points), its window widths (eps) and batches.
 TENSOR_MODES, TENSOR_POINTS = (512, 512), 2_000_000
-TENSOR_EPS = (1e-3, 1e-6)
+TENSOR_EPS = (1e-2, 1e-3, 1e-4, 1e-5, 1e-6)
 TENSOR_BATCHES = (16, 32, 64, 128, 256)
 
 
@@ -137,6 +137,21 @@ def tune_tensor_threshold(torch, w, workloads, native, kind, eps, repeats):
     return 0, width, times
 
 
+def nearest(entries, key):
+    """The entry the library's lookup (csrc/tuning.cpp tuning_for) gives a
+    key: same type, dimensions, precision and width, least 4 |log2 cells
+    difference| + |log2 density difference|, the first on ties; None."""
+    best, best_distance = None, None
+    for e in entries:
+        k = e["key"]
+        if any(k[f] != key[f] for f in ("type", "dimensions", "precision", "width")):
+            continue
+        distance = 4 * abs(k["log2_cells"] - key["log2_cells"]) + abs(k["log2_density"] - key["log2_density"])
+        if best_distance is None or distance < best_distance:
+            best, best_distance = e, distance
+    return best
+
+
 def tensor_entries(torch, w, workloads, native, entries, repeats):
     """Sets the tensor-core threshold of every (type, width) of the batched
     configuration's key: the tuned entry's where the key exists, else a new
@@ -160,11 +175,12 @@ def tensor_entries(torch, w, workloads, native, entries, repeats):
                     e["tensor_min_batch"] = value
                     found = True
             if not found:
-                # Type 2 takes the type-1 entry's launch choices where that
-                # key was tuned (they do not apply to interpolation), else
-                # the plan's defaults; the time noted is the CUDA cores' on
-                # the smallest batch.
-                source = next((e for e in entries if e["key"] == dict(key, type=1)), None)
+                # The launch choices the key got before it had an entry (the
+                # nearest type-1 entry of its width, as the library looks it
+                # up; they do not apply to interpolation), else the plan's
+                # defaults; the time noted is the CUDA cores' on the
+                # smallest batch.
+                source = nearest(entries, dict(key, type=1))
                 best = dict(source["best"]) if source else {"tile": 0, "ctas_per_sm": 4, "crowded_ctas_per_sm": 1}
                 first = TENSOR_BATCHES[0]
                 best["ms"] = times[first]["cuda_cores"]
