@@ -208,7 +208,10 @@ int b200nufft_encode(b200nufft_plan plan, int64_t active_batch, int64_t point_co
  * `permutation` (device, point_count words) receives the original index of
  * every slot and `bin_offsets` (device, bin_count + 1 words) the first slot of
  * every bin followed by the total (NdPointBins::encode,
- * src/gpu_nd_bins.rs:336-471). Either pointer may be null. */
+ * src/gpu_nd_bins.rs:336-471). Either pointer may be null. 3D type-2 plans
+ * interpolate in another order and sort the bin order at the first call after
+ * each set_points, on `stream` (it reserves a device buffer of 3 coordinates
+ * per point the first time). */
 int b200nufft_copy_bin_order(b200nufft_plan plan, uint32_t *permutation,
                              uint32_t *bin_offsets, void *stream);
 

@@ -135,6 +135,9 @@ void gather_sorted_points(const float* points, const uint32_t* perm, int64_t cou
 void gather_sorted_points64(const double* points, const uint32_t* perm, int64_t count,
                             int dimensions, double* sorted, cudaStream_t stream,
                             StageTimer* timer = nullptr);
+// The inverse for 3D coordinates: points[perm[i]] = sorted[i] (float, double).
+template <typename T>
+void scatter_points3(const T* sorted, const uint32_t* perm, int64_t count, T* points, cudaStream_t stream);
 
 // Df64 storage (a (hi, lo) pair of floats per scalar, the reference's
 // double-float format) to and from f64, `count` scalars.

@@ -635,15 +635,8 @@ void NufftPlan::set_points(int64_t count, const void* points, cudaStream_t strea
     geometry_ = -1;
     configure_type2_bins();
   }
-  const size_t words = static_cast<size_t>(std::max<int64_t>(count, 1)) * sizeof(uint32_t);
-  SortBuffers buf;
-  buf.keys_a = static_cast<uint32_t*>(keys_a_.reserve(words, "bin keys"));
-  buf.keys_b = static_cast<uint32_t*>(keys_b_.reserve(words, "bin keys"));
-  buf.vals_a = static_cast<uint32_t*>(vals_a_.reserve(words, "point permutation"));
-  buf.vals_b = static_cast<uint32_t*>(vals_b_.reserve(words, "point permutation"));
-  buf.hist = static_cast<uint32_t*>(hist_.get());
-  buf.status = static_cast<uint32_t*>(status_.reserve(sort_status_bytes(count), "look-back words"));
-  buf.counters = static_cast<uint32_t*>(counters_.get());
+  bin_order_pending_ = false;
+  SortBuffers buf = sort_buffers(count);
   // Type-1 plans sort the points outside the fold's reach after every bin
   // (one more offset word) and mark the others in valid_mask_.
   const bool valid_first = type_ == 1;
@@ -693,8 +686,8 @@ void NufftPlan::set_points(int64_t count, const void* points, cudaStream_t strea
     }
     // 3D type 2: the interpolation takes the points in the order of their
     // support starts' (z, y) rows and 8-cell segments of x, so that a warp's
-    // 32 points gather from few grid rows; that order is sorted first (its
-    // permutation kept), then the reference's bins in the same buffers.
+    // 32 points gather from few grid rows; only that order is sorted here
+    // (its permutation kept), the reference's bins when they are asked for.
     rows_order_ = type_ == 2 && dim_ == 3 && count > 0;
     if (rows_order_) {
       uint64_t stride = 0;
@@ -706,8 +699,8 @@ void NufftPlan::set_points(int64_t count, const void* points, cudaStream_t strea
       sort_points(static_cast<const float*>(points), count, rows, KeyKind::SupportStart, stride, buf, rows_offsets,
                   &order, &keys, stream, &timer_);
       keep_rows_order(order, count, stream);
-    }
-    if (valid_first) {
+      bin_order_pending_ = true;
+    } else if (valid_first) {
       sort_points_valid_first(static_cast<const float*>(points), count, grid_, bins_, buf, offsets, valid_mask,
                               &perm_, &sorted_keys_, stream, &timer_);
     } else {
@@ -735,7 +728,7 @@ void NufftPlan::set_points(int64_t count, const void* points, cudaStream_t strea
       df64_to_f64(static_cast<const float*>(points), count * dim_, converted, stream);
       points64 = converted;
     }
-    // 3D type 2: the interpolation's row order first, as for f32 plans.
+    // 3D type 2: the interpolation's row order alone, as for f32 plans.
     rows_order_ = type_ == 2 && dim_ == 3 && count > 0;
     if (rows_order_) {
       uint64_t stride = 0;
@@ -746,9 +739,11 @@ void NufftPlan::set_points(int64_t count, const void* points, cudaStream_t strea
       uint32_t* keys = nullptr;
       sort_points64(points64, count, rows, stride, buf, rows_offsets, &order, &keys, stream, &timer_, nullptr);
       keep_rows_order(order, count, stream);
+      bin_order_pending_ = true;
+    } else {
+      sort_points64(points64, count, grid_, bins_, buf, offsets, &perm_, &sorted_keys_, stream,
+                    &timer_, valid_mask);
     }
-    sort_points64(points64, count, grid_, bins_, buf, offsets, &perm_, &sorted_keys_, stream,
-                  &timer_, valid_mask);
     double* sorted = static_cast<double*>(sorted_points_.reserve(sorted_bytes, "sorted coordinates"));
     gather_sorted_points64(points64, interp_perm(), count, dim_, sorted, stream, &timer_);
     if (type_ == 2 && dim_ == 2) {
@@ -1269,12 +1264,50 @@ void NufftPlan::keep_rows_order(const uint32_t* order, int64_t count, cudaStream
              "keep row order");
 }
 
+SortBuffers NufftPlan::sort_buffers(int64_t count) {
+  const size_t words = static_cast<size_t>(std::max<int64_t>(count, 1)) * sizeof(uint32_t);
+  SortBuffers buf;
+  buf.keys_a = static_cast<uint32_t*>(keys_a_.reserve(words, "bin keys"));
+  buf.keys_b = static_cast<uint32_t*>(keys_b_.reserve(words, "bin keys"));
+  buf.vals_a = static_cast<uint32_t*>(vals_a_.reserve(words, "point permutation"));
+  buf.vals_b = static_cast<uint32_t*>(vals_b_.reserve(words, "point permutation"));
+  buf.hist = static_cast<uint32_t*>(hist_.get());
+  buf.status = static_cast<uint32_t*>(status_.reserve(sort_status_bytes(count), "look-back words"));
+  buf.counters = static_cast<uint32_t*>(counters_.get());
+  return buf;
+}
+
+void NufftPlan::finish_bin_order(cudaStream_t stream) {
+  if (!bin_order_pending_) return;
+  // The same sort as set_points' (stable, so ties keep the caller's order),
+  // on the coordinates put back in the caller's order from the row order.
+  const int64_t count = point_count_;
+  SortBuffers buf = sort_buffers(count);
+  uint32_t* offsets = static_cast<uint32_t*>(offsets_.get());
+  const uint32_t* rows = static_cast<const uint32_t*>(rows_perm_.get());
+  if (precision_ == B200NUFFT_PRECISION_F32) {
+    float* coords = static_cast<float*>(unsorted_.reserve(static_cast<size_t>(count) * 3 * sizeof(float),
+                                                           "coordinates in the caller's order"));
+    scatter_points3(static_cast<const float*>(sorted_points_.get()), rows, count, coords, stream);
+    sort_points(coords, count, grid_, KeyKind::ApproximateCell, bins_, buf, offsets, &perm_, &sorted_keys_,
+                stream, &timer_);
+  } else {
+    double* coords = static_cast<double*>(unsorted_.reserve(static_cast<size_t>(count) * 3 * sizeof(double),
+                                                             "coordinates in the caller's order"));
+    scatter_points3(static_cast<const double*>(sorted_points_.get()), rows, count, coords, stream);
+    sort_points64(coords, count, grid_, bins_, buf, offsets, &perm_, &sorted_keys_, stream, &timer_, nullptr);
+  }
+  check_cuda(cudaGetLastError(), "bin order launch");
+  bin_order_pending_ = false;
+}
+
 void NufftPlan::copy_bin_order(uint32_t* permutation, uint32_t* bin_offsets, cudaStream_t stream) {
   make_current();
   if (dim_ > 3) throw NufftFailure{B200NUFFT_INVALID_ARGUMENT, "plans of more than three dimensions do not bin"};
   if (point_count_ < 0) {
     throw NufftFailure{B200NUFFT_GPU_EXECUTION_UNAVAILABLE, "no point set"};
   }
+  finish_bin_order(stream);
   const uint32_t* order = perm_;
   const uint32_t* offsets = static_cast<const uint32_t*>(offsets_.get());
   if (type_ == 1) {

@@ -170,6 +170,13 @@ class NufftPlan {
   GridParams rows_grid(uint64_t* bins) const;
   // Copies a sort's permutation into rows_perm_ (the sort buffers are reused).
   void keep_rows_order(const uint32_t* order, int64_t count, cudaStream_t stream);
+  // The reference's bin order (perm_, offsets_, sorted_keys_) of a point set
+  // kept in the row order is sorted only when it is asked for: the
+  // interpolation does not read it.
+  bool bin_order_pending_ = false;
+  DeviceBuffer unsorted_;  // the coordinates back in the caller's order, for that sort
+  void finish_bin_order(cudaStream_t stream);
+  SortBuffers sort_buffers(int64_t count);
 
   // Spreading state.
   DeviceBuffer parts_, part_start_, max_bits_, scratch_, candidates_;

@@ -412,6 +412,18 @@ __global__ void gather_points_kernel(const T* __restrict__ points,
   for (int a = 0; a < D; ++a) sorted[slot * D + a] = points[point * D + a];
 }
 
+// The inverse of gather_points_kernel: the coordinates of slot i back at the
+// point perm[i].
+template <int D, typename T>
+__global__ void scatter_points_kernel(const T* __restrict__ sorted, const uint32_t* __restrict__ perm,
+                                      int64_t count, T* __restrict__ points) {
+  const int64_t slot = static_cast<int64_t>(blockIdx.x) * blockDim.x + threadIdx.x;
+  if (slot >= count) return;
+  const int64_t point = perm[slot];
+#pragma unroll
+  for (int a = 0; a < D; ++a) points[point * D + a] = sorted[slot * D + a];
+}
+
 __global__ void identity_kernel(uint32_t* __restrict__ perm, uint32_t* __restrict__ keys,
                                 int64_t count) {
   const int64_t i = static_cast<int64_t>(blockIdx.x) * blockDim.x + threadIdx.x;
@@ -785,6 +797,16 @@ void sort_from_keys(int64_t count, uint64_t bins, int passes, SortBuffers buf, u
 }
 
 }  // namespace
+
+template <typename T>
+void scatter_points3(const T* sorted, const uint32_t* perm, int64_t count, T* points, cudaStream_t stream) {
+  if (count == 0) return;
+  const unsigned blocks = static_cast<unsigned>((count + 255) / 256);
+  scatter_points_kernel<3, T><<<blocks, 256, 0, stream>>>(sorted, perm, count, points);
+  note_launch();
+}
+template void scatter_points3<float>(const float*, const uint32_t*, int64_t, float*, cudaStream_t);
+template void scatter_points3<double>(const double*, const uint32_t*, int64_t, double*, cudaStream_t);
 
 void gather_sorted_points64(const double* points, const uint32_t* perm, int64_t count,
                             int dimensions, double* sorted, cudaStream_t stream,
