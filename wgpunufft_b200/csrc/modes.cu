@@ -8,6 +8,8 @@
 // is fused into the scatter.
 #include <cuda_runtime.h>
 
+#include <algorithm>
+
 #include "device.h"
 #include "modes.h"
 
@@ -74,6 +76,58 @@ __global__ void predeconvolve_kernel(ModeParams mp, int batch, const Complex* __
   }
 }
 
+// Grids of at least kRowsMinRows rows of at least kRowsMinCells cells along
+// axis 0: a CTA per row, its mode offset along the other axes found once, so
+// a thread does no division; the threads stride along the row.
+constexpr int kRowsMinCells = 64;
+constexpr int64_t kRowsMinRows = 1024;
+
+template <typename Real, typename Complex, typename Index>
+__global__ void __launch_bounds__(256) predeconvolve_rows_kernel(ModeParams mp, int batch,
+                                                                 const Complex* __restrict__ input,
+                                                                 const Real* __restrict__ amplitudes,
+                                                                 Complex* __restrict__ fine) {
+  __shared__ int64_t row_flat;
+  __shared__ int row_mapped;
+  const Index row = static_cast<Index>(blockIdx.x);
+  if (threadIdx.x == 0) {
+    Index rest = row;
+    int64_t flat = 0, stride = mp.modes[0];
+    bool mapped = true;
+    for (int a = 1; a < mp.dimensions; ++a) {
+      const Index n = static_cast<Index>(mp.fine[a]);
+      const int64_t cell = rest % n;
+      rest /= n;
+      const int64_t index = mode_index(cell, mp.modes[a], mp.fine[a], mp.centered);
+      mapped = mapped && index >= 0;
+      flat += index * stride;
+      stride *= mp.modes[a];
+    }
+    row_flat = flat;
+    row_mapped = mapped ? 1 : 0;
+  }
+  __syncthreads();
+  const int64_t n0 = mp.fine[0];
+  const int64_t row_start = n0 * static_cast<int64_t>(row);
+  for (int64_t x = threadIdx.x; x < n0; x += blockDim.x) {
+    const int64_t index = mode_index(x, mp.modes[0], n0, mp.centered);
+    const bool mapped = row_mapped != 0 && index >= 0;
+    const int64_t flat = row_flat + index;
+    const Real amplitude = mapped ? amplitudes[flat] : Real(0);
+    for (int b = 0; b < batch; ++b) {
+      Complex o;
+      o.x = Real(0);
+      o.y = Real(0);
+      if (mapped) {
+        const Complex v = input[static_cast<int64_t>(b) * mp.mode_count + flat];
+        o.x = v.x * amplitude;
+        o.y = v.y * amplitude;
+      }
+      fine[static_cast<int64_t>(b) * mp.fine_count + row_start + x] = o;
+    }
+  }
+}
+
 bool narrow(const ModeParams& mp) {
   return mp.fine_count < (int64_t(1) << 31) && mp.mode_count < (int64_t(1) << 31);
 }
@@ -93,6 +147,20 @@ void deconvolve_any(const ModeParams& mp, int batch, const Complex* fine, const 
 template <typename Real, typename Complex>
 void predeconvolve_any(const ModeParams& mp, int batch, const Complex* input, const Real* amplitudes,
                        Complex* fine, cudaStream_t stream) {
+  // Enough rows to fill the GPU (1D grids are one row).
+  if (mp.fine[0] >= kRowsMinCells && mp.fine_count / mp.fine[0] >= kRowsMinRows) {
+    const unsigned rows = static_cast<unsigned>(mp.fine_count / mp.fine[0]);
+    const int threads = static_cast<int>(std::min<int64_t>(256, (mp.fine[0] + 31) / 32 * 32));
+    if (narrow(mp)) {
+      predeconvolve_rows_kernel<Real, Complex, uint32_t><<<rows, threads, 0, stream>>>(mp, batch, input, amplitudes,
+                                                                                       fine);
+    } else {
+      predeconvolve_rows_kernel<Real, Complex, int64_t><<<rows, threads, 0, stream>>>(mp, batch, input, amplitudes,
+                                                                                      fine);
+    }
+    note_launch();
+    return;
+  }
   const unsigned blocks = static_cast<unsigned>((mp.fine_count + 255) / 256);
   if (narrow(mp)) {
     predeconvolve_kernel<Real, Complex, uint32_t><<<blocks, 256, 0, stream>>>(mp, batch, input, amplitudes, fine);
