@@ -532,11 +532,13 @@ void NufftPlan::configure_tiles() {
       sp.candidate_base[a] = kept_candidate_base[a];
       sp.candidate_count[a] = kept_candidate_count[a];
     }
+    sp.dest_fold = dest_fold_;
     part_upper_bound_ = part_bound;
     return;
   }
   host_candidates_.clear();
   for (int a = 0; a < 3; ++a) candidate_tile_[a] = tile[a];
+  bool dest_fold = dim_ == 3 && tile[0] == 16 && tile[1] == 16 && tile[2] % 4 == 0;
   for (int a = 0; a < dim_; ++a) {
     const int64_t n = fine_[a];
     std::vector<std::vector<int2>> lists(static_cast<size_t>(n));
@@ -548,6 +550,25 @@ void NufftPlan::configure_tiles() {
     }
     size_t most = 1;
     for (const auto& list : lists) most = std::max(most, list.size());
+    // The destination-tile fold walks, per axis, the candidates of the
+    // tile's first cell in their order: every cell of the tile must list an
+    // ordered part of them, each tile once.
+    dest_fold = dest_fold && most <= 2;
+    for (int64_t t = 0; dest_fold && t < sp.ntiles[a]; ++t) {
+      const auto& first = lists[static_cast<size_t>(t * tile[a])];
+      if (first.size() == 2 && first[0].x == first[1].x) dest_fold = false;
+      for (int64_t c = t * tile[a]; dest_fold && c < std::min<int64_t>((t + 1) * tile[a], n); ++c) {
+        size_t at = 0;
+        for (const int2& e : lists[static_cast<size_t>(c)]) {
+          while (at < first.size() && first[at].x != e.x) ++at;
+          if (at == first.size()) {
+            dest_fold = false;
+            break;
+          }
+          ++at;
+        }
+      }
+    }
     sp.candidate_base[a] = static_cast<int64_t>(host_candidates_.size());
     sp.candidate_count[a] = static_cast<int32_t>(most);
     for (const auto& list : lists) {
@@ -556,6 +577,8 @@ void NufftPlan::configure_tiles() {
       }
     }
   }
+  dest_fold_ = dest_fold ? 1 : 0;
+  sp.dest_fold = dest_fold_;
   void* cand = candidates_.reserve(host_candidates_.size() * sizeof(int2), "fold candidates");
   check_cuda(cudaMemcpy(cand, host_candidates_.data(), host_candidates_.size() * sizeof(int2),
                         cudaMemcpyHostToDevice),

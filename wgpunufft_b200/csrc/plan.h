@@ -185,6 +185,7 @@ class NufftPlan {
   int64_t part_upper_bound_ = 0;
   std::vector<int2> host_candidates_;
   int64_t candidate_tile_[3] = {0, 0, 0};
+  int32_t dest_fold_ = 0;  // SpreadParams::dest_fold of the kept candidate table
 
   // Tensor-core spreading (2D f32 type-1 plans of batch >= kTcMinBatch):
   // enabled by the configuration, active when the chosen bins allow it.

@@ -1319,6 +1319,131 @@ __global__ void fold_tiles_kernel(SpreadParams sp, int batch, const Complex* __r
   }
 }
 
+// The fold per destination tile (SpreadParams::dest_fold): a CTA of 256
+// threads takes kDestCells planes of a 16 x 16-cell tile plane stack, a
+// thread the cells (x, y, z0 .. z0 + kDestCells - 1). The CTA walks the
+// covering source tiles in the order of the candidates of the tile's first
+// cell along each axis (z outermost) and each source tile's parts in order;
+// a thread adds a part's value to each of its cells that the source tile
+// covers. Every cell's candidates are an ordered part of those lists, so each
+// cell gets the row fold's sums in the row fold's order, bit for bit; the
+// thread's loads of one part are independent of one another.
+constexpr int kDestCells = 4;
+
+template <typename Complex>
+__global__ void __launch_bounds__(256) fold_dest_kernel(SpreadParams sp, int batch,
+                                                        const Complex* __restrict__ scratch,
+                                                        const uint32_t* __restrict__ part_start, int64_t part_limit,
+                                                        const int2* __restrict__ candidates,
+                                                        Complex* __restrict__ fine) {
+  const int slices = sp.tile[2] / kDestCells;
+  const uint32_t tile = blockIdx.x / static_cast<uint32_t>(slices);
+  const int slice = static_cast<int>(blockIdx.x - tile * static_cast<uint32_t>(slices));
+  const int b = blockIdx.y;
+  const uint32_t n0t = static_cast<uint32_t>(sp.ntiles[0]), n1t = static_cast<uint32_t>(sp.ntiles[1]);
+  const int t0 = static_cast<int>(tile % n0t);
+  const int t1 = static_cast<int>((tile / n0t) % n1t);
+  const int t2 = static_cast<int>(tile / (n0t * n1t));
+  const int x = t0 * 16 + static_cast<int>(threadIdx.x & 15);
+  const int y = t1 * 16 + static_cast<int>(threadIdx.x >> 4);
+  const int z0 = t2 * sp.tile[2] + slice * kDestCells;
+  const int n0 = sp.grid.fine[0], n1 = sp.grid.fine[1], n2 = sp.grid.fine[2];
+  // The source tiles of each axis: the candidates of the tile's first cell.
+  int src[3][2];
+  const int first_cell[3] = {t0 * 16, t1 * 16, t2 * sp.tile[2]};
+#pragma unroll
+  for (int a = 0; a < 3; ++a) {
+    const int2* c = candidates + sp.candidate_base[a] + static_cast<int64_t>(first_cell[a]) * sp.candidate_count[a];
+    src[a][0] = c[0].x;
+    src[a][1] = sp.candidate_count[a] > 1 ? c[1].x : -1;
+  }
+  // A cell's local offset in each source tile along an axis; -1 where that
+  // tile does not cover it.
+  auto offsets = [&](int a, int cell, int& o0, int& o1) {
+    o0 = -1;
+    o1 = -1;
+    const int2* c = candidates + sp.candidate_base[a] + static_cast<int64_t>(cell) * sp.candidate_count[a];
+    const int k = sp.candidate_count[a] > 1 ? 2 : 1;
+    for (int i = 0; i < k; ++i) {
+      const int2 e = c[i];
+      if (e.x < 0) break;
+      if (e.x == src[a][0]) o0 = e.y;
+      else if (e.x == src[a][1]) o1 = e.y;
+    }
+  };
+  const bool xy_inside = x < n0 && y < n1;
+  int ox[2] = {-1, -1}, oy[2] = {-1, -1};
+  if (xy_inside) {
+    offsets(0, x, ox[0], ox[1]);
+    offsets(1, y, oy[0], oy[1]);
+  }
+  int oz[kDestCells][2];
+#pragma unroll
+  for (int k = 0; k < kDestCells; ++k) {
+    oz[k][0] = -1;
+    oz[k][1] = -1;
+    if (z0 + k < n2) offsets(2, z0 + k, oz[k][0], oz[k][1]);
+  }
+  Complex sum[kDestCells];
+#pragma unroll
+  for (int k = 0; k < kDestCells; ++k) {
+    sum[k].x = 0;
+    sum[k].y = 0;
+  }
+  const int plane = sp.pad[0] * sp.pad[1];
+#pragma unroll
+  for (int u2 = 0; u2 < 2; ++u2) {
+    if (src[2][u2] < 0) continue;
+    bool any_z = false;
+#pragma unroll
+    for (int k = 0; k < kDestCells; ++k) any_z = any_z || oz[k][u2] >= 0;
+    if (!any_z) continue;  // the same for the whole CTA
+#pragma unroll
+    for (int u1 = 0; u1 < 2; ++u1) {
+      if (src[1][u1] < 0) continue;
+#pragma unroll
+      for (int u0 = 0; u0 < 2; ++u0) {
+        if (src[0][u0] < 0) continue;
+        const int64_t source = src[0][u0] + static_cast<int64_t>(sp.ntiles[0]) *
+                                                (src[1][u1] + static_cast<int64_t>(sp.ntiles[1]) * src[2][u2]);
+        const uint32_t first = part_start[source];
+        const uint32_t last = min(part_start[source + 1], static_cast<uint32_t>(part_limit));
+        const bool covered = ox[u0] >= 0 && oy[u1] >= 0;
+        const int base = ox[u0] + sp.pad[0] * oy[u1];
+        int at[kDestCells];
+        bool take[kDestCells];
+#pragma unroll
+        for (int k = 0; k < kDestCells; ++k) {
+          take[k] = covered && oz[k][u2] >= 0;
+          at[k] = base + plane * oz[k][u2];
+        }
+        for (uint32_t p = first; p < last; ++p) {
+          const Complex* v = scratch + (static_cast<int64_t>(p) * batch + b) * sp.padded_cells;
+          Complex got[kDestCells];
+#pragma unroll
+          for (int k = 0; k < kDestCells; ++k) {
+            if (take[k]) got[k] = v[at[k]];
+          }
+#pragma unroll
+          for (int k = 0; k < kDestCells; ++k) {
+            if (take[k]) {
+              sum[k].x += got[k].x;
+              sum[k].y += got[k].y;
+            }
+          }
+        }
+      }
+    }
+  }
+  if (!xy_inside) return;
+#pragma unroll
+  for (int k = 0; k < kDestCells; ++k) {
+    if (z0 + k < n2) {
+      fine[static_cast<int64_t>(b) * sp.grid.fine_count + x + static_cast<int64_t>(n0) * (y + static_cast<int64_t>(n1) * (z0 + k))] = sum[k];
+    }
+  }
+}
+
 // Grids of at most kWarpFoldCells cells fold a cell per warp. Small grids
 // holding many points have hundreds of parts per tile, and a thread walking
 // them one after another would leave the GPU idle: here the lanes take every
@@ -1444,6 +1569,10 @@ void fold_any(const SpreadParams& sp, int batch, const Complex* scratch, const u
               int64_t part_limit, const int2* candidates, Complex* fine, cudaStream_t stream) {
   if (sp.grid.fine_count <= kWarpFoldCells) {
     launch_warp_fold(sp, batch, scratch, part_start, part_limit, candidates, fine, stream);
+  } else if (sp.dest_fold && batch < 8) {
+    const dim3 grid(static_cast<unsigned>(sp.tile_count * (sp.tile[2] / kDestCells)), static_cast<unsigned>(batch));
+    fold_dest_kernel<Complex><<<grid, 256, 0, stream>>>(sp, batch, scratch, part_start, part_limit, candidates, fine);
+    note_launch();
   } else if (batch >= 8) {
     launch_fold<8>(sp, batch, scratch, part_start, part_limit, candidates, fine, stream);
   } else {

@@ -49,6 +49,11 @@ struct SpreadParams {
   int32_t pitch01;
   int32_t span;
   const uint32_t* warp_segments;
+  // 3D plans of 16 x 16 x (4 k)-cell tiles whose cells' candidate lists are,
+  // along every axis, ordered parts of the list of their tile's first cell
+  // (checked on the host): single vectors fold per destination tile
+  // (fold_dest_kernel), in the same order as the row fold.
+  int32_t dest_fold;
 };
 
 // Window widths spread by whole warps, one record at a time (3D f32).
