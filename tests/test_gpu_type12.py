@@ -429,3 +429,53 @@ def test_type2_crowded_bins_are_split_over_many_parts():
     assert np.array_equal(outs[0][0].view(np.int64), outs[1][0].view(np.int64))
     ref64 = native.direct_type2(points64[pick], coefficients64[:1], n_modes)
     assert rel_l2(outs[0][0, pick], ref64[0]) < 20 * 1e-12 + 1e-13
+
+
+@pytest.mark.parametrize("precision", ["f32", "f64"])
+def test_3d_type2_bin_order_on_request_leaves_executions_alone(precision):
+    """3D type-2 plans interpolate in their own point order and sort the
+    reference's bins only when bin_order asks: the order is the oracle's for
+    each new point set, and asking for it changes no output bit."""
+    n_modes = (24, 20, 16)
+    eps = 1e-5 if precision == "f32" else 1e-9
+    prec = w.Precision.F32 if precision == "f32" else w.Precision.F64
+    ctype = torch.complex64 if precision == "f32" else torch.complex128
+    rng = np.random.default_rng(77)
+
+    def bits(values):
+        return torch.view_as_real(values).view(torch.int64 if precision == "f64" else torch.int32)
+
+    config = w.NufftConfig(n_modes, eps, precision=prec)
+    plan = w.NufftPlan.type2_gpu(config)
+    coefficients = torch.from_numpy(complex_normal(rng, config.mode_count())).to(ctype).reshape(1, -1).to(DEV)
+    for points in (uniform_points(rng, 30_000, 3), clustered_points(rng, 25_000, 3)):
+        gpu_points = to_gpu(points if precision == "f32" else points.astype(np.float64))
+        plan.set_points_gpu(gpu_points)
+        out = torch.empty((1, points.shape[0]), dtype=ctype, device=DEV)
+        plan.execute_gpu_batch(1, coefficients, out)
+        before = out.clone()
+        perm, offsets = plan.bin_order()
+        if precision == "f32":
+            ref_perm, ref_offsets, *_ = oracle_order(points, plan.fine_grid_shape(), eps, 2)
+            assert np.array_equal(perm.numpy(), ref_perm)
+        else:
+            # As test_f64_bin_order_is_bit_exact: the f64 offsets against the
+            # oracle, the permutation as an order of those keys.
+            fine = list(plan.fine_grid_shape())
+            width = es_kernel.es_parameters(eps, 2.0)[0]
+            keys, bins = binsort.type1_keys64(points.astype(np.float64), fine, width, binsort.type2_sides64(fine))
+            _, ref_offsets = binsort.stable_order(keys, bins)
+            assert np.array_equal(np.sort(perm.numpy()), np.arange(points.shape[0]))
+            assert np.all(np.diff(keys[perm.numpy()].astype(np.int64)) >= 0)
+        assert np.array_equal(offsets.numpy(), ref_offsets)
+        again_perm, _ = plan.bin_order()
+        assert torch.equal(again_perm, perm)
+        plan.execute_gpu_batch(1, coefficients, out)
+        plan.synchronize()
+        assert torch.equal(bits(out), bits(before))
+        fresh = w.NufftPlan.type2_gpu(config)
+        fresh.set_points_gpu(gpu_points)
+        other = torch.empty_like(out)
+        fresh.execute_gpu_batch(1, coefficients, other)
+        fresh.synchronize()
+        assert torch.equal(bits(other), bits(out))
